@@ -1,0 +1,330 @@
+"""Benchmark: Mattes MI value+derivative evaluations per second on one B200.
+
+Workload (one "step" = one value+derivative evaluation through the C ABI): the finest
+level of the 256³ rigid registration — fixed/moving 256³ f32 blob phantoms (60 blobs,
+rotation ±15°, translation ±12 mm, seeded synthetic data), VersorRigid3DTransform,
+32 histogram bins, 10 % random sampling (SplitMix64, 1,677,721 samples). L2 is
+flushed (a 256 MiB write) before every evaluation, outside the timed events.
+
+  value  device time of the evaluations (CUDA events on the library's stream, first
+         kernel to the result copy), inputs resident in HBM
+  e2e    the same call timed end to end through the public C ABI from the host
+         (parameters in from host memory, value+derivative back to host memory)
+
+--impl reference times the reference algorithm's CPU implementation on this host's
+cores (the C++ restatement under oracle/, all threads), since the Rust reference
+cannot be built here. Multi-GPU runs are independent replicas (one registration pair
+per rank): weak scaling, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sitk-rs_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "MI value+derivative evals/sec"
+UNIT = "evals/s"
+WORKLOAD = ("256^3 f32 VersorRigid3D, 32 bins, 10% random sampling (finest pyramid level of the "
+            "256^3 rigid registration), value+derivative")
+N = 256
+BINS = 32
+PCT = 0.10
+SEED = 20261203
+# a pose near the generating transform's inverse (versor right part, translation)
+POSE = [0.021, -0.034, 0.047, 3.1, -4.2, 2.6]
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the run (read-only queries)."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for nm, v in zip(names, s[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _kernel_source_hash() -> str:
+    h = hashlib.sha256()
+    for name in ("sampler.cuh", "mattes.cu"):
+        with open(os.path.join(ROOT, "sitk-rs_b200", "csrc", name), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def _traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary, if it was taken on the
+    current kernel source."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        if d.get("source_hash") != _kernel_source_hash():
+            return None
+        return d["kernels"][kernel]["dram_bytes_per_launch"]
+    except Exception:
+        return None
+
+
+def make_workload(seed: int):
+    from sitk_b200 import synth
+    pair = synth.config1_pair(seed, N)
+    return pair
+
+
+def time_oracle(pair, draw, nthreads: int, budget_s: float, min_evals: int = 1):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    g = oracle.make_geometry((N, N, N))
+    center = [(N - 1) / 2.0] * 3
+    times = []
+    t_start = time.perf_counter()
+    while True:
+        t0 = time.perf_counter()
+        oracle.evaluate(pair.fixed, g, pair.moving, g, BINS, 2, POSE, center, draw=draw, nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= min_evals and time.perf_counter() - t_start >= budget_s:
+            break
+    return times
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    pair = make_workload(SEED)
+    draw = oracle.draw_samples(N ** 3, 2, PCT, SEED)
+    cores = os.cpu_count() or 1
+    times = time_oracle(pair, draw, cores, 0.0, min_evals=args.warmup)  # warm-up
+    times = []
+    for _ in range(args.steps):
+        times += time_oracle(pair, draw, cores, 0.0, min_evals=1)
+    total = sum(times)
+    value = args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "samples": int(draw.size), "bins": BINS},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full evaluations of the workload (C++ FP64 restatement of "
+                                   f"the reference CPU metric, {cores} threads, per-thread histograms "
+                                   "folded in thread order)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import sitk_b200 as sb
+    from sitk_b200.metric import enable_timing, read_timing
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    ctx = sb.Context(dev)
+    pair = make_workload(SEED + rank)
+    f = sb.DeviceImage.upload(pair.fixed, ctx=ctx)
+    m = sb.DeviceImage.upload(pair.moving, ctx=ctx)
+    metric = sb.DeviceMattesMetric.from_device_sampled(f, m, bins=BINS, strategy=sb.SAMPLING_RANDOM,
+                                                       percentage=PCT, seed=SEED)
+    f.free()
+    m.free()
+    info = metric.info()
+    S = int(info["n_samples"])
+    t = sb.VersorRigid3DTransform(POSE[:3], POSE[3:], [(N - 1) / 2.0] * 3)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    l2 = torch.cuda.get_device_properties(dev).L2_cache_size
+    flush = torch.empty(max(2 * l2, 256 << 20) // 4, dtype=torch.float32, device=f"cuda:{dev}")
+
+    sampler = ClockSampler(dev) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    enable_timing(metric, True)
+    for _ in range(max(args.warmup, 3)):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        metric.evaluate(t)
+    # settle clocks under load (untimed)
+    t_end = time.perf_counter() + 1.0
+    while time.perf_counter() < t_end:
+        metric.evaluate(t)
+    read_timing(metric)
+
+    ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    wall0 = time.perf_counter()
+    last = None
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        ev_s[i].record(stream)
+        last = metric.evaluate(t)
+        ev_e[i].record(stream)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - wall0
+    if dist:
+        dist.barrier()
+    ms, nev = read_timing(metric)
+    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(ev_s, ev_e))
+    dev_ms = ms[0]
+    if dist:
+        tt = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_ms, e2e_ms = tt.tolist()
+    if sampler:
+        sampler.stop()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    per_step_ms = dev_ms / args.steps
+    value = world * args.steps / (dev_ms / 1e3)
+    e2e_value = world * args.steps / (e2e_ms / 1e3)
+    kern = {"k_hist": ms[1] / nev, "k_tail": ms[2] / nev, "k_deriv": ms[3] / nev}
+    dom = max(("k_hist", "k_deriv"), key=lambda k: kern[k])
+    vm = N ** 3
+    bytes_alg = S * 4 + min(vm, 8 * S) * 4  # one pass: fixed f32 + moving f32 (per-unit figure × S)
+    peak, peak_kind = _peaks()
+    achieved = bytes_alg / (kern[dom] / 1e3) / 1e9
+    traffic = _traffic(dom)
+
+    # serial CPU baseline on a bounded sample (rank 0, N=1 only)
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        draw = oracle.draw_samples(vm, 2, PCT, SEED)
+        times = time_oracle(pair, draw, 1, args.cpu_budget)
+        cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{len(times)} full evaluations of the same workload, serial C++ FP64 "
+                         f"restatement of the reference CPU metric (~{sum(times):.1f} s)"}
+
+    clocks = sampler.summary() if sampler else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "fixed": [N, N, N], "moving": [N, N, N], "bins": BINS,
+                   "sampling": "random 10%", "samples": S, "transform": "VersorRigid3D",
+                   "l2": "flushed before every evaluation (256 MiB write, untimed)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * (6 + 3),
+                "d2h_bytes_per_step": 8 * (2 + 6)},
+        "gpu_launches": 3 * args.steps,
+        "kernel_ms": kern,
+        "sample_points_per_s": 2 * S * value / world,
+        "wall_ms_per_step": 1e3 * wall / args.steps,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "bytes_alg_per_launch": bytes_alg},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "result": {"value": last.value, "valid": last.valid_points},
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,200 @@
+/*
+ * mi_b200.h — C ABI of the B200 (sm_100a) Mattes mutual-information metric.
+ *
+ * This is the drop-in boundary for the device metric seam of sitk-rs (crate `sitk`,
+ * paths below are inside crates/sitk/src/). Every entry point takes plain pointers
+ * and sizes and returns an mi_status; nothing here names a C++ or torch type, so a
+ * Rust `extern "C"` block, ctypes or cgo can bind it as-is (INTEGRATION.md shows
+ * the Rust and ctypes bindings).
+ *
+ * Threading: a handle (context, image, metric) must not be used from two host
+ * threads at once without external locking. The reference serialises its device
+ * metric behind a Mutex (registration/device.rs:634, :707-712); callers of this
+ * library keep the same discipline. Every call is synchronous on the context's
+ * stream unless stated otherwise.
+ *
+ * Errors: no entry point falls back to the CPU. A refusal is named by its status,
+ * mirroring DeviceMetricError (registration/device.rs:45-110) and CudaError
+ * (cuda/error.rs:11-108); mi_last_error() returns the detail text of the last
+ * failure on a context.
+ */
+#ifndef MI_B200_H
+#define MI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MI_OK = 0,
+    MI_ERR_INVALID_ARGUMENT = 1,      /* null handle/pointer, bad length, bad enum */
+    MI_ERR_NO_DEVICE = 2,             /* CudaError::NoDevice (cuda/error.rs) */
+    MI_ERR_CUDA = 3,                  /* CudaError::Driver: any other runtime failure */
+    MI_ERR_OUT_OF_MEMORY = 4,
+    MI_ERR_UNSUPPORTED_PIXEL_TYPE = 5,/* DeviceImage::upload refuses complex/vector (cuda/image.rs:212-223) */
+    MI_ERR_SINGULAR_DIRECTION = 6,    /* DeviceMetricError::SingularDirection */
+    MI_ERR_TOO_FEW_HISTOGRAM_BINS = 7,/* RegistrationError::TooFewHistogramBins (mattes.rs:158) */
+    MI_ERR_CONSTANT_FIXED = 8,        /* RegistrationError::ConstantIntensity{which:"fixed"} */
+    MI_ERR_CONSTANT_MOVING = 9,       /* RegistrationError::ConstantIntensity{which:"moving"} */
+    MI_ERR_SAMPLE_INDEX_OUT_OF_GRID = 10, /* CudaError::SampleIndexOutOfGrid */
+    MI_ERR_MASK_SIZE_MISMATCH = 11,   /* RegistrationError::MaskSizeMismatch */
+    MI_ERR_NON_AFFINE_TRANSFORM = 12, /* DeviceMetricError::NonAffineTransform */
+    MI_ERR_POINT_MAP_STAGE_COUNT = 13,/* CudaError::PointMapStageCount (more than MI_MAX_STAGES) */
+    MI_ERR_TOO_MANY_HISTOGRAM_BINS = 14, /* bins > MI_MAX_BINS: no reference counterpart */
+    MI_ERR_TIMEOUT = 15,              /* a bounded device wait gave up (batched form) */
+    MI_ERR_NOT_CONVERGED = 16         /* reserved */
+} mi_status;
+
+#define MI_MAX_STAGES 4
+#define MI_MAX_BINS 128
+#define MI_MAX_PARAMS 12
+
+/* DeviceImage pixel types (core PixelId scalar set; cuda/image.rs:182-261).
+ * Every scalar type is cast on the device to f32 as (float)(double)x. */
+typedef enum {
+    MI_U8 = 0, MI_I8 = 1, MI_U16 = 2, MI_I16 = 3, MI_U32 = 4, MI_I32 = 5,
+    MI_U64 = 6, MI_I64 = 7, MI_F32 = 8, MI_F64 = 9,
+    MI_COMPLEX_F32 = 100, MI_VECTOR_F32 = 101  /* refused by name */
+} mi_dtype;
+
+/* 3-D image geometry (cuda/image.rs:122-155): size, spacing, origin, direction
+ * (row-major 3×3). Voxels are stored x-fastest. */
+typedef struct {
+    int64_t size[3];
+    double spacing[3];
+    double origin[3];
+    double direction[9];
+} mi_geometry;
+
+/* Fixed-image sampling (registration/metric.rs:84-94, :419-437). */
+typedef enum {
+    MI_SAMPLING_NONE = 0,     /* every voxel, grid order */
+    MI_SAMPLING_REGULAR = 1,  /* every ceil(1/percentage)-th voxel */
+    MI_SAMPLING_RANDOM = 2,   /* floor(N·percentage) SplitMix64 draws with replacement */
+    MI_SAMPLING_EXPLICIT = 3  /* caller's flat voxel list (FixedSamples::selected_indices) */
+} mi_sampling_strategy;
+
+typedef struct {
+    int strategy;             /* mi_sampling_strategy */
+    double percentage;        /* REGULAR / RANDOM */
+    uint64_t seed;            /* RANDOM */
+    const int64_t* indices;   /* EXPLICIT: host array of flat fixed-grid voxel indices */
+    int64_t n_indices;
+} mi_sampling;
+
+/* Transform families with an analytic Jacobian (transform/parametric.rs). */
+typedef enum {
+    MI_TRANSFORM_AFFINE = 0,          /* 12 params: matrix row-major, translation; fixed: center[3] */
+    MI_TRANSFORM_EULER3D = 1,         /* 6: angles x,y,z, translation; fixed: center[3] (+computeZYX) */
+    MI_TRANSFORM_VERSOR_RIGID3D = 2,  /* 6: versor right part, translation; fixed: center[3] */
+    MI_TRANSFORM_TRANSLATION = 3      /* 3: translation; no fixed params */
+} mi_transform_kind;
+
+/* Histogram geometry and sample count of a metric (MattesGeometry, mattes.rs:133-186). */
+typedef struct {
+    int bins;
+    int64_t n_samples;        /* after the fixed-mask filter */
+    double fixed_min, fixed_max, moving_min, moving_max;
+    double fixed_bin_size, moving_bin_size;
+    double fixed_normalized_min, moving_normalized_min;
+} mi_metric_info;
+
+typedef struct mi_context mi_context;
+typedef struct mi_image mi_image;
+typedef struct mi_metric mi_metric;
+
+/* ---- context (cuda/backend.rs:30-160: Backend / backend()) ---------------- */
+
+/* One context per device; owns one CUDA stream. MI_ERR_NO_DEVICE when absent. */
+mi_status mi_context_create(int device, mi_context** out);
+mi_status mi_context_destroy(mi_context* ctx);
+mi_status mi_context_sync(mi_context* ctx);
+/* Detail text of the last failure on ctx (valid until the next call on ctx). */
+const char* mi_last_error(const mi_context* ctx);
+const char* mi_status_string(mi_status s);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work. */
+void* mi_context_stream(mi_context* ctx);
+
+/* ---- images (cuda/image.rs:182 DeviceImage::upload, :269 to_host) --------- */
+
+mi_status mi_image_upload(mi_context* ctx, const void* host, mi_dtype dtype,
+                          const mi_geometry* geometry, mi_image** out);
+/* Copy an f32 volume that is already in device memory (x-fastest) into a new image. */
+mi_status mi_image_from_device(mi_context* ctx, const float* device_ptr,
+                               const mi_geometry* geometry, mi_image** out);
+mi_status mi_image_to_host(const mi_image* img, float* dst, size_t n_elements);
+mi_status mi_image_geometry(const mi_image* img, mi_geometry* out);
+/* Device address of the image's f32 voxels (borrowed; valid until mi_image_free). */
+const float* mi_image_device_ptr(const mi_image* img);
+mi_status mi_image_free(mi_image* img);
+
+/* ---- metric (registration/device.rs:632-800 DeviceMattesMetric) ----------- */
+
+/* from_device / from_device_sampled (device.rs:644-696). The metric copies both
+ * volumes, so the images may be freed afterwards. fixed_mask: optional image on the
+ * fixed grid, nonzero = inside. moving_mask: optional host array of
+ * size(moving) bytes on the moving grid, nonzero = inside. sampling: NULL means
+ * MI_SAMPLING_NONE. */
+mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_image* moving,
+                           const mi_image* fixed_mask, const uint8_t* moving_mask,
+                           const mi_sampling* sampling, int bins, mi_metric** out);
+mi_status mi_metric_info_get(const mi_metric* m, mi_metric_info* out);
+mi_status mi_metric_destroy(mi_metric* m);
+
+/* DeviceMattesMetric::value (device.rs:734-737): value = −MI at the point map given
+ * as `nstage` stages of 12 doubles (matrix row-major, then offset), replayed in
+ * order: p ← M·p + t (matrix_offset.rs:102-109). `valid` may be NULL. */
+mi_status mi_metric_value(mi_metric* m, const double* stages, int nstage, double* value,
+                          int64_t* valid);
+
+/* DeviceMattesMetric::evaluate (device.rs:767-800) for a transform family:
+ * value = −MI and derivative = +∇(−MI) w.r.t. the family's parameters
+ * (the optimizer subtracts it). Degenerate histograms give value = DBL_MAX and a
+ * zero derivative (mattes.rs:590-609). */
+mi_status mi_metric_value_and_derivative(mi_metric* m, int kind, const double* params,
+                                         int nparams, const double* fixed_params, int nfixed,
+                                         double* value, double* derivative, int64_t* valid);
+
+/* The generic form (registration/cuda.rs:294-363 affine_form + :505-524
+ * contract_mattes): any point map given as stages, plus a Jacobian that is affine in
+ * the fixed point, J(x) = jac0 + Σ_e x_e·jac_c[e], jac0 row-major 3×nparams and
+ * jac_c three such blocks. */
+mi_status mi_metric_value_and_derivative_stages(mi_metric* m, const double* stages, int nstage,
+                                                const double* jac0, const double* jac_c,
+                                                int nparams, double* value, double* derivative,
+                                                int64_t* valid);
+
+/* Device-time accounting (no reference counterpart; used by benchmarks). When
+ * enabled, every evaluation records CUDA events on the context stream around its
+ * kernels. mi_metric_timing_read returns the milliseconds accumulated since the last
+ * read — [0] whole evaluation (first kernel to the result copy), [1] histogram pass,
+ * [2] tail, [3] derivative pass — and the evaluation count, then resets them. */
+mi_status mi_metric_timing_enable(mi_metric* m, int enable);
+mi_status mi_metric_timing_read(mi_metric* m, double* ms4, int64_t* n_evals);
+
+/* The point-map stage (matrix row-major, offset: 12 doubles) a transform family
+ * stores and multiplies (transform/parametric.rs:549-553, :1103-1107, :1331-1335),
+ * and its Jacobian's affine form J(x) = jac0 + Σ_e x_e·jac_c[e] (jac0: 3×nparams
+ * row-major; jac_c: three such blocks), formed on the host in the reference's
+ * operation order. Any output may be NULL. No device work. */
+mi_status mi_transform_form(int kind, const double* params, int nparams, const double* fixed_params,
+                            int nfixed, double* stage12, double* jac0, double* jac_c);
+
+/* Per-sample discrete decisions of the device sampler at a point map, in the
+ * metric's sample order (test hook for the exactness contract): status 0 = outside
+ * the moving buffer or masked, 1 = interpolated value outside the moving range,
+ * 2 = valid; fixed_bin/moving_bin are the Parzen indices of valid samples (−1
+ * otherwise); flat receives each sample's fixed-grid voxel. Any output may be NULL.
+ * n is the capacity of each array and must be ≥ n_samples. */
+mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nstage,
+                                     int8_t* status, int32_t* fixed_bin, int32_t* moving_bin,
+                                     int64_t* flat, int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MI_B200_H */

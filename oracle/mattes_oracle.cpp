@@ -1,0 +1,761 @@
+// CPU ORACLE — test infrastructure only.
+//
+// This file restates, in plain serial FP64 C++, the reference CPU algorithm for the
+// Mattes mutual-information metric of sitk-rs (crate `sitk` v0.0.3). It is the
+// checker for the CUDA library under sitk-rs_b200/: only tests/, the smoke check in
+// __graft_entry__.py and the CPU-baseline legs of bench.py load it. Nothing in the
+// product links or calls it.
+//
+// Parity status: the reference is Rust and cannot be built in this environment
+// (no cargo/rustc, no network for its crates), and its own tests hold no golden
+// vectors for this metric (all of its Mattes pins are relational). This oracle is
+// therefore "parity unpinned" against the reference binary. It is pinned instead by
+// (a) published SplitMix64 vectors, (b) the reference's relational tests re-created
+// in tests/test_oracle.py, and (c) an independent numpy FP64 implementation
+// (oracle/np_oracle.py) that must agree with this file.
+//
+// Arithmetic order follows the reference exactly. Rust never fuses a*b+c, so this
+// file is compiled with -ffp-contract=off, and every sum is written in the
+// reference's accumulation order. Citations are paths inside the reference crate
+// (crates/sitk/src/...).
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cfloat>
+#include <vector>
+#include <algorithm>
+#include <limits>
+#include <thread>
+
+extern "C" {
+
+typedef struct {
+    int64_t size[3];
+    double spacing[3];
+    double origin[3];
+    double direction[9];  // row-major
+} or_geometry;
+
+enum {
+    OR_OK = 0,
+    OR_TOO_FEW_BINS = 1,
+    OR_CONSTANT_FIXED = 2,
+    OR_CONSTANT_MOVING = 3,
+    OR_SINGULAR_DIRECTION = 4,
+    OR_BAD_ARGUMENT = 5,
+};
+
+enum { OR_AFFINE = 0, OR_EULER3D = 1, OR_VERSOR_RIGID3D = 2, OR_TRANSLATION = 3 };
+
+}  // extern "C"
+
+namespace {
+
+const int PADDING = 2;  // registration/mattes.rs:92
+
+// core/matrix.rs:9-21 — accumulator starts at 0.0, terms added in column order.
+void mat_vec(const double* m, const double* v, double* out) {
+    for (int r = 0; r < 3; ++r) {
+        double acc = 0.0;
+        for (int c = 0; c < 3; ++c) acc += m[r * 3 + c] * v[c];
+        out[r] = acc;
+    }
+}
+
+// core/matrix.rs:24-40 — zero entries of `a` are skipped.
+void matmul(const double* a, const double* b, double* out) {
+    for (int i = 0; i < 9; ++i) out[i] = 0.0;
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 3; ++k) {
+            double ark = a[r * 3 + k];
+            if (ark == 0.0) continue;
+            for (int c = 0; c < 3; ++c) out[r * 3 + c] += ark * b[k * 3 + c];
+        }
+}
+
+// core/matrix.rs:44-104 — Gauss–Jordan with partial pivoting, singular below 1e-12.
+bool invert3(const double* m, double* inv) {
+    const int n = 3, w = 6;
+    double a[18];
+    for (int r = 0; r < n; ++r) {
+        for (int c = 0; c < w; ++c) a[r * w + c] = 0.0;
+        for (int c = 0; c < n; ++c) a[r * w + c] = m[r * n + c];
+        a[r * w + n + r] = 1.0;
+    }
+    for (int col = 0; col < n; ++col) {
+        int pivot = col;
+        double best = std::fabs(a[col * w + col]);
+        for (int r = col + 1; r < n; ++r) {
+            double val = std::fabs(a[r * w + col]);
+            if (val > best) { best = val; pivot = r; }
+        }
+        if (best < 1e-12) return false;
+        if (pivot != col)
+            for (int c = 0; c < w; ++c) std::swap(a[col * w + c], a[pivot * w + c]);
+        double diag = a[col * w + col];
+        for (int c = 0; c < w; ++c) a[col * w + c] /= diag;
+        for (int r = 0; r < n; ++r) {
+            if (r == col) continue;
+            double factor = a[r * w + col];
+            if (factor == 0.0) continue;
+            for (int c = 0; c < w; ++c) a[r * w + c] -= factor * a[col * w + c];
+        }
+    }
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) inv[r * n + c] = a[r * w + n + c];
+    return true;
+}
+
+// core/coord.rs:50-88 — index→physical = direction·diag(spacing); physical→index is
+// the Gauss–Jordan inverse of that composed matrix.
+void index_to_physical(const or_geometry& g, double* m) {
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) m[r * 3 + c] = g.direction[r * 3 + c] * g.spacing[c];
+}
+
+// ---------------------------------------------------------------------------
+// Transforms (transform/parametric.rs). Each yields the stored (matrix, offset)
+// its transform_point multiplies, and a per-point dense Jacobian.
+// ---------------------------------------------------------------------------
+struct Transform {
+    int kind = OR_AFFINE;
+    int nparams = 12;
+    double matrix[9];
+    double offset[3];
+    double center[3];
+    double p[12];
+    bool compute_zyx = false;
+    double vx = 0, vy = 0, vz = 0, vw = 1;  // versor (normalised)
+
+    // transform/parametric.rs:549-553 (and :1103-1107, :1331-1335):
+    // mat_vec(matrix, p) then + offset.
+    void transform_point(const double* x, double* y) const {
+        double mx[3];
+        mat_vec(matrix, x, mx);
+        for (int d = 0; d < 3; ++d) y[d] = mx[d] + offset[d];
+    }
+
+    // Jacobian of the mapped point w.r.t. the parameters at point x, row-major 3×P.
+    void jacobian(const double* x, double* j) const {
+        const int P = nparams;
+        for (int i = 0; i < 3 * P; ++i) j[i] = 0.0;
+        if (kind == OR_AFFINE) {
+            // parametric.rs:589-602
+            for (int i = 0; i < 3; ++i) {
+                for (int c = 0; c < 3; ++c) j[i * P + (i * 3 + c)] = x[c] - center[c];
+                j[i * P + (9 + i)] = 1.0;
+            }
+        } else if (kind == OR_TRANSLATION) {
+            for (int i = 0; i < 3; ++i) j[i * P + i] = 1.0;
+        } else if (kind == OR_EULER3D) {
+            // parametric.rs:1125-1166
+            double cx = std::cos(p[0]), sx = std::sin(p[0]);
+            double cy = std::cos(p[1]), sy = std::sin(p[1]);
+            double cz = std::cos(p[2]), sz = std::sin(p[2]);
+            double px = x[0] - center[0], py = x[1] - center[1], pz = x[2] - center[2];
+            if (compute_zyx) {
+                j[0] = (cz * sy * cx + sz * sx) * py + (-cz * sy * sx + sz * cx) * pz;
+                j[6] = (sz * sy * cx - cz * sx) * py + (-sz * sy * sx - cz * cx) * pz;
+                j[12] = (cy * cx) * py + (-cy * sx) * pz;
+                j[1] = (-cz * sy) * px + (cz * cy * sx) * py + (cz * cy * cx) * pz;
+                j[7] = (-sz * sy) * px + (sz * cy * sx) * py + (sz * cy * cx) * pz;
+                j[13] = (-cy) * px + (-sy * sx) * py + (-sy * cx) * pz;
+                j[2] = (-sz * cy) * px + (-sz * sy * sx - cz * cx) * py + (-sz * sy * cx + cz * sx) * pz;
+                j[8] = (cz * cy) * px + (cz * sy * sx - sz * cx) * py + (cz * sy * cx + sz * sx) * pz;
+                j[14] = 0.0;
+            } else {
+                j[0] = (-sz * cx * sy) * px + (sz * sx) * py + (sz * cx * cy) * pz;
+                j[6] = (cz * cx * sy) * px + (-cz * sx) * py + (-cz * cx * cy) * pz;
+                j[12] = (sx * sy) * px + (cx) * py + (-sx * cy) * pz;
+                j[1] = (-cz * sy - sz * sx * cy) * px + (cz * cy - sz * sx * sy) * pz;
+                j[7] = (-sz * sy + cz * sx * cy) * px + (sz * cy + cz * sx * sy) * pz;
+                j[13] = (-cx * cy) * px + (-cx * sy) * pz;
+                j[2] = (-sz * cy - cz * sx * sy) * px + (-cz * cx) * py + (-sz * sy + cz * sx * cy) * pz;
+                j[8] = (cz * cy - sz * sx * sy) * px + (-sz * cx) * py + (cz * sy + sz * sx * cy) * pz;
+                j[14] = 0.0;
+            }
+            j[3] = 1.0; j[10] = 1.0; j[17] = 1.0;
+        } else {
+            // parametric.rs:1355-1384
+            double px = x[0] - center[0], py = x[1] - center[1], pz = x[2] - center[2];
+            double vxx = vx * vx, vyy = vy * vy, vzz = vz * vz, vww = vw * vw;
+            double vxy = vx * vy, vxz = vx * vz, vxw = vx * vw;
+            double vyz = vy * vz, vyw = vy * vw, vzw = vz * vw;
+            j[0] = 2.0 * ((vyw + vxz) * py + (vzw - vxy) * pz) / vw;
+            j[6] = 2.0 * ((vyw - vxz) * px - 2.0 * vxw * py + (vxx - vww) * pz) / vw;
+            j[12] = 2.0 * ((vzw + vxy) * px + (vww - vxx) * py - 2.0 * vxw * pz) / vw;
+            j[1] = 2.0 * (-2.0 * vyw * px + (vxw + vyz) * py + (vww - vyy) * pz) / vw;
+            j[7] = 2.0 * ((vxw - vyz) * px + (vzw + vxy) * pz) / vw;
+            j[13] = 2.0 * ((vyy - vww) * px + (vzw - vxy) * py - 2.0 * vyw * pz) / vw;
+            j[2] = 2.0 * (-2.0 * vzw * px + (vzz - vww) * py + (vxw - vyz) * pz) / vw;
+            j[8] = 2.0 * ((vww - vzz) * px - 2.0 * vzw * py + (vyw + vxz) * pz) / vw;
+            j[14] = 2.0 * ((vxw + vyz) * px + (vyw - vxz) * py) / vw;
+            j[3] = 1.0; j[10] = 1.0; j[17] = 1.0;
+        }
+    }
+};
+
+// Build a transform from (kind, params, fixed params) the way each family's
+// set_parameters / recompute does.
+bool make_transform(int kind, const double* params, const double* fixed, int nfixed, Transform& t) {
+    t.kind = kind;
+    for (int d = 0; d < 3; ++d) t.center[d] = (fixed && nfixed >= 3) ? fixed[d] : 0.0;
+    if (kind == OR_AFFINE) {
+        // parametric.rs:566-573, compute_offset :522-527
+        t.nparams = 12;
+        for (int i = 0; i < 12; ++i) t.p[i] = params[i];
+        for (int i = 0; i < 9; ++i) t.matrix[i] = params[i];
+        double ac[3];
+        mat_vec(t.matrix, t.center, ac);
+        for (int d = 0; d < 3; ++d) t.offset[d] = t.center[d] + params[9 + d] - ac[d];
+    } else if (kind == OR_TRANSLATION) {
+        // parametric.rs:378-391: p + t; the identity matrix form is bitwise equal.
+        t.nparams = 3;
+        for (int i = 0; i < 3; ++i) t.p[i] = params[i];
+        for (int i = 0; i < 9; ++i) t.matrix[i] = (i % 4 == 0) ? 1.0 : 0.0;
+        for (int d = 0; d < 3; ++d) t.offset[d] = params[d];
+    } else if (kind == OR_EULER3D) {
+        // parametric.rs:1063-1086
+        t.nparams = 6;
+        for (int i = 0; i < 6; ++i) t.p[i] = params[i];
+        t.compute_zyx = (fixed && nfixed == 4) ? (fixed[3] != 0.0) : false;
+        double cx = std::cos(params[0]), sx = std::sin(params[0]);
+        double cy = std::cos(params[1]), sy = std::sin(params[1]);
+        double cz = std::cos(params[2]), sz = std::sin(params[2]);
+        double rx[9] = {1.0, 0.0, 0.0, 0.0, cx, -sx, 0.0, sx, cx};
+        double ry[9] = {cy, 0.0, sy, 0.0, 1.0, 0.0, -sy, 0.0, cy};
+        double rz[9] = {cz, -sz, 0.0, sz, cz, 0.0, 0.0, 0.0, 1.0};
+        double tmp[9];
+        if (t.compute_zyx) { matmul(rz, ry, tmp); matmul(tmp, rx, t.matrix); }
+        else { matmul(rz, rx, tmp); matmul(tmp, ry, t.matrix); }
+        double mc[3];
+        mat_vec(t.matrix, t.center, mc);
+        for (int i = 0; i < 3; ++i) t.offset[i] = params[3 + i] + t.center[i] - mc[i];
+    } else if (kind == OR_VERSOR_RIGID3D) {
+        // parametric.rs:1310-1345 (set_versor, recompute)
+        t.nparams = 6;
+        for (int i = 0; i < 6; ++i) t.p[i] = params[i];
+        const double EPS = 1e-10;
+        double vx = params[0], vy = params[1], vz = params[2];
+        double norm = std::sqrt(vx * vx + vy * vy + vz * vz);
+        double ax = vx, ay = vy, az = vz;
+        if (norm >= 1.0 - EPS) {
+            double d = norm + EPS * norm;
+            ax = vx / d; ay = vy / d; az = vz / d;
+        }
+        t.vx = ax; t.vy = ay; t.vz = az;
+        double s = 1.0 - (ax * ax + ay * ay + az * az);
+        t.vw = std::sqrt(s > 0.0 ? s : 0.0);
+        double x = t.vx, y = t.vy, z = t.vz, w = t.vw;
+        double xx = x * x, yy = y * y, zz = z * z;
+        double xy = x * y, xz = x * z, xw = x * w;
+        double yz = y * z, yw = y * w, zw = z * w;
+        double m[9] = {
+            1.0 - 2.0 * (yy + zz), 2.0 * (xy - zw), 2.0 * (xz + yw),
+            2.0 * (xy + zw), 1.0 - 2.0 * (xx + zz), 2.0 * (yz - xw),
+            2.0 * (xz - yw), 2.0 * (yz + xw), 1.0 - 2.0 * (xx + yy)};
+        double mc[3];
+        mat_vec(m, t.center, mc);
+        for (int i = 0; i < 3; ++i) t.offset[i] = params[3 + i] + t.center[i] - mc[i];
+        for (int i = 0; i < 9; ++i) t.matrix[i] = m[i];
+    } else {
+        return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Mattes pieces (registration/mattes.rs)
+// ---------------------------------------------------------------------------
+
+// mattes.rs:96-107
+double cubic_bspline(double u) {
+    double a = std::fabs(u);
+    if (a < 1.0) {
+        double sq = a * a;
+        return (4.0 - 6.0 * sq + 3.0 * sq * a) / 6.0;
+    } else if (a < 2.0) {
+        double sq = a * a;
+        return (8.0 - 12.0 * a + 6.0 * sq - sq * a) / 6.0;
+    }
+    return 0.0;
+}
+
+// mattes.rs:112-124
+double cubic_bspline_derivative(double u) {
+    if (u >= 0.0 && u < 1.0) return -2.0 * u + 1.5 * u * u;
+    if (u > -1.0 && u < 0.0) return -2.0 * u - 1.5 * u * u;
+    if (u >= 1.0 && u < 2.0) return -2.0 + 2.0 * u - 0.5 * u * u;
+    if (u > -2.0 && u <= -1.0) return 2.0 + 2.0 * u + 0.5 * u * u;
+    return 0.0;
+}
+
+struct Geometry {
+    int bins;
+    double moving_true_min, moving_true_max;
+    double fixed_bin_size, moving_bin_size;
+    double fixed_normalized_min, moving_normalized_min;
+};
+
+// mattes.rs:152-186
+int make_geometry(double fmin, double fmax, double mmin, double mmax, int bins, Geometry& g) {
+    if (bins < 2 * PADDING + 1) return OR_TOO_FEW_BINS;
+    if (fmax - fmin <= DBL_EPSILON) return OR_CONSTANT_FIXED;
+    if (mmax - mmin <= DBL_EPSILON) return OR_CONSTANT_MOVING;
+    double denom = (double)(bins - 2 * PADDING);
+    g.bins = bins;
+    g.moving_true_min = mmin;
+    g.moving_true_max = mmax;
+    g.fixed_bin_size = (fmax - fmin) / denom;
+    g.moving_bin_size = (mmax - mmin) / denom;
+    g.fixed_normalized_min = fmin / g.fixed_bin_size - (double)PADDING;
+    g.moving_normalized_min = mmin / g.moving_bin_size - (double)PADDING;
+    return OR_OK;
+}
+
+// mattes.rs:193-206 — truncate toward zero, clamp to [padding, bins − padding − 1].
+int parzen_index(double value, double bin_size, double nmin, int bins) {
+    double term = value / bin_size - nmin;
+    long long index = (long long)term;
+    long long lo = PADDING, hi = (long long)bins - PADDING - 1;
+    if (index < lo) index = lo;
+    else if (index > hi) index = hi;
+    return (int)index;
+}
+
+// core/compensated.rs:112-123 (ITK's Kahan recurrence; the sum is returned
+// without folding the last compensation back in).
+double kahan_sum(const double* v, size_t n) {
+    double sum = 0.0, comp = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        double ci = v[i] - comp;
+        double t = sum + ci;
+        comp = (t - sum) - ci;
+        sum = t;
+    }
+    return sum;
+}
+
+// The prepared sample set and moving image (registration/metric.rs:494-581, 722-924).
+struct Problem {
+    const float* fixed;
+    or_geometry fg;
+    const float* moving;
+    or_geometry mg;
+    const uint8_t* mmask;
+    double f_i2p[9];
+    double m_p2i[9];
+    int64_t mstride[3];
+    std::vector<int64_t> flats;  // selected voxels (after the fixed-mask filter); empty = full grid
+    bool grid;
+    int64_t n;  // sample count
+};
+
+// registration/scales.rs:259-271 — origin-seeded accumulation.
+inline void grid_point(const Problem& P, int64_t flat, double* out) {
+    double idx[3];
+    int64_t f = flat;
+    for (int d = 0; d < 3; ++d) {
+        idx[d] = (double)(f % P.fg.size[d]);
+        f /= P.fg.size[d];
+    }
+    for (int r = 0; r < 3; ++r) {
+        double acc = P.fg.origin[r];
+        for (int c = 0; c < 3; ++c) acc += P.f_i2p[r * 3 + c] * idx[c];
+        out[r] = acc;
+    }
+}
+
+// metric.rs:795-806 — c = M·(p − origin), the difference formed first.
+inline void continuous_index(const Problem& P, const double* p, double* c) {
+    for (int r = 0; r < 3; ++r) {
+        double acc = -0.0;  // Rust's f64 Sum starts from −0.0; a finite result is unaffected
+        for (int j = 0; j < 3; ++j) acc += P.m_p2i[r * 3 + j] * (p[j] - P.mg.origin[j]);
+        c[r] = acc;
+    }
+}
+
+// metric.rs:817-833 + core/coord.rs:185-191 — floor(c + 0.5), reject outside.
+inline bool mask_allows(const Problem& P, const double* c) {
+    if (!P.mmask) return true;
+    int64_t flat = 0;
+    for (int d = 0; d < 3; ++d) {
+        int64_t r = (int64_t)std::floor(c[d] + 0.5);
+        if (r < 0 || r >= P.mg.size[d]) return false;
+        flat += r * P.mstride[d];
+    }
+    return P.mmask[flat] != 0;
+}
+
+// transform/interpolator.rs:29-34
+inline bool is_inside(const Problem& P, const double* c) {
+    for (int d = 0; d < 3; ++d)
+        if (!(c[d] >= -0.5 && c[d] < (double)P.mg.size[d] - 0.5)) return false;
+    return true;
+}
+
+// transform/interpolator.rs:103-152 + metric.rs:848-861 (physical gradient).
+// Returns false when the point is outside the buffer or masked.
+inline bool moving_value_grad(const Problem& P, const double* p, double* value, double* gphys,
+                              bool want_grad) {
+    double c[3];
+    continuous_index(P, p, c);
+    if (!mask_allows(P, c)) return false;
+    if (!is_inside(P, c)) return false;
+    double frac[3];
+    int64_t base[3];
+    for (int d = 0; d < 3; ++d) {
+        double f = std::floor(c[d]);
+        base[d] = (int64_t)f;
+        frac[d] = c[d] - f;
+    }
+    double v = 0.0;
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int corner = 0; corner < 8; ++corner) {
+        int64_t off = 0;
+        double weight = 1.0;
+        for (int d = 0; d < 3; ++d) {
+            int bit = (corner >> d) & 1;
+            weight *= bit ? frac[d] : 1.0 - frac[d];
+            int64_t idx = base[d] + bit;
+            if (idx < 0) idx = 0;
+            if (idx > P.mg.size[d] - 1) idx = P.mg.size[d] - 1;
+            off += idx * P.mstride[d];
+        }
+        double b = (double)P.moving[off];
+        v += weight * b;
+        if (want_grad) {
+            for (int j = 0; j < 3; ++j) {
+                double wj = 1.0;
+                for (int d = 0; d < 3; ++d) {
+                    if (d == j) continue;
+                    int bit = (corner >> d) & 1;
+                    wj *= bit ? frac[d] : 1.0 - frac[d];
+                }
+                double sign = ((corner >> j) & 1) ? 1.0 : -1.0;
+                g[j] += sign * wj * b;
+            }
+        }
+    }
+    *value = v;
+    if (want_grad) {
+        for (int d = 0; d < 3; ++d) {
+            double acc = -0.0;
+            for (int j = 0; j < 3; ++j) acc += g[j] * P.m_p2i[j * 3 + d];
+            gphys[d] = acc;
+        }
+    }
+    return true;
+}
+
+int prepare(const float* fixed, const or_geometry* fg, const float* moving, const or_geometry* mg,
+            const uint8_t* fmask, const uint8_t* mmask, const int64_t* draw, int64_t ndraw,
+            Problem& P) {
+    P.fixed = fixed;
+    P.fg = *fg;
+    P.moving = moving;
+    P.mg = *mg;
+    P.mmask = mmask;
+    index_to_physical(*fg, P.f_i2p);
+    double m_i2p[9];
+    index_to_physical(*mg, m_i2p);
+    if (!invert3(m_i2p, P.m_p2i)) return OR_SINGULAR_DIRECTION;
+    P.mstride[0] = 1;
+    P.mstride[1] = mg->size[0];
+    P.mstride[2] = mg->size[0] * mg->size[1];
+    int64_t nvox = fg->size[0] * fg->size[1] * fg->size[2];
+    // metric.rs:528-540 — the draw, then the fixed-mask filter; no list for the
+    // unmasked full grid.
+    if (!draw && !fmask) {
+        P.grid = true;
+        P.n = nvox;
+        return OR_OK;
+    }
+    P.grid = false;
+    P.flats.clear();
+    if (!draw) {
+        for (int64_t s = 0; s < nvox; ++s)
+            if (fmask[s]) P.flats.push_back(s);
+    } else {
+        for (int64_t i = 0; i < ndraw; ++i) {
+            int64_t f = draw[i];
+            if (f < 0 || f >= nvox) return OR_BAD_ARGUMENT;
+            if (!fmask || fmask[f]) P.flats.push_back(f);
+        }
+    }
+    P.n = (int64_t)P.flats.size();
+    return OR_OK;
+}
+
+inline int64_t sample_flat(const Problem& P, int64_t s) { return P.grid ? s : P.flats[s]; }
+
+// Ranges that size the histogram (metric.rs:633-640 SampledPoints, :913-924 masked moving).
+void ranges(const Problem& P, double* fmin, double* fmax, double* mmin, double* mmax) {
+    double lo = INFINITY, hi = -INFINITY;
+    for (int64_t s = 0; s < P.n; ++s) {
+        double v = (double)P.fixed[sample_flat(P, s)];
+        lo = std::fmin(lo, v);
+        hi = std::fmax(hi, v);
+    }
+    if (P.n == 0) { lo = 0.0; hi = 0.0; }
+    *fmin = lo; *fmax = hi;
+    int64_t nm = P.mg.size[0] * P.mg.size[1] * P.mg.size[2];
+    lo = INFINITY; hi = -INFINITY;
+    bool any = false;
+    for (int64_t i = 0; i < nm; ++i) {
+        if (P.mmask && !P.mmask[i]) continue;
+        double v = (double)P.moving[i];
+        lo = std::fmin(lo, v);
+        hi = std::fmax(hi, v);
+        any = true;
+    }
+    if (!any) { lo = 0.0; hi = 0.0; }
+    *mmin = lo; *mmax = hi;
+}
+
+struct Accum {
+    std::vector<double> joint, fixed_marginal, jpd;
+    int64_t valid = 0;
+};
+
+// The per-sample body of evaluate_global_support (mattes.rs:536-588), or of
+// build_histogram (mattes.rs:451-483) when want_deriv is false.
+inline void sample_body(const Problem& P, const Geometry& G, const Transform& T, int64_t s,
+                        bool want_deriv, Accum& A, int8_t* status, int32_t* fi_out,
+                        int32_t* mi_out) {
+    const int bins = G.bins;
+    const int np = T.nparams;
+    int64_t flat = sample_flat(P, s);
+    double fp[3], mp[3];
+    if (P.grid) grid_point(P, flat, fp);
+    else grid_point(P, flat, fp);  // metric.rs:339-348 — explicit points are write_point's
+    double fv = (double)P.fixed[flat];
+    T.transform_point(fp, mp);
+    double mv, g[3];
+    if (!moving_value_grad(P, mp, &mv, g, want_deriv)) {
+        if (status) status[s] = 0;
+        return;
+    }
+    if (mv < G.moving_true_min || mv > G.moving_true_max) {
+        if (status) status[s] = 1;
+        return;
+    }
+    double moving_term = mv / G.moving_bin_size - G.moving_normalized_min;
+    int mi = parzen_index(mv, G.moving_bin_size, G.moving_normalized_min, bins);
+    int fi = parzen_index(fv, G.fixed_bin_size, G.fixed_normalized_min, bins);
+    if (status) status[s] = 2;
+    if (fi_out) fi_out[s] = fi;
+    if (mi_out) mi_out[s] = mi;
+    A.fixed_marginal[fi] += 1.0;
+    double jac[36];
+    if (want_deriv) T.jacobian(fp, jac);
+    int start = mi - 1;
+    for (int m = start; m < start + 4; ++m) {
+        double arg = (double)m - moving_term;
+        double val = cubic_bspline(arg);
+        A.joint[(size_t)fi * bins + m] += val;
+        if (want_deriv) {
+            double dw = cubic_bspline_derivative(arg);
+            size_t base = ((size_t)fi * bins + m) * np;
+            for (int k = 0; k < np; ++k) {
+                double inner = 0.0;
+                for (int d = 0; d < 3; ++d) inner += jac[d * np + k] * g[d];
+                A.jpd[base + k] += inner * dw;
+            }
+        }
+    }
+    A.valid += 1;
+}
+
+// mattes.rs:590-676 (derivative) and mattes.rs:273-328 (value-only tail).
+void finish(const Geometry& G, Accum& A, int np, bool want_deriv, double* value, double* deriv,
+            int64_t* valid) {
+    const int bins = G.bins;
+    *valid = A.valid;
+    for (int k = 0; k < np && deriv; ++k) deriv[k] = 0.0;
+    if (A.valid == 0) { *value = DBL_MAX; return; }
+    double joint_sum = kahan_sum(A.joint.data(), A.joint.size());
+    if (joint_sum < DBL_EPSILON) { *value = DBL_MAX; return; }
+    double n_factor = 1.0 / (G.moving_bin_size * (double)A.valid);
+    if (want_deriv)
+        for (auto& d : A.jpd) d *= n_factor;
+    double inv_sum = 1.0 / joint_sum;
+    for (auto& p : A.joint) p *= inv_sum;
+    for (auto& p : A.fixed_marginal) p *= inv_sum;
+    std::vector<double> mm(bins, 0.0);
+    for (int f = 0; f < bins; ++f)
+        for (int m = 0; m < bins; ++m) mm[m] += A.joint[(size_t)f * bins + m];
+    const double close = DBL_EPSILON;
+    double sum = 0.0;
+    for (int f = 0; f < bins; ++f) {
+        double fm = A.fixed_marginal[f];
+        if (fm <= close) continue;
+        double log_fm = std::log(fm);
+        for (int m = 0; m < bins; ++m) {
+            double mmv = mm[m];
+            double jp = A.joint[(size_t)f * bins + m];
+            if (mmv > close && jp > close) {
+                double pr = std::log(jp / mmv);
+                sum += jp * (pr - log_fm);
+                if (want_deriv) {
+                    size_t base = ((size_t)f * bins + m) * np;
+                    for (int k = 0; k < np; ++k) deriv[k] += A.jpd[base + k] * pr;
+                }
+            }
+        }
+    }
+    *value = -sum;
+}
+
+}  // namespace
+
+extern "C" {
+
+// One SplitMix64 output (registration/metric.rs:110-116) after `state` has been
+// advanced; exposed so a test can pin it against published vectors.
+uint64_t or_splitmix64_next(uint64_t* state) {
+    *state += 0x9E3779B97F4A7C15ULL;
+    uint64_t z = *state;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// registration/metric.rs:419-437. strategy: 0 None, 1 Regular, 2 Random.
+// Returns the number of drawn voxels (written to `out` when non-null and cap allows),
+// or −1 for the None strategy (the identity selection has no list).
+int64_t or_draw_samples(int64_t voxels, int strategy, double percentage, uint64_t seed,
+                        int64_t* out, int64_t cap) {
+    if (strategy == 0) return -1;
+    if (strategy == 1) {
+        double inv = std::ceil(1.0 / percentage);
+        int64_t stride = (int64_t)inv;
+        if (stride < 1) stride = 1;
+        int64_t n = 0;
+        for (int64_t v = 0; v < voxels; v += stride, ++n)
+            if (out && n < cap) out[n] = v;
+        return n;
+    }
+    int64_t count = (int64_t)((double)voxels * percentage);
+    uint64_t state = seed;
+    for (int64_t i = 0; i < count; ++i) {
+        uint64_t r = or_splitmix64_next(&state) % (uint64_t)voxels;
+        if (out && i < cap) out[i] = (int64_t)r;
+    }
+    return count;
+}
+
+// Histogram geometry for a problem: [fixed_min, fixed_max, moving_min, moving_max,
+// fixed_bin_size, moving_bin_size, fixed_normalized_min, moving_normalized_min],
+// plus the sample count after the fixed-mask filter.
+int or_metric_geometry(const float* fixed, const or_geometry* fg, const float* moving,
+                       const or_geometry* mg, const uint8_t* fmask, const uint8_t* mmask,
+                       const int64_t* draw, int64_t ndraw, int bins, double* out8,
+                       int64_t* nsamples) {
+    Problem P;
+    int st = prepare(fixed, fg, moving, mg, fmask, mmask, draw, ndraw, P);
+    if (st) return st;
+    double fmin, fmax, mmin, mmax;
+    ranges(P, &fmin, &fmax, &mmin, &mmax);
+    Geometry G;
+    out8[0] = fmin; out8[1] = fmax; out8[2] = mmin; out8[3] = mmax;
+    if (nsamples) *nsamples = P.n;
+    st = make_geometry(fmin, fmax, mmin, mmax, bins, G);
+    if (st) return st;
+    out8[4] = G.fixed_bin_size; out8[5] = G.moving_bin_size;
+    out8[6] = G.fixed_normalized_min; out8[7] = G.moving_normalized_min;
+    return OR_OK;
+}
+
+// The whole metric: value = −MI, derivative = +∇(−MI) (mattes.rs:522-676), or the
+// value-only walk (mattes.rs:442-500) when want_derivative is 0.
+//
+// `draw` is the sampling strategy's draw BEFORE the fixed-mask filter (NULL = the
+// whole grid). Per-sample outputs, when non-null, are indexed in post-filter sample
+// order: status 0 = outside/masked, 1 = moving value out of range, 2 = valid; fi/mi
+// are the Parzen bins of a valid sample. `nthreads` > 1 splits the samples into
+// contiguous chunks with private accumulators folded in thread-index order (the
+// reference's deterministic rayon rule, core/parallel.rs:766); 1 is the serial walk.
+int or_mattes_evaluate(const float* fixed, const or_geometry* fg, const float* moving,
+                       const or_geometry* mg, const uint8_t* fmask, const uint8_t* mmask,
+                       const int64_t* draw, int64_t ndraw, int bins, int kind,
+                       const double* params, const double* fixed_params, int nfixed,
+                       int want_derivative, int nthreads, double* value, double* deriv,
+                       int64_t* valid, int8_t* status, int32_t* fi_out, int32_t* mi_out,
+                       double* joint_out, double* fixed_marginal_out) {
+    Problem P;
+    int st = prepare(fixed, fg, moving, mg, fmask, mmask, draw, ndraw, P);
+    if (st) return st;
+    double fmin, fmax, mmin, mmax;
+    ranges(P, &fmin, &fmax, &mmin, &mmax);
+    Geometry G;
+    st = make_geometry(fmin, fmax, mmin, mmax, bins, G);
+    if (st) return st;
+    Transform T;
+    if (!make_transform(kind, params, fixed_params, nfixed, T)) return OR_BAD_ARGUMENT;
+    const bool wd = want_derivative != 0;
+    const int np = T.nparams;
+    if (nthreads < 1) nthreads = 1;
+    std::vector<Accum> parts(nthreads);
+    for (auto& a : parts) {
+        a.joint.assign((size_t)bins * bins, 0.0);
+        a.fixed_marginal.assign(bins, 0.0);
+        if (wd) a.jpd.assign((size_t)bins * bins * np, 0.0);
+    }
+    const int64_t n = P.n;
+    if (nthreads == 1) {
+        for (int64_t s = 0; s < n; ++s) sample_body(P, G, T, s, wd, parts[0], status, fi_out, mi_out);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t) {
+            pool.emplace_back([&, t]() {
+                int64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
+                for (int64_t s = lo; s < hi; ++s)
+                    sample_body(P, G, T, s, wd, parts[t], status, fi_out, mi_out);
+            });
+        }
+        for (auto& th : pool) th.join();
+        for (int t = 1; t < nthreads; ++t) {
+            for (size_t i = 0; i < parts[0].joint.size(); ++i) parts[0].joint[i] += parts[t].joint[i];
+            for (int i = 0; i < bins; ++i) parts[0].fixed_marginal[i] += parts[t].fixed_marginal[i];
+            for (size_t i = 0; i < parts[0].jpd.size(); ++i) parts[0].jpd[i] += parts[t].jpd[i];
+            parts[0].valid += parts[t].valid;
+        }
+    }
+    Accum& A = parts[0];
+    if (joint_out) std::memcpy(joint_out, A.joint.data(), A.joint.size() * sizeof(double));
+    if (fixed_marginal_out) std::memcpy(fixed_marginal_out, A.fixed_marginal.data(), bins * sizeof(double));
+    finish(G, A, np, wd, value, deriv, valid);
+    return OR_OK;
+}
+
+// The transform's stored matrix/offset (one point-map stage) and its Jacobian at a
+// point — exposed so tests can check the product's host-side transform code.
+int or_transform(int kind, const double* params, const double* fixed_params, int nfixed,
+                 const double* point, double* matrix9, double* offset3, double* jac,
+                 double* mapped3) {
+    Transform T;
+    if (!make_transform(kind, params, fixed_params, nfixed, T)) return OR_BAD_ARGUMENT;
+    if (matrix9) std::memcpy(matrix9, T.matrix, sizeof(T.matrix));
+    if (offset3) std::memcpy(offset3, T.offset, sizeof(T.offset));
+    if (point && jac) T.jacobian(point, jac);
+    if (point && mapped3) T.transform_point(point, mapped3);
+    return OR_OK;
+}
+
+int or_cubic_bspline(const double* u, double* val, double* dval, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) {
+        if (val) val[i] = cubic_bspline(u[i]);
+        if (dval) dval[i] = cubic_bspline_derivative(u[i]);
+    }
+    return OR_OK;
+}
+
+double or_kahan_sum(const double* v, int64_t n) { return kahan_sum(v, (size_t)n); }
+
+int64_t or_round_half_integer_up(double x) { return (int64_t)std::floor(x + 0.5); }
+
+int or_invert3(const double* m, double* inv) { return invert3(m, inv) ? OR_OK : OR_SINGULAR_DIRECTION; }
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+The oracle restates the reference's CPU Mattes metric (crates/sitk/src/registration/
+mattes.rs:442-676 and the helpers it calls) in serial FP64 C++; see
+oracle/mattes_oracle.cpp for the per-function citations and the parity status
+("parity unpinned": the Rust reference cannot be built here). Only tests/, the
+smoke check and bench.py's CPU-baseline legs import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmattes_oracle.so")
+
+AFFINE, EULER3D, VERSOR_RIGID3D, TRANSLATION = 0, 1, 2, 3
+NPARAMS = {AFFINE: 12, EULER3D: 6, VERSOR_RIGID3D: 6, TRANSLATION: 3}
+
+STATUS = {0: "ok", 1: "too few bins", 2: "constant fixed", 3: "constant moving",
+          4: "singular direction", 5: "bad argument"}
+
+
+class OrGeometry(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_int64 * 3), ("spacing", ctypes.c_double * 3),
+                ("origin", ctypes.c_double * 3), ("direction", ctypes.c_double * 9)]
+
+
+def make_geometry(size, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
+                  direction=(1, 0, 0, 0, 1, 0, 0, 0, 1)) -> OrGeometry:
+    g = OrGeometry()
+    for i in range(3):
+        g.size[i] = int(size[i])
+        g.spacing[i] = float(spacing[i])
+        g.origin[i] = float(origin[i])
+    for i in range(9):
+        g.direction[i] = float(direction[i])
+    return g
+
+
+def build() -> str:
+    """Compile the oracle library with its Makefile (g++, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    dp, fp, i64p = P(ctypes.c_double), P(ctypes.c_float), P(ctypes.c_int64)
+    u8p, i8p, i32p = P(ctypes.c_uint8), P(ctypes.c_int8), P(ctypes.c_int32)
+    gp = P(OrGeometry)
+    L.or_splitmix64_next.argtypes = [P(ctypes.c_uint64)]
+    L.or_splitmix64_next.restype = ctypes.c_uint64
+    L.or_draw_samples.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_uint64,
+                                  i64p, ctypes.c_int64]
+    L.or_draw_samples.restype = ctypes.c_int64
+    L.or_metric_geometry.argtypes = [fp, gp, fp, gp, u8p, u8p, i64p, ctypes.c_int64, ctypes.c_int,
+                                     dp, i64p]
+    L.or_metric_geometry.restype = ctypes.c_int
+    L.or_mattes_evaluate.argtypes = [fp, gp, fp, gp, u8p, u8p, i64p, ctypes.c_int64, ctypes.c_int,
+                                     ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     dp, dp, i64p, i8p, i32p, i32p, dp, dp]
+    L.or_mattes_evaluate.restype = ctypes.c_int
+    L.or_transform.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp, dp, dp]
+    L.or_transform.restype = ctypes.c_int
+    L.or_cubic_bspline.argtypes = [dp, dp, dp, ctypes.c_int64]
+    L.or_cubic_bspline.restype = ctypes.c_int
+    L.or_kahan_sum.argtypes = [dp, ctypes.c_int64]
+    L.or_kahan_sum.restype = ctypes.c_double
+    L.or_round_half_integer_up.argtypes = [ctypes.c_double]
+    L.or_round_half_integer_up.restype = ctypes.c_int64
+    L.or_invert3.argtypes = [dp, dp]
+    L.or_invert3.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code):
+        super().__init__(f"oracle refused: {STATUS.get(code, code)}")
+        self.code = code
+
+
+def splitmix64(seed: int, n: int) -> list[int]:
+    st = ctypes.c_uint64(seed)
+    return [lib().or_splitmix64_next(ctypes.byref(st)) for _ in range(n)]
+
+
+def draw_samples(voxels: int, strategy: int, percentage: float, seed: int):
+    """metric.rs:419-437 — None (strategy 0) returns None; 1 Regular; 2 Random."""
+    n = lib().or_draw_samples(voxels, strategy, percentage, seed, None, 0)
+    if n < 0:
+        return None
+    out = np.empty(n, dtype=np.int64)
+    lib().or_draw_samples(voxels, strategy, percentage, seed, _ptr(out, ctypes.c_int64), n)
+    return out
+
+
+def geometry_info(fixed, fgeo, moving, mgeo, bins, fmask=None, mmask=None, draw=None):
+    fixed = np.ascontiguousarray(fixed, dtype=np.float32)
+    moving = np.ascontiguousarray(moving, dtype=np.float32)
+    fm = None if fmask is None else np.ascontiguousarray(fmask, dtype=np.uint8)
+    mm = None if mmask is None else np.ascontiguousarray(mmask, dtype=np.uint8)
+    dr = None if draw is None else np.ascontiguousarray(draw, dtype=np.int64)
+    out = np.zeros(8)
+    ns = ctypes.c_int64(0)
+    st = lib().or_metric_geometry(_ptr(fixed, ctypes.c_float), ctypes.byref(fgeo),
+                                  _ptr(moving, ctypes.c_float), ctypes.byref(mgeo),
+                                  _ptr(fm, ctypes.c_uint8), _ptr(mm, ctypes.c_uint8),
+                                  _ptr(dr, ctypes.c_int64), 0 if dr is None else len(dr), bins,
+                                  _ptr(out, ctypes.c_double), ctypes.byref(ns))
+    if st:
+        raise OracleError(st)
+    keys = ["fixed_min", "fixed_max", "moving_min", "moving_max", "fixed_bin_size",
+            "moving_bin_size", "fixed_normalized_min", "moving_normalized_min"]
+    d = dict(zip(keys, out.tolist()))
+    d["nsamples"] = ns.value
+    return d
+
+
+def evaluate(fixed, fgeo, moving, mgeo, bins, kind, params, fixed_params=None, fmask=None,
+             mmask=None, draw=None, derivative=True, nthreads=1, per_sample=False,
+             histogram=False):
+    """value = −MI and derivative (mattes.rs:522-676); returns a dict."""
+    fixed = np.ascontiguousarray(fixed, dtype=np.float32)
+    moving = np.ascontiguousarray(moving, dtype=np.float32)
+    fm = None if fmask is None else np.ascontiguousarray(fmask, dtype=np.uint8)
+    mm = None if mmask is None else np.ascontiguousarray(mmask, dtype=np.uint8)
+    dr = None if draw is None else np.ascontiguousarray(draw, dtype=np.int64)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    fpar = None if fixed_params is None else np.ascontiguousarray(fixed_params, dtype=np.float64)
+    nparams = NPARAMS[kind]
+    deriv = np.zeros(nparams)
+    value = ctypes.c_double(0.0)
+    valid = ctypes.c_int64(0)
+    status = fi = mi = None
+    if per_sample:
+        nvox = int(np.prod([fgeo.size[i] for i in range(3)]))
+        n = nvox if dr is None else len(dr)
+        status = np.full(n, -1, dtype=np.int8)
+        fi = np.full(n, -1, dtype=np.int32)
+        mi = np.full(n, -1, dtype=np.int32)
+    joint = margin = None
+    if histogram:
+        joint = np.zeros(bins * bins)
+        margin = np.zeros(bins)
+    st = lib().or_mattes_evaluate(
+        _ptr(fixed, ctypes.c_float), ctypes.byref(fgeo), _ptr(moving, ctypes.c_float),
+        ctypes.byref(mgeo), _ptr(fm, ctypes.c_uint8), _ptr(mm, ctypes.c_uint8),
+        _ptr(dr, ctypes.c_int64), 0 if dr is None else len(dr), bins, kind,
+        _ptr(params, ctypes.c_double), _ptr(fpar, ctypes.c_double),
+        0 if fpar is None else len(fpar), 1 if derivative else 0, nthreads,
+        ctypes.byref(value), _ptr(deriv, ctypes.c_double), ctypes.byref(valid),
+        _ptr(status, ctypes.c_int8), _ptr(fi, ctypes.c_int32), _ptr(mi, ctypes.c_int32),
+        _ptr(joint, ctypes.c_double), _ptr(margin, ctypes.c_double))
+    if st:
+        raise OracleError(st)
+    out = {"value": value.value, "derivative": deriv, "valid": valid.value}
+    if per_sample:
+        out.update(status=status, fi=fi, mi=mi)
+    if histogram:
+        out.update(joint=joint, fixed_marginal=margin)
+    return out
+
+
+def transform(kind, params, fixed_params=None, point=None):
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    fpar = None if fixed_params is None else np.ascontiguousarray(fixed_params, dtype=np.float64)
+    m = np.zeros(9)
+    o = np.zeros(3)
+    jac = np.zeros(3 * NPARAMS[kind])
+    mapped = np.zeros(3)
+    pt = None if point is None else np.ascontiguousarray(point, dtype=np.float64)
+    st = lib().or_transform(kind, _ptr(params, ctypes.c_double), _ptr(fpar, ctypes.c_double),
+                            0 if fpar is None else len(fpar), _ptr(pt, ctypes.c_double),
+                            _ptr(m, ctypes.c_double), _ptr(o, ctypes.c_double),
+                            _ptr(jac, ctypes.c_double), _ptr(mapped, ctypes.c_double))
+    if st:
+        raise OracleError(st)
+    return {"matrix": m.reshape(3, 3), "offset": o,
+            "jacobian": jac.reshape(3, NPARAMS[kind]), "mapped": mapped}
+
+
+def cubic_bspline(u):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    v = np.zeros_like(u)
+    d = np.zeros_like(u)
+    lib().or_cubic_bspline(_ptr(u, ctypes.c_double), _ptr(v, ctypes.c_double),
+                           _ptr(d, ctypes.c_double), u.size)
+    return v, d
+
+
+def kahan_sum(v):
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    return lib().or_kahan_sum(_ptr(v, ctypes.c_double), v.size)
+
+
+def round_half_integer_up(x: float) -> int:
+    return lib().or_round_half_integer_up(x)

@@ -1,0 +1,113 @@
+// Internal types shared by the translation units of libmi_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "mi_b200.h"
+
+struct mi_context {
+    int device = 0;
+    int num_sms = 0;
+    size_t l2_bytes = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+};
+
+struct mi_image {
+    mi_context* ctx = nullptr;
+    mi_geometry geo{};
+    float* data = nullptr;  // device, x-fastest
+    int64_t n = 0;
+};
+
+namespace mi {
+
+// Sampler constants passed to every metric kernel by value. Matrices are row-major.
+struct SamplerParams {
+    // fixed grid (VirtualGrid, registration/scales.rs:228-271)
+    int64_t fsize0, fsize1, fsize2;
+    double forigin[3];
+    double fi2p[9];
+    // point map stages (matrix_offset.rs:102-109)
+    int nstage;
+    double stage[MI_MAX_STAGES][12];
+    // moving image (MovingImage, registration/metric.rs:681-924)
+    int64_t msize[3];
+    int64_t mstride1, mstride2;
+    double morigin[3];
+    double mp2i[9];
+    double mhi[3];  // (double)size − 0.5, the is_inside upper bound
+    int has_mmask;
+    // histogram geometry (MattesGeometry, mattes.rs:133-186)
+    int bins;
+    double fixed_bin_size, moving_bin_size;
+    double fixed_nmin, moving_nmin;
+    double moving_min, moving_max;
+    // derivative moments are taken about this point to limit cancellation
+    double xref[3];
+};
+
+// Per-metric device scratch and the host-side view of it.
+struct Workspace {
+    unsigned long long* hist = nullptr;  // [bins*bins] joint (2^-32 fixed point), [bins] fixed marginal, [1] valid
+    double* pratio = nullptr;            // [bins*bins] pRatio·nFactor
+    double* tail = nullptr;              // [4]: value, valid, degenerate flag, joint sum
+    double* partials = nullptr;          // [grid_deriv][12]
+    double* result = nullptr;            // [2 + MI_MAX_PARAMS]: value, valid, derivative
+    unsigned int* done_counter = nullptr;
+    double* host_result = nullptr;       // pinned mirror of result
+    int grid_hist = 0, block_hist = 0;
+    int grid_deriv = 0, block_deriv = 0;
+    // optional device-time accounting
+    bool timing = false;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double ms[4] = {0, 0, 0, 0};
+    int64_t timed_evals = 0;
+};
+
+}  // namespace mi
+
+struct mi_metric {
+    mi_context* ctx = nullptr;
+    mi_geometry fgeo{}, mgeo{};
+    float* fixed = nullptr;       // device copy of the fixed volume
+    float* moving = nullptr;      // device copy of the moving volume
+    uint8_t* mmask = nullptr;     // device moving mask or null
+    uint32_t* samples = nullptr;  // device flat indices (sorted); null = the whole grid
+    int64_t n_samples = 0;
+    int bins = 0;
+    mi_metric_info info{};
+    mi::SamplerParams base{};     // everything except the stages
+    mi::Workspace ws;
+};
+
+namespace mi {
+
+mi_status set_error(mi_context* ctx, mi_status s, const std::string& msg);
+mi_status cuda_status(mi_context* ctx, cudaError_t e, const char* where);
+
+// Host-side transform families (transforms.cpp).
+struct AffineForm {
+    int nparams = 0;
+    double stage[12];        // matrix row-major, offset
+    double jac0[3 * MI_MAX_PARAMS];      // J(0), row-major 3×P
+    double jacc[3][3 * MI_MAX_PARAMS];   // ∂J/∂x_e
+};
+mi_status transform_form(int kind, const double* params, int nparams, const double* fixed,
+                         int nfixed, AffineForm* out);
+
+// Core evaluation (mattes.cu).
+mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double* jac0,
+                   const double* jacc, int nparams, bool want_derivative, double* value,
+                   double* derivative, int64_t* valid);
+
+}  // namespace mi
+
+#define MI_CHECK_CUDA(ctx, expr)                                              \
+    do {                                                                      \
+        cudaError_t _e = (expr);                                              \
+        if (_e != cudaSuccess) return mi::cuda_status((ctx), _e, #expr);      \
+    } while (0)

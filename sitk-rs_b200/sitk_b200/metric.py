@@ -1,0 +1,313 @@
+"""Host-side mirror of the reference's device metric seam.
+
+`DeviceImage` follows crates/sitk/src/cuda/image.rs (upload of any scalar pixel type
+to a device f32 volume, to_host), and `DeviceMattesMetric` follows
+registration/device.rs:632-800 (from_device, from_device_sampled, value, evaluate),
+returning a `MetricValue` (registration/metric.rs:1021-1030). Everything runs through
+the C ABI of libmi_b200.so; there is no other compute path.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .transforms import ParametricTransform
+
+_DTYPES = {np.dtype(np.uint8): 0, np.dtype(np.int8): 1, np.dtype(np.uint16): 2,
+           np.dtype(np.int16): 3, np.dtype(np.uint32): 4, np.dtype(np.int32): 5,
+           np.dtype(np.uint64): 6, np.dtype(np.int64): 7, np.dtype(np.float32): 8,
+           np.dtype(np.float64): 9}
+
+SAMPLING_NONE, SAMPLING_REGULAR, SAMPLING_RANDOM, SAMPLING_EXPLICIT = 0, 1, 2, 3
+
+
+def geometry(size, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
+             direction=(1, 0, 0, 0, 1, 0, 0, 0, 1)) -> _lib.MiGeometry:
+    g = _lib.MiGeometry()
+    for i in range(3):
+        g.size[i] = int(size[i])
+        g.spacing[i] = float(spacing[i])
+        g.origin[i] = float(origin[i])
+    for i in range(9):
+        g.direction[i] = float(np.asarray(direction, dtype=np.float64).ravel()[i])
+    return g
+
+
+class Context:
+    """One device, one stream (cuda/backend.rs:30-160)."""
+
+    def __init__(self, device: int = 0):
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(L.mi_context_create(device, ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def sync(self):
+        _lib.check(_lib.load().mi_context_sync(self.handle), self.handle)
+
+    def stream(self) -> int:
+        return _lib.load().mi_context_stream(self.handle) or 0
+
+    def close(self):
+        if self.handle:
+            _lib.load().mi_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Context | None = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class DeviceImage:
+    """A 3-D scalar volume resident on the device as f32 (x-fastest).
+
+    `array` is indexed [z, y, x] (numpy C order of an x-fastest buffer)."""
+
+    def __init__(self, handle, ctx: Context, geo: _lib.MiGeometry):
+        self.handle = handle
+        self.ctx = ctx
+        self.geo = geo
+
+    @classmethod
+    def upload(cls, array, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
+               direction=(1, 0, 0, 0, 1, 0, 0, 0, 1), ctx: Context | None = None) -> "DeviceImage":
+        ctx = ctx or default_context()
+        a = np.ascontiguousarray(array)
+        if a.ndim != 3:
+            raise ValueError("the device metric is 3-D only")  # NotThreeDimensional
+        if np.iscomplexobj(a):
+            code = 100
+        else:
+            code = _DTYPES.get(a.dtype)
+            if code is None:
+                raise TypeError(f"unsupported pixel type {a.dtype}")
+        geo = geometry((a.shape[2], a.shape[1], a.shape[0]), spacing, origin, direction)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mi_image_upload(ctx.handle, a.ctypes.data_as(ctypes.c_void_p), code,
+                                               ctypes.byref(geo), ctypes.byref(h)), ctx.handle)
+        return cls(h, ctx, geo)
+
+    @classmethod
+    def from_device_ptr(cls, ptr: int, size, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
+                        direction=(1, 0, 0, 0, 1, 0, 0, 0, 1), ctx: Context | None = None):
+        ctx = ctx or default_context()
+        geo = geometry(size, spacing, origin, direction)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mi_image_from_device(ctx.handle, ctypes.c_void_p(ptr), ctypes.byref(geo),
+                                                    ctypes.byref(h)), ctx.handle)
+        return cls(h, ctx, geo)
+
+    @property
+    def size(self):
+        return tuple(int(self.geo.size[i]) for i in range(3))
+
+    def to_host(self) -> np.ndarray:
+        nx, ny, nz = self.size
+        out = np.empty((nz, ny, nx), dtype=np.float32)
+        _lib.check(_lib.load().mi_image_to_host(self.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                out.size), self.ctx.handle)
+        return out
+
+    def device_ptr(self) -> int:
+        return _lib.load().mi_image_device_ptr(self.handle) or 0
+
+    def free(self):
+        if self.handle:
+            _lib.load().mi_image_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+@dataclass
+class MetricValue:
+    """registration/metric.rs:1021-1030."""
+    value: float
+    derivative: np.ndarray
+    valid_points: int
+
+
+class DeviceMattesMetric:
+    """Mattes MI over two device-resident images (registration/device.rs:632-800)."""
+
+    def __init__(self, handle, ctx: Context):
+        self.handle = handle
+        self.ctx = ctx
+
+    @classmethod
+    def from_device(cls, fixed: DeviceImage, moving: DeviceImage, bins: int = 50):
+        return cls.from_device_sampled(fixed, moving, None, None, None, bins)
+
+    @classmethod
+    def from_device_sampled(cls, fixed: DeviceImage, moving: DeviceImage, fixed_mask=None,
+                            moving_mask=None, samples=None, bins: int = 50, *,
+                            strategy: int | None = None, percentage: float = 1.0, seed: int = 0):
+        """`samples` is an explicit flat-index list (FixedSamples::selected_indices);
+        alternatively `strategy`/`percentage`/`seed` draw on the device exactly as
+        draw_samples does (registration/metric.rs:419-437)."""
+        ctx = fixed.ctx
+        smp = None
+        keep = []
+        if samples is not None:
+            idx = np.ascontiguousarray(samples, dtype=np.int64)
+            keep.append(idx)
+            smp = _lib.MiSampling(SAMPLING_EXPLICIT, 1.0, 0,
+                                  idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), idx.size)
+        elif strategy is not None and strategy != SAMPLING_NONE:
+            smp = _lib.MiSampling(strategy, float(percentage), int(seed) & (2**64 - 1), None, 0)
+        mm = None
+        if moving_mask is not None:
+            mm = np.ascontiguousarray(np.asarray(moving_mask) != 0, dtype=np.uint8)
+            keep.append(mm)
+        fm_handle = None
+        if fixed_mask is not None:
+            fm_handle = fixed_mask.handle if isinstance(fixed_mask, DeviceImage) else None
+            if fm_handle is None:
+                fmi = DeviceImage.upload(np.asarray(fixed_mask, dtype=np.float32), ctx=ctx)
+                keep.append(fmi)
+                fm_handle = fmi.handle
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mi_metric_create(
+            ctx.handle, fixed.handle, moving.handle, fm_handle,
+            None if mm is None else mm.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+            None if smp is None else ctypes.byref(smp), int(bins), ctypes.byref(h)), ctx.handle)
+        return cls(h, ctx)
+
+    def info(self) -> dict:
+        inf = _lib.MiMetricInfo()
+        _lib.check(_lib.load().mi_metric_info_get(self.handle, ctypes.byref(inf)), self.ctx.handle)
+        return {f: getattr(inf, f) for f, _ in _lib.MiMetricInfo._fields_}
+
+    def sample_count(self) -> int:
+        return int(self.info()["n_samples"])
+
+    def value(self, transform: ParametricTransform) -> float:
+        st = self.stages(transform)
+        v = ctypes.c_double()
+        _lib.check(_lib.load().mi_metric_value(self.handle, st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               st.size // 12, ctypes.byref(v), None), self.ctx.handle)
+        return v.value
+
+    def value_stages(self, stages) -> tuple[float, int]:
+        st = np.ascontiguousarray(stages, dtype=np.float64).ravel()
+        v = ctypes.c_double()
+        n = ctypes.c_int64()
+        _lib.check(_lib.load().mi_metric_value(self.handle, st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               st.size // 12, ctypes.byref(v), ctypes.byref(n)), self.ctx.handle)
+        return v.value, n.value
+
+    def evaluate(self, transform: ParametricTransform) -> MetricValue:
+        p = np.ascontiguousarray(transform.params, dtype=np.float64)
+        fp = np.ascontiguousarray(transform.fixed_params, dtype=np.float64)
+        d = np.zeros(transform.nparams)
+        v = ctypes.c_double()
+        n = ctypes.c_int64()
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.check(_lib.load().mi_metric_value_and_derivative(
+            self.handle, transform.kind, p.ctypes.data_as(dp), p.size,
+            fp.ctypes.data_as(dp) if fp.size else None, fp.size, ctypes.byref(v), d.ctypes.data_as(dp),
+            ctypes.byref(n)), self.ctx.handle)
+        return MetricValue(v.value, d, n.value)
+
+    def evaluate_stages(self, stages, jac0, jacc) -> MetricValue:
+        st = np.ascontiguousarray(stages, dtype=np.float64).ravel()
+        j0 = np.ascontiguousarray(jac0, dtype=np.float64).ravel()
+        jc = np.ascontiguousarray(jacc, dtype=np.float64).ravel()
+        P = j0.size // 3
+        d = np.zeros(P)
+        v = ctypes.c_double()
+        n = ctypes.c_int64()
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.check(_lib.load().mi_metric_value_and_derivative_stages(
+            self.handle, st.ctypes.data_as(dp), st.size // 12, j0.ctypes.data_as(dp), jc.ctypes.data_as(dp),
+            P, ctypes.byref(v), d.ctypes.data_as(dp), ctypes.byref(n)), self.ctx.handle)
+        return MetricValue(v.value, d, n.value)
+
+    def sample_decisions(self, stages):
+        st = np.ascontiguousarray(stages, dtype=np.float64).ravel()
+        n = self.sample_count()
+        status = np.empty(n, dtype=np.int8)
+        fb = np.empty(n, dtype=np.int32)
+        mb = np.empty(n, dtype=np.int32)
+        flat = np.empty(n, dtype=np.int64)
+        P = ctypes.POINTER
+        _lib.check(_lib.load().mi_metric_sample_decisions(
+            self.handle, st.ctypes.data_as(P(ctypes.c_double)), st.size // 12,
+            status.ctypes.data_as(P(ctypes.c_int8)), fb.ctypes.data_as(P(ctypes.c_int32)),
+            mb.ctypes.data_as(P(ctypes.c_int32)), flat.ctypes.data_as(P(ctypes.c_int64)), n), self.ctx.handle)
+        return {"status": status, "fi": fb, "mi": mb, "flat": flat}
+
+    @staticmethod
+    def stages(transform: ParametricTransform) -> np.ndarray:
+        """The transform's point-map stage (matrix row-major, offset), formed by the
+        library's own host code for the family."""
+        return transform_stage(transform)
+
+    def close(self):
+        if self.handle:
+            _lib.load().mi_metric_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def transform_form(transform: ParametricTransform):
+    """(stage[12], jac0[3×P], jacc[3][3×P]) from the library's host transform code
+    (mi_transform_form): the matrix/offset the family multiplies and its Jacobian's
+    affine form, in the reference's operation order."""
+    p = np.ascontiguousarray(transform.params, dtype=np.float64)
+    fp = np.ascontiguousarray(transform.fixed_params, dtype=np.float64)
+    st = np.zeros(12)
+    P = transform.nparams
+    j0 = np.zeros(3 * P)
+    jc = np.zeros(9 * P)
+    dp = ctypes.POINTER(ctypes.c_double)
+    _lib.check(_lib.load().mi_transform_form(transform.kind, p.ctypes.data_as(dp), p.size,
+                                             fp.ctypes.data_as(dp) if fp.size else None, fp.size,
+                                             st.ctypes.data_as(dp), j0.ctypes.data_as(dp),
+                                             jc.ctypes.data_as(dp)))
+    return st, j0.reshape(3, P), jc.reshape(3, 3, P)
+
+
+def transform_stage(transform: ParametricTransform) -> np.ndarray:
+    """The family's point-map stage: matrix row-major then offset."""
+    return transform_form(transform)[0]
+
+
+def enable_timing(metric: DeviceMattesMetric, on: bool = True) -> None:
+    """Record CUDA events around each evaluation's kernels (benchmark accounting)."""
+    _lib.check(_lib.load().mi_metric_timing_enable(metric.handle, 1 if on else 0), metric.ctx.handle)
+
+
+def read_timing(metric: DeviceMattesMetric) -> tuple[np.ndarray, int]:
+    """Accumulated device milliseconds [evaluation, histogram, tail, derivative] and the
+    evaluation count since the last read (then reset)."""
+    ms = np.zeros(4)
+    n = ctypes.c_int64()
+    _lib.check(_lib.load().mi_metric_timing_read(metric.handle, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                 ctypes.byref(n)), metric.ctx.handle)
+    return ms, n.value

