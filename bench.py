@@ -223,7 +223,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         torch.cuda.synchronize(dev)
         metric.evaluate(t)
     # settle clocks under load (untimed)
-    t_end = time.perf_counter() + 1.0
+    t_end = time.perf_counter() + args.settle
     while time.perf_counter() < t_end:
         metric.evaluate(t)
     read_timing(metric)
@@ -317,6 +317,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--settle", type=float, default=1.0,
+                    help="seconds of untimed evaluations before the timed region (clock ramp)")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)

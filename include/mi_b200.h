@@ -187,11 +187,12 @@ mi_status mi_transform_form(int kind, const double* params, int nparams, const d
  * metric's sample order (test hook for the exactness contract): status 0 = outside
  * the moving buffer or masked, 1 = interpolated value outside the moving range,
  * 2 = valid; fixed_bin/moving_bin are the Parzen indices of valid samples (−1
- * otherwise); flat receives each sample's fixed-grid voxel. Any output may be NULL.
- * n is the capacity of each array and must be ≥ n_samples. */
+ * otherwise); flat receives each sample's fixed-grid voxel; exact is 1 where the
+ * sampler's fast path handed the sample to the exact FP64 chain. Any output may be
+ * NULL. n is the capacity of each array and must be ≥ n_samples. */
 mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nstage,
                                      int8_t* status, int32_t* fixed_bin, int32_t* moving_bin,
-                                     int64_t* flat, int64_t n);
+                                     int64_t* flat, int8_t* exact, int64_t n);
 
 #ifdef __cplusplus
 }

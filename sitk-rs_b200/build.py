@@ -46,16 +46,22 @@ def _stale(target, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose: bool = False, force: bool = False, defines: dict | None = None,
+          out: str | None = None, objdir: str | None = None) -> str:
+    """Compile and link the library. `defines` (name → value) override the kernels'
+    compile-time launch-shape constants; `out`/`objdir` place a variant elsewhere."""
+    lib = out or LIB
+    bdir = objdir or BUILD
+    os.makedirs(bdir, exist_ok=True)
     nvcc = _nvcc()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(INCLUDE, "mi_b200.h"))
     objs = []
     common = ["-O3", "-std=c++17", "-I", INCLUDE, "-I", CSRC]
+    common += [f"-D{k}={v}" for k, v in (defines or {}).items()]
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src + ".o")
+        o = os.path.join(bdir, src + ".o")
         if force or _stale(o, [s] + headers):
             cmd = [nvcc, *ARCH, "-lineinfo", *common, "-Xcompiler", "-fPIC,-ffp-contract=off",
                    "-Xptxas", "-v" if verbose else "-O3", "-c", s, "-o", o]
@@ -65,15 +71,15 @@ def build(verbose: bool = False, force: bool = False) -> str:
         objs.append(o)
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src + ".o")
+        o = os.path.join(bdir, src + ".o")
         if force or _stale(o, [s] + headers):
             cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
                    "-I", INCLUDE, "-I", CSRC, "-I", "/usr/local/cuda/include", "-c", s, "-o", o]
             _run(cmd)
         objs.append(o)
-    if force or _stale(LIB, objs):
-        _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs])
-    return LIB
+    if force or _stale(lib, objs):
+        _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", lib, *objs])
+    return lib
 
 
 if __name__ == "__main__":

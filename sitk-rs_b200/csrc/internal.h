@@ -25,12 +25,45 @@ struct mi_image {
 
 namespace mi {
 
+// Division of a u32 by a run-time-invariant divisor through a multiply-high
+// (Granlund & Montgomery, "Division by invariant integers using multiplication",
+// PLDI 1994, round-up variant): q = (umulhi(n, m) + n) >> s with s = ceil(log2 d),
+// m = floor(2^32·(2^s − d)/d) + 1, exact for every n < 2^32.
+struct FastDiv {
+    uint32_t d, m, s;
+};
+
+inline FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f{d, 0, 0};
+    uint32_t s = 0;
+    while (s < 32 && (1ull << s) < d) ++s;
+    f.s = s;
+    f.m = (uint32_t)(((1ull << 32) * ((1ull << s) - d)) / d + 1);
+    return f;
+}
+
 // Sampler constants passed to every metric kernel by value. Matrices are row-major.
 struct SamplerParams {
     // fixed grid (VirtualGrid, registration/scales.rs:228-271)
     int64_t fsize0, fsize1, fsize2;
+    FastDiv div0, div1;
     double forigin[3];
     double fi2p[9];
+    // fast path: the composite map from grid index to moving continuous index,
+    // c ≈ cA·(i, j, k) + cb (FP64 FMAs), within cerr of the exact chain's c
+    double cA[9], cb[3];
+    double cerr;
+    // inside-test bounds with a 2·cerr margin: surely inside c ∈ [ilo, ihi),
+    // surely outside c < olo or c ≥ ohi
+    double ilo, olo, ihi[3], ohi[3];
+    double bin_hi;  // (double)(bins − 3), the top Parzen bin
+    // fast path: fixed physical point relative to xref in FP32, x − xref ≈ xA·(i,j,k) + xb
+    float xA[9], xb[3];
+    float mp2if[9];  // physical→index matrix in FP32 (gradient only)
+    int msz[3];      // moving size, 32-bit (the volume is below 2^32 voxels)
+    uint32_t ms1, ms2;  // moving strides, 32-bit
+    cudaTextureObject_t mtex;  // the moving volume as a 3-D texture (point, clamp, unnormalised)
+    double inv_moving_bin_size;
     // point map stages (matrix_offset.rs:102-109)
     int nstage;
     double stage[MI_MAX_STAGES][12];
@@ -59,6 +92,13 @@ struct Workspace {
     double* result = nullptr;            // [2 + MI_MAX_PARAMS]: value, valid, derivative
     unsigned int* done_counter = nullptr;
     double* host_result = nullptr;       // pinned mirror of result
+    // per-sample records pass 1 hands pass 2 (struct of arrays, sample order):
+    // moving bin (0 = not a valid sample), Parzen fraction, moving gradient
+    uint8_t* rec_mi = nullptr;
+    float* rec_f = nullptr;
+    float* rec_g = nullptr;              // [3][n_samples]
+    float hist_scale = 0.f;              // fixed-point scale of a joint-histogram tap
+    int hist_scale_log2 = 0;
     int grid_hist = 0, block_hist = 0;
     int grid_deriv = 0, block_deriv = 0;
     // optional device-time accounting
@@ -76,7 +116,10 @@ struct mi_metric {
     float* fixed = nullptr;       // device copy of the fixed volume
     float* moving = nullptr;      // device copy of the moving volume
     uint8_t* mmask = nullptr;     // device moving mask or null
+    cudaArray_t marray = nullptr; // the moving volume in a block-linear 3-D array
+    cudaTextureObject_t mtex = 0; // point-sampling, clamp-to-edge texture over marray
     uint32_t* samples = nullptr;  // device flat indices (sorted); null = the whole grid
+    uint8_t* fbin = nullptr;      // device fixed Parzen bin of every sample (exact, set-up time)
     int64_t n_samples = 0;
     int bins = 0;
     mi_metric_info info{};

@@ -1,20 +1,24 @@
 // Mattes mutual information on the device: metric set-up and the per-evaluation
 // kernels.
 //
-// One evaluation (DeviceMattesMetric::evaluate, registration/device.rs:767-800) is
-//   k_hist   pass 1: sampler → Parzen joint histogram in shared memory (per CTA,
-//            2^-32 fixed point in u64, so every add is exact and the result does
-//            not depend on the order), flushed into a global u64 histogram
-//   k_tail   one CTA: normalisation, marginals, −MI, pRatio·nFactor table
-//            (registration/mattes.rs:273-328)
-//   k_deriv  pass 2: sampler with gradient → 12 moments A[d] = Σ w g_d,
-//            B[d][e] = Σ w g_d (x_e − x_ref,e) with w = Σ_taps B₃′·pRatio
-//            (cuda/ops/mattes.rs:319-381 is the reference's form), per-CTA partials
-//            in a fixed shuffle/tree order; the last CTA to finish folds the partials
-//            in CTA order and contracts them with the transform's Jacobian form
-//            (registration/cuda.rs:505-524)
-// and one 8·(2+P)-byte copy back. Every reduction order is a function of the
-// launch shape alone, so repeated evaluations are bit-identical.
+// One evaluation (DeviceMattesMetric::evaluate, registration/device.rs:767-800) is two
+// launches and one 8·(2+P)-byte copy back:
+//   k_hist   pass 1: sampler (value and gradient) → Parzen joint histogram, per CTA
+//            in shared memory as u32 fixed point (native shared atomics), flushed
+//            into a global u64 histogram. Integer adds are exact, so the histogram does
+//            not depend on the order. Each sample also leaves a 17-byte record
+//            (moving bin, Parzen fraction, moving gradient) for pass 2. The last CTA
+//            to finish runs the tail (registration/mattes.rs:273-328): normalisation,
+//            marginals, −MI and the pRatio·nFactor table, and re-zeroes the global
+//            histogram for the next evaluation.
+//   k_deriv  pass 2: streams the records → 12 moments A[d] = Σ w g_d,
+//            B[d][e] = Σ w g_d (x_e − x_ref,e), w = Σ_taps B₃′·pRatio (the form of the
+//            reference's mattes_deriv, cuda/ops/mattes.rs:319-381), FP32 per thread and
+//            FP64 from the warp reduction on, in a fixed shuffle/tree order into per-CTA
+//            partials; the last CTA folds the partials in CTA order and contracts them
+//            with the transform's Jacobian form (registration/cuda.rs:505-524).
+// Every reduction order is a function of the launch shape alone, so repeated
+// evaluations are bit-identical. No kernel waits on another CTA.
 
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
@@ -38,11 +42,19 @@ bool invert3(const double* m, double* inv);
 
 namespace {
 
-constexpr double FIX_SCALE = 4294967296.0;        // 2^32
-constexpr double FIX_INV = 1.0 / 4294967296.0;    // 2^-32
+// Launch shape of the histogram pass: HIST_ILP samples per thread in flight (their
+// corner gathers issued together), and a register cap that keeps HIST_MIN_BLOCKS
+// CTAs of HIST_BLOCK threads resident per SM.
+#ifndef MI_HIST_ILP
+#define MI_HIST_ILP 2
+#endif
+#ifndef MI_HIST_MIN_BLOCKS
+#define MI_HIST_MIN_BLOCKS 4
+#endif
 constexpr int HIST_BLOCK = 256;
+constexpr int HIST_MIN_BLOCKS = MI_HIST_MIN_BLOCKS;
+constexpr int HIST_ILP = MI_HIST_ILP;
 constexpr int DERIV_BLOCK = 256;
-constexpr int TAIL_BLOCK = 1024;
 constexpr int NMOM = 12;
 
 struct JacobianForm {
@@ -51,47 +63,21 @@ struct JacobianForm {
     double jacc[3][3 * MI_MAX_PARAMS];
 };
 
-// ---------------------------------------------------------------------------
-// Pass 1: joint histogram.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(HIST_BLOCK)
-k_hist(SamplerParams P, const float* __restrict__ fixed, const float* __restrict__ moving,
-       const uint8_t* __restrict__ mmask, const uint32_t* __restrict__ samples, int64_t n,
-       unsigned long long* __restrict__ ghist) {
-    extern __shared__ unsigned long long sh[];
-    const int B = P.bins;
-    const int nb = B * B + B;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) sh[i] = 0ull;
-    __syncthreads();
-    unsigned long long* sh_joint = sh;
-    unsigned long long* sh_fixed = sh + B * B;
-    unsigned int valid = 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
-        const uint32_t flat = samples ? __ldg(samples + s) : (uint32_t)s;
-        Sample o;
-        if (take_sample<false>(P, flat, fixed, moving, mmask, o) != SAMPLE_VALID) continue;
-        ++valid;
-        atomicAdd(&sh_fixed[o.fi], 1ull);
-        unsigned long long* row = sh_joint + o.fi * B;
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const int m = o.mi - 1 + t;
-            const double w = bspline3((double)m - o.mterm);
-            const unsigned long long q = __double2ull_rn(w * FIX_SCALE);
-            if (q) atomicAdd(&row[m], q);
-        }
-    }
-    // valid count: one atomic per warp
-    unsigned int wv = valid;
-#pragma unroll
-    for (int off = 16; off; off >>= 1) wv += __shfl_down_sync(0xffffffffu, wv, off);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0 && wv) atomicAdd(&ghist[nb], (unsigned long long)wv);
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-        const unsigned long long v = sh[i];
-        if (v) atomicAdd(&ghist[i], v);
-    }
+// Dynamic shared memory of the tail: jp[B²], fm[B], mm[B], lfm[B], red[32] doubles.
+__host__ __device__ inline size_t tail_doubles(int B) { return (size_t)B * B + 3 * (size_t)B + 32; }
+
+// One histogram copy: B² joint + B fixed-marginal u32 counters, padded so copies
+// start 4 banks apart.
+__host__ __device__ inline int hist_copy_stride(int B) { return ((B * B + B + 31) & ~31) + 4; }
+// Copies that fit in 48 KB (a power of two, 1–8).
+int hist_copies(int B) {
+    int c = 8;
+    while (c > 1 && (size_t)c * hist_copy_stride(B) * sizeof(unsigned int) > 48 * 1024) c >>= 1;
+    return c;
+}
+size_t hist_smem(int B) { return (size_t)hist_copies(B) * hist_copy_stride(B) * sizeof(unsigned int); }
+size_t deriv_smem(int B) {
+    return ((size_t)32 * NMOM + tail_doubles(B)) * sizeof(double) + (size_t)B * B * sizeof(float);
 }
 
 // Block-wide sum of a double in a fixed order (warp shuffles, then warp 0).
@@ -116,43 +102,46 @@ __device__ double block_sum(double v, double* red) {
     return r;
 }
 
-// ---------------------------------------------------------------------------
-// Tail: normalise, marginals, −MI, pRatio (registration/mattes.rs:273-328).
-// tail[0] value, tail[1] valid, tail[2] degenerate flag, tail[3] joint sum;
-// result[0..1] receive value and valid for the value-only path.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(TAIL_BLOCK)
-k_tail(int B, double moving_bin_size, const unsigned long long* __restrict__ ghist,
-       double* __restrict__ pratio, double* __restrict__ tail, double* __restrict__ result) {
-    extern __shared__ double tsh[];
-    double* jp = tsh;              // B*B
-    double* fm = jp + B * B;       // B
-    double* mm = fm + B;           // B
-    double* lfm = mm + B;          // B
-    double* red = lfm + B;         // 32
+struct TailOut {
+    double value;      // −MI, or DBL_MAX for a degenerate histogram
+    double valid;      // valid-sample count
+    bool degenerate;   // no valid sample or no mass (mattes.rs:590-609)
+};
+
+// The tail (registration/mattes.rs:273-328) over the finished global histogram,
+// computed by one CTA into its shared memory: normalisation, marginals, −MI and the
+// pRatio·nFactor table (written to pr, FP32, when non-null). ghist holds the joint
+// taps (fixed point, hist_inv per unit) then the fixed-marginal counts; it is only
+// read. The sums are FP64 block reductions in a fixed order. Every CTA that calls
+// this on the same histogram gets the same bits.
+__device__ TailOut run_tail(int B, double moving_bin_size, double hist_inv,
+                            const unsigned long long* __restrict__ ghist, double* tsh, float* pr) {
+    double* jp = tsh;         // B*B
+    double* fm = jp + B * B;  // B
+    double* mm = fm + B;      // B
+    double* lfm = mm + B;     // B
+    double* red = lfm + B;    // 32
     const int B2 = B * B;
-    const unsigned long long valid = ghist[B2 + B];
-    double part = 0.0;
+    double part = 0.0, cnt = 0.0;
     for (int i = threadIdx.x; i < B2; i += blockDim.x) {
-        const double v = (double)ghist[i] * FIX_INV;
+        const double v = (double)__ldcg(ghist + i) * hist_inv;
         jp[i] = v;
         part += v;
     }
-    for (int i = threadIdx.x; i < B; i += blockDim.x) fm[i] = (double)ghist[B2 + i];
-    const double joint_sum = block_sum(part, red);
-    if (valid == 0 || joint_sum < DBL_EPSILON) {
-        // degenerate histogram (mattes.rs:590-609): value f64::MAX, zero derivative
-        if (threadIdx.x == 0) {
-            tail[0] = DBL_MAX;
-            tail[1] = (double)valid;
-            tail[2] = 1.0;
-            tail[3] = joint_sum;
-            result[0] = DBL_MAX;
-            result[1] = (double)valid;
-        }
-        return;
+    for (int i = threadIdx.x; i < B; i += blockDim.x) {
+        const double c = (double)__ldcg(ghist + B2 + i);
+        fm[i] = c;
+        cnt += c;
     }
-    const double n_factor = 1.0 / (moving_bin_size * (double)valid);
+    TailOut out;
+    const double joint_sum = block_sum(part, red);
+    out.valid = block_sum(cnt, red);
+    out.degenerate = out.valid == 0.0 || joint_sum < DBL_EPSILON;
+    if (out.degenerate) {
+        out.value = DBL_MAX;
+        return out;
+    }
+    const double n_factor = 1.0 / (moving_bin_size * out.valid);
     const double inv_sum = 1.0 / joint_sum;
     for (int i = threadIdx.x; i < B2; i += blockDim.x) jp[i] *= inv_sum;
     for (int i = threadIdx.x; i < B; i += blockDim.x) {
@@ -177,99 +166,245 @@ k_tail(int B, double moving_bin_size, const unsigned long long* __restrict__ ghi
             sum += p * (lr - lfm[f]);
             r = lr * n_factor;
         }
-        pratio[i] = r;
+        if (pr) pr[i] = (float)r;
     }
-    const double total = block_sum(sum, red);
+    out.value = -block_sum(sum, red);
+    return out;
+}
+
+// Value-only tail: one CTA, then the global histogram is re-zeroed.
+__global__ void __launch_bounds__(256)
+k_value(int B, double moving_bin_size, double hist_inv, unsigned long long* __restrict__ ghist,
+        double* __restrict__ result) {
+    extern __shared__ double tsh[];
+    const TailOut t = run_tail(B, moving_bin_size, hist_inv, ghist, tsh, nullptr);
     if (threadIdx.x == 0) {
-        tail[0] = -total;
-        tail[1] = (double)valid;
-        tail[2] = 0.0;
-        tail[3] = joint_sum;
-        result[0] = -total;
-        result[1] = (double)valid;
+        result[0] = t.value;
+        result[1] = t.valid;
+    }
+    for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) ghist[i] = 0ull;
+}
+
+// ---------------------------------------------------------------------------
+// Pass 1: joint histogram (+ per-sample records for pass 2), then the tail in the
+// last CTA. The CTA histogram is u32 fixed point: a tap w is added as
+// round(w·2^k) with k chosen per launch so that no CTA's bin can exceed 2^32
+// (hist_scale = 2^k); the flush into the global histogram is u64.
+// ---------------------------------------------------------------------------
+template <bool RECORD>
+__global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
+k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restrict__ mmask,
+       const uint32_t* __restrict__ samples, const uint8_t* __restrict__ fbin, uint32_t n, uint32_t npad,
+       float hist_scale, int copies, unsigned long long* __restrict__ ghist, uint8_t* __restrict__ rec_mi,
+       float* __restrict__ rec_f, float* __restrict__ rec_g) {
+    extern __shared__ unsigned int sh[];
+    const int B = P.bins;
+    const int nb = B * B + B;
+    const int cstride = hist_copy_stride(B);
+    for (int i = threadIdx.x; i < copies * cstride; i += blockDim.x) sh[i] = 0u;
+    __syncthreads();
+    unsigned int* sh_joint = sh;
+    unsigned int* sh_fixed = sh + B * B;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // Two samples per iteration: both samples' corner gathers are issued (prep) before
+    // either is finished, so each thread keeps two gathers in flight.
+    // The CTA keeps `copies` interleaved copies of the histogram and lane l adds into
+    // copy l mod copies: neighbouring lanes, whose sorted samples usually share a bin
+    // pair, then add to different addresses instead of replaying on one. The copies
+    // are summed at the flush (integer adds: the order does not matter).
+    const int lane = threadIdx.x & 31;
+    unsigned int* my_joint = sh_joint + (lane & (copies - 1)) * cstride;
+    unsigned int* my_fixed = sh_fixed + (lane & (copies - 1)) * cstride;
+    auto account = [&](const Prep& p, uint32_t s, bool real) {
+        if (!real) return;
+        Sample o;
+        o.exact = false;
+        const int st = finish<RECORD>(P, p, moving, o);
+        if (st != SAMPLE_VALID) {
+            if (RECORD) rec_mi[s] = 0;
+            return;
+        }
+        const int fi = __ldg(fbin + s);
+        float w[4];
+        bspline3_taps(o.f, w);
+        unsigned int* row = my_joint + fi * B + (o.mi - 1);
+        // round(w·2^k) by the 1.5·2^23 magic add (w·2^k < 2^22): one FMA, no conversion
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            atomicAdd(row + t, __float_as_uint(fmaf(w[t], hist_scale, 12582912.0f)) - 0x4B400000u);
+        atomicAdd(my_fixed + fi, 1u);
+        if (RECORD) {
+            rec_mi[s] = (uint8_t)o.mi;
+            rec_f[s] = o.f;
+            rec_g[s] = o.g[0];
+            rec_g[(size_t)npad + s] = o.g[1];
+            rec_g[2 * (size_t)npad + s] = o.g[2];
+        }
+    };
+    // whole warps iterate together: the loop bound is the warp's first sample
+    const uint32_t wbase = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    if (HIST_ILP == 2) {
+        for (uint32_t b = wbase; b < n; b += 2 * stride) {
+            const uint32_t s = b + lane, s2 = s + stride;
+            const bool one = s < n, two = s2 < n;
+            const uint32_t fa = one ? (samples ? __ldg(samples + s) : s) : 0u;
+            const uint32_t fb = two ? (samples ? __ldg(samples + s2) : s2) : fa;
+            Prep pa, pb;
+            prep<RECORD>(P, fa, moving, mmask, pa);
+            prep<RECORD>(P, fb, moving, mmask, pb);
+            account(pa, s, one);
+            account(pb, s2, two);
+        }
+    } else {
+        for (uint32_t b = wbase; b < n; b += stride) {
+            const uint32_t s = b + lane;
+            const bool one = s < n;
+            Prep pa;
+            prep<RECORD>(P, one ? (samples ? __ldg(samples + s) : s) : 0u, moving, mmask, pa);
+            account(pa, s, one);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        unsigned long long v = 0ull;
+        for (int c = 0; c < copies; ++c) v += sh[c * cstride + i];
+        if (v) atomicAdd(&ghist[i], v);
     }
 }
 
 // ---------------------------------------------------------------------------
-// Pass 2: derivative moments, with the last CTA folding and contracting.
+// Pass 2: derivative moments streamed from the pass-1 records, FP32 per thread,
+// FP64 from the warp reduction on; the last CTA folds the CTA partials in CTA order
+// and contracts them with the transform's Jacobian form.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void accumulate_moments(const SamplerParams& P, const float* pr, int B, int mi, int fi,
+                                                   float f, float g0, float g1, float g2, uint32_t flat,
+                                                   float* acc) {
+    uint32_t i, j, k;
+    grid_index(P, flat, i, j, k);
+    const float fi_ = (float)i, fj = (float)j, fk = (float)k;
+    float dx[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        dx[d] = fmaf(P.xA[d * 3 + 2], fk, fmaf(P.xA[d * 3 + 1], fj, fmaf(P.xA[d * 3 + 0], fi_, P.xb[d])));
+    float dw[4];
+    bspline3_deriv_taps(f, dw);
+    const float* row = pr + fi * B + (mi - 1);
+    const float w = fmaf(dw[3], row[3], fmaf(dw[2], row[2], fmaf(dw[1], row[1], dw[0] * row[0])));
+    const float wg[3] = {w * g0, w * g1, w * g2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        acc[d] += wg[d];
+        acc[3 + d * 3 + 0] = fmaf(wg[d], dx[0], acc[3 + d * 3 + 0]);
+        acc[3 + d * 3 + 1] = fmaf(wg[d], dx[1], acc[3 + d * 3 + 1]);
+        acc[3 + d * 3 + 2] = fmaf(wg[d], dx[2], acc[3 + d * 3 + 2]);
+    }
+}
+
+// Records are read four samples per thread with 4-, 16- and 16-byte vector loads
+// (every record array is padded to a multiple of four samples; padding records carry
+// moving bin 0 and are skipped).
 __global__ void __launch_bounds__(DERIV_BLOCK)
-k_deriv(SamplerParams P, JacobianForm J, const float* __restrict__ fixed,
-        const float* __restrict__ moving, const uint8_t* __restrict__ mmask,
-        const uint32_t* __restrict__ samples, int64_t n, const double* __restrict__ pratio_g,
-        const double* __restrict__ tail, double* __restrict__ partials,
-        unsigned int* __restrict__ done_counter, double* __restrict__ result) {
+k_deriv(SamplerParams P, JacobianForm J, const uint32_t* __restrict__ samples, const uint8_t* __restrict__ fbin,
+        uint32_t npad, const uint8_t* __restrict__ rec_mi, const float* __restrict__ rec_f,
+        const float* __restrict__ rec_g, double hist_inv, unsigned long long* __restrict__ ghist,
+        double* __restrict__ partials, unsigned int* __restrict__ done_counter, double* __restrict__ result) {
     extern __shared__ double dsh[];
     const int B = P.bins;
-    double* pr = dsh;                 // B*B
-    double* red = dsh + B * B;        // 32 * NMOM
+    double* red = dsh;                                          // 32 * NMOM
+    double* tsh = dsh + 32 * NMOM;                              // tail scratch
+    float* pr = reinterpret_cast<float*>(tsh + tail_doubles(B));  // B*B
     __shared__ bool is_last;
-    const bool degenerate = tail[2] != 0.0;
-    double acc[NMOM];
+    __shared__ double mom[NMOM];
+    // Every CTA forms the tail itself (same histogram, same bits): no CTA waits for
+    // a single one to finish it.
+    const TailOut tail = run_tail(B, P.moving_bin_size, hist_inv, ghist, tsh, pr);
+    const bool degenerate = tail.degenerate;
+    float acc[NMOM];
 #pragma unroll
-    for (int i = 0; i < NMOM; ++i) acc[i] = 0.0;
+    for (int i = 0; i < NMOM; ++i) acc[i] = 0.0f;
     if (!degenerate) {
-        for (int i = threadIdx.x; i < B * B; i += blockDim.x) pr[i] = pratio_g[i];
         __syncthreads();
-        const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-        for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
-            const uint32_t flat = samples ? __ldg(samples + s) : (uint32_t)s;
-            Sample o;
-            if (take_sample<true>(P, flat, fixed, moving, mmask, o) != SAMPLE_VALID) continue;
-            const double* row = pr + o.fi * B;
-            double w = 0.0;
-#pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                const int m = o.mi - 1 + t;
-                w += bspline3_deriv((double)m - o.mterm) * row[m];
-            }
-            if (w == 0.0) continue;
-            const double dx0 = o.x[0] - P.xref[0], dx1 = o.x[1] - P.xref[1], dx2 = o.x[2] - P.xref[2];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double wg = w * o.g[d];
-                acc[d] += wg;
-                acc[3 + d * 3 + 0] += wg * dx0;
-                acc[3 + d * 3 + 1] += wg * dx1;
-                acc[3 + d * 3 + 2] += wg * dx2;
-            }
+        const uint32_t stride = gridDim.x * blockDim.x;
+        const uint32_t ngroups = npad >> 2;
+        const uchar4* mi4p = reinterpret_cast<const uchar4*>(rec_mi);
+        const uchar4* fb4p = reinterpret_cast<const uchar4*>(fbin);
+        const float4* f4p = reinterpret_cast<const float4*>(rec_f);
+        const float4* gx4p = reinterpret_cast<const float4*>(rec_g);
+        const float4* gy4p = reinterpret_cast<const float4*>(rec_g + npad);
+        const float4* gz4p = reinterpret_cast<const float4*>(rec_g + 2 * (size_t)npad);
+        const uint4* s4p = reinterpret_cast<const uint4*>(samples);
+        for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < ngroups; q += stride) {
+            const uchar4 mi4 = __ldg(mi4p + q);
+            if (!(mi4.x | mi4.y | mi4.z | mi4.w)) continue;
+            const float4 f4 = __ldg(f4p + q);
+            const float4 gx = __ldg(gx4p + q), gy = __ldg(gy4p + q), gz = __ldg(gz4p + q);
+            const uchar4 fb4 = __ldg(fb4p + q);
+            const uint4 fl4 = samples ? __ldg(s4p + q) : make_uint4(4 * q, 4 * q + 1, 4 * q + 2, 4 * q + 3);
+            if (mi4.x) accumulate_moments(P, pr, B, mi4.x, fb4.x, f4.x, gx.x, gy.x, gz.x, fl4.x, acc);
+            if (mi4.y) accumulate_moments(P, pr, B, mi4.y, fb4.y, f4.y, gx.y, gy.y, gz.y, fl4.y, acc);
+            if (mi4.z) accumulate_moments(P, pr, B, mi4.z, fb4.z, f4.z, gx.z, gy.z, gz.z, fl4.z, acc);
+            if (mi4.w) accumulate_moments(P, pr, B, mi4.w, fb4.w, f4.w, gx.w, gy.w, gz.w, fl4.w, acc);
         }
     }
-    // CTA reduction in a fixed order: shuffles within a warp, then warp 0 over warps.
+    // CTA reduction in a fixed order: shuffles within a warp, then over warps.
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double accd[NMOM];
 #pragma unroll
     for (int i = 0; i < NMOM; ++i) {
-        double v = acc[i];
+        double v = (double)acc[i];
 #pragma unroll
         for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        acc[i] = v;
+        accd[i] = v;
     }
     if (lane == 0)
-        for (int i = 0; i < NMOM; ++i) red[warp * NMOM + i] = acc[i];
+        for (int i = 0; i < NMOM; ++i) red[warp * NMOM + i] = accd[i];
     __syncthreads();
+    // partials are stored slot-major, [slot][CTA], so the fold reads them coalesced
     if (threadIdx.x < NMOM) {
         double v = 0.0;
         for (int w = 0; w < nw; ++w) v += red[w * NMOM + threadIdx.x];
-        partials[(int64_t)blockIdx.x * NMOM + threadIdx.x] = v;
+        partials[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
     }
-    // Last CTA to arrive folds every CTA's partials in CTA order (no waiting).
+    // The last CTA to arrive folds every CTA's partials (no CTA waits on another),
+    // and — every CTA having read the histogram in its prologue — re-zeroes it for
+    // the next evaluation.
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) is_last = atomicAdd(done_counter, 1u) == gridDim.x - 1;
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    __shared__ double mom[NMOM];
+    for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) ghist[i] = 0ull;
+    // fold in a fixed order: lane l of a slot sums CTAs l, l+21, … four loads at a
+    // time; the 21 lane sums of a slot are then added in lane order
+    constexpr int FOLD = 21;
+    __shared__ double fold[FOLD * NMOM];
+    if (threadIdx.x < FOLD * NMOM) {
+        const int slot = threadIdx.x / FOLD, ln = threadIdx.x % FOLD;
+        const double* src = partials + (int64_t)slot * gridDim.x;
+        double v = 0.0;
+        unsigned int b = ln;
+        for (; b + 3 * FOLD < gridDim.x; b += 4 * FOLD) {
+            const double a0 = __ldcg(src + b), a1 = __ldcg(src + b + FOLD);
+            const double a2 = __ldcg(src + b + 2 * FOLD), a3 = __ldcg(src + b + 3 * FOLD);
+            v += a0;
+            v += a1;
+            v += a2;
+            v += a3;
+        }
+        for (; b < gridDim.x; b += FOLD) v += __ldcg(src + b);
+        fold[slot * FOLD + ln] = v;
+    }
+    __syncthreads();
     if (threadIdx.x < NMOM) {
         double v = 0.0;
-        for (unsigned int b = 0; b < gridDim.x; ++b)
-            v += __ldcg(partials + (int64_t)b * NMOM + threadIdx.x);
+        for (int l = 0; l < FOLD; ++l) v += fold[threadIdx.x * FOLD + l];
         mom[threadIdx.x] = v;
     }
     __syncthreads();
     if (threadIdx.x == 0) *done_counter = 0u;
-    // Contract: ∂/∂p_k = Σ_d J(x_ref)[d][k]·A_d + Σ_{d,e} C_e[d][k]·B[d][e],
-    // with J(x_ref) = J(0) + Σ_e x_ref,e·C_e.
+    // ∂/∂p_k = Σ_d J(x_ref)[d][k]·A_d + Σ_{d,e} C_e[d][k]·B[d][e],  J(x_ref) = J(0) + Σ_e x_ref,e·C_e
     const int np = J.nparams;
     if (threadIdx.x < np) {
         const int k = threadIdx.x;
@@ -285,35 +420,37 @@ k_deriv(SamplerParams P, JacobianForm J, const float* __restrict__ fixed,
         result[2 + k] = dk;
     }
     if (threadIdx.x == 0) {
-        result[0] = tail[0];
-        result[1] = tail[1];
+        result[0] = tail.value;
+        result[1] = tail.valid;
     }
 }
 
-// Per-sample decisions, for the exactness tests.
-__global__ void k_decisions(SamplerParams P, const float* __restrict__ fixed,
-                            const float* __restrict__ moving, const uint8_t* __restrict__ mmask,
-                            const uint32_t* __restrict__ samples, int64_t n,
-                            int8_t* __restrict__ status, int32_t* __restrict__ fbin,
-                            int32_t* __restrict__ mbin, int64_t* __restrict__ flat_out) {
+// Per-sample decisions of the same sampler the kernels use, for the exactness tests.
+__global__ void k_decisions(SamplerParams P, const float* __restrict__ moving,
+                            const uint8_t* __restrict__ mmask, const uint32_t* __restrict__ samples,
+                            const uint8_t* __restrict__ fbin, int64_t n, int8_t* __restrict__ status,
+                            int32_t* __restrict__ fb, int32_t* __restrict__ mb, int64_t* __restrict__ flat_out,
+                            int8_t* __restrict__ exact_out) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
         const uint32_t flat = samples ? samples[s] : (uint32_t)s;
         Sample o;
-        const int st = take_sample<false>(P, flat, fixed, moving, mmask, o);
-        if (status) status[s] = (int8_t)st;
-        if (fbin) fbin[s] = st == SAMPLE_VALID ? o.fi : -1;
-        if (mbin) mbin[s] = st == SAMPLE_VALID ? o.mi : -1;
-        if (flat_out) flat_out[s] = flat;
+        o.exact = false;
+        const int st = sample<false>(P, flat, moving, mmask, o);
+        status[s] = (int8_t)st;
+        fb[s] = st == SAMPLE_VALID ? (int)fbin[s] : -1;
+        mb[s] = st == SAMPLE_VALID ? o.mi : -1;
+        flat_out[s] = flat;
+        exact_out[s] = o.exact ? 1 : 0;
     }
 }
 
 // ---------------------------------------------------------------------------
-// Set-up kernels: the draw, the fixed-mask gate, and the intensity ranges.
+// Set-up kernels: the draw, the fixed-mask gate, the ranges and the fixed bins.
 // ---------------------------------------------------------------------------
 __global__ void k_draw_random(uint64_t seed, uint64_t voxels, int64_t count, uint32_t* out) {
-    // SplitMix64 (registration/metric.rs:101-122): the i-th output follows
-    // i+1 advances of the state, so draw i is mix(seed + (i+1)·γ) mod voxels.
+    // SplitMix64 (registration/metric.rs:101-122): the i-th output follows i+1
+    // advances of the state, so draw i is mix(seed + (i+1)·γ) mod voxels.
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
         uint64_t z = seed + (uint64_t)(i + 1) * 0x9E3779B97F4A7C15ull;
@@ -330,8 +467,8 @@ __global__ void k_iota_stride(int64_t count, uint64_t stride_v, uint32_t* out) {
         out[i] = (uint32_t)((uint64_t)i * stride_v);
 }
 
-__global__ void k_mask_flags(const uint32_t* __restrict__ idx, int64_t count,
-                             const float* __restrict__ fmask, uint8_t* __restrict__ flags) {
+__global__ void k_mask_flags(const uint32_t* __restrict__ idx, int64_t count, const float* __restrict__ fmask,
+                             uint8_t* __restrict__ flags) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
         flags[i] = fmask[idx[i]] != 0.0f ? 1 : 0;
@@ -357,7 +494,10 @@ __global__ void k_minmax(const float* __restrict__ vals, const uint32_t* __restr
         hi = fmaxf(hi, __shfl_down_sync(0xffffffffu, hi, off));
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) { slo[warp] = lo; shi[warp] = hi; }
+    if (lane == 0) {
+        slo[warp] = lo;
+        shi[warp] = hi;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
@@ -369,6 +509,20 @@ __global__ void k_minmax(const float* __restrict__ vals, const uint32_t* __restr
     }
 }
 
+// The exact fixed Parzen bin of every sample, in sample order.
+__global__ void k_fixed_bins(SamplerParams P, const float* __restrict__ fixed, const uint32_t* __restrict__ samples,
+                             int64_t n, uint8_t* __restrict__ fbin) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
+        const uint32_t flat = samples ? samples[s] : (uint32_t)s;
+        fbin[s] = (uint8_t)fixed_bin(P, fixed[flat]);
+    }
+}
+
+// Sample arrays are padded to whole groups of four (the derivative pass reads them
+// with vector loads); at least one group is always allocated.
+size_t pad4(int64_t n) { return (size_t)((std::max<int64_t>(n, 1) + 3) & ~(int64_t)3); }
+
 int grid_for(int64_t n, int block, int cap) {
     int64_t g = (n + block - 1) / block;
     if (g > cap) g = cap;
@@ -376,8 +530,8 @@ int grid_for(int64_t n, int block, int cap) {
     return (int)g;
 }
 
-mi_status minmax(mi_context* ctx, const float* vals, const uint32_t* idx, const uint8_t* mask,
-                 int64_t n, double* lo, double* hi, bool* any) {
+mi_status minmax(mi_context* ctx, const float* vals, const uint32_t* idx, const uint8_t* mask, int64_t n,
+                 double* lo, double* hi, bool* any) {
     const int block = 256;
     const int grid = grid_for(n, block, ctx->num_sms * 4);
     float* d = nullptr;
@@ -402,31 +556,33 @@ mi_status minmax(mi_context* ctx, const float* vals, const uint32_t* idx, const 
 
 void free_metric(mi_metric* m) {
     if (!m) return;
+    if (m->mtex) cudaDestroyTextureObject(m->mtex);
+    if (m->marray) cudaFreeArray(m->marray);
     cudaFree(m->fixed);
     cudaFree(m->moving);
     cudaFree(m->mmask);
     cudaFree(m->samples);
+    cudaFree(m->fbin);
     cudaFree(m->ws.hist);
     cudaFree(m->ws.pratio);
     cudaFree(m->ws.tail);
     cudaFree(m->ws.partials);
     cudaFree(m->ws.result);
     cudaFree(m->ws.done_counter);
+    cudaFree(m->ws.rec_mi);
+    cudaFree(m->ws.rec_f);
+    cudaFree(m->ws.rec_g);
     if (m->ws.host_result) cudaFreeHost(m->ws.host_result);
     for (int i = 0; i < 5; ++i)
         if (m->ws.ev[i]) cudaEventDestroy(m->ws.ev[i]);
     delete m;
 }
 
-size_t hist_smem(int B) { return (size_t)(B * B + B) * sizeof(unsigned long long); }
-size_t tail_smem(int B) { return (size_t)(B * B + 3 * B + 32) * sizeof(double); }
-size_t deriv_smem(int B) { return (size_t)(B * B + 32 * NMOM) * sizeof(double); }
-
 // Build the sample list: the strategy's draw, gated by the fixed mask, sorted
-// ascending. The histogram is a sum of exact integers and so does not depend on
-// the order; sorting only buys locality.
-mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mask,
-                        const mi_sampling* smp, int64_t nvox) {
+// ascending. The histogram is a sum of exact integers and so does not depend on the
+// order; sorting only buys locality.
+mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mask, const mi_sampling* smp,
+                        int64_t nvox) {
     const int strategy = smp ? smp->strategy : MI_SAMPLING_NONE;
     if (strategy == MI_SAMPLING_NONE && !fixed_mask) {
         m->samples = nullptr;
@@ -439,7 +595,7 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
     const int block = 256;
     if (strategy == MI_SAMPLING_NONE) {
         count = nvox;
-        MI_CHECK_CUDA(ctx, cudaMalloc(&draw, (size_t)count * 4));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&draw, pad4(count) * 4));
         k_iota_stride<<<grid_for(count, block, ctx->num_sms * 8), block, 0, st>>>(count, 1, draw);
     } else if (strategy == MI_SAMPLING_REGULAR) {
         if (!(smp->percentage > 0.0) || !std::isfinite(smp->percentage))
@@ -447,20 +603,23 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
         int64_t stride = (int64_t)std::ceil(1.0 / smp->percentage);
         if (stride < 1) stride = 1;
         count = (nvox + stride - 1) / stride;
-        MI_CHECK_CUDA(ctx, cudaMalloc(&draw, (size_t)std::max<int64_t>(count, 1) * 4));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&draw, pad4(count) * 4));
         k_iota_stride<<<grid_for(count, block, ctx->num_sms * 8), block, 0, st>>>(count, (uint64_t)stride, draw);
     } else if (strategy == MI_SAMPLING_RANDOM) {
         if (!(smp->percentage > 0.0) || !std::isfinite(smp->percentage))
             return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "sampling percentage must be positive");
         count = (int64_t)((double)nvox * smp->percentage);
-        if (count >= ((int64_t)1 << 32))
-            return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "sample count exceeds 2^32");
-        MI_CHECK_CUDA(ctx, cudaMalloc(&draw, (size_t)std::max<int64_t>(count, 1) * 4));
+        if (count >= ((int64_t)1 << 31))
+            return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "sample count exceeds 2^31");
+        MI_CHECK_CUDA(ctx, cudaMalloc(&draw, pad4(count) * 4));
         if (count)
-            k_draw_random<<<grid_for(count, block, ctx->num_sms * 8), block, 0, st>>>(smp->seed, (uint64_t)nvox, count, draw);
+            k_draw_random<<<grid_for(count, block, ctx->num_sms * 8), block, 0, st>>>(smp->seed, (uint64_t)nvox,
+                                                                                         count, draw);
     } else if (strategy == MI_SAMPLING_EXPLICIT) {
         if (smp->n_indices < 0 || (smp->n_indices > 0 && !smp->indices))
             return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "explicit sampling needs an index list");
+        if (smp->n_indices >= ((int64_t)1 << 31))
+            return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "sample count exceeds 2^31");
         count = smp->n_indices;
         std::vector<uint32_t> h((size_t)count);
         for (int64_t i = 0; i < count; ++i) {
@@ -471,7 +630,7 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
                                      std::to_string(nvox) + " voxels");
             h[i] = (uint32_t)v;
         }
-        MI_CHECK_CUDA(ctx, cudaMalloc(&draw, (size_t)std::max<int64_t>(count, 1) * 4));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&draw, pad4(count) * 4));
         if (count) MI_CHECK_CUDA(ctx, cudaMemcpyAsync(draw, h.data(), (size_t)count * 4, cudaMemcpyHostToDevice, st));
         MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
     } else {
@@ -488,7 +647,7 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
         uint32_t* out = nullptr;
         int* nsel = nullptr;
         MI_CHECK_CUDA(ctx, cudaMalloc(&flags, (size_t)count));
-        MI_CHECK_CUDA(ctx, cudaMalloc(&out, (size_t)count * 4));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&out, pad4(count) * 4));
         MI_CHECK_CUDA(ctx, cudaMalloc(&nsel, sizeof(int)));
         k_mask_flags<<<grid_for(count, block, ctx->num_sms * 8), block, 0, st>>>(draw, count, fixed_mask->data, flags);
         MI_CHECK_CUDA(ctx, cub::DeviceSelect::Flagged(nullptr, tmp_bytes, draw, flags, out, nsel, (int)count, st));
@@ -507,7 +666,7 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
     }
     if (nkept > 1) {
         uint32_t* sorted = nullptr;
-        MI_CHECK_CUDA(ctx, cudaMalloc(&sorted, (size_t)nkept * 4));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&sorted, pad4(nkept) * 4));
         int bits = 1;
         while (bits < 32 && ((uint64_t)1 << bits) < (uint64_t)nvox) ++bits;
         tmp_bytes = 0;
@@ -524,11 +683,89 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
     return MI_OK;
 }
 
+void mat3_mul(const double* a, const double* b, double* out) {
+    double t[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) t[r * 3 + c] = a[r * 3] * b[c] + a[r * 3 + 1] * b[3 + c] + a[r * 3 + 2] * b[6 + c];
+    std::memcpy(out, t, sizeof(t));
+}
+
+void mat3_vec(const double* a, const double* v, double* out) {
+    double t[3];
+    for (int r = 0; r < 3; ++r) t[r] = a[r * 3] * v[0] + a[r * 3 + 1] * v[1] + a[r * 3 + 2] * v[2];
+    std::memcpy(out, t, sizeof(t));
+}
+
+// Per-evaluation sampler constants: the stages, the composite map grid index →
+// continuous index, and a bound on how far that map can be from the exact chain.
+mi_status fill_params(mi_metric* m, const double* stages, int nstage, SamplerParams& P) {
+    P = m->base;
+    P.nstage = nstage;
+    for (int s = 0; s < nstage; ++s)
+        for (int i = 0; i < 12; ++i) P.stage[s][i] = stages[s * 12 + i];
+    // T(x) = MT·x + tT, the stages folded (for the fast path only; the exact chain
+    // replays them one by one)
+    double MT[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, tT[3] = {0, 0, 0};
+    for (int s = 0; s < nstage; ++s) {
+        const double* S = P.stage[s];
+        double nm[9], nt[3];
+        mat3_mul(S, MT, nm);
+        mat3_vec(S, tT, nt);
+        for (int d = 0; d < 3; ++d) nt[d] += S[9 + d];
+        std::memcpy(MT, nm, sizeof(nm));
+        std::memcpy(tT, nt, sizeof(nt));
+    }
+    double MTf[9], A[9], tmp[3], b[3];
+    mat3_mul(MT, P.fi2p, MTf);
+    mat3_mul(P.mp2i, MTf, A);
+    mat3_vec(MT, P.forigin, tmp);
+    for (int d = 0; d < 3; ++d) tmp[d] += tT[d] - P.morigin[d];
+    mat3_vec(P.mp2i, tmp, b);
+    for (int i = 0; i < 9; ++i) P.cA[i] = A[i];
+    for (int d = 0; d < 3; ++d) P.cb[d] = b[d];
+    // Magnitude bound of every intermediate of the exact chain, in moving voxels,
+    // over the fixed grid's corners; the chain's rounding is ≲ 20·2^-53 of it and
+    // cerr allows 2^-40 (≈ 400× margin).
+    double cmax = 0.0;
+    for (int corner = 0; corner < 8; ++corner) {
+        const double idx[3] = {(corner & 1) ? (double)(P.fsize0 - 1) : 0.0,
+                               (corner & 2) ? (double)(P.fsize1 - 1) : 0.0,
+                               (corner & 4) ? (double)(P.fsize2 - 1) : 0.0};
+        double mag[3];
+        for (int r = 0; r < 3; ++r)
+            mag[r] = std::fabs(P.forigin[r]) + std::fabs(P.fi2p[r * 3]) * idx[0] +
+                     std::fabs(P.fi2p[r * 3 + 1]) * idx[1] + std::fabs(P.fi2p[r * 3 + 2]) * idx[2];
+        for (int s = 0; s < nstage; ++s) {
+            const double* S = P.stage[s];
+            double nmag[3];
+            for (int r = 0; r < 3; ++r)
+                nmag[r] = std::fabs(S[r * 3]) * mag[0] + std::fabs(S[r * 3 + 1]) * mag[1] +
+                          std::fabs(S[r * 3 + 2]) * mag[2] + std::fabs(S[9 + r]);
+            std::memcpy(mag, nmag, sizeof(mag));
+        }
+        for (int r = 0; r < 3; ++r) mag[r] += std::fabs(P.morigin[r]);
+        for (int r = 0; r < 3; ++r) {
+            const double cm = std::fabs(P.mp2i[r * 3]) * mag[0] + std::fabs(P.mp2i[r * 3 + 1]) * mag[1] +
+                              std::fabs(P.mp2i[r * 3 + 2]) * mag[2];
+            cmax = std::max(cmax, cm);
+        }
+    }
+    if (!std::isfinite(cmax)) return set_error(m->ctx, MI_ERR_INVALID_ARGUMENT, "non-finite point map");
+    P.cerr = std::ldexp(1.0, -40) * (1.0 + cmax) * (double)(1 + nstage);
+    P.ilo = -0.5 + 2.0 * P.cerr;
+    P.olo = -0.5 - 2.0 * P.cerr;
+    for (int d = 0; d < 3; ++d) {
+        P.ihi[d] = P.mhi[d] - 2.0 * P.cerr;
+        P.ohi[d] = P.mhi[d] + 2.0 * P.cerr;
+    }
+    P.bin_hi = (double)(P.bins - PADDING - 1);
+    return MI_OK;
+}
+
 }  // namespace
 
-mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double* jac0,
-                   const double* jacc, int nparams, bool want_derivative, double* value,
-                   double* derivative, int64_t* valid) {
+mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double* jac0, const double* jacc,
+                   int nparams, bool want_derivative, double* value, double* derivative, int64_t* valid) {
     mi_context* ctx = m->ctx;
     if (nstage < 0 || nstage > MI_MAX_STAGES)
         return set_error(ctx, MI_ERR_POINT_MAP_STAGE_COUNT,
@@ -537,33 +774,42 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     if (want_derivative && (nparams < 1 || nparams > MI_MAX_PARAMS || !jac0 || !jacc || !derivative))
         return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "bad Jacobian form");
     MI_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
-    SamplerParams P = m->base;
-    P.nstage = nstage;
-    for (int s = 0; s < nstage; ++s)
-        for (int i = 0; i < 12; ++i) P.stage[s][i] = stages[s * 12 + i];
+    SamplerParams P;
+    mi_status s = fill_params(m, stages, nstage, P);
+    if (s != MI_OK) return s;
     const int B = m->bins;
     cudaStream_t st = ctx->stream;
     Workspace& ws = m->ws;
     const bool timing = ws.timing;
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[0], st));
-    MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + B + 1) * 8, st));
-    k_hist<<<ws.grid_hist, ws.block_hist, hist_smem(B), st>>>(P, m->fixed, m->moving, m->mmask, m->samples,
-                                                              m->n_samples, ws.hist);
+    const uint32_t n = (uint32_t)m->n_samples;
+    const uint32_t npad = (n + 3u) & ~3u;
+    const double hist_inv = std::ldexp(1.0, -ws.hist_scale_log2);
+    if (want_derivative)
+        k_hist<true><<<ws.grid_hist, ws.block_hist, hist_smem(B), st>>>(
+            P, m->moving, m->mmask, m->samples, m->fbin, n, npad, ws.hist_scale, hist_copies(B), ws.hist, ws.rec_mi, ws.rec_f,
+            ws.rec_g);
+    else
+        k_hist<false><<<ws.grid_hist, ws.block_hist, hist_smem(B), st>>>(
+            P, m->moving, m->mmask, m->samples, m->fbin, n, npad, ws.hist_scale, hist_copies(B), ws.hist, nullptr, nullptr,
+            nullptr);
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
-    k_tail<<<1, TAIL_BLOCK, tail_smem(B), st>>>(B, P.moving_bin_size, ws.hist, ws.pratio, ws.tail, ws.result);
-    if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[2], st));
     int nout = 2;
     if (want_derivative) {
+        if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[2], st));
         JacobianForm J;
         J.nparams = nparams;
         for (int i = 0; i < 3 * nparams; ++i) {
             J.jac0[i] = jac0[i];
             for (int e = 0; e < 3; ++e) J.jacc[e][i] = jacc[e * 3 * nparams + i];
         }
-        k_deriv<<<ws.grid_deriv, ws.block_deriv, deriv_smem(B), st>>>(
-            P, J, m->fixed, m->moving, m->mmask, m->samples, m->n_samples, ws.pratio, ws.tail,
-            ws.partials, ws.done_counter, ws.result);
+        k_deriv<<<ws.grid_deriv, ws.block_deriv, deriv_smem(B), st>>>(P, J, m->samples, m->fbin, npad, ws.rec_mi,
+                                                                      ws.rec_f, ws.rec_g, hist_inv, ws.hist,
+                                                                      ws.partials, ws.done_counter, ws.result);
         nout = 2 + nparams;
+    } else {
+        k_value<<<1, 256, tail_doubles(B) * sizeof(double), st>>>(B, P.moving_bin_size, hist_inv, ws.hist, ws.result);
+        if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[2], st));
     }
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[3], st));
     MI_CHECK_CUDA(ctx, cudaGetLastError());
@@ -593,9 +839,8 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
 
 extern "C" {
 
-mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_image* moving,
-                           const mi_image* fixed_mask, const uint8_t* moving_mask,
-                           const mi_sampling* sampling, int bins, mi_metric** out) {
+mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_image* moving, const mi_image* fixed_mask,
+                           const uint8_t* moving_mask, const mi_sampling* sampling, int bins, mi_metric** out) {
     using namespace mi;
     if (!ctx || !fixed || !moving || !out) return MI_ERR_INVALID_ARGUMENT;
     *out = nullptr;
@@ -613,8 +858,10 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
             if (fixed_mask->geo.size[d] != fixed->geo.size[d])
                 return set_error(ctx, MI_ERR_MASK_SIZE_MISMATCH, "fixed mask size differs from the fixed image");
     const int64_t nvox = fixed->n, mvox = moving->n;
-    if (nvox >= ((int64_t)1 << 32) || mvox >= ((int64_t)1 << 40))
-        return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "volume too large for 32-bit sample indices");
+    if (nvox >= ((int64_t)1 << 31) || mvox >= ((int64_t)1 << 32))
+        return set_error(ctx, MI_ERR_INVALID_ARGUMENT,
+                         "volume too large: the fixed grid must hold fewer than 2^31 voxels and the moving "
+                         "volume fewer than 2^32");
     double m_i2p[9], m_p2i[9], f_i2p[9];
     index_to_physical(moving->geo, m_i2p);
     if (!invert3(m_i2p, m_p2i)) return set_error(ctx, MI_ERR_SINGULAR_DIRECTION, "moving direction is singular");
@@ -677,6 +924,8 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     P.fsize0 = fixed->geo.size[0];
     P.fsize1 = fixed->geo.size[1];
     P.fsize2 = fixed->geo.size[2];
+    P.div0 = make_fastdiv((uint32_t)P.fsize0);
+    P.div1 = make_fastdiv((uint32_t)P.fsize1);
     for (int i = 0; i < 3; ++i) P.forigin[i] = fixed->geo.origin[i];
     for (int i = 0; i < 9; ++i) P.fi2p[i] = f_i2p[i];
     for (int d = 0; d < 3; ++d) {
@@ -686,40 +935,106 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     }
     P.mstride1 = moving->geo.size[0];
     P.mstride2 = moving->geo.size[0] * moving->geo.size[1];
-    for (int i = 0; i < 9; ++i) P.mp2i[i] = m_p2i[i];
+    for (int i = 0; i < 9; ++i) {
+        P.mp2i[i] = m_p2i[i];
+        P.mp2if[i] = (float)m_p2i[i];
+    }
     P.has_mmask = moving_mask ? 1 : 0;
+    for (int d = 0; d < 3; ++d) P.msz[d] = (int)moving->geo.size[d];
+    P.ms1 = (uint32_t)P.mstride1;
+    P.ms2 = (uint32_t)P.mstride2;
+    {
+        // the moving volume as a block-linear 3-D array behind a point-sampling,
+        // clamp-to-edge, unnormalised-coordinate texture (the fast path's corner fetch)
+        const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float>();
+        const cudaExtent ext = make_cudaExtent((size_t)moving->geo.size[0], (size_t)moving->geo.size[1],
+                                               (size_t)moving->geo.size[2]);
+        TRY_CUDA(cudaMalloc3DArray(&m->marray, &fmt, ext));
+        cudaMemcpy3DParms cp = {};
+        cp.srcPtr = make_cudaPitchedPtr(m->moving, (size_t)moving->geo.size[0] * sizeof(float),
+                                        (size_t)moving->geo.size[0], (size_t)moving->geo.size[1]);
+        cp.dstArray = m->marray;
+        cp.extent = ext;
+        cp.kind = cudaMemcpyDeviceToDevice;
+        TRY_CUDA(cudaMemcpy3DAsync(&cp, st));
+        cudaResourceDesc res = {};
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = m->marray;
+        cudaTextureDesc td = {};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModePoint;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        TRY_CUDA(cudaCreateTextureObject(&m->mtex, &res, &td, nullptr));
+        P.mtex = m->mtex;
+    }
     P.bins = bins;
     P.fixed_bin_size = info.fixed_bin_size;
     P.moving_bin_size = info.moving_bin_size;
+    P.inv_moving_bin_size = 1.0 / info.moving_bin_size;
     P.fixed_nmin = info.fixed_normalized_min;
     P.moving_nmin = info.moving_normalized_min;
     P.moving_min = mmin;
     P.moving_max = mmax;
-    // x_ref: the fixed grid's physical centre.
+    // x_ref: the fixed grid's physical centre; x − x_ref = M_f·idx + (o_f − x_ref)
     const double mid[3] = {0.5 * (double)(P.fsize0 - 1), 0.5 * (double)(P.fsize1 - 1), 0.5 * (double)(P.fsize2 - 1)};
-    for (int r = 0; r < 3; ++r)
+    for (int r = 0; r < 3; ++r) {
         P.xref[r] = P.forigin[r] + f_i2p[r * 3] * mid[0] + f_i2p[r * 3 + 1] * mid[1] + f_i2p[r * 3 + 2] * mid[2];
+        P.xb[r] = (float)(P.forigin[r] - P.xref[r]);
+        for (int c = 0; c < 3; ++c) P.xA[r * 3 + c] = (float)f_i2p[r * 3 + c];
+    }
+
+    // The exact fixed bin of every sample (a pure function of the fixed value).
+    TRY_CUDA(cudaMalloc(&m->fbin, pad4(m->n_samples)));
+    k_fixed_bins<<<grid_for(m->n_samples, 256, ctx->num_sms * 8), 256, 0, st>>>(P, m->fixed, m->samples,
+                                                                              m->n_samples, m->fbin);
+    TRY_CUDA(cudaGetLastError());
 
     // Workspace and launch shapes.
     Workspace& ws = m->ws;
     const int B = bins;
-    TRY_CUDA(cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tail_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_smem(B)));
     TRY_CUDA(cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)deriv_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_value, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(tail_doubles(B) * sizeof(double))));
     int occ_h = 0, occ_d = 0;
-    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist, HIST_BLOCK, hist_smem(B)));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK, hist_smem(B)));
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_deriv, DERIV_BLOCK, deriv_smem(B)));
     ws.block_hist = HIST_BLOCK;
     ws.block_deriv = DERIV_BLOCK;
     ws.grid_hist = grid_for(m->n_samples, HIST_BLOCK, ctx->num_sms * std::max(occ_h, 1));
-    ws.grid_deriv = grid_for(m->n_samples, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
-    TRY_CUDA(cudaMalloc(&ws.hist, (size_t)(B * B + B + 1) * 8));
+    ws.grid_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
+    // Fixed-point scale of a histogram tap: a CTA takes at most cta_max samples, each
+    // adding at most 2/3 to one bin, so 2^k·(2/3)·cta_max (+ rounding) must stay below
+    // 2^32 (a copy of the CTA histogram sees at most as many samples as the CTA);
+    // k is capped at 22 so that the magic-add rounding stays exact.
+    {
+        const int64_t per_thread = (m->n_samples + (int64_t)ws.grid_hist * HIST_BLOCK - 1) /
+                                   ((int64_t)ws.grid_hist * HIST_BLOCK);
+        const double cta_max = (double)std::max<int64_t>(per_thread * HIST_BLOCK, 1);
+        int k = 22;  // w·2^k < 2^22 keeps the magic-add rounding exact
+        while (k > 0 && std::ldexp(1.0, k) * (2.0 / 3.0) * cta_max + cta_max >= 4294967295.0 * 0.98) --k;
+        ws.hist_scale_log2 = k;
+        ws.hist_scale = (float)std::ldexp(1.0, k);
+    }
+    {
+        // padded to whole groups of four samples; padding records keep moving bin 0
+        const size_t ns = pad4(m->n_samples);
+        TRY_CUDA(cudaMalloc(&ws.rec_mi, ns));
+        TRY_CUDA(cudaMemsetAsync(ws.rec_mi, 0, ns, st));
+        TRY_CUDA(cudaMalloc(&ws.rec_f, ns * sizeof(float)));
+        TRY_CUDA(cudaMalloc(&ws.rec_g, 3 * ns * sizeof(float)));
+    }
+    TRY_CUDA(cudaMalloc(&ws.hist, (size_t)(B * B + B) * 8));
+    TRY_CUDA(cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + B) * 8, st));
     TRY_CUDA(cudaMalloc(&ws.pratio, (size_t)B * B * 8));
     TRY_CUDA(cudaMalloc(&ws.tail, 4 * 8));
+    TRY_CUDA(cudaMemsetAsync(ws.tail, 0, 4 * 8, st));
     TRY_CUDA(cudaMalloc(&ws.partials, (size_t)ws.grid_deriv * NMOM * 8));
     TRY_CUDA(cudaMalloc(&ws.result, (2 + MI_MAX_PARAMS) * 8));
-    TRY_CUDA(cudaMalloc(&ws.done_counter, sizeof(unsigned int)));
-    TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, sizeof(unsigned int), st));
+    TRY_CUDA(cudaMalloc(&ws.done_counter, 2 * sizeof(unsigned int)));
+    TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, 2 * sizeof(unsigned int), st));
     TRY_CUDA(cudaMemsetAsync(ws.result, 0, (2 + MI_MAX_PARAMS) * 8, st));
     TRY_CUDA(cudaMallocHost(&ws.host_result, (2 + MI_MAX_PARAMS) * 8));
     TRY_CUDA(cudaStreamSynchronize(st));
@@ -748,18 +1063,22 @@ mi_status mi_metric_value(mi_metric* m, const double* stages, int nstage, double
 }
 
 mi_status mi_metric_value_and_derivative(mi_metric* m, int kind, const double* params, int nparams,
-                                         const double* fixed_params, int nfixed, double* value,
-                                         double* derivative, int64_t* valid) {
+                                         const double* fixed_params, int nfixed, double* value, double* derivative,
+                                         int64_t* valid) {
     if (!m || !params || !value || !derivative) return MI_ERR_INVALID_ARGUMENT;
     mi::AffineForm f;
     mi_status s = mi::transform_form(kind, params, nparams, fixed_params, nfixed, &f);
     if (s != MI_OK) return mi::set_error(m->ctx, s, "bad transform kind or parameter count");
-    return mi::evaluate(m, f.stage, 1, f.jac0, &f.jacc[0][0], f.nparams, true, value, derivative, valid);
+    // pack C_e contiguously with stride 3·P, the layout evaluate() takes
+    double jc[3 * 3 * MI_MAX_PARAMS];
+    for (int e = 0; e < 3; ++e)
+        for (int i = 0; i < 3 * f.nparams; ++i) jc[e * 3 * f.nparams + i] = f.jacc[e][i];
+    return mi::evaluate(m, f.stage, 1, f.jac0, jc, f.nparams, true, value, derivative, valid);
 }
 
-mi_status mi_metric_value_and_derivative_stages(mi_metric* m, const double* stages, int nstage,
-                                                const double* jac0, const double* jac_c, int nparams,
-                                                double* value, double* derivative, int64_t* valid) {
+mi_status mi_metric_value_and_derivative_stages(mi_metric* m, const double* stages, int nstage, const double* jac0,
+                                                const double* jac_c, int nparams, double* value, double* derivative,
+                                                int64_t* valid) {
     if (!m || !value || !derivative || !jac0 || !jac_c) return MI_ERR_INVALID_ARGUMENT;
     return mi::evaluate(m, stages, nstage, jac0, jac_c, nparams, true, value, derivative, valid);
 }
@@ -786,8 +1105,8 @@ mi_status mi_metric_timing_read(mi_metric* m, double* ms4, int64_t* n_evals) {
     return MI_OK;
 }
 
-mi_status mi_transform_form(int kind, const double* params, int nparams, const double* fixed_params,
-                            int nfixed, double* stage12, double* jac0, double* jac_c) {
+mi_status mi_transform_form(int kind, const double* params, int nparams, const double* fixed_params, int nfixed,
+                            double* stage12, double* jac0, double* jac_c) {
     mi::AffineForm f;
     mi_status s = mi::transform_form(kind, params, nparams, fixed_params, nfixed, &f);
     if (s != MI_OK) return s;
@@ -799,36 +1118,41 @@ mi_status mi_transform_form(int kind, const double* params, int nparams, const d
 }
 
 mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nstage, int8_t* status,
-                                     int32_t* fixed_bin, int32_t* moving_bin, int64_t* flat, int64_t n) {
+                                     int32_t* fixed_bin, int32_t* moving_bin, int64_t* flat, int8_t* exact, int64_t n) {
     using namespace mi;
     if (!m) return MI_ERR_INVALID_ARGUMENT;
     mi_context* ctx = m->ctx;
     if (n < m->n_samples) return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "output arrays shorter than the sample count");
     if (nstage < 0 || nstage > MI_MAX_STAGES) return set_error(ctx, MI_ERR_POINT_MAP_STAGE_COUNT, "too many stages");
     MI_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
-    SamplerParams P = m->base;
-    P.nstage = nstage;
-    for (int s = 0; s < nstage; ++s)
-        for (int i = 0; i < 12; ++i) P.stage[s][i] = stages[s * 12 + i];
+    SamplerParams P;
+    mi_status s = fill_params(m, stages, nstage, P);
+    if (s != MI_OK) return s;
     const int64_t ns = m->n_samples;
-    int8_t* d_st = nullptr;
+    const size_t cap = (size_t)std::max<int64_t>(ns, 1);
+    int8_t *d_st = nullptr, *d_ex = nullptr;
     int32_t *d_fb = nullptr, *d_mb = nullptr;
     int64_t* d_fl = nullptr;
     cudaStream_t st = ctx->stream;
-    MI_CHECK_CUDA(ctx, cudaMalloc(&d_st, (size_t)std::max<int64_t>(ns, 1)));
-    MI_CHECK_CUDA(ctx, cudaMalloc(&d_fb, (size_t)std::max<int64_t>(ns, 1) * 4));
-    MI_CHECK_CUDA(ctx, cudaMalloc(&d_mb, (size_t)std::max<int64_t>(ns, 1) * 4));
-    MI_CHECK_CUDA(ctx, cudaMalloc(&d_fl, (size_t)std::max<int64_t>(ns, 1) * 8));
-    const int block = 256;
-    k_decisions<<<grid_for(ns, block, ctx->num_sms * 8), block, 0, st>>>(P, m->fixed, m->moving, m->mmask,
-                                                                         m->samples, ns, d_st, d_fb, d_mb, d_fl);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaMalloc(&d_st, cap);
+    if (e == cudaSuccess) e = cudaMalloc(&d_ex, cap);
+    if (e == cudaSuccess) e = cudaMalloc(&d_fb, cap * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&d_mb, cap * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&d_fl, cap * 8);
+    if (e == cudaSuccess) {
+        const int block = 256;
+        k_decisions<<<grid_for(ns, block, ctx->num_sms * 8), block, 0, st>>>(P, m->moving, m->mmask, m->samples, m->fbin,
+                                                                             ns, d_st, d_fb, d_mb, d_fl, d_ex);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess && status) e = cudaMemcpyAsync(status, d_st, (size_t)ns, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && exact) e = cudaMemcpyAsync(exact, d_ex, (size_t)ns, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && fixed_bin) e = cudaMemcpyAsync(fixed_bin, d_fb, (size_t)ns * 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && moving_bin) e = cudaMemcpyAsync(moving_bin, d_mb, (size_t)ns * 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && flat) e = cudaMemcpyAsync(flat, d_fl, (size_t)ns * 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(d_st);
+    cudaFree(d_ex);
     cudaFree(d_fb);
     cudaFree(d_mb);
     cudaFree(d_fl);

@@ -2,10 +2,13 @@
 // point-map stages → continuous index → moving mask / inside test → trilinear value
 // (and gradient) → moving-range reject → Parzen bins.
 //
-// Every step that feeds a discrete decision (the inside test, the mask rounding, the
-// range reject and both Parzen truncations) is computed in FP64 with each multiply,
-// add and divide rounded separately (__dmul_rn / __dadd_rn / __ddiv_rn, which nvcc
-// never contracts into an FMA), in the reference host's operation order:
+// Two evaluations of the chain share this file.
+//
+// exact_index() and exact_value() compute every step that feeds a discrete decision
+// (the inside test, the mask rounding, the range reject and the moving Parzen
+// truncation) in FP64 with each multiply, add and divide rounded separately
+// (__dmul_rn / __dadd_rn / __ddiv_rn, which nvcc never contracts into an FMA), in
+// the reference host's operation order:
 //   point      registration/scales.rs:259-271 (origin-seeded accumulation)
 //   stages     core/matrix.rs:9-21 + transform/parametric.rs:549-553
 //   index      registration/metric.rs:795-806 (origin subtracted first)
@@ -13,10 +16,20 @@
 //   inside     transform/interpolator.rs:29-34
 //   trilinear  transform/interpolator.rs:103-152 (corner order, clamping, products)
 //   bins       registration/mattes.rs:193-206, :464-478
-// so validity and bin indices equal the host's exactly. The single liberty taken is
-// the sign of an exact zero (a chain seeded with x rather than 0.0 + x), on which no
-// decision depends. The interpolant gradient is not a decision input and is formed
-// with FMAs.
+// so its decisions are the host's exactly. The one liberty is the sign of an exact
+// zero (a chain seeded with x rather than 0.0 + x), on which no decision depends.
+//
+// sample() is the fast path every kernel calls. It forms the continuous index with
+// three FP64 FMAs per axis from the composite map (within cerr of the exact chain),
+// interpolates in FP32, and carries a rigorous bound on how far each quantity can
+// be from the exact chain's. Each decision is taken from the fast values only when
+// the bound cannot straddle its threshold; otherwise the quantity is recomputed by
+// the exact functions. The interpolant gradient is discontinuous across cell faces,
+// so the gradient pass also recomputes c exactly whenever c lies within the bound of
+// an integer. Either way the decisions and the gradient's cell equal the reference's;
+// only the continuous weights (B-spline taps, gradient, fractions) carry FP32
+// rounding, inside the metric's tolerance. The fixed bin is exact by construction:
+// it is computed once per metric by exact arithmetic (fixed_bin()).
 #pragma once
 
 #include <cstdint>
@@ -30,12 +43,23 @@ constexpr int PADDING = 2;  // registration/mattes.rs:92
 enum : int { SAMPLE_OUTSIDE = 0, SAMPLE_OUT_OF_RANGE = 1, SAMPLE_VALID = 2 };
 
 struct Sample {
-    double x[3];    // fixed physical point
-    double mv;      // interpolated moving value
-    double mterm;   // moving Parzen term
-    double g[3];    // moving physical gradient (GRAD only)
-    int fi, mi;     // Parzen bins
+    float g[3];     // moving physical gradient (GRAD)
+    float f;        // Parzen fraction: moving term − moving bin
+    int mi;         // moving Parzen bin
+    bool exact;     // a decision or the gradient's cell came from the exact chain
 };
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+    return (uint32_t)(((uint64_t)__umulhi(n, f.m) + n) >> f.s);
+}
+
+__device__ __forceinline__ void grid_index(const SamplerParams& P, uint32_t flat, uint32_t& i,
+                                           uint32_t& j, uint32_t& k) {
+    const uint32_t row = fdiv(flat, P.div0);
+    i = flat - row * P.div0.d;
+    k = fdiv(row, P.div1);
+    j = row - k * P.div1.d;
+}
 
 __device__ __forceinline__ int parzen_bin(double term, int bins) {
     long long idx = (long long)term;  // truncation toward zero
@@ -44,18 +68,16 @@ __device__ __forceinline__ int parzen_bin(double term, int bins) {
     return (int)idx;
 }
 
-template <bool GRAD>
-__device__ __forceinline__ int take_sample(const SamplerParams& P, uint32_t flat,
-                                           const float* __restrict__ fixed,
-                                           const float* __restrict__ moving,
-                                           const uint8_t* __restrict__ mmask, Sample& o) {
-    // Fixed-grid voxel of this sample (x-fastest).
-    const uint32_t s0 = (uint32_t)P.fsize0, s1 = (uint32_t)P.fsize1;
-    const uint32_t row = flat / s0;
-    const double di = (double)(flat - row * s0);
-    const uint32_t k = row / s1;
-    const double dj = (double)(row - k * s1);
-    const double dk = (double)k;
+// The fixed bin of a fixed value (mattes.rs:193-206), exact.
+__device__ __forceinline__ int fixed_bin(const SamplerParams& P, float fv) {
+    return parzen_bin(__dsub_rn(__ddiv_rn((double)fv, P.fixed_bin_size), P.fixed_nmin), P.bins);
+}
+
+// The reference's continuous index, exact: fixed-grid point (origin-seeded), the
+// stages one by one, then M·(p − origin) with the origin subtracted first.
+__device__ __forceinline__ void exact_index(const SamplerParams& P, uint32_t i, uint32_t j, uint32_t k,
+                                            double* c) {
+    const double di = (double)i, dj = (double)j, dk = (double)k;
     double x[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
@@ -65,7 +87,6 @@ __device__ __forceinline__ int take_sample(const SamplerParams& P, uint32_t flat
         acc = __dadd_rn(acc, __dmul_rn(P.fi2p[r * 3 + 2], dk));
         x[r] = acc;
     }
-    // Point-map stages, each p ← mat_vec(M, p) + t.
     double p0 = x[0], p1 = x[1], p2 = x[2];
     for (int st = 0; st < P.nstage; ++st) {
         const double* a = P.stage[st];
@@ -77,13 +98,13 @@ __device__ __forceinline__ int take_sample(const SamplerParams& P, uint32_t flat
             acc = __dadd_rn(acc, __dmul_rn(a[d * 3 + 2], p2));
             q[d] = __dadd_rn(acc, a[9 + d]);
         }
-        p0 = q[0]; p1 = q[1]; p2 = q[2];
+        p0 = q[0];
+        p1 = q[1];
+        p2 = q[2];
     }
-    // Continuous index in the moving image.
     const double e0 = __dsub_rn(p0, P.morigin[0]);
     const double e1 = __dsub_rn(p1, P.morigin[1]);
     const double e2 = __dsub_rn(p2, P.morigin[2]);
-    double c[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
         double acc = __dmul_rn(P.mp2i[r * 3 + 0], e0);
@@ -91,24 +112,13 @@ __device__ __forceinline__ int take_sample(const SamplerParams& P, uint32_t flat
         acc = __dadd_rn(acc, __dmul_rn(P.mp2i[r * 3 + 2], e2));
         c[r] = acc;
     }
-    if (P.has_mmask) {
-        int64_t mflat = 0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double r = floor(__dadd_rn(c[d], 0.5));
-            if (!(r >= 0.0 && r < (double)P.msize[d])) return SAMPLE_OUTSIDE;
-            const int64_t ri = (int64_t)r;
-            mflat += d == 0 ? ri : (d == 1 ? ri * P.mstride1 : ri * P.mstride2);
-        }
-        if (!mmask[mflat]) return SAMPLE_OUTSIDE;
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-        if (!(c[d] >= -0.5 && c[d] < P.mhi[d])) return SAMPLE_OUTSIDE;
+}
 
-    // Trilinear interpolation: weights w_d[0] = 1 − frac, w_d[1] = frac; the corner
-    // weight is ((w0·w1)·w2) exactly as the host's running product (its leading
-    // 1.0· is exact); the value is summed in corner order.
+// The reference's trilinear value at an exact continuous index that has passed the
+// inside test: weights w_d[0] = 1 − frac, w_d[1] = frac, the corner weight the host's
+// running product ((w0·w1)·w2) (its leading 1.0· is exact), summed in corner order.
+__device__ __forceinline__ double exact_value(const SamplerParams& P, const double* c,
+                                              const float* __restrict__ moving) {
     double fr[3], om[3];
     int64_t b0[3], b1[3];
 #pragma unroll
@@ -118,81 +128,243 @@ __device__ __forceinline__ int take_sample(const SamplerParams& P, uint32_t flat
         om[d] = __dsub_rn(1.0, fr[d]);
         const int64_t base = (int64_t)f;
         const int64_t hi = P.msize[d] - 1;
-        int64_t i0 = base, i1 = base + 1;
-        i0 = i0 < 0 ? 0 : (i0 > hi ? hi : i0);
-        i1 = i1 < 0 ? 0 : (i1 > hi ? hi : i1);
-        b0[d] = i0;
-        b1[d] = i1;
+        b0[d] = base < 0 ? 0 : (base > hi ? hi : base);
+        b1[d] = base + 1 < 0 ? 0 : (base + 1 > hi ? hi : base + 1);
     }
     const int64_t oy0 = b0[1] * P.mstride1, oy1 = b1[1] * P.mstride1;
     const int64_t oz0 = b0[2] * P.mstride2, oz1 = b1[2] * P.mstride2;
-    double v[8];
-    v[0] = (double)__ldg(moving + (b0[0] + oy0 + oz0));
-    v[1] = (double)__ldg(moving + (b1[0] + oy0 + oz0));
-    v[2] = (double)__ldg(moving + (b0[0] + oy1 + oz0));
-    v[3] = (double)__ldg(moving + (b1[0] + oy1 + oz0));
-    v[4] = (double)__ldg(moving + (b0[0] + oy0 + oz1));
-    v[5] = (double)__ldg(moving + (b1[0] + oy0 + oz1));
-    v[6] = (double)__ldg(moving + (b0[0] + oy1 + oz1));
-    v[7] = (double)__ldg(moving + (b1[0] + oy1 + oz1));
     const double w00 = __dmul_rn(om[0], om[1]);
     const double w10 = __dmul_rn(fr[0], om[1]);
     const double w01 = __dmul_rn(om[0], fr[1]);
     const double w11 = __dmul_rn(fr[0], fr[1]);
-    double mv = __dmul_rn(__dmul_rn(w00, om[2]), v[0]);
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, om[2]), v[1]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, om[2]), v[2]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, om[2]), v[3]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w00, fr[2]), v[4]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, fr[2]), v[5]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, fr[2]), v[6]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, fr[2]), v[7]));
+    double mv = __dmul_rn(__dmul_rn(w00, om[2]), (double)__ldg(moving + (b0[0] + oy0 + oz0)));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, om[2]), (double)__ldg(moving + (b1[0] + oy0 + oz0))));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, om[2]), (double)__ldg(moving + (b0[0] + oy1 + oz0))));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, om[2]), (double)__ldg(moving + (b1[0] + oy1 + oz0))));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w00, fr[2]), (double)__ldg(moving + (b0[0] + oy0 + oz1))));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, fr[2]), (double)__ldg(moving + (b1[0] + oy0 + oz1))));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, fr[2]), (double)__ldg(moving + (b0[0] + oy1 + oz1))));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, fr[2]), (double)__ldg(moving + (b1[0] + oy1 + oz1))));
+    return mv;
+}
 
-    if (mv < P.moving_min || mv > P.moving_max) return SAMPLE_OUT_OF_RANGE;
+// The sampler: fast path with exact fallback (see the file comment), in two stages
+// so a kernel can keep several samples' gathers in flight.
+//
+// prep():
+// 1. c from the composite map (3 FP64 FMAs per axis), within ce of the exact c.
+// 2. If a geometric decision (mask rounding, inside test) could flip within ±ce, or —
+//    for the gradient, which is discontinuous across cell faces — c is within ce of
+//    an integer, c is recomputed exactly (exact_index) and ce becomes 0.
+// 3. Geometric decisions on c; the mask byte and the eight corners are loaded.
+// finish():
+// 4. FP32 trilinear value (and gradient) on the cell of c, with a bound dv on its
+//    distance from the reference's FP64 value.
+// 5. Range reject and Parzen bin from the FP32 value when dv cannot flip them;
+//    otherwise the reference's value is recomputed exactly (exact_value).
+struct Prep {
+    uint32_t flat;
+    float fr[3];
+    float v[8];
+    uint8_t mval;  // moving-mask byte at round(c) (1 without a mask)
+    bool ok;       // not decided outside
+    bool exact_c;  // c was recomputed exactly
+};
 
-    o.mv = mv;
-    o.mterm = __dsub_rn(__ddiv_rn(mv, P.moving_bin_size), P.moving_nmin);
-    o.mi = parzen_bin(o.mterm, P.bins);
-    const double fv = (double)__ldg(fixed + flat);
-    o.fi = parzen_bin(__dsub_rn(__ddiv_rn(fv, P.fixed_bin_size), P.fixed_nmin), P.bins);
-    o.x[0] = x[0];
-    o.x[1] = x[1];
-    o.x[2] = x[2];
+template <bool GRAD>
+__device__ __forceinline__ void prep(const SamplerParams& P, uint32_t flat, const float* __restrict__ moving,
+                                     const uint8_t* __restrict__ mmask, Prep& p) {
+    p.flat = flat;
+    p.ok = false;
+    p.exact_c = false;
+    p.mval = 1;
+    uint32_t i, j, k;
+    grid_index(P, flat, i, j, k);
+    double c[3];
+    {
+        const double di = (double)i, dj = (double)j, dk = (double)k;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+            c[r] = fma(P.cA[r * 3 + 2], dk, fma(P.cA[r * 3 + 1], dj, fma(P.cA[r * 3 + 0], di, P.cb[r])));
+    }
+    const double ce = P.cerr;
+    bool need_index = false;
+    // inside test [−0.5, size − 0.5): the bounds ilo/ihi (surely inside) and olo/ohi
+    // (surely outside) carry a margin of 2·ce
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (!(c[d] >= P.ilo && c[d] < P.ihi[d])) {
+            if (c[d] < P.olo || c[d] >= P.ohi[d]) return;
+            need_index = true;
+        }
+    }
+    if (P.has_mmask) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double h = c[d] + 0.5;
+            if (floor(h - ce) != floor(h + ce)) need_index = true;
+        }
+    }
+    double fl[3], frd[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        fl[d] = floor(c[d]);
+        frd[d] = c[d] - fl[d];
+        if (GRAD && (frd[d] <= ce || frd[d] >= 1.0 - ce)) need_index = true;
+    }
+    if (need_index) {
+        exact_index(P, i, j, k, c);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (!(c[d] >= -0.5 && c[d] < P.mhi[d])) return;
+            fl[d] = floor(c[d]);
+            frd[d] = c[d] - fl[d];
+        }
+        p.exact_c = true;
+    }
+    if (P.has_mmask) {
+        // decided on c (certain, or exact)
+        uint32_t mflat = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double r = floor(c[d] + 0.5);
+            if (!(r >= 0.0 && r < (double)P.msz[d])) return;
+            const uint32_t ri = (uint32_t)r;
+            mflat += d == 0 ? ri : (d == 1 ? ri * P.ms1 : ri * P.ms2);
+        }
+        p.mval = __ldg(mmask + mflat);
+    }
+    // The eight corners of the cell of c. c passed the inside test, so floor(c) ∈
+    // [−1, size − 1]. They are fetched from the moving volume's 3-D texture: point
+    // sampling at voxel centres returns the stored f32 voxel unchanged, clamp
+    // addressing is exactly the reference's clamp-to-edge of each corner index, and
+    // the block-linear layout keeps a cell's corners on a few cache lines.
+    float cx[2], cy[2], cz[2];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) p.fr[d] = (float)frd[d];
+    cx[0] = (float)fl[0] + 0.5f;
+    cy[0] = (float)fl[1] + 0.5f;
+    cz[0] = (float)fl[2] + 0.5f;
+    cx[1] = cx[0] + 1.0f;
+    cy[1] = cy[0] + 1.0f;
+    cz[1] = cz[0] + 1.0f;
+    p.v[0] = tex3D<float>(P.mtex, cx[0], cy[0], cz[0]);
+    p.v[1] = tex3D<float>(P.mtex, cx[1], cy[0], cz[0]);
+    p.v[2] = tex3D<float>(P.mtex, cx[0], cy[1], cz[0]);
+    p.v[3] = tex3D<float>(P.mtex, cx[1], cy[1], cz[0]);
+    p.v[4] = tex3D<float>(P.mtex, cx[0], cy[0], cz[1]);
+    p.v[5] = tex3D<float>(P.mtex, cx[1], cy[0], cz[1]);
+    p.v[6] = tex3D<float>(P.mtex, cx[0], cy[1], cz[1]);
+    p.v[7] = tex3D<float>(P.mtex, cx[1], cy[1], cz[1]);
+    p.ok = true;
+}
+
+template <bool GRAD>
+__device__ __forceinline__ int finish(const SamplerParams& P, const Prep& p, const float* __restrict__ moving,
+                                      Sample& o) {
+    if (!p.ok || !p.mval) return SAMPLE_OUTSIDE;
+    o.exact = p.exact_c;
+    const float* v = p.v;
+    const float* fr = p.fr;
+    // x-lerps, then y, then z
+    const float x00 = fmaf(fr[0], v[1] - v[0], v[0]);
+    const float x10 = fmaf(fr[0], v[3] - v[2], v[2]);
+    const float x01 = fmaf(fr[0], v[5] - v[4], v[4]);
+    const float x11 = fmaf(fr[0], v[7] - v[6], v[6]);
+    const float y0 = fmaf(fr[1], x10 - x00, x00);
+    const float y1 = fmaf(fr[1], x11 - x01, x01);
     if (GRAD) {
-        // Exact gradient of the trilinear interpolant in index space, then
-        // g_phys[d] = Σ_j g_idx[j]·M[j][d] (registration/metric.rs:848-861).
-        const double gx = om[1] * om[2] * (v[1] - v[0]) + fr[1] * om[2] * (v[3] - v[2]) +
-                          om[1] * fr[2] * (v[5] - v[4]) + fr[1] * fr[2] * (v[7] - v[6]);
-        const double gy = om[0] * om[2] * (v[2] - v[0]) + fr[0] * om[2] * (v[3] - v[1]) +
-                          om[0] * fr[2] * (v[6] - v[4]) + fr[0] * fr[2] * (v[7] - v[5]);
-        const double gz = om[0] * om[1] * (v[4] - v[0]) + fr[0] * om[1] * (v[5] - v[1]) +
-                          om[0] * fr[1] * (v[6] - v[2]) + fr[0] * fr[1] * (v[7] - v[3]);
+        // exact gradient of the trilinear interpolant in index space, then
+        // g_phys[d] = Σ_j g_idx[j]·M[j][d] (registration/metric.rs:848-861)
+        const float gz = y1 - y0;
+        const float gy = fmaf(fr[2], (x11 - x01) - (x10 - x00), x10 - x00);
+        const float a0 = fmaf(fr[1], (v[3] - v[2]) - (v[1] - v[0]), v[1] - v[0]);
+        const float a1 = fmaf(fr[1], (v[7] - v[6]) - (v[5] - v[4]), v[5] - v[4]);
+        const float gx = fmaf(fr[2], a1 - a0, a0);
 #pragma unroll
         for (int d = 0; d < 3; ++d)
-            o.g[d] = gx * P.mp2i[0 * 3 + d] + gy * P.mp2i[1 * 3 + d] + gz * P.mp2i[2 * 3 + d];
+            o.g[d] = gx * P.mp2if[0 * 3 + d] + gy * P.mp2if[1 * 3 + d] + gz * P.mp2if[2 * 3 + d];
     }
+    const float mv = fmaf(fr[2], y1 - y0, y0);
+    // |mv − reference value| ≤ dv: three levels of FP32 lerps add at most 12 units of
+    // 2^-24 of the largest corner magnitude (32 allowed), plus the Lipschitz effect
+    // (≤ 6·vmax per voxel) of the continuous-index error ce.
+    const double ce = p.exact_c ? 0.0 : P.cerr;
+    float vmax = fabsf(v[0]);
+#pragma unroll
+    for (int t = 1; t < 8; ++t) vmax = fmaxf(vmax, fabsf(v[t]));
+    const double dv = (double)vmax * (32.0 * 5.9604644775390625e-08 + 8.0 * ce) + 1e-300;
+    const double mvd = (double)mv;
+    bool certain = true;
+    double term = 0.0;
+    int mi = 0;
+    if (!(dv < 1e300) || !isfinite(mvd)) {
+        certain = false;
+    } else if (mvd + dv < P.moving_min || mvd - dv > P.moving_max) {
+        return SAMPLE_OUT_OF_RANGE;
+    } else if (!(mvd - dv >= P.moving_min && mvd + dv <= P.moving_max)) {
+        certain = false;
+    }
+    if (certain) {
+        // truncation then clamp to [2, bins − 3] equals floor then clamp for every
+        // term (anything below 2 clamps to 2)
+        term = fma(mvd, P.inv_moving_bin_size, -P.moving_nmin);
+        const double dt = dv * P.inv_moving_bin_size * 1.0000001 +
+                          (fabs(term) + fabs(mvd * P.inv_moving_bin_size) + 1.0) * 1e-13;
+        const double lo = fmin(fmax(floor(term - dt), (double)PADDING), P.bin_hi);
+        const double hi = fmin(fmax(floor(term + dt), (double)PADDING), P.bin_hi);
+        if (lo != hi) certain = false;
+        else mi = (int)lo;
+    }
+    if (!certain) {
+        uint32_t i, j, k;
+        grid_index(P, p.flat, i, j, k);
+        double c[3];
+        exact_index(P, i, j, k, c);
+        o.exact = true;
+        const double mvx = exact_value(P, c, moving);
+        if (mvx < P.moving_min || mvx > P.moving_max) return SAMPLE_OUT_OF_RANGE;
+        term = __dsub_rn(__ddiv_rn(mvx, P.moving_bin_size), P.moving_nmin);
+        mi = parzen_bin(term, P.bins);
+    }
+    o.f = (float)(term - (double)mi);
+    o.mi = mi;
     return SAMPLE_VALID;
 }
 
-// Cubic B-spline Parzen window B₃(u) and its derivative (mattes.rs:96-124; ITK's
-// BSplineKernelFunction<3> / BSplineDerivativeKernelFunction<3>). These weights are
-// not decision inputs, so FMAs are allowed.
-__device__ __forceinline__ double bspline3(double u) {
-    const double a = fabs(u);
-    if (a < 1.0) return (4.0 - 6.0 * a * a + 3.0 * a * a * a) * (1.0 / 6.0);
-    if (a < 2.0) {
-        const double t = 2.0 - a;
-        return t * t * t * (1.0 / 6.0);
-    }
-    return 0.0;
+template <bool GRAD>
+__device__ __forceinline__ int sample(const SamplerParams& P, uint32_t flat, const float* __restrict__ moving,
+                                      const uint8_t* __restrict__ mmask, Sample& o) {
+    Prep p;
+    prep<GRAD>(P, flat, moving, mmask, p);
+    o.exact = false;
+    return finish<GRAD>(P, p, moving, o);
 }
 
-__device__ __forceinline__ double bspline3_deriv(double u) {
-    if (u >= 0.0 && u < 1.0) return -2.0 * u + 1.5 * u * u;
-    if (u > -1.0 && u < 0.0) return -2.0 * u - 1.5 * u * u;
-    if (u >= 1.0 && u < 2.0) return -2.0 + 2.0 * u - 0.5 * u * u;
-    if (u > -2.0 && u <= -1.0) return 2.0 + 2.0 * u + 0.5 * u * u;
-    return 0.0;
+// The four Parzen taps of a sample. With f = term − mi ∈ [0, 1] the taps sit at
+// u = m − term = −1−f, −f, 1−f, 2−f (m = mi−1 … mi+2), where the cubic B-spline
+// B₃(u) and its derivative B₃′(u) (mattes.rs:96-124; ITK's BSplineKernelFunction<3>
+// and BSplineDerivativeKernelFunction<3>) reduce to one polynomial piece each:
+//   B₃:  (1−f)³/6, (4 − 6f² + 3f³)/6, (1 + 3f + 3f² − 3f³)/6, f³/6
+//   B₃′: (1−f)²/2, 2f − 3f²/2, −1/2 − f + 3f²/2, −f²/2
+// (at f = 0 and f = 1 these equal the reference's branch values). The taps are
+// continuous weights, not decision inputs, and are formed in FP32.
+__device__ __forceinline__ void bspline3_taps(float f, float* w) {
+    const float g = 1.0f - f;
+    const float f2 = f * f, f3 = f2 * f;
+    w[0] = g * g * g * (1.0f / 6.0f);
+    w[1] = fmaf(3.0f, f3, fmaf(-6.0f, f2, 4.0f)) * (1.0f / 6.0f);
+    w[2] = fmaf(-3.0f, f3, fmaf(3.0f, f2, fmaf(3.0f, f, 1.0f))) * (1.0f / 6.0f);
+    w[3] = f3 * (1.0f / 6.0f);
+}
+
+__device__ __forceinline__ void bspline3_deriv_taps(float f, float* d) {
+    const float g = 1.0f - f;
+    const float f2 = f * f;
+    d[0] = 0.5f * g * g;
+    d[1] = fmaf(-1.5f, f2, 2.0f * f);
+    d[2] = fmaf(1.5f, f2, -0.5f - f);
+    d[3] = -0.5f * f2;
 }
 
 }  // namespace mi

@@ -103,7 +103,7 @@ def load(path: str | None = None):
     L.mi_metric_value_and_derivative_stages.argtypes = [vp, dp, ctypes.c_int, dp, dp, ctypes.c_int,
                                                         dp, dp, i64p]
     L.mi_metric_sample_decisions.argtypes = [vp, dp, ctypes.c_int, P(ctypes.c_int8), P(ctypes.c_int32),
-                                             P(ctypes.c_int32), i64p, ctypes.c_int64]
+                                             P(ctypes.c_int32), i64p, P(ctypes.c_int8), ctypes.c_int64]
     L.mi_transform_form.argtypes = [ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int, dp, dp, dp]
     L.mi_metric_timing_enable.argtypes = [vp, ctypes.c_int]
     L.mi_metric_timing_read.argtypes = [vp, dp, i64p]

@@ -250,12 +250,14 @@ class DeviceMattesMetric:
         fb = np.empty(n, dtype=np.int32)
         mb = np.empty(n, dtype=np.int32)
         flat = np.empty(n, dtype=np.int64)
+        exact = np.empty(n, dtype=np.int8)
         P = ctypes.POINTER
         _lib.check(_lib.load().mi_metric_sample_decisions(
             self.handle, st.ctypes.data_as(P(ctypes.c_double)), st.size // 12,
             status.ctypes.data_as(P(ctypes.c_int8)), fb.ctypes.data_as(P(ctypes.c_int32)),
-            mb.ctypes.data_as(P(ctypes.c_int32)), flat.ctypes.data_as(P(ctypes.c_int64)), n), self.ctx.handle)
-        return {"status": status, "fi": fb, "mi": mb, "flat": flat}
+            mb.ctypes.data_as(P(ctypes.c_int32)), flat.ctypes.data_as(P(ctypes.c_int64)),
+            exact.ctypes.data_as(P(ctypes.c_int8)), n), self.ctx.handle)
+        return {"status": status, "fi": fb, "mi": mb, "flat": flat, "exact": exact}
 
     @staticmethod
     def stages(transform: ParametricTransform) -> np.ndarray:

@@ -69,3 +69,20 @@ def test_transform_stage_is_the_oracles_to_the_bit(oracle_lib, kind, params, fix
     x = np.array([3.0, -4.0, 5.5])
     jx = j0 + sum(x[e] * jc[e] for e in range(3))
     np.testing.assert_allclose(jx, ref["jacobian"], rtol=1e-12, atol=1e-12)
+
+
+def test_fastdiv_multiplier_divides_exactly():
+    # csrc/internal.h make_fastdiv + sampler.cuh fdiv: q = (umulhi(n, m) + n) >> s
+    rng = np.random.default_rng(0)
+    divisors = [1, 2, 3, 5, 7, 48, 64, 100, 127, 192, 255, 256, 257, 511, 512, 1000, 4093, 65535, 65536]
+    ns = np.concatenate([rng.integers(0, 2 ** 32, 20000, dtype=np.uint64),
+                         np.array([0, 1, 2 ** 32 - 1, 2 ** 31, 2 ** 24 - 1, 2 ** 24], dtype=np.uint64)])
+    for d in divisors:
+        s = 0
+        while (1 << s) < d:
+            s += 1
+        m = ((1 << 32) * ((1 << s) - d)) // d + 1
+        assert m < (1 << 32)
+        for n in ns.tolist():
+            q = (((n * m) >> 32) + n) >> s
+            assert q == n // d, (n, d)
