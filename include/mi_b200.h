@@ -194,6 +194,36 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
                                      int8_t* status, int32_t* fixed_bin, int32_t* moving_bin,
                                      int64_t* flat, int8_t* exact, int64_t n);
 
+/* ---- allocation-free value (no counterpart in the reference) --------------- */
+
+/* Largest histogram the allocation-free entry point can hold. */
+#define MI_NOALLOC_MAX_BINS 64
+
+/* The metric value for callers that cannot allocate device memory: code running
+ * while a CUDA graph is captured, hosts that give the library a fixed memory budget,
+ * real-time loops that must not reach the allocator. It calls no cudaMalloc,
+ * cudaFree or allocating routine; its only scratch is one fixed-size array in the
+ * library's device memory (a joint histogram of at most MI_NOALLOC_MAX_BINS bins,
+ * 33 KB), which every GPU that loads the library holds until the process exits.
+ *
+ * Inputs and outputs belong to the caller and are device pointers: the fixed and
+ * moving volumes (f32, x-fastest) with their geometries; an optional list of
+ * n_samples flat fixed-grid voxels (NULL = every voxel); the histogram geometry
+ * `info` (bins and intensity ranges, e.g. from mi_metric_info_get); the point map as
+ * `nstage` stages of 12 doubles; and `result`, two doubles that receive −MI and the
+ * valid-sample count. No masks. Work is queued on the context's stream and the
+ * call returns without waiting: result is ready once that stream has reached it.
+ *
+ * The first call on a device looks the scratch array up for that device; make that
+ * first call before any stream capture begins. Every call on a device shares the
+ * array (each call clears it first), so calls whose work overlaps on the GPU race:
+ * serialise them. bins > MI_NOALLOC_MAX_BINS is refused with
+ * MI_ERR_TOO_MANY_HISTOGRAM_BINS. */
+mi_status mi_metric_value_noalloc(mi_context* ctx, const float* fixed, const mi_geometry* fixed_geometry,
+                                  const float* moving, const mi_geometry* moving_geometry,
+                                  const uint32_t* samples, int64_t n_samples, const mi_metric_info* info,
+                                  const double* stages, int nstage, double* result);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,7 +29,7 @@ EXPORTED = [
     "mi_metric_create", "mi_metric_info_get", "mi_metric_destroy", "mi_metric_value",
     "mi_metric_value_and_derivative", "mi_metric_value_and_derivative_stages",
     "mi_metric_sample_decisions", "mi_transform_form", "mi_metric_timing_enable",
-    "mi_metric_timing_read",
+    "mi_metric_timing_read", "mi_metric_value_noalloc",
 ]
 
 
@@ -105,6 +105,9 @@ def load(path: str | None = None):
     L.mi_metric_sample_decisions.argtypes = [vp, dp, ctypes.c_int, P(ctypes.c_int8), P(ctypes.c_int32),
                                              P(ctypes.c_int32), i64p, P(ctypes.c_int8), ctypes.c_int64]
     L.mi_transform_form.argtypes = [ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int, dp, dp, dp]
+    L.mi_metric_value_noalloc.argtypes = [vp, vp, P(MiGeometry), vp, P(MiGeometry), vp, ctypes.c_int64,
+                                          P(MiMetricInfo), dp, ctypes.c_int, vp]
+    L.mi_metric_value_noalloc.restype = ctypes.c_int
     L.mi_metric_timing_enable.argtypes = [vp, ctypes.c_int]
     L.mi_metric_timing_read.argtypes = [vp, dp, i64p]
     for name in ["mi_metric_timing_enable", "mi_metric_timing_read", "mi_transform_form", "mi_context_create", "mi_context_destroy", "mi_context_sync", "mi_image_upload",
