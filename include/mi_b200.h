@@ -194,6 +194,54 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
                                      int8_t* status, int32_t* fixed_bin, int32_t* moving_bin,
                                      int64_t* flat, int8_t* exact, int64_t n);
 
+/* ---- registration driver (registration/optimizer.rs, scales.rs, method.rs) ---- */
+
+/* Why an optimisation stopped (optimizer.rs:73-93, same order). */
+typedef enum {
+    MI_STOP_MAX_ITERATIONS = 0,
+    MI_STOP_STEP_TOO_SMALL = 1,
+    MI_STOP_CONVERGED = 2,
+    MI_STOP_GRADIENT_CONVERGED = 3
+} mi_stop_reason;
+
+/* RegularStepGradientDescentOptimizer (optimizer.rs:271-440) as the driver runs it
+ * (method.rs:3140-3400). */
+typedef struct {
+    int iterations;              /* number_of_iterations */
+    double minimum_step;         /* minimum_step_length */
+    double gradient_tolerance;   /* gradient_magnitude_tolerance (ITK default 1e-4) */
+    double relaxation;           /* relaxation_factor (ITK default 0.5) */
+    double learning_rate;        /* step-length scale when estimate_learning_rate == 0 */
+    int estimate_learning_rate;  /* 1: EstimateLearningRate::Once (scales.rs estimate_learning_rate) */
+    int physical_shift_scales;   /* 1: scales from physical shift (scales.rs:572-871); 0: unit */
+    /* Optional evaluation record (no counterpart in the reference): when non-NULL,
+     * evaluation k < trace_rows writes row k = [value, params[nparams],
+     * derivative[nparams]] (1 + 2·nparams doubles, host memory). */
+    double* trace;
+    int trace_rows;
+} mi_rsgd_config;
+
+typedef struct {
+    double value;       /* metric value at the returned parameters */
+    int64_t valid;      /* valid samples at the returned parameters */
+    int iterations;     /* steps taken */
+    int stop_reason;    /* mi_stop_reason */
+    int evaluations;    /* metric evaluations made */
+} mi_rsgd_result;
+
+/* One level of registration: regular-step gradient descent over the device metric
+ * from params_inout (updated in place), for a transform family with the given fixed
+ * parameters (method.rs:3140 `drive`, optimizer.rs:352-440). */
+mi_status mi_register_rsgd(mi_metric* m, int kind, const double* fixed_params, int nfixed,
+                           const mi_rsgd_config* cfg, double* params_inout, int nparams,
+                           mi_rsgd_result* out);
+
+/* CenteredTransformInitializer in Geometry mode (registration/initializer.rs:56-105):
+ * center = the fixed image's geometric centre, translation = moving centre − fixed
+ * centre. Host only. */
+mi_status mi_centered_initialize(const mi_geometry* fixed, const mi_geometry* moving, double* center3,
+                                 double* translation3);
+
 /* ---- allocation-free value (no counterpart in the reference) --------------- */
 
 /* Largest histogram the allocation-free entry point can hold. */

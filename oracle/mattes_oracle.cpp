@@ -730,6 +730,147 @@ int or_mattes_evaluate(const float* fixed, const or_geometry* fg, const float* m
     return OR_OK;
 }
 
+// One level of registration with the reference's regular-step gradient descent
+// (registration/optimizer.rs:352-440) as its driver runs it (method.rs:3140-3400):
+// physical-shift scales over the fixed grid's corners (scales.rs:423-441, 668-722)
+// and, when estimate_lr, the learning rate estimated once (scales.rs:779-824;
+// method.rs EstimateLearningRate::Once). The objective is this file's metric.
+// stop: 0 MaxIterations, 1 StepTooSmall, 3 GradientConverged.
+int or_register(const float* fixed, const or_geometry* fg, const float* moving, const or_geometry* mg,
+                const uint8_t* fmask, const uint8_t* mmask, const int64_t* draw, int64_t ndraw, int bins,
+                int kind, double* params_inout, const double* fixed_params, int nfixed, int iterations,
+                double minimum_step, double gradient_tolerance, double relaxation_factor, double learning_rate,
+                int estimate_lr, int shift_scales, int nthreads, double* value_out, int* iterations_out,
+                int* stop_out) {
+    Problem P;
+    int st = prepare(fixed, fg, moving, mg, fmask, mmask, draw, ndraw, P);
+    if (st) return st;
+    double fmin, fmax, mmin, mmax;
+    ranges(P, &fmin, &fmax, &mmin, &mmax);
+    Geometry G;
+    st = make_geometry(fmin, fmax, mmin, mmax, bins, G);
+    if (st) return st;
+    Transform T0;
+    if (!make_transform(kind, params_inout, fixed_params, nfixed, T0)) return OR_BAD_ARGUMENT;
+    const int n = T0.nparams;
+    if (nthreads < 1) nthreads = 1;
+    std::vector<double> grad(n), scales(n, 1.0), scaled(n), prev(n, 0.0), p(params_inout, params_inout + n);
+    double value = 0.0;
+    auto eval = [&](const double* at) {
+        Transform T;
+        make_transform(kind, at, fixed_params, nfixed, T);
+        std::vector<Accum> parts(nthreads);
+        for (auto& a : parts) {
+            a.joint.assign((size_t)bins * bins, 0.0);
+            a.fixed_marginal.assign(bins, 0.0);
+            a.jpd.assign((size_t)bins * bins * n, 0.0);
+        }
+        const int64_t ns = P.n;
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t)
+            pool.emplace_back([&, t]() {
+                const int64_t lo = ns * t / nthreads, hi = ns * (t + 1) / nthreads;
+                for (int64_t s = lo; s < hi; ++s) sample_body(P, G, T, s, true, parts[t], nullptr, nullptr, nullptr);
+            });
+        for (auto& th : pool) th.join();
+        for (int t = 1; t < nthreads; ++t) {
+            for (size_t i = 0; i < parts[0].joint.size(); ++i) parts[0].joint[i] += parts[t].joint[i];
+            for (int i = 0; i < bins; ++i) parts[0].fixed_marginal[i] += parts[t].fixed_marginal[i];
+            for (size_t i = 0; i < parts[0].jpd.size(); ++i) parts[0].jpd[i] += parts[t].jpd[i];
+            parts[0].valid += parts[t].valid;
+        }
+        int64_t valid = 0;
+        finish(G, parts[0], n, true, &value, grad.data(), &valid);
+    };
+    // the estimator's Jacobians at the initial transform, at the 8 grid corners
+    std::vector<double> jac((size_t)8 * 3 * n);
+    double i2p[9];
+    index_to_physical(*fg, i2p);
+    for (int corner = 0; corner < 8; ++corner) {
+        double idx[3], x[3];
+        for (int d = 0; d < 3; ++d) idx[d] = ((corner >> d) & 1) ? (double)(fg->size[d] - 1) : 0.0;
+        for (int r = 0; r < 3; ++r) {
+            double v = fg->origin[r];
+            for (int c = 0; c < 3; ++c) v += i2p[r * 3 + c] * idx[c];
+            x[r] = v;
+        }
+        T0.jacobian(x, jac.data() + (size_t)corner * 3 * n);
+    }
+    const double dsmall = 0.01;
+    if (shift_scales) {
+        std::vector<double> shifts(n, 0.0);
+        for (int s = 0; s < 8; ++s)
+            for (int k = 0; k < n; ++k) {
+                double sq = 0.0;
+                for (int r = 0; r < 3; ++r) {
+                    double v = jac[(size_t)s * 3 * n + r * n + k];
+                    sq += v * v;
+                }
+                shifts[k] = std::fmax(shifts[k], dsmall * std::sqrt(sq));
+            }
+        double mn = INFINITY;
+        for (int k = 0; k < n; ++k)
+            if (shifts[k] > DBL_EPSILON) mn = std::fmin(mn, shifts[k]);
+        if (std::isfinite(mn)) {
+            double inv_d2 = 1.0 / (dsmall * dsmall);
+            for (int k = 0; k < n; ++k)
+                scales[k] = (shifts[k] <= DBL_EPSILON ? mn * mn : shifts[k] * shifts[k]) * inv_d2;
+        }
+    }
+    double max_step_size = INFINITY;
+    for (int d = 0; d < 3; ++d) max_step_size = std::fmin(max_step_size, fg->spacing[d]);
+    auto est_lr = [&](const double* step) {
+        double max_step = 0.0;
+        for (int k = 0; k < n; ++k) max_step = std::fmax(max_step, std::fabs(step[k]));
+        if (max_step <= DBL_EPSILON) return 1.0;
+        double factor = dsmall / max_step;
+        double max_sq = 0.0;
+        for (int s = 0; s < 8; ++s) {
+            double sq = 0.0;
+            for (int r = 0; r < 3; ++r) {
+                double dot = -0.0;
+                for (int c = 0; c < n; ++c) dot += jac[(size_t)s * 3 * n + r * n + c] * (step[c] * factor);
+                sq += dot * dot;
+            }
+            max_sq = std::fmax(max_sq, sq);
+        }
+        double step_scale = std::sqrt(max_sq) / factor;
+        return step_scale <= DBL_EPSILON ? 1.0 : max_step_size / step_scale;
+    };
+    eval(p.data());
+    double lr = learning_rate;
+    if (estimate_lr) {
+        for (int k = 0; k < n; ++k) scaled[k] = grad[k] / scales[k];
+        double sq = -0.0;
+        for (int k = 0; k < n; ++k) sq += scaled[k] * scaled[k];
+        lr = est_lr(scaled.data()) * std::sqrt(sq);
+    }
+    double relaxation = 1.0;
+    int stop = 0, taken = 0;
+    for (;;) {
+        for (int k = 0; k < n; ++k) scaled[k] = grad[k] / scales[k];
+        std::vector<double> sq(n);
+        for (int k = 0; k < n; ++k) sq[k] = scaled[k] * scaled[k];
+        const double gm = std::sqrt(kahan_sum(sq.data(), n));
+        if (gm < gradient_tolerance) { stop = 3; break; }
+        for (int k = 0; k < n; ++k) sq[k] = scaled[k] * prev[k];
+        if (kahan_sum(sq.data(), n) < 0.0) relaxation *= relaxation_factor;
+        const double step_length = relaxation * lr;
+        if (step_length < minimum_step) { stop = 1; break; }
+        if (taken >= iterations) break;
+        const double factor = step_length / gm;
+        for (int k = 0; k < n; ++k) p[k] -= factor * scaled[k];
+        prev = scaled;
+        ++taken;
+        eval(p.data());
+    }
+    std::memcpy(params_inout, p.data(), sizeof(double) * n);
+    *value_out = value;
+    *iterations_out = taken;
+    *stop_out = stop;
+    return OR_OK;
+}
+
 // The transform's stored matrix/offset (one point-map stage) and its Jacobian at a
 // point — exposed so tests can check the product's host-side transform code.
 int or_transform(int kind, const double* params, const double* fixed_params, int nfixed,

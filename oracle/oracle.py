@@ -215,3 +215,44 @@ def kahan_sum(v):
 
 def round_half_integer_up(x: float) -> int:
     return lib().or_round_half_integer_up(x)
+
+
+def register(fixed, fgeo, moving, mgeo, bins, kind, params, fixed_params=None, fmask=None,
+             mmask=None, draw=None, iterations=100, minimum_step=1e-4, gradient_tolerance=1e-4,
+             relaxation=0.5, learning_rate=1.0, estimate_learning_rate=True, shift_scales=True,
+             nthreads=1):
+    """One level of regular-step gradient descent with physical-shift scales
+    (registration/optimizer.rs:352-440, scales.rs:572-871, method.rs:3140-3400)."""
+    L = lib()
+    if not hasattr(L.or_register, "_typed"):
+        P = ctypes.POINTER
+        dp = P(ctypes.c_double)
+        L.or_register.argtypes = [P(ctypes.c_float), P(OrGeometry), P(ctypes.c_float), P(OrGeometry),
+                                  P(ctypes.c_uint8), P(ctypes.c_uint8), P(ctypes.c_int64), ctypes.c_int64,
+                                  ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, P(ctypes.c_int),
+                                  P(ctypes.c_int)]
+        L.or_register.restype = ctypes.c_int
+        L.or_register._typed = True
+    fixed = np.ascontiguousarray(fixed, dtype=np.float32)
+    moving = np.ascontiguousarray(moving, dtype=np.float32)
+    fm = None if fmask is None else np.ascontiguousarray(fmask, dtype=np.uint8)
+    mm = None if mmask is None else np.ascontiguousarray(mmask, dtype=np.uint8)
+    dr = None if draw is None else np.ascontiguousarray(draw, dtype=np.int64)
+    p = np.array(params, dtype=np.float64)
+    fpar = None if fixed_params is None else np.ascontiguousarray(fixed_params, dtype=np.float64)
+    value = ctypes.c_double()
+    iters = ctypes.c_int()
+    stop = ctypes.c_int()
+    st = L.or_register(_ptr(fixed, ctypes.c_float), ctypes.byref(fgeo), _ptr(moving, ctypes.c_float),
+                       ctypes.byref(mgeo), _ptr(fm, ctypes.c_uint8), _ptr(mm, ctypes.c_uint8),
+                       _ptr(dr, ctypes.c_int64), 0 if dr is None else len(dr), bins, kind,
+                       _ptr(p, ctypes.c_double), _ptr(fpar, ctypes.c_double),
+                       0 if fpar is None else len(fpar), iterations, minimum_step, gradient_tolerance,
+                       relaxation, learning_rate, 1 if estimate_learning_rate else 0,
+                       1 if shift_scales else 0, nthreads, ctypes.byref(value), ctypes.byref(iters),
+                       ctypes.byref(stop))
+    if st:
+        raise OracleError(st)
+    return {"params": p, "value": value.value, "iterations": iters.value, "stop_reason": stop.value}

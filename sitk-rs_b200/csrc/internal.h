@@ -99,6 +99,7 @@ struct Workspace {
     float* rec_g = nullptr;              // [3][n_samples]
     float hist_scale = 0.f;              // fixed-point scale of a joint-histogram tap
     int hist_scale_log2 = 0;
+    int fine_scale_log2 = 0;              // scale of the fine part; the global bins' unit is 2^-this
     int grid_hist = 0, block_hist = 0;
     int grid_deriv = 0, block_deriv = 0;
     // optional device-time accounting
@@ -141,6 +142,9 @@ struct AffineForm {
 };
 mi_status transform_form(int kind, const double* params, int nparams, const double* fixed,
                          int nfixed, AffineForm* out);
+// The family's own jacobian_wrt_parameters at point x, row-major 3×P.
+mi_status transform_jacobian(int kind, const double* params, int nparams, const double* fixed, int nfixed,
+                             const double* x, double* jac);
 
 // Core evaluation (mattes.cu).
 mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double* jac0,

@@ -51,6 +51,17 @@ namespace {
 #ifndef MI_HIST_MIN_BLOCKS
 #define MI_HIST_MIN_BLOCKS 4
 #endif
+// Histogram copies per CTA (coarse and fine parts) and the fine part's threshold
+// 2^-MI_HIST_FINE_T (see k_hist).
+#ifndef MI_HIST_COPIES
+#define MI_HIST_COPIES 4
+#endif
+#ifndef MI_HIST_FINE_COPIES
+#define MI_HIST_FINE_COPIES 2
+#endif
+#ifndef MI_HIST_FINE_T
+#define MI_HIST_FINE_T 10
+#endif
 constexpr int HIST_BLOCK = 256;
 constexpr int HIST_MIN_BLOCKS = MI_HIST_MIN_BLOCKS;
 constexpr int HIST_ILP = MI_HIST_ILP;
@@ -69,13 +80,26 @@ __host__ __device__ inline size_t tail_doubles(int B) { return (size_t)B * B + 3
 // One histogram copy: B² joint + B fixed-marginal u32 counters, padded so copies
 // start 4 banks apart.
 __host__ __device__ inline int hist_copy_stride(int B) { return ((B * B + B + 31) & ~31) + 4; }
-// Copies that fit in 48 KB (a power of two, 1–8).
+// Copies that fit in 48 KB (a power of two, 1–MI_HIST_COPIES).
 int hist_copies(int B) {
-    int c = 8;
+    int c = MI_HIST_COPIES;
     while (c > 1 && (size_t)c * hist_copy_stride(B) * sizeof(unsigned int) > 48 * 1024) c >>= 1;
     return c;
 }
-size_t hist_smem(int B) { return (size_t)hist_copies(B) * hist_copy_stride(B) * sizeof(unsigned int); }
+// The fine histogram (B² u32 counters per copy) that takes the small outer taps.
+__host__ __device__ inline int hist_fine_stride(int B) { return ((B * B + 31) & ~31) + 4; }
+// Fine copies: up to MI_HIST_FINE_COPIES, fewer if the two parts together pass
+// 52 KB (four 256-thread CTAs resident per SM at 32 bins).
+int hist_fine_copies(int B) {
+    const size_t coarse = (size_t)hist_copies(B) * hist_copy_stride(B) * sizeof(unsigned int);
+    int c = MI_HIST_FINE_COPIES;
+    while (c > 1 && coarse + (size_t)c * hist_fine_stride(B) * sizeof(unsigned int) > 52 * 1024) c >>= 1;
+    return c;
+}
+size_t hist_smem(int B) {
+    return ((size_t)hist_copies(B) * hist_copy_stride(B) + (size_t)hist_fine_copies(B) * hist_fine_stride(B)) *
+           sizeof(unsigned int);
+}
 size_t deriv_smem(int B) {
     return ((size_t)32 * NMOM + tail_doubles(B)) * sizeof(double) + (size_t)B * B * sizeof(float);
 }
@@ -186,22 +210,36 @@ k_value(int B, double moving_bin_size, double hist_inv, unsigned long long* __re
 }
 
 // ---------------------------------------------------------------------------
-// Pass 1: joint histogram (+ per-sample records for pass 2), then the tail in the
-// last CTA. The CTA histogram is u32 fixed point: a tap w is added as
-// round(w·2^k) with k chosen per launch so that no CTA's bin can exceed 2^32
-// (hist_scale = 2^k); the flush into the global histogram is u64.
+// Pass 1: joint histogram (+ per-sample records for pass 2). The CTA histogram is
+// u32 fixed point in two parts, both exact integer sums:
+//   coarse: the two inner taps (always ≥ 1/6) and outer taps ≥ 2^-FINE_T, added as
+//           round(w·2^k) (hist_scale = 2^k);
+//   fine:   outer taps below 2^-FINE_T (a cubic B-spline's end taps, f³/6 and
+//           (1−f)³/6, near a bin edge), added as round(w·2^kf) with kf > k
+//           (fine_scale = 2^kf, fine_shift = kf − k).
+// A sparse bin whose mass is made of end taps is where pRatio = log p is steep: a
+// 2^-k quantum there moves the derivative by far more than FP32 rounding does, so
+// those taps get the fine quantum. k and kf are chosen per launch so that no copy's
+// counter can pass 2^32; the flush adds (coarse << fine_shift) + fine into the u64
+// global histogram, whose unit is 2^-kf.
 // ---------------------------------------------------------------------------
+constexpr int FINE_T = MI_HIST_FINE_T;
+constexpr float FINE_LIMIT = 1.0f / (float)(1u << FINE_T);
+
 template <bool RECORD>
 __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
 k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restrict__ mmask,
        const uint32_t* __restrict__ samples, const uint8_t* __restrict__ fbin, uint32_t n, uint32_t npad,
-       float hist_scale, int copies, unsigned long long* __restrict__ ghist, uint8_t* __restrict__ rec_mi,
-       float* __restrict__ rec_f, float* __restrict__ rec_g) {
+       float hist_scale, float fine_scale, int fine_shift, int copies, int fine_copies,
+       unsigned long long* __restrict__ ghist, uint8_t* __restrict__ rec_mi, float* __restrict__ rec_f,
+       float* __restrict__ rec_g) {
     extern __shared__ unsigned int sh[];
     const int B = P.bins;
     const int nb = B * B + B;
     const int cstride = hist_copy_stride(B);
-    for (int i = threadIdx.x; i < copies * cstride; i += blockDim.x) sh[i] = 0u;
+    const int fstride = hist_fine_stride(B);
+    unsigned int* sh_fine = sh + copies * cstride;
+    for (int i = threadIdx.x; i < copies * cstride + fine_copies * fstride; i += blockDim.x) sh[i] = 0u;
     __syncthreads();
     unsigned int* sh_joint = sh;
     unsigned int* sh_fixed = sh + B * B;
@@ -215,6 +253,7 @@ k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restr
     const int lane = threadIdx.x & 31;
     unsigned int* my_joint = sh_joint + (lane & (copies - 1)) * cstride;
     unsigned int* my_fixed = sh_fixed + (lane & (copies - 1)) * cstride;
+    unsigned int* my_fine = sh_fine + (lane & (fine_copies - 1)) * fstride;
     auto account = [&](const Prep& p, uint32_t s, bool real) {
         if (!real) return;
         Sample o;
@@ -227,11 +266,19 @@ k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restr
         const int fi = __ldg(fbin + s);
         float w[4];
         bspline3_taps(o.f, w);
-        unsigned int* row = my_joint + fi * B + (o.mi - 1);
-        // round(w·2^k) by the 1.5·2^23 magic add (w·2^k < 2^22): one FMA, no conversion
+        const int off = fi * B + (o.mi - 1);
+        unsigned int* row = my_joint + off;
+        unsigned int* frow = my_fine + off;
+        // round(w·scale) by the 1.5·2^23 magic add (w·scale < 2^22 for both parts):
+        // one FMA, no conversion
+        atomicAdd(row + 1, __float_as_uint(fmaf(w[1], hist_scale, 12582912.0f)) - 0x4B400000u);
+        atomicAdd(row + 2, __float_as_uint(fmaf(w[2], hist_scale, 12582912.0f)) - 0x4B400000u);
 #pragma unroll
-        for (int t = 0; t < 4; ++t)
-            atomicAdd(row + t, __float_as_uint(fmaf(w[t], hist_scale, 12582912.0f)) - 0x4B400000u);
+        for (int t = 0; t < 4; t += 3) {
+            const bool fine = w[t] < FINE_LIMIT;
+            atomicAdd((fine ? frow : row) + t,
+                      __float_as_uint(fmaf(w[t], fine ? fine_scale : hist_scale, 12582912.0f)) - 0x4B400000u);
+        }
         atomicAdd(my_fixed + fi, 1u);
         if (RECORD) {
             rec_mi[s] = (uint8_t)o.mi;
@@ -268,6 +315,11 @@ k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restr
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
         unsigned long long v = 0ull;
         for (int c = 0; c < copies; ++c) v += sh[c * cstride + i];
+        if (i < B * B) {
+            unsigned long long f = 0ull;
+            for (int c = 0; c < fine_copies; ++c) f += sh_fine[c * fstride + i];
+            v = (v << fine_shift) + f;
+        }
         if (v) atomicAdd(&ghist[i], v);
     }
 }
@@ -784,15 +836,17 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[0], st));
     const uint32_t n = (uint32_t)m->n_samples;
     const uint32_t npad = (n + 3u) & ~3u;
-    const double hist_inv = std::ldexp(1.0, -ws.hist_scale_log2);
+    const double hist_inv = std::ldexp(1.0, -ws.fine_scale_log2);
+    const float fine_scale = (float)std::ldexp(1.0, ws.fine_scale_log2);
+    const int fine_shift = ws.fine_scale_log2 - ws.hist_scale_log2;
     if (want_derivative)
         k_hist<true><<<ws.grid_hist, ws.block_hist, hist_smem(B), st>>>(
-            P, m->moving, m->mmask, m->samples, m->fbin, n, npad, ws.hist_scale, hist_copies(B), ws.hist, ws.rec_mi, ws.rec_f,
-            ws.rec_g);
+            P, m->moving, m->mmask, m->samples, m->fbin, n, npad, ws.hist_scale, fine_scale, fine_shift,
+            hist_copies(B), hist_fine_copies(B), ws.hist, ws.rec_mi, ws.rec_f, ws.rec_g);
     else
         k_hist<false><<<ws.grid_hist, ws.block_hist, hist_smem(B), st>>>(
-            P, m->moving, m->mmask, m->samples, m->fbin, n, npad, ws.hist_scale, hist_copies(B), ws.hist, nullptr, nullptr,
-            nullptr);
+            P, m->moving, m->mmask, m->samples, m->fbin, n, npad, ws.hist_scale, fine_scale, fine_shift,
+            hist_copies(B), hist_fine_copies(B), ws.hist, nullptr, nullptr, nullptr);
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
     int nout = 2;
     if (want_derivative) {
@@ -1005,18 +1059,27 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     ws.block_deriv = DERIV_BLOCK;
     ws.grid_hist = grid_for(m->n_samples, HIST_BLOCK, ctx->num_sms * std::max(occ_h, 1));
     ws.grid_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
-    // Fixed-point scale of a histogram tap: a CTA takes at most cta_max samples, each
-    // adding at most 2/3 to one bin, so 2^k·(2/3)·cta_max (+ rounding) must stay below
-    // 2^32 (a copy of the CTA histogram sees at most as many samples as the CTA);
-    // k is capped at 22 so that the magic-add rounding stays exact.
+    // Fixed-point scales of the histogram taps. A thread takes at most per_thread
+    // samples, and a copy of the CTA histogram is fed by HIST_BLOCK/copies threads, so
+    // it sees at most copy_max samples; each adds at most one tap to a bin (coarse
+    // taps ≤ 2/3, fine taps < 2^-FINE_T). Every counter must stay below 2^32 and every
+    // rounded tap below 2^22 (the magic-add rounding): k ≤ 22, kf ≤ FINE_T + 22. The global
+    // u64 bin, in units of 2^-kf, takes at most n_samples·(2/3)·2^kf.
     {
         const int64_t per_thread = (m->n_samples + (int64_t)ws.grid_hist * HIST_BLOCK - 1) /
                                    ((int64_t)ws.grid_hist * HIST_BLOCK);
-        const double cta_max = (double)std::max<int64_t>(per_thread * HIST_BLOCK, 1);
-        int k = 22;  // w·2^k < 2^22 keeps the magic-add rounding exact
-        while (k > 0 && std::ldexp(1.0, k) * (2.0 / 3.0) * cta_max + cta_max >= 4294967295.0 * 0.98) --k;
+        const double lim = 4294967295.0 * 0.98;
+        const double coarse_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_copies(B)), 1);
+        const double fine_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_fine_copies(B)), 1);
+        int k = 22;
+        while (k > 0 && std::ldexp(1.0, k) * (2.0 / 3.0) * coarse_max + coarse_max >= lim) --k;
+        int kf = FINE_T + 22;
+        while (kf > k && (std::ldexp(1.0, kf - FINE_T) * fine_max + fine_max >= lim ||
+                          std::ldexp(1.0, kf) * (double)(m->n_samples + 1) >= 0x1p63))
+            --kf;
         ws.hist_scale_log2 = k;
         ws.hist_scale = (float)std::ldexp(1.0, k);
+        ws.fine_scale_log2 = kf;
     }
     {
         // padded to whole groups of four samples; padding records keep moving bin 0

@@ -105,6 +105,9 @@ struct Family {
     }
 };
 
+mi_status build_family(int kind, const double* params, int nparams, const double* fixed, int nfixed,
+                       Family& f);
+
 }  // namespace
 
 namespace mi {
@@ -113,6 +116,42 @@ mi_status transform_form(int kind, const double* params, int nparams, const doub
                          int nfixed, AffineForm* out) {
     if (!params || !out) return MI_ERR_INVALID_ARGUMENT;
     Family f{};
+    const mi_status s = build_family(kind, params, nparams, fixed, nfixed, f);
+    if (s != MI_OK) return s;
+    out->nparams = f.P;
+    for (int i = 0; i < 9; ++i) out->stage[i] = f.m[i];
+    for (int d = 0; d < 3; ++d) out->stage[9 + d] = f.off[d];
+    // J is linear in p = x − center plus a constant translation block.
+    double jt[3 * MI_MAX_PARAMS];
+    f.jac_centered(0.0, 0.0, 0.0, jt);  // the constant part
+    for (int e = 0; e < 3; ++e) {
+        double unit[3] = {0.0, 0.0, 0.0};
+        unit[e] = 1.0;
+        double je[3 * MI_MAX_PARAMS];
+        f.jac_centered(unit[0], unit[1], unit[2], je);
+        for (int i = 0; i < 3 * f.P; ++i) out->jacc[e][i] = je[i] - jt[i];
+    }
+    f.jac_centered(-f.center[0], -f.center[1], -f.center[2], out->jac0);
+    return MI_OK;
+}
+
+mi_status transform_jacobian(int kind, const double* params, int nparams, const double* fixed, int nfixed,
+                             const double* x, double* jac) {
+    if (!params || !x || !jac) return MI_ERR_INVALID_ARGUMENT;
+    Family f{};
+    const mi_status s = build_family(kind, params, nparams, fixed, nfixed, f);
+    if (s != MI_OK) return s;
+    // jacobian_wrt_parameters(point): p = point − center first, as each family does
+    f.jac_centered(x[0] - f.center[0], x[1] - f.center[1], x[2] - f.center[2], jac);
+    return MI_OK;
+}
+
+}  // namespace mi
+
+namespace {
+
+mi_status build_family(int kind, const double* params, int nparams, const double* fixed, int nfixed,
+                       Family& f) {
     f.kind = kind;
     for (int d = 0; d < 3; ++d) f.center[d] = (fixed && nfixed >= 3) ? fixed[d] : 0.0;
     switch (kind) {
@@ -184,21 +223,7 @@ mi_status transform_form(int kind, const double* params, int nparams, const doub
         default:
             return MI_ERR_INVALID_ARGUMENT;
     }
-    out->nparams = f.P;
-    for (int i = 0; i < 9; ++i) out->stage[i] = f.m[i];
-    for (int d = 0; d < 3; ++d) out->stage[9 + d] = f.off[d];
-    // J is linear in p = x − center plus a constant translation block.
-    double jt[3 * MI_MAX_PARAMS];
-    f.jac_centered(0.0, 0.0, 0.0, jt);  // the constant part
-    for (int e = 0; e < 3; ++e) {
-        double unit[3] = {0.0, 0.0, 0.0};
-        unit[e] = 1.0;
-        double je[3 * MI_MAX_PARAMS];
-        f.jac_centered(unit[0], unit[1], unit[2], je);
-        for (int i = 0; i < 3 * f.P; ++i) out->jacc[e][i] = je[i] - jt[i];
-    }
-    f.jac_centered(-f.center[0], -f.center[1], -f.center[2], out->jac0);
     return MI_OK;
 }
 
-}  // namespace mi
+}  // namespace

@@ -29,7 +29,8 @@ EXPORTED = [
     "mi_metric_create", "mi_metric_info_get", "mi_metric_destroy", "mi_metric_value",
     "mi_metric_value_and_derivative", "mi_metric_value_and_derivative_stages",
     "mi_metric_sample_decisions", "mi_transform_form", "mi_metric_timing_enable",
-    "mi_metric_timing_read", "mi_metric_value_noalloc",
+    "mi_metric_timing_read", "mi_metric_value_noalloc", "mi_register_rsgd",
+    "mi_centered_initialize",
 ]
 
 

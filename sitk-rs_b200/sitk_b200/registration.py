@@ -1,0 +1,97 @@
+"""Registration driver over the device metric (the reference's kept callers).
+
+`register_rsgd` is one level of `ImageRegistrationMethod` as the reference drives
+its device metric (registration/method.rs:3140-3400): regular-step gradient descent
+(optimizer.rs:271-440) with physical-shift scales and a once-estimated learning rate
+(scales.rs:572-871, `set_optimizer_as_regular_step_gradient_descent_estimated` +
+`set_optimizer_scales_from_physical_shift`). `centered_initialize` is
+CenteredTransformInitializer in Geometry mode (initializer.rs:56-105). The loop runs
+in the library (csrc/register.cpp); every objective call is the device metric.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .metric import DeviceImage, DeviceMattesMetric
+from .transforms import ParametricTransform
+
+STOP_REASONS = {0: "MaxIterations", 1: "StepTooSmall", 2: "Converged", 3: "GradientConverged"}
+
+
+class MiRsgdConfig(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("minimum_step", ctypes.c_double),
+                ("gradient_tolerance", ctypes.c_double), ("relaxation", ctypes.c_double),
+                ("learning_rate", ctypes.c_double), ("estimate_learning_rate", ctypes.c_int),
+                ("physical_shift_scales", ctypes.c_int), ("trace", ctypes.POINTER(ctypes.c_double)),
+                ("trace_rows", ctypes.c_int)]
+
+
+class MiRsgdResult(ctypes.Structure):
+    _fields_ = [("value", ctypes.c_double), ("valid", ctypes.c_int64), ("iterations", ctypes.c_int),
+                ("stop_reason", ctypes.c_int), ("evaluations", ctypes.c_int)]
+
+
+@dataclass
+class LevelResult:
+    """registration/method.rs:728-800 (per level)."""
+    value: float
+    iterations: int
+    stop_reason: str
+    valid_points: int
+    evaluations: int
+    trace: np.ndarray | None = None  # rows [value, params, derivative] per evaluation
+
+
+def _bind():
+    L = _lib.load()
+    if getattr(L, "_rsgd_bound", False):
+        return L
+    P = ctypes.POINTER
+    L.mi_register_rsgd.argtypes = [ctypes.c_void_p, ctypes.c_int, P(ctypes.c_double), ctypes.c_int,
+                                   P(MiRsgdConfig), P(ctypes.c_double), ctypes.c_int, P(MiRsgdResult)]
+    L.mi_register_rsgd.restype = ctypes.c_int
+    L.mi_centered_initialize.argtypes = [P(_lib.MiGeometry), P(_lib.MiGeometry), P(ctypes.c_double),
+                                         P(ctypes.c_double)]
+    L.mi_centered_initialize.restype = ctypes.c_int
+    L._rsgd_bound = True
+    return L
+
+
+def centered_initialize(fixed: DeviceImage, moving: DeviceImage):
+    """(center, translation) of CenteredTransformInitializer(Geometry)."""
+    L = _bind()
+    c = np.zeros(3)
+    t = np.zeros(3)
+    dp = ctypes.POINTER(ctypes.c_double)
+    _lib.check(L.mi_centered_initialize(ctypes.byref(fixed.geo), ctypes.byref(moving.geo),
+                                        c.ctypes.data_as(dp), t.ctypes.data_as(dp)))
+    return c, t
+
+
+def register_rsgd(metric: DeviceMattesMetric, transform: ParametricTransform, iterations: int = 100,
+                  minimum_step: float = 1e-4, gradient_tolerance: float = 1e-4, relaxation: float = 0.5,
+                  learning_rate: float | None = None, physical_shift_scales: bool = True,
+                  record: bool = False) -> LevelResult:
+    """Optimise `transform` in place (its parameters are updated). With `record`, the
+    result carries every evaluation's value, parameters and derivative."""
+    L = _bind()
+    p = np.ascontiguousarray(transform.params, dtype=np.float64).copy()
+    rows = int(iterations) + 1 if record else 0
+    trace = np.zeros((rows, 1 + 2 * p.size)) if record else None
+    cfg = MiRsgdConfig(int(iterations), float(minimum_step), float(gradient_tolerance), float(relaxation),
+                       1.0 if learning_rate is None else float(learning_rate),
+                       1 if learning_rate is None else 0, 1 if physical_shift_scales else 0,
+                       trace.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if record else None, rows)
+    fp = np.ascontiguousarray(transform.fixed_params, dtype=np.float64)
+    res = MiRsgdResult()
+    dp = ctypes.POINTER(ctypes.c_double)
+    _lib.check(L.mi_register_rsgd(metric.handle, transform.kind, fp.ctypes.data_as(dp) if fp.size else None,
+                                  fp.size, ctypes.byref(cfg), p.ctypes.data_as(dp), p.size, ctypes.byref(res)),
+               metric.ctx.handle)
+    transform.set_parameters(p)
+    return LevelResult(res.value, res.iterations, STOP_REASONS.get(res.stop_reason, str(res.stop_reason)),
+                       res.valid, res.evaluations, None if trace is None else trace[:res.evaluations])
