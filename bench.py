@@ -7,9 +7,11 @@ rotation ±15°, translation ±12 mm, seeded synthetic data), VersorRigid3DTrans
 flushed (a 256 MiB write) before every evaluation, outside the timed events.
 
   value  device time of the evaluations (CUDA events on the library's stream, first
-         kernel to the result copy), inputs resident in HBM
-  e2e    the same call timed end to end through the public C ABI from the host
-         (parameters in from host memory, value+derivative back to host memory)
+         kernel to the result copy), inputs resident in HBM; the flush is queued on
+         the same stream, so the launches of an evaluation wait behind it
+  e2e    the same call timed end to end through the public C ABI from the host,
+         starting from an idle stream (parameters in from host memory, value and
+         derivative back to host memory, launch latency and host wait included)
 
 --impl reference times the reference algorithm's CPU implementation on this host's
 cores (the C++ restatement under oracle/, all threads), since the Rust reference
@@ -211,43 +213,82 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     S = int(info["n_samples"])
     t = sb.VersorRigid3DTransform(POSE[:3], POSE[3:], [(N - 1) / 2.0] * 3)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    from sitk_b200.metric import get_fused, set_fused
+    if args.form == "fused":
+        set_fused(metric, True)
+    fused = get_fused(metric)
+    launches_per_eval = 1 if fused else 2
     l2 = torch.cuda.get_device_properties(dev).L2_cache_size
-    flush = torch.empty(max(2 * l2, 256 << 20) // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    nflush = max(2 * l2, 256 << 20) // 4
+    flush_w = torch.empty(nflush, dtype=torch.float32, device=f"cuda:{dev}")
+    flush_r = torch.zeros(nflush, dtype=torch.float32, device=f"cuda:{dev}")
+
+    def l2_flush():
+        # write a buffer larger than L2 (evicts every line of the evaluation's data),
+        # then read another one, so the write's dirty lines are written back here and
+        # not during the next evaluation; queued on the evaluation's stream
+        with torch.cuda.stream(stream):
+            flush_w.zero_()
+            torch.sum(flush_r)
 
     sampler = ClockSampler(dev) if rank == 0 else None
     if sampler:
         sampler.start()
-    enable_timing(metric, True)
     for _ in range(max(args.warmup, 3)):
-        flush.zero_()
-        torch.cuda.synchronize(dev)
+        l2_flush()
         metric.evaluate(t)
     # settle clocks under load (untimed)
     t_end = time.perf_counter() + args.settle
     while time.perf_counter() < t_end:
         metric.evaluate(t)
-    read_timing(metric)
 
+    def timed_loop(per_kernel: bool):
+        # The flush is queued on the evaluation's own stream with no host wait after
+        # it: an evaluation's launches queue while the flush runs, and its events
+        # (recorded by the library before its first launch and after its result copy)
+        # measure the evaluation on the device, not the host's launch latency.
+        enable_timing(metric, True, per_kernel=per_kernel)
+        read_timing(metric)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            l2_flush()
+            metric.evaluate(t)
+        torch.cuda.synchronize(dev)
+        w = time.perf_counter() - w0
+        if dist:
+            dist.barrier()
+        ms, nev = read_timing(metric)
+        enable_timing(metric, False)
+        return ms, nev, w
+
+    # value: whole evaluations, two events each
+    ms, nev, wall = timed_loop(False)
+    dev_ms = ms[0]
+    # kernel durations for the roofline: events after every kernel as well
+    ms_k, nev_k, _ = timed_loop(True)
+
+    # End to end: the call as a user makes it, from an idle stream: torch events
+    # bracket the whole synchronous call (parameter upload as kernel arguments,
+    # launches, the device-to-host copy of value and derivative, the host wait).
     ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    wall0 = time.perf_counter()
     last = None
     for i in range(args.steps):
-        flush.zero_()
+        l2_flush()
         torch.cuda.synchronize(dev)
         ev_s[i].record(stream)
         last = metric.evaluate(t)
         ev_e[i].record(stream)
     torch.cuda.synchronize(dev)
-    wall = time.perf_counter() - wall0
     if dist:
         dist.barrier()
-    ms, nev = read_timing(metric)
     e2e_ms = sum(a.elapsed_time(b) for a, b in zip(ev_s, ev_e))
-    dev_ms = ms[0]
     if dist:
         tt = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -262,11 +303,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     per_step_ms = dev_ms / args.steps
     value = world * args.steps / (dev_ms / 1e3)
     e2e_value = world * args.steps / (e2e_ms / 1e3)
-    # ms[2] is the gap between the two passes (the tail runs inside k_deriv)
-    kern = {"k_hist": ms[1] / nev, "between_passes": ms[2] / nev, "k_deriv": ms[3] / nev}
-    dom = max(("k_hist", "k_deriv"), key=lambda k: kern[k])
     vm = N ** 3
-    bytes_alg = S * 4 + min(vm, 8 * S) * 4  # one pass: fixed f32 + moving f32 (per-unit figure × S)
+    pass_bytes = S * 4 + min(vm, 8 * S) * 4  # one pass: fixed f32 + moving f32 (per-unit figure × S)
+    if fused:
+        kern = {"k_eval": ms_k[1] / nev_k}
+        dom, bytes_alg = "k_eval", 2 * pass_bytes  # both passes in one launch
+    else:
+        kern = {"k_hist": ms_k[1] / nev_k, "k_deriv": ms_k[2] / nev_k}  # k_deriv forms the tail itself
+        dom, bytes_alg = "k_hist", pass_bytes
     peak, peak_kind = _peaks()
     achieved = bytes_alg / (kern[dom] / 1e3) / 1e9
     traffic = _traffic(dom)
@@ -289,11 +333,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "fixed": [N, N, N], "moving": [N, N, N], "bins": BINS,
                    "sampling": "random 10%", "samples": S, "transform": "VersorRigid3D",
-                   "l2": "flushed before every evaluation (256 MiB write, untimed)",
+                   "l2": "flushed before every evaluation (256 MiB write, then a 256 MiB read of "
+                         "another buffer so the write-backs fall outside the timed region)",
+                   "form": "fused (one cooperative kernel)" if fused else "split (two kernels)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * (6 + 3),
                 "d2h_bytes_per_step": 8 * (2 + 6)},
-        "gpu_launches": 2 * args.steps,  # k_hist + k_deriv per evaluation
+        "gpu_launches": launches_per_eval * args.steps,  # in the timed loop of `value`
         "kernel_ms": kern,
         "sample_points_per_s": 2 * S * value / world,
         "wall_ms_per_step": 1e3 * wall / args.steps,
@@ -318,6 +364,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="split", choices=["split", "fused"],
+                    help="launch form of an evaluation: two kernels, or one cooperative kernel")
     ap.add_argument("--settle", type=float, default=1.0,
                     help="seconds of untimed evaluations before the timed region (clock ramp)")
     args = ap.parse_args()

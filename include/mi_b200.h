@@ -44,7 +44,7 @@ typedef enum {
     MI_ERR_NON_AFFINE_TRANSFORM = 12, /* DeviceMetricError::NonAffineTransform */
     MI_ERR_POINT_MAP_STAGE_COUNT = 13,/* CudaError::PointMapStageCount (more than MI_MAX_STAGES) */
     MI_ERR_TOO_MANY_HISTOGRAM_BINS = 14, /* bins > MI_MAX_BINS: no reference counterpart */
-    MI_ERR_TIMEOUT = 15,              /* a bounded device wait gave up (batched form) */
+    MI_ERR_TIMEOUT = 15,              /* a bounded device wait gave up (fused form's grid barrier) */
     MI_ERR_NOT_CONVERGED = 16         /* reserved */
 } mi_status;
 
@@ -167,13 +167,28 @@ mi_status mi_metric_value_and_derivative_stages(mi_metric* m, const double* stag
                                                 int nparams, double* value, double* derivative,
                                                 int64_t* valid);
 
-/* Device-time accounting (no reference counterpart; used by benchmarks). When
- * enabled, every evaluation records CUDA events on the context stream around its
- * kernels. mi_metric_timing_read returns the milliseconds accumulated since the last
- * read — [0] whole evaluation (first kernel to the result copy), [1] histogram pass,
- * [2] tail, [3] derivative pass — and the evaluation count, then resets them. */
+/* Device-time accounting (no reference counterpart; used by benchmarks). enable = 1
+ * records a CUDA event on the context stream before an evaluation's first launch and
+ * one after its result copy; enable = 2 also records one after each kernel (each
+ * event adds a little device time of its own); 0 turns it off. mi_metric_timing_read
+ * returns the milliseconds accumulated since the last read — [0] whole evaluation
+ * (first launch to the result copy), and with enable = 2 [1] histogram pass (the
+ * whole fused kernel in the fused form), [2] the second kernel of the split form
+ * (tail and derivative pass, or the value-only tail), [3] unused — and the
+ * evaluation count, then resets them. */
 mi_status mi_metric_timing_enable(mi_metric* m, int enable);
 mi_status mi_metric_timing_read(mi_metric* m, double* ms4, int64_t* n_evals);
+
+/* Launch form of an evaluation (no reference counterpart). The fused form is one
+ * cooperative kernel (histogram, grid barrier, tail and derivative); the split form
+ * is two kernels (histogram; tail and derivative) with the same arithmetic and the
+ * same value bits. The split form is the default: the device time is the same and
+ * a cooperative launch adds its latency to a synchronous call. mi_metric_set_fused(m,
+ * 1) fails with MI_ERR_INVALID_ARGUMENT where a cooperative launch is not available;
+ * mi_metric_get_fused reports the current form. A fused evaluation whose grid
+ * barrier does not complete within its wait limit returns MI_ERR_TIMEOUT. */
+mi_status mi_metric_set_fused(mi_metric* m, int fused);
+mi_status mi_metric_get_fused(const mi_metric* m, int* fused);
 
 /* The point-map stage (matrix row-major, offset: 12 doubles) a transform family
  * stores and multiplies (transform/parametric.rs:549-553, :1103-1107, :1331-1335),

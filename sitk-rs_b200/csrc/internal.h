@@ -86,15 +86,14 @@ struct SamplerParams {
 // Per-metric device scratch and the host-side view of it.
 struct Workspace {
     unsigned long long* hist = nullptr;  // [bins*bins] joint (2^-32 fixed point), [bins] fixed marginal, [1] valid
-    double* pratio = nullptr;            // [bins*bins] pRatio·nFactor
-    double* tail = nullptr;              // [4]: value, valid, degenerate flag, joint sum
     double* partials = nullptr;          // [grid_deriv][12]
+    double* vsum = nullptr;              // value slice sums
     double* result = nullptr;            // [2 + MI_MAX_PARAMS]: value, valid, derivative
     unsigned int* done_counter = nullptr;
     double* host_result = nullptr;       // pinned mirror of result
     // per-sample records pass 1 hands pass 2 (struct of arrays, sample order):
     // moving bin (0 = not a valid sample), Parzen fraction, moving gradient
-    uint8_t* rec_mi = nullptr;
+    uint16_t* rec_bins = nullptr;
     float* rec_f = nullptr;
     float* rec_g = nullptr;              // [3][n_samples]
     float hist_scale = 0.f;              // fixed-point scale of a joint-histogram tap
@@ -102,8 +101,12 @@ struct Workspace {
     int fine_scale_log2 = 0;              // scale of the fine part; the global bins' unit is 2^-this
     int grid_hist = 0, block_hist = 0;
     int grid_deriv = 0, block_deriv = 0;
+    int grid_eval = 0;                    // fused form's cooperative grid (0: not available)
+    int grid_split_hist = 0, grid_split_deriv = 0;
+    bool fused = false;                   // evaluate with the fused cooperative kernel
+    bool can_fuse = false;
     // optional device-time accounting
-    bool timing = false;
+    int timing = 0;                      // 0 off, 1 whole evaluation, 2 also per kernel
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double ms[4] = {0, 0, 0, 0};
     int64_t timed_evals = 0;

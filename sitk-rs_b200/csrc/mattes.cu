@@ -74,9 +74,6 @@ struct JacobianForm {
     double jacc[3][3 * MI_MAX_PARAMS];
 };
 
-// Dynamic shared memory of the tail: jp[B²], fm[B], mm[B], lfm[B], red[32] doubles.
-__host__ __device__ inline size_t tail_doubles(int B) { return (size_t)B * B + 3 * (size_t)B + 32; }
-
 // One histogram copy: B² joint + B fixed-marginal u32 counters, padded so copies
 // start 4 banks apart.
 __host__ __device__ inline int hist_copy_stride(int B) { return ((B * B + B + 31) & ~31) + 4; }
@@ -100,9 +97,17 @@ size_t hist_smem(int B) {
     return ((size_t)hist_copies(B) * hist_copy_stride(B) + (size_t)hist_fine_copies(B) * hist_fine_stride(B)) *
            sizeof(unsigned int);
 }
-size_t deriv_smem(int B) {
-    return ((size_t)32 * NMOM + tail_doubles(B)) * sizeof(double) + (size_t)B * B * sizeof(float);
+// Shared memory of the tail (see TailSmem).
+constexpr int TAIL_BLOCK = 256;
+__host__ __device__ inline int tail_groups(int B) { return TAIL_BLOCK / B; }
+__host__ __device__ inline size_t tail_smem(int B) {
+    return ((size_t)B * B + B + (size_t)tail_groups(B) * B + B) * 8 + ((2 * (size_t)B + 7) & ~(size_t)7);
 }
+size_t deriv_smem(int B) { return 32 * (size_t)NMOM * sizeof(double) + tail_smem(B) + (size_t)B * B * sizeof(float); }
+// The fused kernel reuses one dynamic allocation for its phases. The derivative
+// pass's layout: moment reduction scratch (32·NMOM doubles), the tail's state
+// (tail_smem), then the pRatio table (B² floats).
+size_t eval_smem(int B) { return std::max(hist_smem(B), std::max(deriv_smem(B), tail_smem(B))); }
 
 // Block-wide sum of a double in a fixed order (warp shuffles, then warp 0).
 __device__ double block_sum(double v, double* red) {
@@ -126,87 +131,38 @@ __device__ double block_sum(double v, double* red) {
     return r;
 }
 
-struct TailOut {
-    double value;      // −MI, or DBL_MAX for a degenerate histogram
-    double valid;      // valid-sample count
-    bool degenerate;   // no valid sample or no mass (mattes.rs:590-609)
-};
-
-// The tail (registration/mattes.rs:273-328) over the finished global histogram,
-// computed by one CTA into its shared memory: normalisation, marginals, −MI and the
-// pRatio·nFactor table (written to pr, FP32, when non-null). ghist holds the joint
-// taps (fixed point, hist_inv per unit) then the fixed-marginal counts; it is only
-// read. The sums are FP64 block reductions in a fixed order. Every CTA that calls
-// this on the same histogram gets the same bits.
-__device__ TailOut run_tail(int B, double moving_bin_size, double hist_inv,
-                            const unsigned long long* __restrict__ ghist, double* tsh, float* pr) {
-    double* jp = tsh;         // B*B
-    double* fm = jp + B * B;  // B
-    double* mm = fm + B;      // B
-    double* lfm = mm + B;     // B
-    double* red = lfm + B;    // 32
-    const int B2 = B * B;
-    double part = 0.0, cnt = 0.0;
-    for (int i = threadIdx.x; i < B2; i += blockDim.x) {
-        const double v = (double)__ldcg(ghist + i) * hist_inv;
-        jp[i] = v;
-        part += v;
-    }
-    for (int i = threadIdx.x; i < B; i += blockDim.x) {
-        const double c = (double)__ldcg(ghist + B2 + i);
-        fm[i] = c;
-        cnt += c;
-    }
-    TailOut out;
-    const double joint_sum = block_sum(part, red);
-    out.valid = block_sum(cnt, red);
-    out.degenerate = out.valid == 0.0 || joint_sum < DBL_EPSILON;
-    if (out.degenerate) {
-        out.value = DBL_MAX;
-        return out;
-    }
-    const double n_factor = 1.0 / (moving_bin_size * out.valid);
-    const double inv_sum = 1.0 / joint_sum;
-    for (int i = threadIdx.x; i < B2; i += blockDim.x) jp[i] *= inv_sum;
-    for (int i = threadIdx.x; i < B; i += blockDim.x) {
-        const double f = fm[i] * inv_sum;
-        fm[i] = f;
-        lfm[i] = f > DBL_EPSILON ? log(f) : 0.0;
-    }
-    __syncthreads();
-    for (int m = threadIdx.x; m < B; m += blockDim.x) {
-        double acc = 0.0;
-        for (int f = 0; f < B; ++f) acc += jp[f * B + m];
-        mm[m] = acc;
-    }
-    __syncthreads();
-    double sum = 0.0;
-    for (int i = threadIdx.x; i < B2; i += blockDim.x) {
-        const int f = i / B, m = i - f * B;
-        const double p = jp[i], mmv = mm[m];
-        double r = 0.0;
-        if (fm[f] > DBL_EPSILON && mmv > DBL_EPSILON && p > DBL_EPSILON) {
-            const double lr = log(p / mmv);
-            sum += p * (lr - lfm[f]);
-            r = lr * n_factor;
-        }
-        if (pr) pr[i] = (float)r;
-    }
-    out.value = -block_sum(sum, red);
-    return out;
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
 }
 
-// Value-only tail: one CTA, then the global histogram is re-zeroed.
-__global__ void __launch_bounds__(256)
-k_value(int B, double moving_bin_size, double hist_inv, unsigned long long* __restrict__ ghist,
-        double* __restrict__ result) {
-    extern __shared__ double tsh[];
-    const TailOut t = run_tail(B, moving_bin_size, hist_inv, ghist, tsh, nullptr);
-    if (threadIdx.x == 0) {
-        result[0] = t.value;
-        result[1] = t.valid;
-    }
-    for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) ghist[i] = 0ull;
+// Device buffers and per-launch constants shared by the evaluation kernels.
+//   sync[0] done counter of the final phase, sync[2] grid-barrier counter of the
+//   fused kernel.
+//   result: value, valid, derivative[MI_MAX_PARAMS], then the error word.
+struct EvalArgs {
+    const float* moving;
+    const uint8_t* mmask;
+    const uint32_t* samples;
+    const uint8_t* fbin;
+    uint32_t n, npad;
+    float hist_scale, fine_scale;
+    int fine_shift, copies, fine_copies;
+    double hist_inv;
+    unsigned long long* ghist;
+    uint16_t* rec_bins;  // per sample: moving bin | fixed bin << 8 (0 = not valid)
+    float* rec_f;
+    float* rec_g;
+    double* partials;
+    double* vsum;  // value slice sums (value_slices(B))
+    unsigned int* sync;
+    double* result;
+};
+constexpr int RESULT_ERR = 2 + MI_MAX_PARAMS;  // result slot holding the error word
+constexpr int RESULT_DOUBLES = RESULT_ERR + 2;
+__device__ __forceinline__ unsigned int* error_word(const EvalArgs& a) {
+    return reinterpret_cast<unsigned int*>(a.result + RESULT_ERR);
 }
 
 // ---------------------------------------------------------------------------
@@ -227,15 +183,10 @@ constexpr int FINE_T = MI_HIST_FINE_T;
 constexpr float FINE_LIMIT = 1.0f / (float)(1u << FINE_T);
 
 template <bool RECORD>
-__global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
-k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restrict__ mmask,
-       const uint32_t* __restrict__ samples, const uint8_t* __restrict__ fbin, uint32_t n, uint32_t npad,
-       float hist_scale, float fine_scale, int fine_shift, int copies, int fine_copies,
-       unsigned long long* __restrict__ ghist, uint8_t* __restrict__ rec_mi, float* __restrict__ rec_f,
-       float* __restrict__ rec_g) {
-    extern __shared__ unsigned int sh[];
+__device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArgs& a, unsigned int* sh) {
     const int B = P.bins;
     const int nb = B * B + B;
+    const int copies = a.copies, fine_copies = a.fine_copies;
     const int cstride = hist_copy_stride(B);
     const int fstride = hist_fine_stride(B);
     unsigned int* sh_fine = sh + copies * cstride;
@@ -244,6 +195,12 @@ k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restr
     unsigned int* sh_joint = sh;
     unsigned int* sh_fixed = sh + B * B;
     const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t n = a.n, npad = a.npad;
+    const float* __restrict__ moving = a.moving;
+    const uint8_t* __restrict__ mmask = a.mmask;
+    const uint32_t* __restrict__ samples = a.samples;
+    const uint8_t* __restrict__ fbin = a.fbin;
+    const float hist_scale = a.hist_scale, fine_scale = a.fine_scale;
     // Two samples per iteration: both samples' corner gathers are issued (prep) before
     // either is finished, so each thread keeps two gathers in flight.
     // The CTA keeps `copies` interleaved copies of the histogram and lane l adds into
@@ -260,7 +217,7 @@ k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restr
         o.exact = false;
         const int st = finish<RECORD>(P, p, moving, o);
         if (st != SAMPLE_VALID) {
-            if (RECORD) rec_mi[s] = 0;
+            if (RECORD) a.rec_bins[s] = 0;
             return;
         }
         const int fi = __ldg(fbin + s);
@@ -281,11 +238,11 @@ k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restr
         }
         atomicAdd(my_fixed + fi, 1u);
         if (RECORD) {
-            rec_mi[s] = (uint8_t)o.mi;
-            rec_f[s] = o.f;
-            rec_g[s] = o.g[0];
-            rec_g[(size_t)npad + s] = o.g[1];
-            rec_g[2 * (size_t)npad + s] = o.g[2];
+            a.rec_bins[s] = (uint16_t)(o.mi | (fi << 8));
+            a.rec_f[s] = o.f;
+            a.rec_g[s] = o.g[0];
+            a.rec_g[(size_t)npad + s] = o.g[1];
+            a.rec_g[2 * (size_t)npad + s] = o.g[2];
         }
     };
     // whole warps iterate together: the loop bound is the warp's first sample
@@ -318,9 +275,174 @@ k_hist(SamplerParams P, const float* __restrict__ moving, const uint8_t* __restr
         if (i < B * B) {
             unsigned long long f = 0ull;
             for (int c = 0; c < fine_copies; ++c) f += sh_fine[c * fstride + i];
-            v = (v << fine_shift) + f;
+            v = (v << a.fine_shift) + f;
         }
-        if (v) atomicAdd(&ghist[i], v);
+        if (v) atomicAdd(&a.ghist[i], v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The tail (registration/mattes.rs:273-328) over the finished global histogram. The
+// marginals are sums of the integer histogram, so every CTA forms them exactly (any
+// order, same bits):
+//   total = Σ joint, col[m] = Σ_f joint[f][m], valid = Σ_f count[f].
+// With p = joint/total the reference's quantities are
+//   joint_sum = total·2^-kf, jp = joint/total, mm = col/total, fm = count/joint_sum,
+//   pRatio = ln(jp/mm) = ln(joint/col), −MI = −Σ jp·(pRatio − ln fm),
+// the ratio inside the logarithm formed from the exact integers; nFactor =
+// 1/(moving bin size·valid); degenerate (value DBL_MAX, zero derivative) when there
+// is no valid sample or Σ joint < ε (mattes.rs:590-609).
+// ---------------------------------------------------------------------------
+// The tail's shared-memory state, carved from `base` (tail_smem(B) bytes): a copy of
+// the global histogram (B² joint + B counts, u64), per-group column partials, the
+// column sums and fixed counts, and the column/row flags mm > ε, fm > ε.
+struct TailSmem {
+    unsigned long long* hist;  // B*B + B
+    unsigned long long* part;  // tail_groups(B) * B
+    unsigned long long* col;   // B
+    uint8_t* okm;              // B
+    uint8_t* okf;              // B
+};
+__device__ __forceinline__ TailSmem tail_layout(int B, unsigned char* base) {
+    TailSmem t;
+    t.hist = reinterpret_cast<unsigned long long*>(base);
+    t.part = t.hist + B * B + B;
+    t.col = t.part + tail_groups(B) * B;
+    t.okm = reinterpret_cast<uint8_t*>(t.col + B);
+    t.okf = t.okm + B;
+    return t;
+}
+
+// Per-CTA tail state: the integer marginals, the normalisers and the degenerate flag.
+struct TailCtx {
+    unsigned long long total, valid;
+    double dt;         // total, as a double
+    double joint_sum;  // total·2^-kf
+    double n_factor;   // 1/(moving bin size·valid)
+    bool degenerate;
+};
+
+// Every CTA copies the histogram into shared memory with coalesced loads and forms
+// the marginals from the copy: column m's sum in tail_groups(B) row groups, then over
+// the groups; counts are read in place. Integer sums, so any order gives the same
+// bits.
+__device__ TailCtx tail_prepare(int B, double moving_bin_size, const EvalArgs& a, const TailSmem& ts) {
+    const int B2 = B * B, nb = B2 + B;
+    const unsigned long long* __restrict__ gh = a.ghist;
+    for (int i0 = threadIdx.x; i0 < nb; i0 += 4 * blockDim.x) {
+        unsigned long long v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * blockDim.x;
+            v[u] = i < nb ? __ldcg(gh + i) : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * blockDim.x;
+            if (i < nb) ts.hist[i] = v[u];
+        }
+    }
+    __syncthreads();
+    const int G = tail_groups(B);
+    if ((int)threadIdx.x < G * B) {
+        const int m = threadIdx.x % B, g = threadIdx.x / B;
+        unsigned long long v = 0ull;
+        for (int f = g; f < B; f += G) v += ts.hist[f * B + m];
+        ts.part[g * B + m] = v;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < B) {
+        unsigned long long v = 0ull;
+        for (int g = 0; g < G; ++g) v += ts.part[g * B + threadIdx.x];
+        ts.col[threadIdx.x] = v;
+    }
+    __syncthreads();
+    const unsigned long long* cnt = ts.hist + B2;
+    const int lane = threadIdx.x & 31;
+    TailCtx t;
+    t.total = 0ull;
+    t.valid = 0ull;
+    for (int m = lane; m < B; m += 32) {
+        t.total += ts.col[m];
+        t.valid += cnt[m];
+    }
+    t.total = warp_sum_u64(t.total);
+    t.valid = warp_sum_u64(t.valid);
+    t.dt = (double)t.total;
+    t.joint_sum = t.dt * a.hist_inv;
+    t.degenerate = t.valid == 0ull || t.joint_sum < DBL_EPSILON;
+    t.n_factor = t.degenerate ? 0.0 : 1.0 / (moving_bin_size * (double)t.valid);
+    if ((int)threadIdx.x < B) {
+        ts.okm[threadIdx.x] = (double)ts.col[threadIdx.x] / t.dt > DBL_EPSILON;
+        ts.okf[threadIdx.x] = (double)cnt[threadIdx.x] / t.joint_sum > DBL_EPSILON;
+    }
+    __syncthreads();
+    return t;
+}
+
+// pRatio·nFactor of every bin into pr (shared memory, FP32): 0 where the reference
+// skips the bin, else ln(joint/col)·nFactor with the ratio formed in FP64 and the
+// logarithm taken in FP32 (the table is FP32).
+__device__ void pr_table(int B, const TailCtx& t, const TailSmem& ts, float* pr) {
+    const int B2 = B * B;
+    const float nf = (float)t.n_factor;
+    for (int i = threadIdx.x; i < B2; i += blockDim.x) {
+        const int f = i / B, m = i - f * B;
+        const unsigned long long jv = ts.hist[i];
+        float r = 0.0f;
+        if (ts.okf[f] && ts.okm[m] && jv && (double)jv / t.dt > DBL_EPSILON)
+            r = logf((float)((double)jv / (double)ts.col[m])) * nf;
+        pr[i] = r;
+    }
+}
+
+// −MI is summed in value slices of 32 bins, one warp each (lane l takes bin
+// 32·s + l, then a fixed xor tree), and the slice sums are folded in slice order
+// (fold_value). Whichever warp of whichever kernel computes a slice, it gets the
+// same bits, so every launch form reports the same value.
+__host__ __device__ inline int value_slices(int B) { return (B * B + 31) / 32; }
+
+__device__ double value_slice(int B, const TailCtx& t, const TailSmem& ts, int slice) {
+    const int lane = threadIdx.x & 31;
+    const int i = slice * 32 + lane;
+    double term = 0.0;
+    if (i < B * B) {
+        const unsigned long long jv = ts.hist[i];
+        const int f = i / B, m = i - f * B;
+        const double jp = (double)jv / t.dt;
+        const double mm = (double)ts.col[m] / t.dt;
+        const double fm = (double)ts.hist[B * B + f] / t.joint_sum;
+        if (fm > DBL_EPSILON && mm > DBL_EPSILON && jp > DBL_EPSILON)
+            term = jp * (log((double)jv / (double)ts.col[m]) - log(fm));
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);
+    return term;
+}
+
+// This CTA's share of the value slices (global warp w takes slices w, w + W, …),
+// their sums stored in a.vsum.
+__device__ void value_slices_share(int B, const EvalArgs& a, const TailCtx& t, const TailSmem& ts) {
+    const int lane = threadIdx.x & 31;
+    const int nw = blockDim.x >> 5;
+    const int ns = value_slices(B);
+    for (int s = blockIdx.x * nw + (threadIdx.x >> 5); s < ns; s += gridDim.x * nw) {
+        const double v = value_slice(B, t, ts, s);
+        if (lane == 0) a.vsum[s] = v;
+    }
+}
+
+// One warp: value and valid into result (lane 0), from the slice sums.
+__device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
+    const int lane = threadIdx.x & 31;
+    const int ns = value_slices(B);
+    double v = 0.0;
+    for (int s = lane; s < ns; s += 32) v += __ldcg(a.vsum + s);
+#pragma unroll
+    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0) {
+        a.result[0] = t.degenerate ? DBL_MAX : -v;
+        a.result[1] = (double)t.valid;
     }
 }
 
@@ -353,50 +475,68 @@ __device__ __forceinline__ void accumulate_moments(const SamplerParams& P, const
     }
 }
 
-// Records are read four samples per thread with 4-, 16- and 16-byte vector loads
-// (every record array is padded to a multiple of four samples; padding records carry
-// moving bin 0 and are skipped).
-__global__ void __launch_bounds__(DERIV_BLOCK)
-k_deriv(SamplerParams P, JacobianForm J, const uint32_t* __restrict__ samples, const uint8_t* __restrict__ fbin,
-        uint32_t npad, const uint8_t* __restrict__ rec_mi, const float* __restrict__ rec_f,
-        const float* __restrict__ rec_g, double hist_inv, unsigned long long* __restrict__ ghist,
-        double* __restrict__ partials, unsigned int* __restrict__ done_counter, double* __restrict__ result) {
-    extern __shared__ double dsh[];
+// The moments of this CTA's share of the samples, stored into partials[slot][CTA].
+// The CTA first forms the tail itself (tail_prepare, pr_table) and its share of the
+// value slices; the first group of records is requested before that so its loads
+// overlap the tail. Records are read four samples
+// per thread with 8- and 16-byte vector loads (every record array is padded to a
+// multiple of four samples; padding records carry bins 0 and are skipped). Returns
+// the tail state.
+__device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double* dsh) {
     const int B = P.bins;
-    double* red = dsh;                                          // 32 * NMOM
-    double* tsh = dsh + 32 * NMOM;                              // tail scratch
-    float* pr = reinterpret_cast<float*>(tsh + tail_doubles(B));  // B*B
-    __shared__ bool is_last;
-    __shared__ double mom[NMOM];
-    // Every CTA forms the tail itself (same histogram, same bits): no CTA waits for
-    // a single one to finish it.
-    const TailOut tail = run_tail(B, P.moving_bin_size, hist_inv, ghist, tsh, pr);
-    const bool degenerate = tail.degenerate;
+    double* red = dsh;  // 32 * NMOM
+    unsigned char* tbase = reinterpret_cast<unsigned char*>(dsh + 32 * NMOM);
+    const TailSmem ts = tail_layout(B, tbase);
+    float* pr = reinterpret_cast<float*>(tbase + tail_smem(B));  // B*B
     float acc[NMOM];
 #pragma unroll
     for (int i = 0; i < NMOM; ++i) acc[i] = 0.0f;
-    if (!degenerate) {
-        __syncthreads();
-        const uint32_t stride = gridDim.x * blockDim.x;
-        const uint32_t ngroups = npad >> 2;
-        const uchar4* mi4p = reinterpret_cast<const uchar4*>(rec_mi);
-        const uchar4* fb4p = reinterpret_cast<const uchar4*>(fbin);
-        const float4* f4p = reinterpret_cast<const float4*>(rec_f);
-        const float4* gx4p = reinterpret_cast<const float4*>(rec_g);
-        const float4* gy4p = reinterpret_cast<const float4*>(rec_g + npad);
-        const float4* gz4p = reinterpret_cast<const float4*>(rec_g + 2 * (size_t)npad);
-        const uint4* s4p = reinterpret_cast<const uint4*>(samples);
-        for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < ngroups; q += stride) {
-            const uchar4 mi4 = __ldg(mi4p + q);
-            if (!(mi4.x | mi4.y | mi4.z | mi4.w)) continue;
-            const float4 f4 = __ldg(f4p + q);
-            const float4 gx = __ldg(gx4p + q), gy = __ldg(gy4p + q), gz = __ldg(gz4p + q);
-            const uchar4 fb4 = __ldg(fb4p + q);
-            const uint4 fl4 = samples ? __ldg(s4p + q) : make_uint4(4 * q, 4 * q + 1, 4 * q + 2, 4 * q + 3);
-            if (mi4.x) accumulate_moments(P, pr, B, mi4.x, fb4.x, f4.x, gx.x, gy.x, gz.x, fl4.x, acc);
-            if (mi4.y) accumulate_moments(P, pr, B, mi4.y, fb4.y, f4.y, gx.y, gy.y, gz.y, fl4.y, acc);
-            if (mi4.z) accumulate_moments(P, pr, B, mi4.z, fb4.z, f4.z, gx.z, gy.z, gz.z, fl4.z, acc);
-            if (mi4.w) accumulate_moments(P, pr, B, mi4.w, fb4.w, f4.w, gx.w, gy.w, gz.w, fl4.w, acc);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t npad = a.npad;
+    const uint32_t ngroups = npad >> 2;
+    const uint2* b4p = reinterpret_cast<const uint2*>(a.rec_bins);
+    const float4* f4p = reinterpret_cast<const float4*>(a.rec_f);
+    const float4* gx4p = reinterpret_cast<const float4*>(a.rec_g);
+    const float4* gy4p = reinterpret_cast<const float4*>(a.rec_g + npad);
+    const float4* gz4p = reinterpret_cast<const float4*>(a.rec_g + 2 * (size_t)npad);
+    const uint4* s4p = reinterpret_cast<const uint4*>(a.samples);
+    // the next group's records are loaded before the current group is accumulated
+    struct Group {
+        uint2 b;
+        float4 f, gx, gy, gz;
+        uint4 fl;
+    };
+    auto load = [&](uint32_t q, Group& g) {
+        g.b = __ldcg(b4p + q);
+        g.f = __ldcg(f4p + q);
+        g.gx = __ldcg(gx4p + q);
+        g.gy = __ldcg(gy4p + q);
+        g.gz = __ldcg(gz4p + q);
+        g.fl = a.samples ? __ldg(s4p + q) : make_uint4(4 * q, 4 * q + 1, 4 * q + 2, 4 * q + 3);
+    };
+    auto one = [&](uint32_t bins, float f, float gx, float gy, float gz, uint32_t flat) {
+        if (bins & 0xffu) accumulate_moments(P, pr, B, bins & 0xffu, bins >> 8, f, gx, gy, gz, flat, acc);
+    };
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    Group cur;
+    if (q < ngroups) load(q, cur);
+    const TailCtx t = tail_prepare(B, P.moving_bin_size, a, ts);
+    if (!t.degenerate) {
+        pr_table(B, t, ts, pr);
+        value_slices_share(B, a, t, ts);
+    }
+    __syncthreads();
+    if (!t.degenerate) {
+        while (q < ngroups) {
+            const uint32_t qn = q + stride;
+            Group nxt;
+            if (qn < ngroups) load(qn, nxt);
+            one(cur.b.x & 0xffffu, cur.f.x, cur.gx.x, cur.gy.x, cur.gz.x, cur.fl.x);
+            one(cur.b.x >> 16, cur.f.y, cur.gx.y, cur.gy.y, cur.gz.y, cur.fl.y);
+            one(cur.b.y & 0xffffu, cur.f.z, cur.gx.z, cur.gy.z, cur.gz.z, cur.fl.z);
+            one(cur.b.y >> 16, cur.f.w, cur.gx.w, cur.gy.w, cur.gz.w, cur.fl.w);
+            cur = nxt;
+            q = qn;
         }
     }
     // CTA reduction in a fixed order: shuffles within a warp, then over warps.
@@ -416,34 +556,31 @@ k_deriv(SamplerParams P, JacobianForm J, const uint32_t* __restrict__ samples, c
     if (threadIdx.x < NMOM) {
         double v = 0.0;
         for (int w = 0; w < nw; ++w) v += red[w * NMOM + threadIdx.x];
-        partials[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
+        a.partials[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
     }
-    // The last CTA to arrive folds every CTA's partials (no CTA waits on another),
-    // and — every CTA having read the histogram in its prologue — re-zeroes it for
-    // the next evaluation.
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) is_last = atomicAdd(done_counter, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!is_last) return;
-    __threadfence();
-    for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) ghist[i] = 0ull;
-    // fold in a fixed order: lane l of a slot sums CTAs l, l+21, … four loads at a
-    // time; the 21 lane sums of a slot are then added in lane order
+    return t;
+}
+
+// Run by the last CTA to finish the derivative phase: fold every CTA's partials in
+// a fixed order (lane l of a slot sums CTAs l, l+21, … eight loads at a time; the 21
+// lane sums of a slot are then added in lane order) and contract with the Jacobian
+// form: ∂/∂p_k = Σ_d J(x_ref)[d][k]·A_d + Σ_{d,e} C_e[d][k]·B[d][e],
+// J(x_ref) = J(0) + Σ_e x_ref,e·C_e.
+__device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const EvalArgs& a, bool degenerate) {
     constexpr int FOLD = 21;
     __shared__ double fold[FOLD * NMOM];
+    __shared__ double mom[NMOM];
     if (threadIdx.x < FOLD * NMOM) {
         const int slot = threadIdx.x / FOLD, ln = threadIdx.x % FOLD;
-        const double* src = partials + (int64_t)slot * gridDim.x;
+        const double* src = a.partials + (int64_t)slot * gridDim.x;
         double v = 0.0;
         unsigned int b = ln;
-        for (; b + 3 * FOLD < gridDim.x; b += 4 * FOLD) {
-            const double a0 = __ldcg(src + b), a1 = __ldcg(src + b + FOLD);
-            const double a2 = __ldcg(src + b + 2 * FOLD), a3 = __ldcg(src + b + 3 * FOLD);
-            v += a0;
-            v += a1;
-            v += a2;
-            v += a3;
+        for (; b + 7 * FOLD < gridDim.x; b += 8 * FOLD) {
+            double t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t[u] = __ldcg(src + b + u * FOLD);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v += t[u];
         }
         for (; b < gridDim.x; b += FOLD) v += __ldcg(src + b);
         fold[slot * FOLD + ln] = v;
@@ -455,8 +592,6 @@ k_deriv(SamplerParams P, JacobianForm J, const uint32_t* __restrict__ samples, c
         mom[threadIdx.x] = v;
     }
     __syncthreads();
-    if (threadIdx.x == 0) *done_counter = 0u;
-    // ∂/∂p_k = Σ_d J(x_ref)[d][k]·A_d + Σ_{d,e} C_e[d][k]·B[d][e],  J(x_ref) = J(0) + Σ_e x_ref,e·C_e
     const int np = J.nparams;
     if (threadIdx.x < np) {
         const int k = threadIdx.x;
@@ -469,12 +604,124 @@ k_deriv(SamplerParams P, JacobianForm J, const uint32_t* __restrict__ samples, c
                 for (int e = 0; e < 3; ++e) dk += J.jacc[e][d * np + k] * mom[3 + d * 3 + e];
             }
         }
-        result[2 + k] = dk;
+        a.result[2 + k] = dk;
     }
+}
+
+// Arrival at the end of a kernel: returns true in the last CTA to arrive (after
+// which every other CTA's global writes are visible to it).
+__device__ __forceinline__ bool last_to_arrive(unsigned int* counter) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+__device__ __forceinline__ unsigned int load_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of the fused kernel (a cooperative launch, so every CTA is
+// resident). Arrivals count up across the kernel: barrier k waits for k·gridDim.x.
+// The wait is bounded: after BARRIER_SPINS polls the CTA raises the error word and
+// every CTA that sees it leaves, so a launch that lost a CTA ends instead of hanging.
+constexpr unsigned int BARRIER_SPINS = 1u << 22;
+__device__ __forceinline__ bool grid_barrier(const EvalArgs& a, unsigned int k) {
+    __shared__ int ok;
+    __threadfence();
+    __syncthreads();
     if (threadIdx.x == 0) {
-        result[0] = tail.value;
-        result[1] = tail.valid;
+        unsigned int* count = a.sync + 2;
+        unsigned int* err = error_word(a);
+        const unsigned int target = k * gridDim.x;
+        atomicAdd(count, 1u);
+        int good = 1;
+        unsigned int spins = 0;
+        while (load_acquire(count) < target) {
+            if (load_acquire(err) != 0u || ++spins > BARRIER_SPINS) {
+                good = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+        if (!good) atomicOr(err, 1u);
+        ok = good;
     }
+    __syncthreads();
+    return ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels. The fused evaluation is one cooperative launch:
+//   histogram → grid barrier → every CTA forms the tail (CTA 0 writes value and
+//   valid) and its share of the derivative moments → the last CTA to finish folds
+//   the moments, writes the derivative, re-zeroes the global histogram and resets
+//   the counters. The value-only form runs the tail in CTA 0 alone.
+// The split form (k_hist, then k_deriv or k_tail) does the same work with a kernel
+// boundary in place of the barrier.
+// ---------------------------------------------------------------------------
+template <bool DERIV>
+__global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
+k_eval(SamplerParams P, JacobianForm J, EvalArgs a) {
+    extern __shared__ __align__(16) unsigned char esh[];
+    unsigned int* sh = reinterpret_cast<unsigned int*>(esh);
+    double* dsh = reinterpret_cast<double*>(esh);
+    const int B = P.bins;
+    hist_phase<DERIV>(P, a, sh);
+    if (!grid_barrier(a, 1)) return;
+    TailCtx t;
+    if (DERIV) {
+        t = deriv_phase(P, a, dsh);
+    } else {
+        const TailSmem ts = tail_layout(B, esh);
+        t = tail_prepare(B, P.moving_bin_size, a, ts);
+        if (!t.degenerate) value_slices_share(B, a, t, ts);
+    }
+    if (!last_to_arrive(a.sync)) return;
+    // every CTA has left the barrier and is done with the histogram
+    if (DERIV) deriv_fold(P, J, a, t.degenerate);
+    if (threadIdx.x < 32) fold_value(B, a, t);
+    if (threadIdx.x == 0) {
+        a.sync[0] = 0u;
+        a.sync[2] = 0u;
+    }
+    for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) a.ghist[i] = 0ull;
+}
+
+template <bool RECORD>
+__global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
+k_hist(SamplerParams P, EvalArgs a) {
+    extern __shared__ unsigned int sh[];
+    hist_phase<RECORD>(P, a, sh);
+}
+
+// Value-only tail of the split form: one CTA.
+__global__ void __launch_bounds__(TAIL_BLOCK)
+k_tail(int B, double moving_bin_size, EvalArgs a) {
+    extern __shared__ __align__(16) unsigned char tsh[];
+    const TailSmem ts = tail_layout(B, tsh);
+    const TailCtx t = tail_prepare(B, moving_bin_size, a, ts);
+    if (!t.degenerate) value_slices_share(B, a, t, ts);
+    __syncthreads();
+    if (threadIdx.x < 32) fold_value(B, a, t);
+    for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) a.ghist[i] = 0ull;
+}
+
+// Tail and derivative pass of the split form.
+__global__ void __launch_bounds__(DERIV_BLOCK)
+k_deriv(SamplerParams P, JacobianForm J, EvalArgs a) {
+    extern __shared__ double dsh[];
+    const TailCtx t = deriv_phase(P, a, dsh);
+    if (!last_to_arrive(a.sync)) return;
+    deriv_fold(P, J, a, t.degenerate);
+    if (threadIdx.x < 32) fold_value(P.bins, a, t);
+    if (threadIdx.x == 0) a.sync[0] = 0u;
+    for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
 }
 
 // Per-sample decisions of the same sampler the kernels use, for the exactness tests.
@@ -616,12 +863,11 @@ void free_metric(mi_metric* m) {
     cudaFree(m->samples);
     cudaFree(m->fbin);
     cudaFree(m->ws.hist);
-    cudaFree(m->ws.pratio);
-    cudaFree(m->ws.tail);
     cudaFree(m->ws.partials);
+    cudaFree(m->ws.vsum);
     cudaFree(m->ws.result);
     cudaFree(m->ws.done_counter);
-    cudaFree(m->ws.rec_mi);
+    cudaFree(m->ws.rec_bins);
     cudaFree(m->ws.rec_f);
     cudaFree(m->ws.rec_g);
     if (m->ws.host_result) cudaFreeHost(m->ws.host_result);
@@ -832,54 +1078,98 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     const int B = m->bins;
     cudaStream_t st = ctx->stream;
     Workspace& ws = m->ws;
-    const bool timing = ws.timing;
-    if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[0], st));
+    const bool timing = ws.timing != 0;
+    const bool per_kernel = ws.timing == 2;
     const uint32_t n = (uint32_t)m->n_samples;
-    const uint32_t npad = (n + 3u) & ~3u;
-    const double hist_inv = std::ldexp(1.0, -ws.fine_scale_log2);
-    const float fine_scale = (float)std::ldexp(1.0, ws.fine_scale_log2);
-    const int fine_shift = ws.fine_scale_log2 - ws.hist_scale_log2;
-    if (want_derivative)
-        k_hist<true><<<ws.grid_hist, ws.block_hist, hist_smem(B), st>>>(
-            P, m->moving, m->mmask, m->samples, m->fbin, n, npad, ws.hist_scale, fine_scale, fine_shift,
-            hist_copies(B), hist_fine_copies(B), ws.hist, ws.rec_mi, ws.rec_f, ws.rec_g);
-    else
-        k_hist<false><<<ws.grid_hist, ws.block_hist, hist_smem(B), st>>>(
-            P, m->moving, m->mmask, m->samples, m->fbin, n, npad, ws.hist_scale, fine_scale, fine_shift,
-            hist_copies(B), hist_fine_copies(B), ws.hist, nullptr, nullptr, nullptr);
-    if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
-    int nout = 2;
-    if (want_derivative) {
-        if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[2], st));
-        JacobianForm J;
-        J.nparams = nparams;
-        for (int i = 0; i < 3 * nparams; ++i) {
-            J.jac0[i] = jac0[i];
-            for (int e = 0; e < 3; ++e) J.jacc[e][i] = jacc[e * 3 * nparams + i];
-        }
-        k_deriv<<<ws.grid_deriv, ws.block_deriv, deriv_smem(B), st>>>(P, J, m->samples, m->fbin, npad, ws.rec_mi,
-                                                                      ws.rec_f, ws.rec_g, hist_inv, ws.hist,
-                                                                      ws.partials, ws.done_counter, ws.result);
-        nout = 2 + nparams;
-    } else {
-        k_value<<<1, 256, tail_doubles(B) * sizeof(double), st>>>(B, P.moving_bin_size, hist_inv, ws.hist, ws.result);
-        if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[2], st));
+    EvalArgs a;
+    a.moving = m->moving;
+    a.mmask = m->mmask;
+    a.samples = m->samples;
+    a.fbin = m->fbin;
+    a.n = n;
+    a.npad = (n + 3u) & ~3u;
+    a.hist_scale = ws.hist_scale;
+    a.fine_scale = (float)std::ldexp(1.0, ws.fine_scale_log2);
+    a.fine_shift = ws.fine_scale_log2 - ws.hist_scale_log2;
+    a.copies = hist_copies(B);
+    a.fine_copies = hist_fine_copies(B);
+    a.hist_inv = std::ldexp(1.0, -ws.fine_scale_log2);
+    a.ghist = ws.hist;
+    a.rec_bins = want_derivative ? ws.rec_bins : nullptr;
+    a.rec_f = want_derivative ? ws.rec_f : nullptr;
+    a.rec_g = want_derivative ? ws.rec_g : nullptr;
+    a.partials = ws.partials;
+    a.vsum = ws.vsum;
+    a.sync = ws.done_counter;
+    a.result = ws.result;
+    JacobianForm J;
+    J.nparams = want_derivative ? nparams : 0;
+    for (int i = 0; i < 3 * J.nparams; ++i) {
+        J.jac0[i] = jac0[i];
+        for (int e = 0; e < 3; ++e) J.jacc[e][i] = jacc[e * 3 * nparams + i];
     }
-    if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[3], st));
+    if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[0], st));
+    if (ws.fused) {
+        // one cooperative launch: every CTA resident, so the in-kernel barriers hold
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)ws.grid_eval);
+        cfg.blockDim = dim3(HIST_BLOCK);
+        cfg.dynamicSmemBytes = eval_smem(B);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (want_derivative)
+            MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_eval<true>, P, J, a));
+        else
+            MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_eval<false>, P, J, a));
+        if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
+    } else {
+        if (want_derivative)
+            k_hist<true><<<ws.grid_hist, HIST_BLOCK, hist_smem(B), st>>>(P, a);
+        else
+            k_hist<false><<<ws.grid_hist, HIST_BLOCK, hist_smem(B), st>>>(P, a);
+        if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
+        if (want_derivative)
+            k_deriv<<<ws.grid_deriv, DERIV_BLOCK, deriv_smem(B), st>>>(P, J, a);
+        else
+            k_tail<<<1, TAIL_BLOCK, tail_smem(B), st>>>(B, P.moving_bin_size, a);
+        if (per_kernel) {
+            MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[2], st));
+            MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[3], st));
+        }
+    }
     MI_CHECK_CUDA(ctx, cudaGetLastError());
-    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(ws.host_result, ws.result, (size_t)nout * 8, cudaMemcpyDeviceToHost, st));
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(ws.host_result, ws.result, RESULT_DOUBLES * sizeof(double),
+                                       cudaMemcpyDeviceToHost, st));
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[4], st));
     MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+    unsigned int err = 0;
+    std::memcpy(&err, ws.host_result + RESULT_ERR, sizeof(err));
+    if (err) {
+        // a barrier gave up: clear the counters, the error word and the histogram
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.result, 0, RESULT_DOUBLES * sizeof(double), st));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + B) * 8, st));
+        MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+        return set_error(ctx, MI_ERR_TIMEOUT, "a grid barrier of the fused evaluation timed out");
+    }
     if (timing) {
         float t = 0.f;
         MI_CHECK_CUDA(ctx, cudaEventElapsedTime(&t, ws.ev[0], ws.ev[4]));
         ws.ms[0] += t;
-        MI_CHECK_CUDA(ctx, cudaEventElapsedTime(&t, ws.ev[0], ws.ev[1]));
-        ws.ms[1] += t;
-        MI_CHECK_CUDA(ctx, cudaEventElapsedTime(&t, ws.ev[1], ws.ev[2]));
-        ws.ms[2] += t;
-        MI_CHECK_CUDA(ctx, cudaEventElapsedTime(&t, ws.ev[2], ws.ev[3]));
-        ws.ms[3] += t;
+        if (per_kernel) {
+            MI_CHECK_CUDA(ctx, cudaEventElapsedTime(&t, ws.ev[0], ws.ev[1]));
+            ws.ms[1] += t;
+            if (!ws.fused) {
+                MI_CHECK_CUDA(ctx, cudaEventElapsedTime(&t, ws.ev[1], ws.ev[2]));
+                ws.ms[2] += t;
+                MI_CHECK_CUDA(ctx, cudaEventElapsedTime(&t, ws.ev[2], ws.ev[3]));
+                ws.ms[3] += t;
+            }
+        }
         ws.timed_evals += 1;
     }
     if (value) *value = ws.host_result[0];
@@ -1050,15 +1340,27 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     TRY_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_smem(B)));
     TRY_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_smem(B)));
     TRY_CUDA(cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)deriv_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_value, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(tail_doubles(B) * sizeof(double))));
-    int occ_h = 0, occ_d = 0;
+    TRY_CUDA(cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tail_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_eval<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_eval<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
+    int occ_h = 0, occ_d = 0, occ_e1 = 0, occ_e0 = 0, coop = 0;
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK, hist_smem(B)));
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_deriv, DERIV_BLOCK, deriv_smem(B)));
-    ws.block_hist = HIST_BLOCK;
-    ws.block_deriv = DERIV_BLOCK;
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e1, k_eval<true>, HIST_BLOCK, eval_smem(B)));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e0, k_eval<false>, HIST_BLOCK, eval_smem(B)));
+    TRY_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+    // The fused form needs every CTA resident (a cooperative launch).
+    const int resident = ctx->num_sms * std::min(occ_e1, occ_e0);
+    // The split form is the default: the fused kernel's device time is the same, and
+    // a cooperative launch waits for the stream to drain, which adds its latency to
+    // every synchronous evaluation.
+    ws.can_fuse = coop != 0 && resident >= 1;
+    ws.fused = false;
+    ws.grid_eval = ws.can_fuse ? grid_for(m->n_samples, HIST_BLOCK, resident) : 0;
     ws.grid_hist = grid_for(m->n_samples, HIST_BLOCK, ctx->num_sms * std::max(occ_h, 1));
     ws.grid_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
+    ws.block_hist = HIST_BLOCK;
+    ws.block_deriv = DERIV_BLOCK;
     // Fixed-point scales of the histogram taps. A thread takes at most per_thread
     // samples, and a copy of the CTA histogram is fed by HIST_BLOCK/copies threads, so
     // it sees at most copy_max samples; each adds at most one tap to a bin (coarse
@@ -1066,8 +1368,9 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     // rounded tap below 2^22 (the magic-add rounding): k ≤ 22, kf ≤ FINE_T + 22. The global
     // u64 bin, in units of 2^-kf, takes at most n_samples·(2/3)·2^kf.
     {
-        const int64_t per_thread = (m->n_samples + (int64_t)ws.grid_hist * HIST_BLOCK - 1) /
-                                   ((int64_t)ws.grid_hist * HIST_BLOCK);
+        // both forms' histogram grids (the form can be switched after creation)
+        const int64_t hgrid = ws.can_fuse ? std::min(ws.grid_hist, ws.grid_eval) : ws.grid_hist;
+        const int64_t per_thread = (m->n_samples + hgrid * HIST_BLOCK - 1) / (hgrid * HIST_BLOCK);
         const double lim = 4294967295.0 * 0.98;
         const double coarse_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_copies(B)), 1);
         const double fine_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_fine_copies(B)), 1);
@@ -1084,22 +1387,28 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     {
         // padded to whole groups of four samples; padding records keep moving bin 0
         const size_t ns = pad4(m->n_samples);
-        TRY_CUDA(cudaMalloc(&ws.rec_mi, ns));
-        TRY_CUDA(cudaMemsetAsync(ws.rec_mi, 0, ns, st));
+        TRY_CUDA(cudaMalloc(&ws.rec_bins, ns * sizeof(uint16_t)));
+        TRY_CUDA(cudaMemsetAsync(ws.rec_bins, 0, ns * sizeof(uint16_t), st));
         TRY_CUDA(cudaMalloc(&ws.rec_f, ns * sizeof(float)));
         TRY_CUDA(cudaMalloc(&ws.rec_g, 3 * ns * sizeof(float)));
     }
     TRY_CUDA(cudaMalloc(&ws.hist, (size_t)(B * B + B) * 8));
     TRY_CUDA(cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + B) * 8, st));
-    TRY_CUDA(cudaMalloc(&ws.pratio, (size_t)B * B * 8));
-    TRY_CUDA(cudaMalloc(&ws.tail, 4 * 8));
-    TRY_CUDA(cudaMemsetAsync(ws.tail, 0, 4 * 8, st));
-    TRY_CUDA(cudaMalloc(&ws.partials, (size_t)ws.grid_deriv * NMOM * 8));
-    TRY_CUDA(cudaMalloc(&ws.result, (2 + MI_MAX_PARAMS) * 8));
-    TRY_CUDA(cudaMalloc(&ws.done_counter, 2 * sizeof(unsigned int)));
-    TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, 2 * sizeof(unsigned int), st));
-    TRY_CUDA(cudaMemsetAsync(ws.result, 0, (2 + MI_MAX_PARAMS) * 8, st));
-    TRY_CUDA(cudaMallocHost(&ws.host_result, (2 + MI_MAX_PARAMS) * 8));
+    // partials serve both forms: the split form's k_deriv grid and, should the form
+    // be switched, the fused grid
+    {
+        const int pgrid = std::max(ws.grid_deriv, std::max(ws.grid_eval,
+            grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1))));
+        ws.grid_split_hist = grid_for(m->n_samples, HIST_BLOCK, ctx->num_sms * std::max(occ_h, 1));
+        ws.grid_split_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
+        TRY_CUDA(cudaMalloc(&ws.partials, (size_t)pgrid * NMOM * 8));
+    }
+    TRY_CUDA(cudaMalloc(&ws.vsum, (size_t)value_slices(B) * 8));
+    TRY_CUDA(cudaMalloc(&ws.result, RESULT_DOUBLES * 8));
+    TRY_CUDA(cudaMalloc(&ws.done_counter, 4 * sizeof(unsigned int)));
+    TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));
+    TRY_CUDA(cudaMemsetAsync(ws.result, 0, RESULT_DOUBLES * 8, st));
+    TRY_CUDA(cudaMallocHost(&ws.host_result, RESULT_DOUBLES * 8));
     TRY_CUDA(cudaStreamSynchronize(st));
 #undef TRY_CUDA
     *out = m;
@@ -1153,7 +1462,24 @@ mi_status mi_metric_timing_enable(mi_metric* m, int enable) {
         MI_CHECK_CUDA(m->ctx, cudaSetDevice(m->ctx->device));
         for (int i = 0; i < 5; ++i) MI_CHECK_CUDA(m->ctx, cudaEventCreate(&ws.ev[i]));
     }
-    ws.timing = enable != 0;
+    ws.timing = enable < 0 ? 0 : (enable > 2 ? 2 : enable);
+    return MI_OK;
+}
+
+mi_status mi_metric_set_fused(mi_metric* m, int fused) {
+    if (!m) return MI_ERR_INVALID_ARGUMENT;
+    mi::Workspace& ws = m->ws;
+    if (fused && !ws.can_fuse)
+        return mi::set_error(m->ctx, MI_ERR_INVALID_ARGUMENT, "a cooperative launch is not available here");
+    ws.fused = fused != 0;
+    ws.grid_hist = ws.fused ? ws.grid_eval : ws.grid_split_hist;
+    ws.grid_deriv = ws.fused ? ws.grid_eval : ws.grid_split_deriv;
+    return MI_OK;
+}
+
+mi_status mi_metric_get_fused(const mi_metric* m, int* fused) {
+    if (!m || !fused) return MI_ERR_INVALID_ARGUMENT;
+    *fused = m->ws.fused ? 1 : 0;
     return MI_OK;
 }
 

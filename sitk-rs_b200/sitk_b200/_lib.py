@@ -30,7 +30,7 @@ EXPORTED = [
     "mi_metric_value_and_derivative", "mi_metric_value_and_derivative_stages",
     "mi_metric_sample_decisions", "mi_transform_form", "mi_metric_timing_enable",
     "mi_metric_timing_read", "mi_metric_value_noalloc", "mi_register_rsgd",
-    "mi_centered_initialize",
+    "mi_centered_initialize", "mi_metric_set_fused", "mi_metric_get_fused",
 ]
 
 
@@ -111,7 +111,9 @@ def load(path: str | None = None):
     L.mi_metric_value_noalloc.restype = ctypes.c_int
     L.mi_metric_timing_enable.argtypes = [vp, ctypes.c_int]
     L.mi_metric_timing_read.argtypes = [vp, dp, i64p]
-    for name in ["mi_metric_timing_enable", "mi_metric_timing_read", "mi_transform_form", "mi_context_create", "mi_context_destroy", "mi_context_sync", "mi_image_upload",
+    L.mi_metric_set_fused.argtypes = [vp, ctypes.c_int]
+    L.mi_metric_get_fused.argtypes = [vp, P(ctypes.c_int)]
+    for name in ["mi_metric_set_fused", "mi_metric_get_fused", "mi_metric_timing_enable", "mi_metric_timing_read", "mi_transform_form", "mi_context_create", "mi_context_destroy", "mi_context_sync", "mi_image_upload",
                  "mi_image_from_device", "mi_image_to_host", "mi_image_geometry", "mi_image_free",
                  "mi_metric_create", "mi_metric_info_get", "mi_metric_destroy", "mi_metric_value",
                  "mi_metric_value_and_derivative", "mi_metric_value_and_derivative_stages",

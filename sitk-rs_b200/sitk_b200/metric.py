@@ -300,9 +300,11 @@ def transform_stage(transform: ParametricTransform) -> np.ndarray:
     return transform_form(transform)[0]
 
 
-def enable_timing(metric: DeviceMattesMetric, on: bool = True) -> None:
-    """Record CUDA events around each evaluation's kernels (benchmark accounting)."""
-    _lib.check(_lib.load().mi_metric_timing_enable(metric.handle, 1 if on else 0), metric.ctx.handle)
+def enable_timing(metric: DeviceMattesMetric, on: bool = True, per_kernel: bool = False) -> None:
+    """Record CUDA events around each evaluation (and, with per_kernel, after each of
+    its kernels) for benchmark accounting."""
+    mode = 0 if not on else (2 if per_kernel else 1)
+    _lib.check(_lib.load().mi_metric_timing_enable(metric.handle, mode), metric.ctx.handle)
 
 
 def read_timing(metric: DeviceMattesMetric) -> tuple[np.ndarray, int]:
@@ -313,3 +315,15 @@ def read_timing(metric: DeviceMattesMetric) -> tuple[np.ndarray, int]:
     _lib.check(_lib.load().mi_metric_timing_read(metric.handle, ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                                  ctypes.byref(n)), metric.ctx.handle)
     return ms, n.value
+
+
+def set_fused(metric: DeviceMattesMetric, fused: bool) -> None:
+    """Choose the launch form: one cooperative kernel (True) or two kernels (False).
+    Both compute the same histogram, tail and moments."""
+    _lib.check(_lib.load().mi_metric_set_fused(metric.handle, 1 if fused else 0), metric.ctx.handle)
+
+
+def get_fused(metric: DeviceMattesMetric) -> bool:
+    f = ctypes.c_int()
+    _lib.check(_lib.load().mi_metric_get_fused(metric.handle, ctypes.byref(f)), metric.ctx.handle)
+    return bool(f.value)
