@@ -257,6 +257,37 @@ mi_status mi_register_rsgd(mi_metric* m, int kind, const double* fixed_params, i
 mi_status mi_centered_initialize(const mi_geometry* fixed, const mi_geometry* moving, double* center3,
                                  double* translation3);
 
+/* ---- pyramid level (registration/method.rs:2416 prepare_level; device
+ *      counterpart cuda/ops/pyramid.rs) ---------------------------------------- */
+
+/* Recursive (IIR, Deriche) Gaussian smoothing of an image, zero order on every axis
+ * (filters/recursive_gaussian.rs:81 recursive_gaussian): sigma3 in physical units
+ * per axis, 0 = that axis untouched. FP64 throughout, narrowed to f32 once; the
+ * result is a new image on the same grid. An axis with sigma > 0 needs at least 4
+ * voxels (AxisTooShortForRecursion → MI_ERR_INVALID_ARGUMENT). */
+mi_status mi_image_smooth(mi_context* ctx, const mi_image* in, const double* sigma3, mi_image** out);
+
+/* ShrinkImageFilter's output geometry (filters/shrink.rs:51-95): size/f (at least
+ * 1), spacing·f, origin moved by Direction·diag(spacing)·δ with δ the
+ * centre-preserving shift. Host only. */
+mi_status mi_shrink_geometry(const mi_geometry* in, const int64_t* factors3, mi_geometry* out);
+
+/* ResampleImageFilter through the identity with the linear interpolator
+ * (transform/resample.rs:226-290): a new image on `grid`, `fill` outside the input
+ * buffer. */
+mi_status mi_image_resample(mi_context* ctx, const mi_image* in, const mi_geometry* grid, double fill,
+                            mi_image** out);
+
+/* One level of the multi-resolution schedule as prepare_level builds it without a
+ * virtual domain, fixed-initial transform or masks: both images smoothed with
+ * `sigma` (physical units when sigma_physical, else voxels scaled by the fixed
+ * spacing, method.rs:2344-2350), the smoothed fixed image resampled onto its own
+ * shrunk grid (skipped when every factor is 1); the moving image is only smoothed.
+ * Returns two new images. */
+mi_status mi_pyramid_level(mi_context* ctx, const mi_image* fixed, const mi_image* moving, double sigma,
+                           int sigma_physical, const int64_t* factors3, mi_image** fixed_level,
+                           mi_image** moving_level);
+
 /* ---- allocation-free value (no counterpart in the reference) --------------- */
 
 /* Largest histogram the allocation-free entry point can hold. */

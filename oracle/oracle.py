@@ -256,3 +256,69 @@ def register(fixed, fgeo, moving, mgeo, bins, kind, params, fixed_params=None, f
     if st:
         raise OracleError(st)
     return {"params": p, "value": value.value, "iterations": iters.value, "stop_reason": stop.value}
+
+
+def _pyr_bind():
+    L = lib()
+    if getattr(L, "_pyr_typed", False):
+        return L
+    P = ctypes.POINTER
+    gp = P(OrGeometry)
+    L.or_recursive_gaussian.argtypes = [P(ctypes.c_float), gp, P(ctypes.c_double), P(ctypes.c_float)]
+    L.or_recursive_gaussian.restype = ctypes.c_int
+    L.or_shrink_geometry.argtypes = [gp, P(ctypes.c_int64), gp]
+    L.or_shrink_geometry.restype = ctypes.c_int
+    L.or_resample_linear.argtypes = [P(ctypes.c_float), gp, gp, ctypes.c_double, P(ctypes.c_float)]
+    L.or_resample_linear.restype = ctypes.c_int
+    L._pyr_typed = True
+    return L
+
+
+def recursive_gaussian(volume, geo, sigma3):
+    """Zero-order recursive Gaussian (filters/recursive_gaussian.rs), physical sigma per axis."""
+    L = _pyr_bind()
+    v = np.ascontiguousarray(volume, dtype=np.float32)
+    s = np.ascontiguousarray(sigma3, dtype=np.float64)
+    out = np.empty_like(v)
+    st = L.or_recursive_gaussian(_ptr(v, ctypes.c_float), ctypes.byref(geo), _ptr(s, ctypes.c_double),
+                                 _ptr(out, ctypes.c_float))
+    if st:
+        raise OracleError(st)
+    return out
+
+
+def shrink_geometry(geo, factors):
+    """ShrinkImageFilter output grid (filters/shrink.rs:51-95)."""
+    L = _pyr_bind()
+    f = np.ascontiguousarray(factors, dtype=np.int64)
+    out = OrGeometry()
+    st = L.or_shrink_geometry(ctypes.byref(geo), _ptr(f, ctypes.c_int64), ctypes.byref(out))
+    if st:
+        raise OracleError(st)
+    return out
+
+
+def resample_linear(volume, geo_in, geo_out, fill=0.0):
+    """ResampleImageFilter through the identity, linear (transform/resample.rs:226-290)."""
+    L = _pyr_bind()
+    v = np.ascontiguousarray(volume, dtype=np.float32)
+    n = int(geo_out.size[0] * geo_out.size[1] * geo_out.size[2])
+    out = np.empty(n, dtype=np.float32)
+    st = L.or_resample_linear(_ptr(v, ctypes.c_float), ctypes.byref(geo_in), ctypes.byref(geo_out), float(fill),
+                              _ptr(out, ctypes.c_float))
+    if st:
+        raise OracleError(st)
+    return out.reshape(int(geo_out.size[2]), int(geo_out.size[1]), int(geo_out.size[0]))
+
+
+def pyramid_level(fixed, fgeo, moving, mgeo, sigma, factors, sigma_physical=True):
+    """prepare_level (registration/method.rs:2416) without virtual domain, fixed-initial
+    transform or masks: returns (fixed_level, fixed_level_geo, moving_level)."""
+    s3 = [sigma if sigma_physical else sigma * fgeo.spacing[d] for d in range(3)]
+    smooth = any(v != 0.0 for v in s3)
+    sf = recursive_gaussian(fixed, fgeo, s3) if smooth else np.ascontiguousarray(fixed, dtype=np.float32)
+    sm = recursive_gaussian(moving, mgeo, s3) if smooth else np.ascontiguousarray(moving, dtype=np.float32)
+    if all(int(f) == 1 for f in factors):
+        return sf, fgeo, sm
+    cg = shrink_geometry(fgeo, factors)
+    return resample_linear(sf, fgeo, cg, 0.0), cg, sm

@@ -30,7 +30,8 @@ EXPORTED = [
     "mi_metric_value_and_derivative", "mi_metric_value_and_derivative_stages",
     "mi_metric_sample_decisions", "mi_transform_form", "mi_metric_timing_enable",
     "mi_metric_timing_read", "mi_metric_value_noalloc", "mi_register_rsgd",
-    "mi_centered_initialize", "mi_metric_set_fused", "mi_metric_get_fused",
+    "mi_centered_initialize", "mi_metric_set_fused", "mi_metric_get_fused", "mi_image_smooth",
+    "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level",
 ]
 
 
@@ -112,8 +113,13 @@ def load(path: str | None = None):
     L.mi_metric_timing_enable.argtypes = [vp, ctypes.c_int]
     L.mi_metric_timing_read.argtypes = [vp, dp, i64p]
     L.mi_metric_set_fused.argtypes = [vp, ctypes.c_int]
+    L.mi_image_smooth.argtypes = [vp, vp, dp, P(vp)]
+    L.mi_shrink_geometry.argtypes = [P(MiGeometry), i64p, P(MiGeometry)]
+    L.mi_image_resample.argtypes = [vp, vp, P(MiGeometry), ctypes.c_double, P(vp)]
+    L.mi_pyramid_level.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int, i64p, P(vp), P(vp)]
     L.mi_metric_get_fused.argtypes = [vp, P(ctypes.c_int)]
-    for name in ["mi_metric_set_fused", "mi_metric_get_fused", "mi_metric_timing_enable", "mi_metric_timing_read", "mi_transform_form", "mi_context_create", "mi_context_destroy", "mi_context_sync", "mi_image_upload",
+    for name in ["mi_image_smooth", "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level",
+                 "mi_metric_set_fused", "mi_metric_get_fused", "mi_metric_timing_enable", "mi_metric_timing_read", "mi_transform_form", "mi_context_create", "mi_context_destroy", "mi_context_sync", "mi_image_upload",
                  "mi_image_from_device", "mi_image_to_host", "mi_image_geometry", "mi_image_free",
                  "mi_metric_create", "mi_metric_info_get", "mi_metric_destroy", "mi_metric_value",
                  "mi_metric_value_and_derivative", "mi_metric_value_and_derivative_stages",

@@ -127,6 +127,23 @@ class DeviceImage:
     def device_ptr(self) -> int:
         return _lib.load().mi_image_device_ptr(self.handle) or 0
 
+    def smooth(self, sigma) -> "DeviceImage":
+        """Zero-order recursive Gaussian (filters/recursive_gaussian.rs); `sigma` is a
+        physical sigma per axis (or one for all)."""
+        s = np.broadcast_to(np.asarray(sigma, dtype=np.float64), (3,)).copy()
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mi_image_smooth(self.ctx.handle, self.handle,
+                                               s.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(h)),
+                   self.ctx.handle)
+        return DeviceImage(h, self.ctx, _copy_geo(self.geo))
+
+    def resample(self, grid: _lib.MiGeometry, fill: float = 0.0) -> "DeviceImage":
+        """Linear resampling onto `grid` through the identity (transform/resample.rs)."""
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mi_image_resample(self.ctx.handle, self.handle, ctypes.byref(grid), float(fill),
+                                                 ctypes.byref(h)), self.ctx.handle)
+        return DeviceImage(h, self.ctx, _copy_geo(grid))
+
     def free(self):
         if self.handle:
             _lib.load().mi_image_free(self.handle)
@@ -327,3 +344,33 @@ def get_fused(metric: DeviceMattesMetric) -> bool:
     f = ctypes.c_int()
     _lib.check(_lib.load().mi_metric_get_fused(metric.handle, ctypes.byref(f)), metric.ctx.handle)
     return bool(f.value)
+
+
+def _copy_geo(g: _lib.MiGeometry) -> _lib.MiGeometry:
+    out = _lib.MiGeometry()
+    ctypes.pointer(out)[0] = g
+    return out
+
+
+def shrink_geometry(geo: _lib.MiGeometry, factors) -> _lib.MiGeometry:
+    """ShrinkImageFilter's output grid (filters/shrink.rs:51-95)."""
+    f = np.broadcast_to(np.asarray(factors, dtype=np.int64), (3,)).copy()
+    out = _lib.MiGeometry()
+    _lib.check(_lib.load().mi_shrink_geometry(ctypes.byref(geo), f.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                              ctypes.byref(out)))
+    return out
+
+
+def pyramid_level(fixed: DeviceImage, moving: DeviceImage, sigma: float, factors, sigma_physical: bool = True):
+    """One level of prepare_level (registration/method.rs:2416): (fixed_level, moving_level)."""
+    f = np.broadcast_to(np.asarray(factors, dtype=np.int64), (3,)).copy()
+    hf, hm = ctypes.c_void_p(), ctypes.c_void_p()
+    _lib.check(_lib.load().mi_pyramid_level(fixed.ctx.handle, fixed.handle, moving.handle, float(sigma),
+                                            1 if sigma_physical else 0,
+                                            f.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(hf),
+                                            ctypes.byref(hm)), fixed.ctx.handle)
+    L = _lib.load()
+    gf, gm = _lib.MiGeometry(), _lib.MiGeometry()
+    _lib.check(L.mi_image_geometry(hf, ctypes.byref(gf)))
+    _lib.check(L.mi_image_geometry(hm, ctypes.byref(gm)))
+    return DeviceImage(hf, fixed.ctx, gf), DeviceImage(hm, moving.ctx, gm)

@@ -95,3 +95,36 @@ def register_rsgd(metric: DeviceMattesMetric, transform: ParametricTransform, it
     transform.set_parameters(p)
     return LevelResult(res.value, res.iterations, STOP_REASONS.get(res.stop_reason, str(res.stop_reason)),
                        res.valid, res.evaluations, None if trace is None else trace[:res.evaluations])
+
+
+@dataclass
+class MultiLevelResult:
+    """RegistrationResult::from_levels (registration/method.rs): the final parameters
+    and one record per level, coarsest first."""
+    params: np.ndarray
+    levels: list
+
+
+def register_multilevel(fixed: DeviceImage, moving: DeviceImage, transform: ParametricTransform,
+                        shrink_factors=(4, 2, 1), smoothing_sigmas=(2.0, 1.0, 0.0), sigmas_physical: bool = True,
+                        bins: int = 32, strategy: int | None = 2, percentage: float = 0.1, seed: int = 0,
+                        iterations: int = 200, **rsgd) -> MultiLevelResult:
+    """The device registration loop of ImageRegistrationMethod::execute_on_device
+    (registration/method.rs:2698-2880) for the Mattes metric: per level, the
+    pyramid level (prepare_level: smoothed fixed resampled onto its shrunk grid,
+    smoothed moving), the level's sample draw (same strategy, percentage and seed,
+    over the level's fixed grid), then one regular-step gradient descent run from
+    the previous level's parameters. `transform` is updated in place."""
+    from .metric import pyramid_level
+    if len(shrink_factors) != len(smoothing_sigmas):
+        raise ValueError("PyramidScheduleLength: shrink and smoothing schedules differ in length")
+    records = []
+    for f, s in zip(shrink_factors, smoothing_sigmas):
+        fl, ml = pyramid_level(fixed, moving, s, f, sigmas_physical)
+        metric = DeviceMattesMetric.from_device_sampled(fl, ml, bins=bins, strategy=strategy, percentage=percentage,
+                                                        seed=seed)
+        fl.free()
+        ml.free()
+        records.append(register_rsgd(metric, transform, iterations=iterations, **rsgd))
+        metric.close()
+    return MultiLevelResult(np.array(transform.params, dtype=np.float64), records)

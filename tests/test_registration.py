@@ -178,3 +178,33 @@ def test_versor_registration_random_sampling_every_step_checked(oracle_lib):
     np.testing.assert_allclose(tr[4, 1:1 + n], early["params"], rtol=0, atol=1e-6)
     # and the run lands in the oracle's basin
     assert abs(res.value - ref["value"]) <= 2e-3 * abs(ref["value"])
+
+
+@pytest.mark.gpu
+def test_multilevel_registration_matches_the_oracle_level_by_level(oracle_lib):
+    # execute_on_device's level loop (method.rs:2698-2880) on the contrast-inverted pair
+    # of tests/mattes_device.rs:459 with a two-level pyramid (shrink 2/1, sigma 1/0)
+    import sitk_b200 as sb
+    from sitk_b200 import registration
+    n = 48
+    sp, org = (0.8, 0.9, 1.1), (-3.0, 2.0, 1.0)
+    fixed = _analytic_volume(n, (0.0, 0.0, 0.0))
+    moving = (120.0 - _analytic_volume(n, (-2.0, 1.0, 0.0)).astype(np.float64)).astype(np.float32)
+    f = sb.DeviceImage.upload(fixed, sp, org)
+    m = sb.DeviceImage.upload(moving, sp, org)
+    t = sb.TranslationTransform((0.0, 0.0, 0.0))
+    schedule = ((2, 1.0), (1, 0.0))
+    res = registration.register_multilevel(f, m, t, shrink_factors=[s[0] for s in schedule],
+                                           smoothing_sigmas=[s[1] for s in schedule], bins=50, strategy=None,
+                                           iterations=200, minimum_step=0.01, gradient_tolerance=1e-6)
+    g = oracle_lib.make_geometry((n, n, n), sp, org)
+    p = np.zeros(3)
+    for (factor, sigma), level in zip(schedule, res.levels):
+        ofl, ogeo, oml = oracle_lib.pyramid_level(fixed, g, moving, g, sigma, (factor,) * 3)
+        ref = oracle_lib.register(ofl, ogeo, oml, g, 50, 3, p, None, iterations=200, minimum_step=0.01,
+                                  gradient_tolerance=1e-6, nthreads=8)
+        assert level.iterations == ref["iterations"], (factor, level, ref)
+        assert abs(level.value - ref["value"]) <= 1e-3 * abs(ref["value"])
+        p = ref["params"]
+    assert np.max(np.abs(res.params - p)) < 1e-3, (res.params, p)
+    assert np.max(np.abs(res.params)) > 0.5
