@@ -288,6 +288,35 @@ mi_status mi_pyramid_level(mi_context* ctx, const mi_image* fixed, const mi_imag
                            int sigma_physical, const int64_t* factors3, mi_image** fixed_level,
                            mi_image** moving_level);
 
+/* ---- batched registration (no reference counterpart) ----------------------- */
+
+/* Many registrations of uneven image sizes advanced together: every optimizer
+ * iteration is one pass of three launches over all still-active pairs (histogram
+ * pass, tail and derivative pass, the regular-step gradient descent step of every
+ * pair, with all optimizer state on the device), several passes captured in one CUDA
+ * graph that is replayed until every pair has stopped. Per pair the sampler,
+ * histogram, tail, moments, optimizer step and point-map constants are the
+ * single-pair code; a pair's samples are cut into chunks, and the histogram's
+ * fixed-point unit follows the chunk size, so values agree with mi_register_rsgd on
+ * the same pair to that unit.
+ *
+ * mi_batch_create builds one metric per pair (fixed[p], moving[p], sampling[p] — an
+ * array of npairs, or NULL for the whole grid — and the common bin count) for the
+ * affine (fixed_params: npairs × 3 centres) or translation family (nfixed = 0).
+ * mi_batch_register runs from params_inout (npairs × nparams, updated in place) with
+ * one configuration for every pair (trace unused) and fills results[npairs];
+ * autotune != 0 first times candidate shapes (chunk size, privatised histogram copies)
+ * on this batch and keeps the fastest, cached per (bins, sample-count class).
+ * mi_batch_shape reports the shape in use. */
+typedef struct mi_batch mi_batch;
+mi_status mi_batch_create(mi_context* ctx, int npairs, const mi_image* const* fixed, const mi_image* const* moving,
+                          const mi_sampling* sampling, int bins, int kind, const double* fixed_params, int nfixed,
+                          mi_batch** out);
+mi_status mi_batch_register(mi_batch* b, const mi_rsgd_config* cfg, int autotune, double* params_inout,
+                            mi_rsgd_result* results);
+mi_status mi_batch_shape(const mi_batch* b, int* chunk, int* copies, int* nchunks);
+mi_status mi_batch_destroy(mi_batch* b);
+
 /* ---- allocation-free value (no counterpart in the reference) --------------- */
 
 /* Largest histogram the allocation-free entry point can hold. */

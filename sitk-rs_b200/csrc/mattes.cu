@@ -33,6 +33,8 @@
 
 #include "internal.h"
 #include "sampler.cuh"
+#include "eval_device.cuh"
+#include "point_map.h"
 
 namespace mi {
 
@@ -41,620 +43,6 @@ void index_to_physical(const mi_geometry& g, double* m);
 bool invert3(const double* m, double* inv);
 
 namespace {
-
-// Launch shape of the histogram pass: HIST_ILP samples per thread in flight (their
-// corner gathers issued together), and a register cap that keeps HIST_MIN_BLOCKS
-// CTAs of HIST_BLOCK threads resident per SM.
-#ifndef MI_HIST_ILP
-#define MI_HIST_ILP 2
-#endif
-#ifndef MI_HIST_MIN_BLOCKS
-#define MI_HIST_MIN_BLOCKS 4
-#endif
-// Histogram copies per CTA (coarse and fine parts) and the fine part's threshold
-// 2^-MI_HIST_FINE_T (see k_hist).
-#ifndef MI_HIST_COPIES
-#define MI_HIST_COPIES 4
-#endif
-#ifndef MI_HIST_FINE_COPIES
-#define MI_HIST_FINE_COPIES 2
-#endif
-#ifndef MI_HIST_FINE_T
-#define MI_HIST_FINE_T 10
-#endif
-constexpr int HIST_BLOCK = 256;
-constexpr int HIST_MIN_BLOCKS = MI_HIST_MIN_BLOCKS;
-constexpr int HIST_ILP = MI_HIST_ILP;
-constexpr int DERIV_BLOCK = 256;
-constexpr int NMOM = 12;
-
-struct JacobianForm {
-    int nparams;
-    double jac0[3 * MI_MAX_PARAMS];
-    double jacc[3][3 * MI_MAX_PARAMS];
-};
-
-// One histogram copy: B² joint + B fixed-marginal u32 counters, padded so copies
-// start 4 banks apart.
-__host__ __device__ inline int hist_copy_stride(int B) { return ((B * B + B + 31) & ~31) + 4; }
-// Copies that fit in 48 KB (a power of two, 1–MI_HIST_COPIES).
-int hist_copies(int B) {
-    int c = MI_HIST_COPIES;
-    while (c > 1 && (size_t)c * hist_copy_stride(B) * sizeof(unsigned int) > 48 * 1024) c >>= 1;
-    return c;
-}
-// The fine histogram (B² u32 counters per copy) that takes the small outer taps.
-__host__ __device__ inline int hist_fine_stride(int B) { return ((B * B + 31) & ~31) + 4; }
-// Fine copies: up to MI_HIST_FINE_COPIES, fewer if the two parts together pass
-// 52 KB (four 256-thread CTAs resident per SM at 32 bins).
-int hist_fine_copies(int B) {
-    const size_t coarse = (size_t)hist_copies(B) * hist_copy_stride(B) * sizeof(unsigned int);
-    int c = MI_HIST_FINE_COPIES;
-    while (c > 1 && coarse + (size_t)c * hist_fine_stride(B) * sizeof(unsigned int) > 52 * 1024) c >>= 1;
-    return c;
-}
-size_t hist_smem(int B) {
-    return ((size_t)hist_copies(B) * hist_copy_stride(B) + (size_t)hist_fine_copies(B) * hist_fine_stride(B)) *
-           sizeof(unsigned int);
-}
-// Shared memory of the tail (see TailSmem).
-constexpr int TAIL_BLOCK = 256;
-__host__ __device__ inline int tail_groups(int B) { return TAIL_BLOCK / B; }
-__host__ __device__ inline size_t tail_smem(int B) {
-    return ((size_t)B * B + B + (size_t)tail_groups(B) * B + B) * 8 + ((2 * (size_t)B + 7) & ~(size_t)7);
-}
-size_t deriv_smem(int B) { return 32 * (size_t)NMOM * sizeof(double) + tail_smem(B) + (size_t)B * B * sizeof(float); }
-// The fused kernel reuses one dynamic allocation for its phases. The derivative
-// pass's layout: moment reduction scratch (32·NMOM doubles), the tail's state
-// (tail_smem), then the pRatio table (B² floats).
-size_t eval_smem(int B) { return std::max(hist_smem(B), std::max(deriv_smem(B), tail_smem(B))); }
-
-// Block-wide sum of a double in a fixed order (warp shuffles, then warp 0).
-__device__ double block_sum(double v, double* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    __syncthreads();
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    const int nw = (blockDim.x + 31) >> 5;
-    double r = 0.0;
-    if (warp == 0) {
-        r = lane < nw ? red[lane] : 0.0;
-#pragma unroll
-        for (int off = 16; off; off >>= 1) r += __shfl_down_sync(0xffffffffu, r, off);
-        if (lane == 0) red[0] = r;
-    }
-    __syncthreads();
-    r = red[0];
-    __syncthreads();
-    return r;
-}
-
-__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
-#pragma unroll
-    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    return v;
-}
-
-// Device buffers and per-launch constants shared by the evaluation kernels.
-//   sync[0] done counter of the final phase, sync[2] grid-barrier counter of the
-//   fused kernel.
-//   result: value, valid, derivative[MI_MAX_PARAMS], then the error word.
-struct EvalArgs {
-    const float* moving;
-    const uint8_t* mmask;
-    const uint32_t* samples;
-    const uint8_t* fbin;
-    uint32_t n, npad;
-    float hist_scale, fine_scale;
-    int fine_shift, copies, fine_copies;
-    double hist_inv;
-    unsigned long long* ghist;
-    uint16_t* rec_bins;  // per sample: moving bin | fixed bin << 8 (0 = not valid)
-    float* rec_f;
-    float* rec_g;
-    double* partials;
-    double* vsum;  // value slice sums (value_slices(B))
-    unsigned int* sync;
-    double* result;
-};
-constexpr int RESULT_ERR = 2 + MI_MAX_PARAMS;  // result slot holding the error word
-constexpr int RESULT_DOUBLES = RESULT_ERR + 2;
-__device__ __forceinline__ unsigned int* error_word(const EvalArgs& a) {
-    return reinterpret_cast<unsigned int*>(a.result + RESULT_ERR);
-}
-
-// ---------------------------------------------------------------------------
-// Pass 1: joint histogram (+ per-sample records for pass 2). The CTA histogram is
-// u32 fixed point in two parts, both exact integer sums:
-//   coarse: the two inner taps (always ≥ 1/6) and outer taps ≥ 2^-FINE_T, added as
-//           round(w·2^k) (hist_scale = 2^k);
-//   fine:   outer taps below 2^-FINE_T (a cubic B-spline's end taps, f³/6 and
-//           (1−f)³/6, near a bin edge), added as round(w·2^kf) with kf > k
-//           (fine_scale = 2^kf, fine_shift = kf − k).
-// A sparse bin whose mass is made of end taps is where pRatio = log p is steep: a
-// 2^-k quantum there moves the derivative by far more than FP32 rounding does, so
-// those taps get the fine quantum. k and kf are chosen per launch so that no copy's
-// counter can pass 2^32; the flush adds (coarse << fine_shift) + fine into the u64
-// global histogram, whose unit is 2^-kf.
-// ---------------------------------------------------------------------------
-constexpr int FINE_T = MI_HIST_FINE_T;
-constexpr float FINE_LIMIT = 1.0f / (float)(1u << FINE_T);
-
-template <bool RECORD>
-__device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArgs& a, unsigned int* sh) {
-    const int B = P.bins;
-    const int nb = B * B + B;
-    const int copies = a.copies, fine_copies = a.fine_copies;
-    const int cstride = hist_copy_stride(B);
-    const int fstride = hist_fine_stride(B);
-    unsigned int* sh_fine = sh + copies * cstride;
-    for (int i = threadIdx.x; i < copies * cstride + fine_copies * fstride; i += blockDim.x) sh[i] = 0u;
-    __syncthreads();
-    unsigned int* sh_joint = sh;
-    unsigned int* sh_fixed = sh + B * B;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t n = a.n, npad = a.npad;
-    const float* __restrict__ moving = a.moving;
-    const uint8_t* __restrict__ mmask = a.mmask;
-    const uint32_t* __restrict__ samples = a.samples;
-    const uint8_t* __restrict__ fbin = a.fbin;
-    const float hist_scale = a.hist_scale, fine_scale = a.fine_scale;
-    // Two samples per iteration: both samples' corner gathers are issued (prep) before
-    // either is finished, so each thread keeps two gathers in flight.
-    // The CTA keeps `copies` interleaved copies of the histogram and lane l adds into
-    // copy l mod copies: neighbouring lanes, whose sorted samples usually share a bin
-    // pair, then add to different addresses instead of replaying on one. The copies
-    // are summed at the flush (integer adds: the order does not matter).
-    const int lane = threadIdx.x & 31;
-    unsigned int* my_joint = sh_joint + (lane & (copies - 1)) * cstride;
-    unsigned int* my_fixed = sh_fixed + (lane & (copies - 1)) * cstride;
-    unsigned int* my_fine = sh_fine + (lane & (fine_copies - 1)) * fstride;
-    auto account = [&](const Prep& p, uint32_t s, bool real) {
-        if (!real) return;
-        Sample o;
-        o.exact = false;
-        const int st = finish<RECORD>(P, p, moving, o);
-        if (st != SAMPLE_VALID) {
-            if (RECORD) a.rec_bins[s] = 0;
-            return;
-        }
-        const int fi = __ldg(fbin + s);
-        float w[4];
-        bspline3_taps(o.f, w);
-        const int off = fi * B + (o.mi - 1);
-        unsigned int* row = my_joint + off;
-        unsigned int* frow = my_fine + off;
-        // round(w·scale) by the 1.5·2^23 magic add (w·scale < 2^22 for both parts):
-        // one FMA, no conversion
-        atomicAdd(row + 1, __float_as_uint(fmaf(w[1], hist_scale, 12582912.0f)) - 0x4B400000u);
-        atomicAdd(row + 2, __float_as_uint(fmaf(w[2], hist_scale, 12582912.0f)) - 0x4B400000u);
-#pragma unroll
-        for (int t = 0; t < 4; t += 3) {
-            const bool fine = w[t] < FINE_LIMIT;
-            atomicAdd((fine ? frow : row) + t,
-                      __float_as_uint(fmaf(w[t], fine ? fine_scale : hist_scale, 12582912.0f)) - 0x4B400000u);
-        }
-        atomicAdd(my_fixed + fi, 1u);
-        if (RECORD) {
-            a.rec_bins[s] = (uint16_t)(o.mi | (fi << 8));
-            a.rec_f[s] = o.f;
-            a.rec_g[s] = o.g[0];
-            a.rec_g[(size_t)npad + s] = o.g[1];
-            a.rec_g[2 * (size_t)npad + s] = o.g[2];
-        }
-    };
-    // whole warps iterate together: the loop bound is the warp's first sample
-    const uint32_t wbase = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
-    if (HIST_ILP == 2) {
-        for (uint32_t b = wbase; b < n; b += 2 * stride) {
-            const uint32_t s = b + lane, s2 = s + stride;
-            const bool one = s < n, two = s2 < n;
-            const uint32_t fa = one ? (samples ? __ldg(samples + s) : s) : 0u;
-            const uint32_t fb = two ? (samples ? __ldg(samples + s2) : s2) : fa;
-            Prep pa, pb;
-            prep<RECORD>(P, fa, moving, mmask, pa);
-            prep<RECORD>(P, fb, moving, mmask, pb);
-            account(pa, s, one);
-            account(pb, s2, two);
-        }
-    } else {
-        for (uint32_t b = wbase; b < n; b += stride) {
-            const uint32_t s = b + lane;
-            const bool one = s < n;
-            Prep pa;
-            prep<RECORD>(P, one ? (samples ? __ldg(samples + s) : s) : 0u, moving, mmask, pa);
-            account(pa, s, one);
-        }
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-        unsigned long long v = 0ull;
-        for (int c = 0; c < copies; ++c) v += sh[c * cstride + i];
-        if (i < B * B) {
-            unsigned long long f = 0ull;
-            for (int c = 0; c < fine_copies; ++c) f += sh_fine[c * fstride + i];
-            v = (v << a.fine_shift) + f;
-        }
-        if (v) atomicAdd(&a.ghist[i], v);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// The tail (registration/mattes.rs:273-328) over the finished global histogram. The
-// marginals are sums of the integer histogram, so every CTA forms them exactly (any
-// order, same bits):
-//   total = Σ joint, col[m] = Σ_f joint[f][m], valid = Σ_f count[f].
-// With p = joint/total the reference's quantities are
-//   joint_sum = total·2^-kf, jp = joint/total, mm = col/total, fm = count/joint_sum,
-//   pRatio = ln(jp/mm) = ln(joint/col), −MI = −Σ jp·(pRatio − ln fm),
-// the ratio inside the logarithm formed from the exact integers; nFactor =
-// 1/(moving bin size·valid); degenerate (value DBL_MAX, zero derivative) when there
-// is no valid sample or Σ joint < ε (mattes.rs:590-609).
-// ---------------------------------------------------------------------------
-// The tail's shared-memory state, carved from `base` (tail_smem(B) bytes): a copy of
-// the global histogram (B² joint + B counts, u64), per-group column partials, the
-// column sums and fixed counts, and the column/row flags mm > ε, fm > ε.
-struct TailSmem {
-    unsigned long long* hist;  // B*B + B
-    unsigned long long* part;  // tail_groups(B) * B
-    unsigned long long* col;   // B
-    uint8_t* okm;              // B
-    uint8_t* okf;              // B
-};
-__device__ __forceinline__ TailSmem tail_layout(int B, unsigned char* base) {
-    TailSmem t;
-    t.hist = reinterpret_cast<unsigned long long*>(base);
-    t.part = t.hist + B * B + B;
-    t.col = t.part + tail_groups(B) * B;
-    t.okm = reinterpret_cast<uint8_t*>(t.col + B);
-    t.okf = t.okm + B;
-    return t;
-}
-
-// Per-CTA tail state: the integer marginals, the normalisers and the degenerate flag.
-struct TailCtx {
-    unsigned long long total, valid;
-    double dt;         // total, as a double
-    double joint_sum;  // total·2^-kf
-    double n_factor;   // 1/(moving bin size·valid)
-    bool degenerate;
-};
-
-// Every CTA copies the histogram into shared memory with coalesced loads and forms
-// the marginals from the copy: column m's sum in tail_groups(B) row groups, then over
-// the groups; counts are read in place. Integer sums, so any order gives the same
-// bits.
-__device__ TailCtx tail_prepare(int B, double moving_bin_size, const EvalArgs& a, const TailSmem& ts) {
-    const int B2 = B * B, nb = B2 + B;
-    const unsigned long long* __restrict__ gh = a.ghist;
-    for (int i0 = threadIdx.x; i0 < nb; i0 += 4 * blockDim.x) {
-        unsigned long long v[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int i = i0 + u * blockDim.x;
-            v[u] = i < nb ? __ldcg(gh + i) : 0ull;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int i = i0 + u * blockDim.x;
-            if (i < nb) ts.hist[i] = v[u];
-        }
-    }
-    __syncthreads();
-    const int G = tail_groups(B);
-    if ((int)threadIdx.x < G * B) {
-        const int m = threadIdx.x % B, g = threadIdx.x / B;
-        unsigned long long v = 0ull;
-        for (int f = g; f < B; f += G) v += ts.hist[f * B + m];
-        ts.part[g * B + m] = v;
-    }
-    __syncthreads();
-    if ((int)threadIdx.x < B) {
-        unsigned long long v = 0ull;
-        for (int g = 0; g < G; ++g) v += ts.part[g * B + threadIdx.x];
-        ts.col[threadIdx.x] = v;
-    }
-    __syncthreads();
-    const unsigned long long* cnt = ts.hist + B2;
-    const int lane = threadIdx.x & 31;
-    TailCtx t;
-    t.total = 0ull;
-    t.valid = 0ull;
-    for (int m = lane; m < B; m += 32) {
-        t.total += ts.col[m];
-        t.valid += cnt[m];
-    }
-    t.total = warp_sum_u64(t.total);
-    t.valid = warp_sum_u64(t.valid);
-    t.dt = (double)t.total;
-    t.joint_sum = t.dt * a.hist_inv;
-    t.degenerate = t.valid == 0ull || t.joint_sum < DBL_EPSILON;
-    t.n_factor = t.degenerate ? 0.0 : 1.0 / (moving_bin_size * (double)t.valid);
-    if ((int)threadIdx.x < B) {
-        ts.okm[threadIdx.x] = (double)ts.col[threadIdx.x] / t.dt > DBL_EPSILON;
-        ts.okf[threadIdx.x] = (double)cnt[threadIdx.x] / t.joint_sum > DBL_EPSILON;
-    }
-    __syncthreads();
-    return t;
-}
-
-// pRatio·nFactor of every bin into pr (shared memory, FP32): 0 where the reference
-// skips the bin, else ln(joint/col)·nFactor with the ratio formed in FP64 and the
-// logarithm taken in FP32 (the table is FP32).
-__device__ void pr_table(int B, const TailCtx& t, const TailSmem& ts, float* pr) {
-    const int B2 = B * B;
-    const float nf = (float)t.n_factor;
-    for (int i = threadIdx.x; i < B2; i += blockDim.x) {
-        const int f = i / B, m = i - f * B;
-        const unsigned long long jv = ts.hist[i];
-        float r = 0.0f;
-        if (ts.okf[f] && ts.okm[m] && jv && (double)jv / t.dt > DBL_EPSILON)
-            r = logf((float)((double)jv / (double)ts.col[m])) * nf;
-        pr[i] = r;
-    }
-}
-
-// −MI is summed in value slices of 32 bins, one warp each (lane l takes bin
-// 32·s + l, then a fixed xor tree), and the slice sums are folded in slice order
-// (fold_value). Whichever warp of whichever kernel computes a slice, it gets the
-// same bits, so every launch form reports the same value.
-__host__ __device__ inline int value_slices(int B) { return (B * B + 31) / 32; }
-
-__device__ double value_slice(int B, const TailCtx& t, const TailSmem& ts, int slice) {
-    const int lane = threadIdx.x & 31;
-    const int i = slice * 32 + lane;
-    double term = 0.0;
-    if (i < B * B) {
-        const unsigned long long jv = ts.hist[i];
-        const int f = i / B, m = i - f * B;
-        const double jp = (double)jv / t.dt;
-        const double mm = (double)ts.col[m] / t.dt;
-        const double fm = (double)ts.hist[B * B + f] / t.joint_sum;
-        if (fm > DBL_EPSILON && mm > DBL_EPSILON && jp > DBL_EPSILON)
-            term = jp * (log((double)jv / (double)ts.col[m]) - log(fm));
-    }
-#pragma unroll
-    for (int off = 16; off; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);
-    return term;
-}
-
-// This CTA's share of the value slices (global warp w takes slices w, w + W, …),
-// their sums stored in a.vsum.
-__device__ void value_slices_share(int B, const EvalArgs& a, const TailCtx& t, const TailSmem& ts) {
-    const int lane = threadIdx.x & 31;
-    const int nw = blockDim.x >> 5;
-    const int ns = value_slices(B);
-    for (int s = blockIdx.x * nw + (threadIdx.x >> 5); s < ns; s += gridDim.x * nw) {
-        const double v = value_slice(B, t, ts, s);
-        if (lane == 0) a.vsum[s] = v;
-    }
-}
-
-// One warp: value and valid into result (lane 0), from the slice sums.
-__device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
-    const int lane = threadIdx.x & 31;
-    const int ns = value_slices(B);
-    double v = 0.0;
-    for (int s = lane; s < ns; s += 32) v += __ldcg(a.vsum + s);
-#pragma unroll
-    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    if (lane == 0) {
-        a.result[0] = t.degenerate ? DBL_MAX : -v;
-        a.result[1] = (double)t.valid;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Pass 2: derivative moments streamed from the pass-1 records, FP32 per thread,
-// FP64 from the warp reduction on; the last CTA folds the CTA partials in CTA order
-// and contracts them with the transform's Jacobian form.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void accumulate_moments(const SamplerParams& P, const float* pr, int B, int mi, int fi,
-                                                   float f, float g0, float g1, float g2, uint32_t flat,
-                                                   float* acc) {
-    uint32_t i, j, k;
-    grid_index(P, flat, i, j, k);
-    const float fi_ = (float)i, fj = (float)j, fk = (float)k;
-    float dx[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-        dx[d] = fmaf(P.xA[d * 3 + 2], fk, fmaf(P.xA[d * 3 + 1], fj, fmaf(P.xA[d * 3 + 0], fi_, P.xb[d])));
-    float dw[4];
-    bspline3_deriv_taps(f, dw);
-    const float* row = pr + fi * B + (mi - 1);
-    const float w = fmaf(dw[3], row[3], fmaf(dw[2], row[2], fmaf(dw[1], row[1], dw[0] * row[0])));
-    const float wg[3] = {w * g0, w * g1, w * g2};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        acc[d] += wg[d];
-        acc[3 + d * 3 + 0] = fmaf(wg[d], dx[0], acc[3 + d * 3 + 0]);
-        acc[3 + d * 3 + 1] = fmaf(wg[d], dx[1], acc[3 + d * 3 + 1]);
-        acc[3 + d * 3 + 2] = fmaf(wg[d], dx[2], acc[3 + d * 3 + 2]);
-    }
-}
-
-// The moments of this CTA's share of the samples, stored into partials[slot][CTA].
-// The CTA first forms the tail itself (tail_prepare, pr_table) and its share of the
-// value slices; the first group of records is requested before that so its loads
-// overlap the tail. Records are read four samples
-// per thread with 8- and 16-byte vector loads (every record array is padded to a
-// multiple of four samples; padding records carry bins 0 and are skipped). Returns
-// the tail state.
-__device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double* dsh) {
-    const int B = P.bins;
-    double* red = dsh;  // 32 * NMOM
-    unsigned char* tbase = reinterpret_cast<unsigned char*>(dsh + 32 * NMOM);
-    const TailSmem ts = tail_layout(B, tbase);
-    float* pr = reinterpret_cast<float*>(tbase + tail_smem(B));  // B*B
-    float acc[NMOM];
-#pragma unroll
-    for (int i = 0; i < NMOM; ++i) acc[i] = 0.0f;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t npad = a.npad;
-    const uint32_t ngroups = npad >> 2;
-    const uint2* b4p = reinterpret_cast<const uint2*>(a.rec_bins);
-    const float4* f4p = reinterpret_cast<const float4*>(a.rec_f);
-    const float4* gx4p = reinterpret_cast<const float4*>(a.rec_g);
-    const float4* gy4p = reinterpret_cast<const float4*>(a.rec_g + npad);
-    const float4* gz4p = reinterpret_cast<const float4*>(a.rec_g + 2 * (size_t)npad);
-    const uint4* s4p = reinterpret_cast<const uint4*>(a.samples);
-    // the next group's records are loaded before the current group is accumulated
-    struct Group {
-        uint2 b;
-        float4 f, gx, gy, gz;
-        uint4 fl;
-    };
-    auto load = [&](uint32_t q, Group& g) {
-        g.b = __ldcg(b4p + q);
-        g.f = __ldcg(f4p + q);
-        g.gx = __ldcg(gx4p + q);
-        g.gy = __ldcg(gy4p + q);
-        g.gz = __ldcg(gz4p + q);
-        g.fl = a.samples ? __ldg(s4p + q) : make_uint4(4 * q, 4 * q + 1, 4 * q + 2, 4 * q + 3);
-    };
-    auto one = [&](uint32_t bins, float f, float gx, float gy, float gz, uint32_t flat) {
-        if (bins & 0xffu) accumulate_moments(P, pr, B, bins & 0xffu, bins >> 8, f, gx, gy, gz, flat, acc);
-    };
-    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    Group cur;
-    if (q < ngroups) load(q, cur);
-    const TailCtx t = tail_prepare(B, P.moving_bin_size, a, ts);
-    if (!t.degenerate) {
-        pr_table(B, t, ts, pr);
-        value_slices_share(B, a, t, ts);
-    }
-    __syncthreads();
-    if (!t.degenerate) {
-        while (q < ngroups) {
-            const uint32_t qn = q + stride;
-            Group nxt;
-            if (qn < ngroups) load(qn, nxt);
-            one(cur.b.x & 0xffffu, cur.f.x, cur.gx.x, cur.gy.x, cur.gz.x, cur.fl.x);
-            one(cur.b.x >> 16, cur.f.y, cur.gx.y, cur.gy.y, cur.gz.y, cur.fl.y);
-            one(cur.b.y & 0xffffu, cur.f.z, cur.gx.z, cur.gy.z, cur.gz.z, cur.fl.z);
-            one(cur.b.y >> 16, cur.f.w, cur.gx.w, cur.gy.w, cur.gz.w, cur.fl.w);
-            cur = nxt;
-            q = qn;
-        }
-    }
-    // CTA reduction in a fixed order: shuffles within a warp, then over warps.
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    double accd[NMOM];
-#pragma unroll
-    for (int i = 0; i < NMOM; ++i) {
-        double v = (double)acc[i];
-#pragma unroll
-        for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        accd[i] = v;
-    }
-    if (lane == 0)
-        for (int i = 0; i < NMOM; ++i) red[warp * NMOM + i] = accd[i];
-    __syncthreads();
-    // partials are stored slot-major, [slot][CTA], so the fold reads them coalesced
-    if (threadIdx.x < NMOM) {
-        double v = 0.0;
-        for (int w = 0; w < nw; ++w) v += red[w * NMOM + threadIdx.x];
-        a.partials[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
-    }
-    return t;
-}
-
-// Run by the last CTA to finish the derivative phase: fold every CTA's partials in
-// a fixed order (lane l of a slot sums CTAs l, l+21, … eight loads at a time; the 21
-// lane sums of a slot are then added in lane order) and contract with the Jacobian
-// form: ∂/∂p_k = Σ_d J(x_ref)[d][k]·A_d + Σ_{d,e} C_e[d][k]·B[d][e],
-// J(x_ref) = J(0) + Σ_e x_ref,e·C_e.
-__device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const EvalArgs& a, bool degenerate) {
-    constexpr int FOLD = 21;
-    __shared__ double fold[FOLD * NMOM];
-    __shared__ double mom[NMOM];
-    if (threadIdx.x < FOLD * NMOM) {
-        const int slot = threadIdx.x / FOLD, ln = threadIdx.x % FOLD;
-        const double* src = a.partials + (int64_t)slot * gridDim.x;
-        double v = 0.0;
-        unsigned int b = ln;
-        for (; b + 7 * FOLD < gridDim.x; b += 8 * FOLD) {
-            double t[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) t[u] = __ldcg(src + b + u * FOLD);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) v += t[u];
-        }
-        for (; b < gridDim.x; b += FOLD) v += __ldcg(src + b);
-        fold[slot * FOLD + ln] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < NMOM) {
-        double v = 0.0;
-        for (int l = 0; l < FOLD; ++l) v += fold[threadIdx.x * FOLD + l];
-        mom[threadIdx.x] = v;
-    }
-    __syncthreads();
-    const int np = J.nparams;
-    if (threadIdx.x < np) {
-        const int k = threadIdx.x;
-        double dk = 0.0;
-        if (!degenerate) {
-            for (int d = 0; d < 3; ++d) {
-                double jr = J.jac0[d * np + k];
-                for (int e = 0; e < 3; ++e) jr += P.xref[e] * J.jacc[e][d * np + k];
-                dk += jr * mom[d];
-                for (int e = 0; e < 3; ++e) dk += J.jacc[e][d * np + k] * mom[3 + d * 3 + e];
-            }
-        }
-        a.result[2 + k] = dk;
-    }
-}
-
-// Arrival at the end of a kernel: returns true in the last CTA to arrive (after
-// which every other CTA's global writes are visible to it).
-__device__ __forceinline__ bool last_to_arrive(unsigned int* counter) {
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (last) __threadfence();
-    return last;
-}
-
-__device__ __forceinline__ unsigned int load_acquire(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Grid-wide barrier of the fused kernel (a cooperative launch, so every CTA is
-// resident). Arrivals count up across the kernel: barrier k waits for k·gridDim.x.
-// The wait is bounded: after BARRIER_SPINS polls the CTA raises the error word and
-// every CTA that sees it leaves, so a launch that lost a CTA ends instead of hanging.
-constexpr unsigned int BARRIER_SPINS = 1u << 22;
-__device__ __forceinline__ bool grid_barrier(const EvalArgs& a, unsigned int k) {
-    __shared__ int ok;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned int* count = a.sync + 2;
-        unsigned int* err = error_word(a);
-        const unsigned int target = k * gridDim.x;
-        atomicAdd(count, 1u);
-        int good = 1;
-        unsigned int spins = 0;
-        while (load_acquire(count) < target) {
-            if (load_acquire(err) != 0u || ++spins > BARRIER_SPINS) {
-                good = 0;
-                break;
-            }
-            __nanosleep(64);
-        }
-        if (!good) atomicOr(err, 1u);
-        ok = good;
-    }
-    __syncthreads();
-    return ok != 0;
-}
 
 // ---------------------------------------------------------------------------
 // Kernels. The fused evaluation is one cooperative launch:
@@ -672,19 +60,19 @@ k_eval(SamplerParams P, JacobianForm J, EvalArgs a) {
     unsigned int* sh = reinterpret_cast<unsigned int*>(esh);
     double* dsh = reinterpret_cast<double*>(esh);
     const int B = P.bins;
-    hist_phase<DERIV>(P, a, sh);
+    hist_phase<DERIV>(P, a, sh, grid_samples(a.n));
     if (!grid_barrier(a, 1)) return;
     TailCtx t;
     if (DERIV) {
-        t = deriv_phase(P, a, dsh);
+        t = deriv_phase(P, a, dsh, grid_groups(a));
     } else {
         const TailSmem ts = tail_layout(B, esh);
         t = tail_prepare(B, P.moving_bin_size, a, ts);
-        if (!t.degenerate) value_slices_share(B, a, t, ts);
+        if (!t.degenerate) value_slices_share(B, a, t, ts, (int)blockIdx.x, (int)gridDim.x);
     }
     if (!last_to_arrive(a.sync)) return;
     // every CTA has left the barrier and is done with the histogram
-    if (DERIV) deriv_fold(P, J, a, t.degenerate);
+    if (DERIV) deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
     if (threadIdx.x < 32) fold_value(B, a, t);
     if (threadIdx.x == 0) {
         a.sync[0] = 0u;
@@ -697,7 +85,7 @@ template <bool RECORD>
 __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
 k_hist(SamplerParams P, EvalArgs a) {
     extern __shared__ unsigned int sh[];
-    hist_phase<RECORD>(P, a, sh);
+    hist_phase<RECORD>(P, a, sh, grid_samples(a.n));
 }
 
 // Value-only tail of the split form: one CTA.
@@ -706,7 +94,7 @@ k_tail(int B, double moving_bin_size, EvalArgs a) {
     extern __shared__ __align__(16) unsigned char tsh[];
     const TailSmem ts = tail_layout(B, tsh);
     const TailCtx t = tail_prepare(B, moving_bin_size, a, ts);
-    if (!t.degenerate) value_slices_share(B, a, t, ts);
+    if (!t.degenerate) value_slices_share(B, a, t, ts, (int)blockIdx.x, (int)gridDim.x);
     __syncthreads();
     if (threadIdx.x < 32) fold_value(B, a, t);
     for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) a.ghist[i] = 0ull;
@@ -716,9 +104,9 @@ k_tail(int B, double moving_bin_size, EvalArgs a) {
 __global__ void __launch_bounds__(DERIV_BLOCK)
 k_deriv(SamplerParams P, JacobianForm J, EvalArgs a) {
     extern __shared__ double dsh[];
-    const TailCtx t = deriv_phase(P, a, dsh);
+    const TailCtx t = deriv_phase(P, a, dsh, grid_groups(a));
     if (!last_to_arrive(a.sync)) return;
-    deriv_fold(P, J, a, t.degenerate);
+    deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
     if (threadIdx.x < 32) fold_value(P.bins, a, t);
     if (threadIdx.x == 0) a.sync[0] = 0u;
     for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
@@ -981,82 +369,11 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
     return MI_OK;
 }
 
-void mat3_mul(const double* a, const double* b, double* out) {
-    double t[9];
-    for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) t[r * 3 + c] = a[r * 3] * b[c] + a[r * 3 + 1] * b[3 + c] + a[r * 3 + 2] * b[6 + c];
-    std::memcpy(out, t, sizeof(t));
-}
-
-void mat3_vec(const double* a, const double* v, double* out) {
-    double t[3];
-    for (int r = 0; r < 3; ++r) t[r] = a[r * 3] * v[0] + a[r * 3 + 1] * v[1] + a[r * 3 + 2] * v[2];
-    std::memcpy(out, t, sizeof(t));
-}
-
-// Per-evaluation sampler constants: the stages, the composite map grid index →
-// continuous index, and a bound on how far that map can be from the exact chain.
+// Per-evaluation sampler constants: the stages and the composite map (point_map.h).
 mi_status fill_params(mi_metric* m, const double* stages, int nstage, SamplerParams& P) {
     P = m->base;
-    P.nstage = nstage;
-    for (int s = 0; s < nstage; ++s)
-        for (int i = 0; i < 12; ++i) P.stage[s][i] = stages[s * 12 + i];
-    // T(x) = MT·x + tT, the stages folded (for the fast path only; the exact chain
-    // replays them one by one)
-    double MT[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, tT[3] = {0, 0, 0};
-    for (int s = 0; s < nstage; ++s) {
-        const double* S = P.stage[s];
-        double nm[9], nt[3];
-        mat3_mul(S, MT, nm);
-        mat3_vec(S, tT, nt);
-        for (int d = 0; d < 3; ++d) nt[d] += S[9 + d];
-        std::memcpy(MT, nm, sizeof(nm));
-        std::memcpy(tT, nt, sizeof(nt));
-    }
-    double MTf[9], A[9], tmp[3], b[3];
-    mat3_mul(MT, P.fi2p, MTf);
-    mat3_mul(P.mp2i, MTf, A);
-    mat3_vec(MT, P.forigin, tmp);
-    for (int d = 0; d < 3; ++d) tmp[d] += tT[d] - P.morigin[d];
-    mat3_vec(P.mp2i, tmp, b);
-    for (int i = 0; i < 9; ++i) P.cA[i] = A[i];
-    for (int d = 0; d < 3; ++d) P.cb[d] = b[d];
-    // Magnitude bound of every intermediate of the exact chain, in moving voxels,
-    // over the fixed grid's corners; the chain's rounding is ≲ 20·2^-53 of it and
-    // cerr allows 2^-40 (≈ 400× margin).
-    double cmax = 0.0;
-    for (int corner = 0; corner < 8; ++corner) {
-        const double idx[3] = {(corner & 1) ? (double)(P.fsize0 - 1) : 0.0,
-                               (corner & 2) ? (double)(P.fsize1 - 1) : 0.0,
-                               (corner & 4) ? (double)(P.fsize2 - 1) : 0.0};
-        double mag[3];
-        for (int r = 0; r < 3; ++r)
-            mag[r] = std::fabs(P.forigin[r]) + std::fabs(P.fi2p[r * 3]) * idx[0] +
-                     std::fabs(P.fi2p[r * 3 + 1]) * idx[1] + std::fabs(P.fi2p[r * 3 + 2]) * idx[2];
-        for (int s = 0; s < nstage; ++s) {
-            const double* S = P.stage[s];
-            double nmag[3];
-            for (int r = 0; r < 3; ++r)
-                nmag[r] = std::fabs(S[r * 3]) * mag[0] + std::fabs(S[r * 3 + 1]) * mag[1] +
-                          std::fabs(S[r * 3 + 2]) * mag[2] + std::fabs(S[9 + r]);
-            std::memcpy(mag, nmag, sizeof(mag));
-        }
-        for (int r = 0; r < 3; ++r) mag[r] += std::fabs(P.morigin[r]);
-        for (int r = 0; r < 3; ++r) {
-            const double cm = std::fabs(P.mp2i[r * 3]) * mag[0] + std::fabs(P.mp2i[r * 3 + 1]) * mag[1] +
-                              std::fabs(P.mp2i[r * 3 + 2]) * mag[2];
-            cmax = std::max(cmax, cm);
-        }
-    }
-    if (!std::isfinite(cmax)) return set_error(m->ctx, MI_ERR_INVALID_ARGUMENT, "non-finite point map");
-    P.cerr = std::ldexp(1.0, -40) * (1.0 + cmax) * (double)(1 + nstage);
-    P.ilo = -0.5 + 2.0 * P.cerr;
-    P.olo = -0.5 - 2.0 * P.cerr;
-    for (int d = 0; d < 3; ++d) {
-        P.ihi[d] = P.mhi[d] - 2.0 * P.cerr;
-        P.ohi[d] = P.mhi[d] + 2.0 * P.cerr;
-    }
-    P.bin_hi = (double)(P.bins - PADDING - 1);
+    if (!point_map_fill(P, stages, nstage))
+        return set_error(m->ctx, MI_ERR_INVALID_ARGUMENT, "non-finite point map");
     return MI_OK;
 }
 

@@ -128,3 +128,87 @@ def register_multilevel(fixed: DeviceImage, moving: DeviceImage, transform: Para
         records.append(register_rsgd(metric, transform, iterations=iterations, **rsgd))
         metric.close()
     return MultiLevelResult(np.array(transform.params, dtype=np.float64), records)
+
+
+class BatchRegistration:
+    """Many registrations of uneven sizes advanced together on the device (mi_batch_*):
+    one pass of histogram, derivative and optimizer-step launches per iteration for
+    every still-active pair, replayed from a CUDA graph until all pairs have stopped.
+    Affine (centres given per pair) or translation family; one bin count, one
+    sampling rule per pair."""
+
+    def __init__(self, fixed_images, moving_images, bins: int = 50, kind: int = 0, centers=None,
+                 strategy: int | None = None, percentage: float = 1.0, seeds=None):
+        from .metric import SAMPLING_NONE
+        L = _lib.load()
+        if not getattr(L, "_batch_bound", False):
+            P = ctypes.POINTER
+            vp = ctypes.c_void_p
+            L.mi_batch_create.argtypes = [vp, ctypes.c_int, P(vp), P(vp), P(_lib.MiSampling), ctypes.c_int,
+                                          ctypes.c_int, P(ctypes.c_double), ctypes.c_int, P(vp)]
+            L.mi_batch_register.argtypes = [vp, P(MiRsgdConfig), ctypes.c_int, P(ctypes.c_double), P(MiRsgdResult)]
+            L.mi_batch_shape.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+            L.mi_batch_destroy.argtypes = [vp]
+            for f in ("mi_batch_create", "mi_batch_register", "mi_batch_shape", "mi_batch_destroy"):
+                getattr(L, f).restype = ctypes.c_int
+            L._batch_bound = True
+        n = len(fixed_images)
+        if len(moving_images) != n:
+            raise ValueError("one moving image per fixed image")
+        self.n = n
+        self.kind = kind
+        self.nparams = {0: 12, 3: 3}.get(kind)
+        if self.nparams is None:
+            raise ValueError("the batched form takes affine (0) or translation (3)")
+        self.ctx = fixed_images[0].ctx
+        fx = (ctypes.c_void_p * n)(*[f.handle for f in fixed_images])
+        mv = (ctypes.c_void_p * n)(*[m.handle for m in moving_images])
+        smp = None
+        if strategy is not None and strategy != SAMPLING_NONE:
+            seeds = seeds if seeds is not None else [0] * n
+            smp = (_lib.MiSampling * n)(*[_lib.MiSampling(strategy, float(percentage), int(s) & (2**64 - 1), None, 0)
+                                          for s in seeds])
+        fp = None
+        nfixed = 0
+        if kind == 0:
+            c = np.ascontiguousarray(centers, dtype=np.float64).reshape(n, 3)
+            self._centers = c
+            fp = c.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            nfixed = 3
+        h = ctypes.c_void_p()
+        _lib.check(L.mi_batch_create(self.ctx.handle, n, fx, mv, smp, int(bins), kind, fp, nfixed, ctypes.byref(h)),
+                   self.ctx.handle)
+        self.handle = h
+
+    def register(self, params, iterations: int = 100, minimum_step: float = 1e-4, gradient_tolerance: float = 1e-4,
+                 relaxation: float = 0.5, learning_rate: float | None = None, physical_shift_scales: bool = True,
+                 autotune: bool = True):
+        """Runs every pair from `params` (n × nparams); returns (params, [LevelResult])."""
+        p = np.ascontiguousarray(params, dtype=np.float64).reshape(self.n, self.nparams).copy()
+        cfg = MiRsgdConfig(int(iterations), float(minimum_step), float(gradient_tolerance), float(relaxation),
+                           1.0 if learning_rate is None else float(learning_rate),
+                           1 if learning_rate is None else 0, 1 if physical_shift_scales else 0, None, 0)
+        res = (MiRsgdResult * self.n)()
+        _lib.check(_lib.load().mi_batch_register(self.handle, ctypes.byref(cfg), 1 if autotune else 0,
+                                                 p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), res),
+                   self.ctx.handle)
+        out = [LevelResult(r.value, r.iterations, STOP_REASONS.get(r.stop_reason, str(r.stop_reason)), r.valid,
+                           r.evaluations) for r in res]
+        return p, out
+
+    def shape(self):
+        """(chunk size, histogram copies, chunk count) in use."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(_lib.load().mi_batch_shape(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().mi_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
