@@ -232,6 +232,64 @@ def time_registration(pair, ctx, dev):
             "tre_corners_mm": {"mean": float(np.mean(err)), "max": float(np.max(err))}}
 
 
+def time_batch(ctx, dev, seed: int):
+    """The batched workload: 64 affine pairs, edge n ~ U{48..192} per pair (seeded),
+    50 bins, 20 % random sampling, regular-step gradient descent (≤ 100 iterations)
+    from the identity, all pairs advanced together (mi_batch_*: CUDA-graph replay,
+    autotuned shape). Pairs are generated on the device (mi_synth_pair). Reported
+    beside the single-pair driver run pair by pair on the same pairs."""
+    import torch
+    import sitk_b200 as sb
+    from sitk_b200 import registration, synth
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = [int(v) for v in rng.integers(48, 193, size=64)]
+    fixed, moving = [], []
+    t0 = time.perf_counter()
+    for i, n in enumerate(sizes):
+        f, m, _ = synth.make_pair_device(n, 20, seed + i, 10.0, 5.0, (0.95, 1.05), ctx=ctx)
+        fixed.append(f)
+        moving.append(m)
+    torch.cuda.synchronize(dev)
+    gen_s = time.perf_counter() - t0
+    centers = [[(n - 1) / 2.0] * 3 for n in sizes]
+    start = np.tile(np.concatenate([np.eye(3).ravel(), np.zeros(3)]), (64, 1))
+    batch = registration.BatchRegistration(fixed, moving, bins=50, kind=0, centers=centers,
+                                           strategy=sb.SAMPLING_RANDOM, percentage=0.2,
+                                           seeds=[seed + i for i in range(64)])
+    t0 = time.perf_counter()
+    batch.register(start, iterations=100, autotune=True)  # first call: autotune + graph build
+    tune_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    params, res = batch.register(start, iterations=100, autotune=True)  # cached shape and graph
+    wall = time.perf_counter() - t0
+    chunk, copies, nchunks = batch.shape()
+    ev = np.array([r.evaluations for r in res], dtype=np.float64)
+    per_pair = ev * (wall / ev.max())
+    batch.close()
+    # the single-pair driver, pair after pair
+    plain = []
+    for i, n in enumerate(sizes):
+        metric = sb.DeviceMattesMetric.from_device_sampled(fixed[i], moving[i], bins=50, strategy=sb.SAMPLING_RANDOM,
+                                                           percentage=0.2, seed=seed + i)
+        t = sb.AffineTransform(np.eye(3), (0.0, 0.0, 0.0), centers[i])
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        registration.register_rsgd(metric, t, iterations=100)
+        plain.append(time.perf_counter() - t1)
+        metric.close()
+    for img in fixed + moving:
+        img.free()
+    return {"pairs": 64, "edge": [min(sizes), max(sizes)], "bins": 50, "sampling": "random 20%",
+            "samples_total": int(sum(int(0.2 * n ** 3) for n in sizes)),
+            "generate_s": gen_s, "first_call_s": tune_s, "wall_s": wall, "registrations_per_s": 64 / wall,
+            "per_pair_s": {"p50": float(np.percentile(per_pair, 50)), "p99": float(np.percentile(per_pair, 99))},
+            "evaluations": {"mean": float(ev.mean()), "max": int(ev.max())},
+            "shape": {"chunk": chunk, "copies": copies, "chunks": nchunks},
+            "single_pair_driver": {"wall_s": float(sum(plain)), "registrations_per_s": 64 / sum(plain),
+                                   "per_pair_s": {"p50": float(np.percentile(plain, 50)),
+                                                  "p99": float(np.percentile(plain, 99))}}}
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
     import sitk_b200 as sb
@@ -372,6 +430,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     clocks = sampler.summary() if sampler else None
     reg = None if args.no_registration else time_registration(pair, ctx, dev)
+    batch = None if args.no_batch else time_batch(ctx, dev, SEED)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True, "scaling": "weak",
@@ -395,6 +454,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "clocks": clocks,
         "result": {"value": last.value, "valid": last.valid_points},
         "registration": reg,
+        "batch": batch,
     }
     print(json.dumps(line), flush=True)
     if dist:
@@ -412,6 +472,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-registration", action="store_true",
                     help="skip the full three-level registration run reported beside the metric")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the 64-pair batched registration run reported beside the metric")
     ap.add_argument("--form", default="split", choices=["split", "fused"],
                     help="launch form of an evaluation: two kernels, or one cooperative kernel")
     ap.add_argument("--settle", type=float, default=1.0,

@@ -317,6 +317,19 @@ mi_status mi_batch_register(mi_batch* b, const mi_rsgd_config* cfg, int autotune
 mi_status mi_batch_shape(const mi_batch* b, int* chunk, int* copies, int* nchunks);
 mi_status mi_batch_destroy(mi_batch* b);
 
+/* ---- synthetic pairs (no reference counterpart) ------------------------------ */
+
+/* The counter-based synthetic registration pair built on the device (the CPU twin is
+ * sitk_b200/synth.py make_pair_counter): an n³ volume with unit spacing and zero
+ * origin, a ramp plus nblobs Gaussian blobs (blobs5: σ, amplitude, cx, cy, cz per
+ * blob, added in order inside their ±3.5σ boxes); fixed = volume + noise·N(0,1); moving
+ * = the noiseless volume resampled (trilinear, clamp-to-edge) at m·(x − c) + c + t
+ * (affine12: m row-major, then t; c the grid centre) + its own noise. The noise of
+ * voxel i is a function of (seed, field, i) only: SplitMix64-mixed counters, Box–Muller.
+ * Returns two new images. */
+mi_status mi_synth_pair(mi_context* ctx, int n, int nblobs, const double* blobs5, const double* affine12,
+                        uint64_t seed, double noise, mi_image** fixed, mi_image** moving);
+
 /* ---- allocation-free value (no counterpart in the reference) --------------- */
 
 /* Largest histogram the allocation-free entry point can hold. */
