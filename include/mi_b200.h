@@ -330,6 +330,15 @@ mi_status mi_batch_destroy(mi_batch* b);
 mi_status mi_synth_pair(mi_context* ctx, int n, int nblobs, const double* blobs5, const double* affine12,
                         uint64_t seed, double noise, mi_image** fixed, mi_image** moving);
 
+/* ---- learned initialiser (no reference counterpart) ------------------------- */
+
+/* C[M×N] (FP32, leading dimension ldc) = A[M×K]·B[N×K]ᵀ with A and B BF16, row-major,
+ * K contiguous (leading dimensions lda, ldb ≥ K): the tensor-core GEMM the
+ * initialiser's convolution-as-GEMM layers run on (tcgen05.mma, FP32 accumulation in
+ * tensor memory). All pointers are device memory; the call is synchronous. */
+mi_status mi_gemm_bf16_tn(mi_context* ctx, int M, int N, int K, const void* A, int lda, const void* B, int ldb,
+                          float* C, int ldc);
+
 /* ---- allocation-free value (no counterpart in the reference) --------------- */
 
 /* Largest histogram the allocation-free entry point can hold. */

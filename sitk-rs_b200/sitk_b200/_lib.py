@@ -32,7 +32,7 @@ EXPORTED = [
     "mi_metric_timing_read", "mi_metric_value_noalloc", "mi_register_rsgd",
     "mi_centered_initialize", "mi_metric_set_fused", "mi_metric_get_fused", "mi_image_smooth",
     "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level", "mi_batch_create", "mi_batch_register",
-    "mi_batch_shape", "mi_batch_destroy", "mi_synth_pair",
+    "mi_batch_shape", "mi_batch_destroy", "mi_synth_pair", "mi_gemm_bf16_tn",
 ]
 
 
