@@ -339,6 +339,36 @@ mi_status mi_synth_pair(mi_context* ctx, int n, int nblobs, const double* blobs5
 mi_status mi_gemm_bf16_tn(mi_context* ctx, int M, int N, int K, const void* A, int lda, const void* B, int ldb,
                           float* C, int ldc);
 
+/* The initialiser network: a 3-D convolutional encoder (2 → 16 → 32 → 64 → 128
+ * channels, 3³ kernels, stride 2, padding 1, ReLU; 32³ → 2³) and an MLP head (1024 →
+ * 256 ReLU → 12) that maps a fixed/moving pair resampled to 32³ onto 12 normalised
+ * affine parameters. Every layer runs on the tensor-core GEMM (BF16 operands, FP32
+ * accumulation); master weights and Adam moments are FP32. Layers are numbered 0–3
+ * (convolutions; W is out × 27·in with column ((kz·3 + ky)·3 + kx)·in + c), 4 and 5
+ * (fully connected; W is out × in, fc1's input index ((z·2 + y)·2 + x)·128 + c).
+ * Network inputs are device arrays of B × 32³ × 2 FP32, channels last (x fastest
+ * over the grid, then the two channels per voxel: fixed, moving). */
+typedef struct mi_initnet mi_initnet;
+
+/* Weights He-uniform from a SplitMix64 stream keyed by seed (the last layer scaled by
+ * 0.1), biases 0; buffers for batches of up to max_batch pairs. */
+mi_status mi_initnet_create(mi_context* ctx, uint64_t seed, int max_batch, mi_initnet** out);
+mi_status mi_initnet_destroy(mi_initnet* net);
+/* Copies layer `which`'s weights (out × in, row-major) and bias out — or, with grads
+ * != 0, the gradients of the last training step. Either pointer may be NULL. */
+mi_status mi_initnet_get(mi_initnet* net, int which, int grads, float* w, float* b);
+mi_status mi_initnet_set(mi_initnet* net, int which, const float* w, const float* b);
+/* out (device, B × 12) = the network on x (device, B × 32³ × 2). */
+mi_status mi_initnet_forward(mi_initnet* net, int batch, const float* x, float* out);
+/* Forward, mean squared error against target (device, B × 12), backward; then one
+ * Adam step (β1 0.9, β2 0.999, ε 1e-8) when lr > 0. loss (host) may be NULL. */
+mi_status mi_initnet_train_step(mi_initnet* net, int batch, const float* x, const float* target, float lr,
+                                float* loss);
+/* One pair's network input (device, 32³ × 2): fixed and moving resampled (linear, fill
+ * 0) onto the 32³ grid with the fixed image's centre and direction and spacing ·
+ * size / 32, each normalised to zero mean and unit variance. */
+mi_status mi_initnet_prepare(mi_context* ctx, const mi_image* fixed, const mi_image* moving, float* out);
+
 /* ---- allocation-free value (no counterpart in the reference) --------------- */
 
 /* Largest histogram the allocation-free entry point can hold. */

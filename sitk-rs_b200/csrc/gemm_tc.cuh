@@ -108,8 +108,13 @@ k_gemm_tn(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda, con
     uint32_t phase = 0;
     bool ok = true;
 
+    // split K: slice blockIdx.z of gridDim.z covers k tiles [kt0, kt1) and writes its
+    // partial product to the blockIdx.z-th M × ldc block of C
     const int ktiles = (K + TILE_K - 1) / TILE_K;
-    for (int kt = 0; kt < ktiles && ok; ++kt) {  // `ok` is uniform over the CTA
+    const int per = (ktiles + (int)gridDim.z - 1) / (int)gridDim.z;
+    const int kt0 = (int)blockIdx.z * per, kt1 = min(ktiles, kt0 + per);
+    C += (size_t)blockIdx.z * (size_t)M * (size_t)ldc;
+    for (int kt = kt0; kt < kt1 && ok; ++kt) {  // `ok` is uniform over the CTA
         load_tile<TILE_M>(A, lda, M, K, m0, kt * TILE_K, As);
         load_tile<NT>(B, ldb, N, K, n0, kt * TILE_K, Bs);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -121,7 +126,7 @@ k_gemm_tn(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda, con
                 // k step s reads k chunks 2s and 2s + 1: 256 bytes further per step
                 const uint64_t ad = smem_desc(a_addr + s * 256, 128, 1024);
                 const uint64_t bd = smem_desc(b_addr + s * 256, 128, 1024);
-                const uint32_t acc = (kt > 0 || s > 0) ? 1u : 0u;
+                const uint32_t acc = (kt > kt0 || s > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
@@ -169,7 +174,8 @@ k_gemm_tn(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda, con
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const int col = n0 + c0 + j;
-                    if (col < N) C[(size_t)row * ldc + col] = __uint_as_float(r[j]);
+                    // an empty K slice wrote no accumulator: its partial product is 0
+                    if (col < N) C[(size_t)row * ldc + col] = kt1 > kt0 ? __uint_as_float(r[j]) : 0.0f;
                 }
             }
         }
