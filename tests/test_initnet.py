@@ -182,3 +182,25 @@ def test_initnet_prepare_matches_oracle_resample(oracle_lib):
         r = oracle.resample_linear(vol, gi, go).astype(np.float64)
         r = (r - r.mean()) / r.std()
         assert np.max(np.abs(x[..., ch] - r)) < 1e-4
+
+
+def test_trained_initialiser_beats_centred_start():
+    """A network trained on 1,024 labelled 64³ pairs (rotation ±20°, translation
+    ±10 mm, scale 0.9–1.1): refined proposals reach the plain run's final metric value
+    within 1e-3 on nearly every held-out pair, in fewer optimizer iterations, and land
+    within 1 mm of the truth at least as often as the centred start does."""
+    from sitk_b200 import initnet as I
+    spec = I.PairSpec(n=64, nblobs=20, rot_deg=20.0, trans_mm=10.0)
+    run = I.PlainRun(bins=32, percentage=0.2, iterations=200)
+    data = I.labelled_set(range(100, 1124), spec, run)
+    # the labels are the metric's optimum next to the generating affine
+    c = [31.5] * 3
+    assert np.median([I.target_error(l, t, c, 19.2) for l, t in zip(data["labels"], data["truth"])]) < 0.5
+    net = I.InitNet(seed=2, max_batch=64)
+    losses, _ = I.train(net, data["x"], data["labels"], epochs=10)
+    assert losses[-1] < 0.5 * losses[0]
+    ev = I.evaluate(net, range(500000, 500064), spec, run, single_pairs=2)
+    assert ev["accepted"] >= 0.9, ev
+    assert ev["iterations"]["learned"]["mean"] < ev["iterations"]["plain"]["mean"], ev
+    assert ev["within_1mm"]["learned"] >= ev["within_1mm"]["plain"], ev
+    net.close()
