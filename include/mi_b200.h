@@ -4,8 +4,7 @@
  * This is the drop-in boundary for the device metric seam of sitk-rs (crate `sitk`,
  * paths below are inside crates/sitk/src/). Every entry point takes plain pointers
  * and sizes and returns an mi_status; nothing here names a C++ or torch type, so a
- * Rust `extern "C"` block, ctypes or cgo can bind it as-is (INTEGRATION.md shows
- * the Rust and ctypes bindings).
+ * Rust `extern "C"` block, ctypes or cgo can bind it as-is.
  *
  * Threading: a handle (context, image, metric) must not be used from two host
  * threads at once without external locking. The reference serialises its device
@@ -43,7 +42,7 @@ typedef enum {
     MI_ERR_MASK_SIZE_MISMATCH = 11,   /* RegistrationError::MaskSizeMismatch */
     MI_ERR_NON_AFFINE_TRANSFORM = 12, /* DeviceMetricError::NonAffineTransform */
     MI_ERR_POINT_MAP_STAGE_COUNT = 13,/* CudaError::PointMapStageCount (more than MI_MAX_STAGES) */
-    MI_ERR_TOO_MANY_HISTOGRAM_BINS = 14, /* bins > MI_MAX_BINS: no reference counterpart */
+    MI_ERR_TOO_MANY_HISTOGRAM_BINS = 14, /* bins > MI_MAX_BINS (the shared-memory histogram's limit): no reference counterpart */
     MI_ERR_TIMEOUT = 15,              /* a bounded device wait gave up (fused form's grid barrier) */
     MI_ERR_NOT_CONVERGED = 16         /* reserved */
 } mi_status;
@@ -141,6 +140,23 @@ mi_status mi_image_free(mi_image* img);
 mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_image* moving,
                            const mi_image* fixed_mask, const uint8_t* moving_mask,
                            const mi_sampling* sampling, int bins, mi_metric** out);
+
+/* How the metric stores the moving volume it samples (no reference counterpart: the
+ * reference widens it to f64, resident.rs:406-417). MI_STORAGE_BF16 rounds every
+ * voxel to BF16 (to nearest, ties to even) once at creation; the range, the bins and
+ * every interpolation then use the rounded values, exactly as an f32 volume holding
+ * them would, and the corner gathers move half the bytes. */
+#define MI_STORAGE_F32 0
+#define MI_STORAGE_BF16 1
+typedef struct mi_metric_options {
+    int moving_storage; /* MI_STORAGE_F32 (default) or MI_STORAGE_BF16 */
+} mi_metric_options;
+
+/* mi_metric_create with options (NULL: the defaults). */
+mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_image* moving,
+                              const mi_image* fixed_mask, const uint8_t* moving_mask,
+                              const mi_sampling* sampling, int bins, const mi_metric_options* options,
+                              mi_metric** out);
 mi_status mi_metric_info_get(const mi_metric* m, mi_metric_info* out);
 mi_status mi_metric_destroy(mi_metric* m);
 

@@ -63,6 +63,7 @@ struct SamplerParams {
     int msz[3];      // moving size, 32-bit (the volume is below 2^32 voxels)
     uint32_t ms1, ms2;  // moving strides, 32-bit
     cudaTextureObject_t mtex;  // the moving volume as a 3-D texture (point, clamp, unnormalised)
+    int mbf16;                 // the texture holds BF16 bits (u16), widened exactly on fetch
     double inv_moving_bin_size;
     // point map stages (matrix_offset.rs:102-109)
     int nstage;

@@ -20,11 +20,13 @@
 // Every reduction order is a function of the launch shape alone, so repeated
 // evaluations are bit-identical. No kernel waits on another CTA.
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_select.cuh>
 
 #include <algorithm>
+
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -159,6 +161,16 @@ __global__ void k_mask_flags(const uint32_t* __restrict__ idx, int64_t count, co
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
         flags[i] = fmask[idx[i]] != 0.0f ? 1 : 0;
+}
+
+// v ← v rounded to BF16 (to nearest, ties to even; NaN stays NaN), bits[i] its upper
+// 16 bits
+__global__ void k_round_bf16(float* __restrict__ v, int64_t n, uint16_t* __restrict__ bits) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint16_t b = __bfloat16_as_ushort(__float2bfloat16_rn(v[i]));
+        bits[i] = b;
+        v[i] = __uint_as_float((uint32_t)b << 16);
+    }
 }
 
 // min/max over the selected fixed samples (or all voxels) and over the moving voxels
@@ -502,8 +514,17 @@ extern "C" {
 
 mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_image* moving, const mi_image* fixed_mask,
                            const uint8_t* moving_mask, const mi_sampling* sampling, int bins, mi_metric** out) {
+    return mi_metric_create_ex(ctx, fixed, moving, fixed_mask, moving_mask, sampling, bins, nullptr, out);
+}
+
+mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_image* moving,
+                              const mi_image* fixed_mask, const uint8_t* moving_mask, const mi_sampling* sampling,
+                              int bins, const mi_metric_options* options, mi_metric** out) {
     using namespace mi;
     if (!ctx || !fixed || !moving || !out) return MI_ERR_INVALID_ARGUMENT;
+    const int storage = options ? options->moving_storage : MI_STORAGE_F32;
+    if (storage != MI_STORAGE_F32 && storage != MI_STORAGE_BF16)
+        return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "moving_storage must be MI_STORAGE_F32 or MI_STORAGE_BF16");
     *out = nullptr;
     if (fixed->ctx != ctx || moving->ctx != ctx || (fixed_mask && fixed_mask->ctx != ctx))
         return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "images belong to another context");
@@ -536,8 +557,10 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     m->mgeo = moving->geo;
     m->bins = bins;
     cudaStream_t st = ctx->stream;
+    uint16_t* mbits = nullptr;  // BF16 storage: the rounded volume's bits, for the texture
     auto fail = [&](mi_status s) {
         cudaStreamSynchronize(st);
+        cudaFree(mbits);
         free_metric(m);
         return s;
     };
@@ -550,6 +573,13 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     TRY_CUDA(cudaMalloc(&m->moving, (size_t)mvox * 4));
     TRY_CUDA(cudaMemcpyAsync(m->fixed, fixed->data, (size_t)nvox * 4, cudaMemcpyDeviceToDevice, st));
     TRY_CUDA(cudaMemcpyAsync(m->moving, moving->data, (size_t)mvox * 4, cudaMemcpyDeviceToDevice, st));
+    if (storage == MI_STORAGE_BF16) {
+        // the metric sees the volume rounded to BF16 everywhere: the range, the exact
+        // fallback's copy (the widened values) and the texture (the bits)
+        TRY_CUDA(cudaMalloc(&mbits, (size_t)mvox * 2));
+        k_round_bf16<<<grid_for(mvox, 256, ctx->num_sms * 8), 256, 0, st>>>(m->moving, mvox, mbits);
+        TRY_CUDA(cudaGetLastError());
+    }
     if (moving_mask) {
         TRY_CUDA(cudaMalloc(&m->mmask, (size_t)mvox));
         TRY_CUDA(cudaMemcpyAsync(m->mmask, moving_mask, (size_t)mvox, cudaMemcpyHostToDevice, st));
@@ -607,17 +637,26 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
     {
         // the moving volume as a block-linear 3-D array behind a point-sampling,
         // clamp-to-edge, unnormalised-coordinate texture (the fast path's corner fetch)
-        const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float>();
+        const bool b16 = storage == MI_STORAGE_BF16;
+        const cudaChannelFormatDesc fmt = b16 ? cudaCreateChannelDesc<unsigned short>() : cudaCreateChannelDesc<float>();
+        const size_t esize = b16 ? 2 : 4;
         const cudaExtent ext = make_cudaExtent((size_t)moving->geo.size[0], (size_t)moving->geo.size[1],
                                                (size_t)moving->geo.size[2]);
         TRY_CUDA(cudaMalloc3DArray(&m->marray, &fmt, ext));
         cudaMemcpy3DParms cp = {};
-        cp.srcPtr = make_cudaPitchedPtr(m->moving, (size_t)moving->geo.size[0] * sizeof(float),
+        cp.srcPtr = make_cudaPitchedPtr(b16 ? (void*)mbits : (void*)m->moving, (size_t)moving->geo.size[0] * esize,
                                         (size_t)moving->geo.size[0], (size_t)moving->geo.size[1]);
         cp.dstArray = m->marray;
         cp.extent = ext;
         cp.kind = cudaMemcpyDeviceToDevice;
-        TRY_CUDA(cudaMemcpy3DAsync(&cp, st));
+        const cudaError_t ce = cudaMemcpy3DAsync(&cp, st);
+        if (mbits) {
+            cudaStreamSynchronize(st);
+            cudaFree(mbits);
+            mbits = nullptr;
+        }
+        TRY_CUDA(ce);
+        P.mbf16 = b16 ? 1 : 0;
         cudaResourceDesc res = {};
         res.resType = cudaResourceTypeArray;
         res.res.array.array = m->marray;

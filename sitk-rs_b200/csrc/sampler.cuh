@@ -248,14 +248,16 @@ __device__ __forceinline__ void prep(const SamplerParams& P, uint32_t flat, cons
     cx[1] = cx[0] + 1.0f;
     cy[1] = cy[0] + 1.0f;
     cz[1] = cz[0] + 1.0f;
-    p.v[0] = tex3D<float>(P.mtex, cx[0], cy[0], cz[0]);
-    p.v[1] = tex3D<float>(P.mtex, cx[1], cy[0], cz[0]);
-    p.v[2] = tex3D<float>(P.mtex, cx[0], cy[1], cz[0]);
-    p.v[3] = tex3D<float>(P.mtex, cx[1], cy[1], cz[0]);
-    p.v[4] = tex3D<float>(P.mtex, cx[0], cy[0], cz[1]);
-    p.v[5] = tex3D<float>(P.mtex, cx[1], cy[0], cz[1]);
-    p.v[6] = tex3D<float>(P.mtex, cx[0], cy[1], cz[1]);
-    p.v[7] = tex3D<float>(P.mtex, cx[1], cy[1], cz[1]);
+    if (P.mbf16) {
+        // BF16 storage: the upper half of an f32, so the widening is exact
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+            p.v[t] = __uint_as_float((uint32_t)tex3D<unsigned short>(P.mtex, cx[t & 1], cy[(t >> 1) & 1], cz[t >> 2])
+                                     << 16);
+    } else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) p.v[t] = tex3D<float>(P.mtex, cx[t & 1], cy[(t >> 1) & 1], cz[t >> 2]);
+    }
     p.ok = true;
 }
 

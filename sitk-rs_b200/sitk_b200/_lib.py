@@ -34,7 +34,7 @@ EXPORTED = [
     "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level", "mi_batch_create", "mi_batch_register",
     "mi_batch_shape", "mi_batch_destroy", "mi_synth_pair", "mi_gemm_bf16_tn", "mi_initnet_create",
     "mi_initnet_destroy", "mi_initnet_get", "mi_initnet_set", "mi_initnet_forward", "mi_initnet_train_step",
-    "mi_initnet_prepare",
+    "mi_initnet_prepare", "mi_metric_create_ex",
 ]
 
 
@@ -100,6 +100,9 @@ def load(path: str | None = None):
     L.mi_image_device_ptr.restype = vp
     L.mi_image_free.argtypes = [vp]
     L.mi_metric_create.argtypes = [vp, vp, vp, vp, P(ctypes.c_uint8), P(MiSampling), ctypes.c_int, P(vp)]
+    L.mi_metric_create_ex.argtypes = [vp, vp, vp, vp, P(ctypes.c_uint8), P(MiSampling), ctypes.c_int,
+                                      P(ctypes.c_int), P(vp)]
+    L.mi_metric_create_ex.restype = ctypes.c_int
     L.mi_metric_info_get.argtypes = [vp, P(MiMetricInfo)]
     L.mi_metric_destroy.argtypes = [vp]
     L.mi_metric_value.argtypes = [vp, dp, ctypes.c_int, dp, i64p]

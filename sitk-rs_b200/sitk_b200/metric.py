@@ -178,10 +178,15 @@ class DeviceMattesMetric:
     @classmethod
     def from_device_sampled(cls, fixed: DeviceImage, moving: DeviceImage, fixed_mask=None,
                             moving_mask=None, samples=None, bins: int = 50, *,
-                            strategy: int | None = None, percentage: float = 1.0, seed: int = 0):
+                            strategy: int | None = None, percentage: float = 1.0, seed: int = 0,
+                            moving_storage: str = "f32"):
         """`samples` is an explicit flat-index list (FixedSamples::selected_indices);
         alternatively `strategy`/`percentage`/`seed` draw on the device exactly as
-        draw_samples does (registration/metric.rs:419-437)."""
+        draw_samples does (registration/metric.rs:419-437). `moving_storage` "bf16"
+        keeps the moving volume rounded to BF16 (mi_metric_create_ex)."""
+        storage = {"f32": 0, "bf16": 1}.get(moving_storage)
+        if storage is None:
+            raise ValueError("moving_storage is 'f32' or 'bf16'")
         ctx = fixed.ctx
         smp = None
         keep = []
@@ -204,10 +209,11 @@ class DeviceMattesMetric:
                 keep.append(fmi)
                 fm_handle = fmi.handle
         h = ctypes.c_void_p()
-        _lib.check(_lib.load().mi_metric_create(
+        opts = ctypes.c_int(storage)  # mi_metric_options{moving_storage}
+        _lib.check(_lib.load().mi_metric_create_ex(
             ctx.handle, fixed.handle, moving.handle, fm_handle,
             None if mm is None else mm.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
-            None if smp is None else ctypes.byref(smp), int(bins), ctypes.byref(h)), ctx.handle)
+            None if smp is None else ctypes.byref(smp), int(bins), ctypes.byref(opts), ctypes.byref(h)), ctx.handle)
         return cls(h, ctx)
 
     def info(self) -> dict:

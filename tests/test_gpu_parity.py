@@ -32,10 +32,22 @@ def _oracle_geo(oracle, n, spacing, origin):
     return oracle.make_geometry((n, n, n), spacing=spacing, origin=origin)
 
 
+def bf16_round(v):
+    """f32 → nearest BF16 (ties to even), widened back to f32 (finite inputs)."""
+    b = np.ascontiguousarray(v, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).reshape(np.shape(v))
+
+
 def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
-             strategy=None, pct=1.0, seed=0, mmask=None, fmask=None, explicit=None):
+             strategy=None, pct=1.0, seed=0, mmask=None, fmask=None, explicit=None, moving_storage="f32"):
+    """With moving_storage "bf16" the oracle runs on the moving volume rounded to BF16
+    (the values the device metric samples), so the same exact contract applies."""
     sb = _sb()
     f, m = _upload_pair(p, spacing, origin)
+    if moving_storage == "bf16":
+        import dataclasses
+        p = dataclasses.replace(p, moving=bf16_round(p.moving))
     kw = {}
     draw = None
     if explicit is not None:
@@ -44,7 +56,7 @@ def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0
         draw = oracle.draw_samples(n ** 3, strategy, pct, seed)
     metric = sb.DeviceMattesMetric.from_device_sampled(
         f, m, fixed_mask=fmask, moving_mask=mmask, samples=explicit, bins=bins,
-        strategy=strategy, percentage=pct, seed=seed)
+        strategy=strategy, percentage=pct, seed=seed, moving_storage=moving_storage)
     g = _oracle_geo(oracle, n, spacing, origin)
     ref = oracle.evaluate(p.fixed, g, p.moving, g, bins, transform.kind, transform.params,
                           transform.fixed_params, fmask=fmask, mmask=mmask, draw=draw,
@@ -250,3 +262,21 @@ def test_two_stage_point_map(oracle_lib):
     dec = metric.sample_decisions(np.concatenate([s1, s2]))
     assert n2 == int((dec["status"] == 2).sum())
     assert np.isfinite(v2)
+
+
+def test_bf16_moving_storage_euler_64_bins(oracle_lib):
+    """The large-volume form at reduced size (Euler3D, 64 bins, 20 % random sampling)
+    with the moving volume stored as BF16: exact decisions and the usual tolerances
+    against the oracle on the rounded volume; the storage error itself (against the
+    oracle on the f32 volume) is a property of BF16, bounded loosely here."""
+    sb = _sb()
+    p = small_pair(n=96, seed=33, nblobs=24, rot=10.0, trans=5.0, scale=None)
+    c = [47.5] * 3
+    t = sb.Euler3DTransform((0.04, -0.03, 0.06), (1.1, -0.8, 0.5), c)
+    draw = oracle_lib.draw_samples(96 ** 3, 2, 0.2, 7)
+    _, mv, ref_b, _ = _compare(oracle_lib, p, 96, t, 64, strategy=2, pct=0.2, seed=7, moving_storage="bf16")
+    g = _oracle_geo(oracle_lib, 96, (1.0, 1.0, 1.0), (0.0, 0.0, 0.0))
+    ref_f = oracle_lib.evaluate(p.fixed, g, p.moving, g, 64, t.kind, t.params, t.fixed_params, draw=draw)
+    assert abs(mv.value - ref_f["value"]) <= 1e-2 * abs(ref_f["value"])
+    scale = np.max(np.abs(ref_f["derivative"]))
+    assert np.max(np.abs(mv.derivative - ref_f["derivative"])) <= 0.1 * scale
