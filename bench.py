@@ -116,7 +116,7 @@ def _peaks():
 
 def _kernel_source_hash() -> str:
     h = hashlib.sha256()
-    for name in ("sampler.cuh", "mattes.cu"):
+    for name in ("sampler.cuh", "eval_device.cuh", "mattes.cu"):
         with open(os.path.join(ROOT, "sitk-rs_b200", "csrc", name), "rb") as f:
             h.update(f.read())
     return h.hexdigest()[:16]
@@ -509,6 +509,109 @@ def run_initnet(args, rank: int, world: int, local_rank: int):
     return 0
 
 
+def bf16_round(v):
+    """f32 → nearest BF16 (ties to even), widened back to f32 (finite inputs)."""
+    b = np.ascontiguousarray(v, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).reshape(np.shape(v))
+
+
+def run_storage_study(args, rank: int, world: int, local_rank: int):
+    """The large-volume case: n³ (default 512³) f32 blob pair (120 blobs, rotation
+    ±10°, translation ±5 mm), Euler3D, 64 bins, 20 % random sampling. The metric runs
+    with the moving volume stored as f32 and as BF16; each is timed (device events,
+    L2 flushed before every evaluation) and compared with the FP64 oracle on the f32
+    volumes (the storage error) — and the BF16 form also with the oracle on the
+    rounded volume (the parity contract). One GPU; other ranks exit."""
+    import torch
+
+    import sitk_b200 as sb
+    from sitk_b200 import synth
+    from sitk_b200.metric import enable_timing, read_timing
+    if rank != 0:
+        return 0
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    ctx = sb.Context(dev)
+    n = args.storage_n
+    bins, pct = 64, 0.2
+    f, m, _ = synth.make_pair_device(n, 120, SEED + 3, 10.0, 5.0, None, ctx=ctx)
+    c = [(n - 1) / 2.0] * 3
+    t = sb.Euler3DTransform((0.02, -0.015, 0.03), (0.8, -0.6, 0.4), c)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    l2 = torch.cuda.get_device_properties(dev).L2_cache_size
+    nflush = max(2 * l2, 256 << 20) // 4
+    flush_w = torch.empty(nflush, dtype=torch.float32, device=f"cuda:{dev}")
+    flush_r = torch.zeros(nflush, dtype=torch.float32, device=f"cuda:{dev}")
+    peak, peak_kind = _peaks()
+    runs = {}
+    for storage in ("f32", "bf16"):
+        metric = sb.DeviceMattesMetric.from_device_sampled(f, m, bins=bins, strategy=sb.SAMPLING_RANDOM,
+                                                           percentage=pct, seed=SEED, moving_storage=storage)
+        S = int(metric.info()["n_samples"])
+        for _ in range(3):
+            metric.evaluate(t)
+        enable_timing(metric, True, per_kernel=True)
+        read_timing(metric)
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush_w.zero_()
+                torch.sum(flush_r)
+            mv = metric.evaluate(t)
+        torch.cuda.synchronize(dev)
+        ms, nev = read_timing(metric)
+        enable_timing(metric, False)
+        b_m = 4 if storage == "f32" else 2
+        pass_bytes = S * 4 + min(n ** 3, 8 * S) * b_m
+        k_hist = ms[1] / nev
+        runs[storage] = {"value": mv.value, "derivative": [float(x) for x in mv.derivative],
+                         "valid": mv.valid_points, "ms_per_eval": ms[0] / nev, "evals_per_s": nev / (ms[0] / 1e3),
+                         "kernel_ms": {"k_hist": k_hist, "k_deriv": ms[2] / nev},
+                         "roofline_k_hist": {"bytes_alg": pass_bytes,
+                                             "achieved_gbs": pass_bytes / (k_hist / 1e3) / 1e9,
+                                             "frac": pass_bytes / (k_hist / 1e3) / 1e9 / peak}}
+        metric.close()
+    fixed_h = f.to_host()
+    moving_h = m.to_host()
+    f.free()
+    m.free()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    g = oracle.make_geometry((n, n, n))
+    draw = oracle.draw_samples(n ** 3, 2, pct, SEED)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ref = oracle.evaluate(fixed_h, g, moving_h, g, bins, t.kind, t.params, t.fixed_params, draw=draw, nthreads=cores)
+    oracle_s = time.perf_counter() - t0
+    ref_b = oracle.evaluate(fixed_h, g, bf16_round(moving_h), g, bins, t.kind, t.params, t.fixed_params, draw=draw,
+                            nthreads=cores)
+
+    def err(run, r):
+        d = np.asarray(run["derivative"])
+        rd = np.asarray(r["derivative"])
+        return {"value_rel": abs(run["value"] - r["value"]) / abs(r["value"]),
+                "derivative_max_abs_over_max": float(np.max(np.abs(d - rd)) / np.max(np.abs(rd))),
+                "valid_equal": run["valid"] == r["valid"]}
+
+    line = {
+        "metric": "MI value+derivative evals/sec, moving volume stored f32 and bf16",
+        "value": runs["bf16"]["evals_per_s"], "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": 3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (bf16 storage)",
+        "data": "synthetic",
+        "config": {"workload": f"{n}^3 f32 blob pair, Euler3D, 64 bins, 20% random sampling, value+derivative",
+                   "samples": int(draw.size), "l2": "flushed before every evaluation"},
+        "runs": runs,
+        "error_vs_fp64_oracle_on_f32_volumes": {"f32": err(runs["f32"], ref), "bf16": err(runs["bf16"], ref)},
+        "bf16_vs_oracle_on_rounded_volume": err(runs["bf16"], ref_b),
+        "oracle": {"value": ref["value"], "derivative": [float(x) for x in ref["derivative"]],
+                   "seconds": oracle_s, "threads": cores},
+        "peak": {"hbm_gbs": peak, "source": peak_kind},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -531,6 +634,9 @@ def main():
     ap.add_argument("--initnet-test", type=int, default=512)
     ap.add_argument("--initnet-epochs", type=int, default=20)
     ap.add_argument("--initnet-single", type=int, default=32)
+    ap.add_argument("--storage-study", action="store_true",
+                    help="run the f32/bf16 moving-storage study (512^3) instead of the metric benchmark")
+    ap.add_argument("--storage-n", type=int, default=512)
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
@@ -539,6 +645,8 @@ def main():
         return run_reference(args, rank, world)
     if args.initnet:
         return run_initnet(args, rank, world, local_rank)
+    if args.storage_study:
+        return run_storage_study(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 
