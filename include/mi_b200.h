@@ -148,8 +148,27 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
  * them would, and the corner gathers move half the bytes. */
 #define MI_STORAGE_F32 0
 #define MI_STORAGE_BF16 1
+
+/* Which metric a handle evaluates. The Mattes metric is the default; mean squares
+ * and normalised cross-correlation are the reference's other device metrics
+ * (registration/device.rs:203-620 DeviceMeanSquaresMetric, DeviceCorrelationMetric)
+ * over the same sample set, masks and sampler, behind the same value / derivative
+ * entry points:
+ *   mean squares: value = Σ(m − f)²/count, derivative = +∂value/∂p
+ *   correlation:  value = −sfm²/(sff·smm) over mean-subtracted samples, derivative
+ *                 = +∂value/∂p; a degenerate sample set (m2·f2 ≤ DBL_EPSILON)
+ *                 gives DBL_MAX and a zero derivative.
+ * No valid sample gives DBL_MAX for every metric. `bins` is ignored for these two,
+ * and they refuse no constant image (the reference does not). mi_metric_info_get
+ * reports bins = 0 and only the sample count for them. The Mattes-only hooks
+ * (mi_metric_sample_decisions, mi_metric_set_fused) refuse them. */
+#define MI_METRIC_MATTES 0
+#define MI_METRIC_MEAN_SQUARES 1
+#define MI_METRIC_CORRELATION 2
+
 typedef struct mi_metric_options {
     int moving_storage; /* MI_STORAGE_F32 (default) or MI_STORAGE_BF16 */
+    int metric;         /* MI_METRIC_MATTES (default), MI_METRIC_MEAN_SQUARES, MI_METRIC_CORRELATION */
 } mi_metric_options;
 
 /* mi_metric_create with options (NULL: the defaults). */

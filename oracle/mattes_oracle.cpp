@@ -899,4 +899,139 @@ int64_t or_round_half_integer_up(double x) { return (int64_t)std::floor(x + 0.5)
 
 int or_invert3(const double* m, double* inv) { return invert3(m, inv) ? OR_OK : OR_SINGULAR_DIRECTION; }
 
+// ---------------------------------------------------------------------------
+// The shared-sampler siblings of the Mattes metric, over the same Problem (sample
+// set, masks, moving image) and the same per-sample sampler (moving_value_grad).
+// ---------------------------------------------------------------------------
+
+// Mean squares: CpuBackend::mean_squares, dense branch (registration/metric.rs:1064-
+// 1160), and mean_squares_value (:1162-1196) when want_derivative is 0. Per valid
+// sample, in sample order: diff = mv − f; value_sum += diff²; for each parameter k,
+// deriv[k] += 2·diff·(Σ_d ∇M[d]·J[d][k]) (the Σ from 0.0, d ascending). Then both
+// are scaled by 1/valid; no valid sample gives f64::MAX and a zero derivative.
+int or_ms_evaluate(const float* fixed, const or_geometry* fg, const float* moving, const or_geometry* mg,
+                   const uint8_t* fmask, const uint8_t* mmask, const int64_t* draw, int64_t ndraw, int kind,
+                   const double* params, const double* fixed_params, int nfixed, int want_derivative,
+                   double* value, double* deriv, int64_t* valid) {
+    Problem P;
+    int st = prepare(fixed, fg, moving, mg, fmask, mmask, draw, ndraw, P);
+    if (st) return st;
+    Transform T;
+    if (!make_transform(kind, params, fixed_params, nfixed, T)) return OR_BAD_ARGUMENT;
+    const int np = T.nparams;
+    const bool wd = want_derivative != 0;
+    double value_sum = 0.0;
+    std::vector<double> d(np, 0.0);
+    int64_t nv = 0;
+    double jac[36];
+    for (int64_t s = 0; s < P.n; ++s) {
+        const int64_t flat = sample_flat(P, s);
+        double fp[3], mp[3], mv, g[3];
+        grid_point(P, flat, fp);
+        T.transform_point(fp, mp);
+        if (!moving_value_grad(P, mp, &mv, g, wd)) continue;
+        const double diff = mv - (double)P.fixed[flat];
+        value_sum += diff * diff;
+        if (wd) {
+            T.jacobian(fp, jac);
+            for (int k = 0; k < np; ++k) {
+                double gk = 0.0;
+                for (int q = 0; q < 3; ++q) gk += g[q] * jac[q * np + k];
+                d[k] += 2.0 * diff * gk;
+            }
+        }
+        nv += 1;
+    }
+    *valid = nv;
+    if (nv == 0) {
+        *value = DBL_MAX;
+        if (wd) for (int k = 0; k < np; ++k) deriv[k] = 0.0;
+        return OR_OK;
+    }
+    const double inv = 1.0 / (double)nv;
+    if (wd) {
+        *value = value_sum * inv;
+        for (int k = 0; k < np; ++k) deriv[k] = d[k] * inv;
+    } else {
+        *value = value_sum / (double)nv;  // mean_squares_value divides
+    }
+    return OR_OK;
+}
+
+// Normalised cross-correlation: CorrelationMetric (registration/correlation.rs).
+// Pass 1, means() (:260-295): Σf, Σm over the valid samples in sample order, each
+// divided by the count. Pass 2, evaluate() (:297-410): f1 = f − f̄, m1 = m − m̄;
+// fm += f1·m1, f2 += f1², m2 += m1², fdm[k] += f1·inner, mdm[k] += m1·inner with
+// inner = Σ_d ∇M[d]·J[d][k]; value = −fm²/(m2·f2), derivative
+// −2·fm/(f2·m2)·(fdm − fm/m2·mdm). value() (:200-257) is pass 2 without the
+// derivative sums. No valid sample, or m2·f2 ≤ ε, gives f64::MAX and a zero
+// derivative (valid = the count in the second case).
+int or_ncc_evaluate(const float* fixed, const or_geometry* fg, const float* moving, const or_geometry* mg,
+                    const uint8_t* fmask, const uint8_t* mmask, const int64_t* draw, int64_t ndraw, int kind,
+                    const double* params, const double* fixed_params, int nfixed, int want_derivative,
+                    double* value, double* deriv, int64_t* valid) {
+    Problem P;
+    int st = prepare(fixed, fg, moving, mg, fmask, mmask, draw, ndraw, P);
+    if (st) return st;
+    Transform T;
+    if (!make_transform(kind, params, fixed_params, nfixed, T)) return OR_BAD_ARGUMENT;
+    const int np = T.nparams;
+    const bool wd = want_derivative != 0;
+    if (wd) for (int k = 0; k < np; ++k) deriv[k] = 0.0;
+    double fix_sum = 0.0, mov_sum = 0.0;
+    int64_t n1 = 0;
+    for (int64_t s = 0; s < P.n; ++s) {
+        const int64_t flat = sample_flat(P, s);
+        double fp[3], mp[3], mv, g[3];
+        grid_point(P, flat, fp);
+        T.transform_point(fp, mp);
+        if (!moving_value_grad(P, mp, &mv, g, false)) continue;
+        fix_sum += (double)P.fixed[flat];
+        mov_sum += mv;
+        n1 += 1;
+    }
+    if (n1 == 0) {
+        *value = DBL_MAX;
+        *valid = 0;
+        return OR_OK;
+    }
+    const double avg_fix = fix_sum / (double)n1, avg_mov = mov_sum / (double)n1;
+    double fm = 0.0, f2 = 0.0, m2 = 0.0;
+    std::vector<double> fdm(np, 0.0), mdm(np, 0.0);
+    int64_t nv = 0;
+    double jac[36];
+    for (int64_t s = 0; s < P.n; ++s) {
+        const int64_t flat = sample_flat(P, s);
+        double fp[3], mp[3], mv, g[3];
+        grid_point(P, flat, fp);
+        T.transform_point(fp, mp);
+        if (!moving_value_grad(P, mp, &mv, g, wd)) continue;
+        const double f1 = (double)P.fixed[flat] - avg_fix;
+        const double m1 = mv - avg_mov;
+        fm += f1 * m1;
+        f2 += f1 * f1;
+        m2 += m1 * m1;
+        if (wd) {
+            T.jacobian(fp, jac);
+            for (int k = 0; k < np; ++k) {
+                double inner = 0.0;
+                for (int q = 0; q < 3; ++q) inner += g[q] * jac[q * np + k];
+                fdm[k] += f1 * inner;
+                mdm[k] += m1 * inner;
+            }
+        }
+        nv += 1;
+    }
+    *valid = nv;
+    const double m2f2 = m2 * f2;
+    if (nv == 0 || m2f2 <= DBL_EPSILON) {
+        *value = DBL_MAX;
+        return OR_OK;
+    }
+    *value = -fm * fm / m2f2;
+    if (wd)
+        for (int k = 0; k < np; ++k) deriv[k] = -2.0 * fm / (f2 * m2) * (fdm[k] - fm / m2 * mdm[k]);
+    return OR_OK;
+}
+
 }  // extern "C"

@@ -83,6 +83,11 @@ def lib():
     L.or_round_half_integer_up.restype = ctypes.c_int64
     L.or_invert3.argtypes = [dp, dp]
     L.or_invert3.restype = ctypes.c_int
+    for name in ("or_ms_evaluate", "or_ncc_evaluate"):
+        f = getattr(L, name)
+        f.argtypes = [fp, gp, fp, gp, u8p, u8p, i64p, ctypes.c_int64, ctypes.c_int, dp, dp, ctypes.c_int,
+                      ctypes.c_int, dp, dp, i64p]
+        f.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -179,6 +184,41 @@ def evaluate(fixed, fgeo, moving, mgeo, bins, kind, params, fixed_params=None, f
     if histogram:
         out.update(joint=joint, fixed_marginal=margin)
     return out
+
+
+def _moments_metric(fn, fixed, fgeo, moving, mgeo, kind, params, fixed_params, fmask, mmask, draw, derivative):
+    fixed = np.ascontiguousarray(fixed, dtype=np.float32)
+    moving = np.ascontiguousarray(moving, dtype=np.float32)
+    fm = None if fmask is None else np.ascontiguousarray(np.asarray(fmask) != 0, dtype=np.uint8)
+    mm = None if mmask is None else np.ascontiguousarray(np.asarray(mmask) != 0, dtype=np.uint8)
+    dr = None if draw is None else np.ascontiguousarray(draw, dtype=np.int64)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    fpar = None if fixed_params is None else np.ascontiguousarray(fixed_params, dtype=np.float64)
+    deriv = np.zeros(NPARAMS[kind])
+    value = ctypes.c_double(0.0)
+    valid = ctypes.c_int64(0)
+    st = fn(_ptr(fixed, ctypes.c_float), ctypes.byref(fgeo), _ptr(moving, ctypes.c_float), ctypes.byref(mgeo),
+            _ptr(fm, ctypes.c_uint8), _ptr(mm, ctypes.c_uint8), _ptr(dr, ctypes.c_int64),
+            0 if dr is None else len(dr), kind, _ptr(params, ctypes.c_double), _ptr(fpar, ctypes.c_double),
+            0 if fpar is None else len(fpar), 1 if derivative else 0, ctypes.byref(value),
+            _ptr(deriv, ctypes.c_double), ctypes.byref(valid))
+    if st:
+        raise OracleError(st)
+    return {"value": value.value, "derivative": deriv, "valid": valid.value}
+
+
+def mean_squares(fixed, fgeo, moving, mgeo, kind, params, fixed_params=None, fmask=None, mmask=None, draw=None,
+                 derivative=True):
+    """CpuBackend::mean_squares / mean_squares_value (registration/metric.rs:1064-1196)."""
+    return _moments_metric(lib().or_ms_evaluate, fixed, fgeo, moving, mgeo, kind, params, fixed_params, fmask,
+                           mmask, draw, derivative)
+
+
+def correlation(fixed, fgeo, moving, mgeo, kind, params, fixed_params=None, fmask=None, mmask=None, draw=None,
+                derivative=True):
+    """CorrelationMetric::evaluate / value (registration/correlation.rs:200-410)."""
+    return _moments_metric(lib().or_ncc_evaluate, fixed, fgeo, moving, mgeo, kind, params, fixed_params, fmask,
+                           mmask, draw, derivative)
 
 
 def transform(kind, params, fixed_params=None, point=None):

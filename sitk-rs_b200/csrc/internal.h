@@ -115,8 +115,20 @@ struct Workspace {
 
 }  // namespace mi
 
+namespace mi {
+// Buffers of the mean-squares and correlation reductions (moments.cu).
+struct MomentsWs {
+    int grid = 0;
+    double* partials = nullptr;      // [grid][slots]
+    double* result = nullptr;        // [2][28]: the folded moments, then correlation's pass-1 sums
+    unsigned int* counter = nullptr; // [2] arrival counters
+    double* host = nullptr;          // pinned copy of the folded moments
+};
+}  // namespace mi
+
 struct mi_metric {
     mi_context* ctx = nullptr;
+    int metric_kind = 0;          // MI_METRIC_MATTES, MI_METRIC_MEAN_SQUARES, MI_METRIC_CORRELATION
     mi_geometry fgeo{}, mgeo{};
     float* fixed = nullptr;       // device copy of the fixed volume
     float* moving = nullptr;      // device copy of the moving volume
@@ -130,6 +142,7 @@ struct mi_metric {
     mi_metric_info info{};
     mi::SamplerParams base{};     // everything except the stages
     mi::Workspace ws;
+    mi::MomentsWs mom;
 };
 
 namespace mi {
@@ -149,6 +162,12 @@ mi_status transform_form(int kind, const double* params, int nparams, const doub
 // The family's own jacobian_wrt_parameters at point x, row-major 3×P.
 mi_status transform_jacobian(int kind, const double* params, int nparams, const double* fixed, int nfixed,
                              const double* x, double* jac);
+
+// Mean squares and correlation (moments.cu).
+mi_status moments_setup(mi_metric* m);
+void moments_free(mi_metric* m);
+mi_status evaluate_moments(mi_metric* m, const SamplerParams& P, const double* jac0, const double* jacc, int nparams,
+                           bool want_derivative, double* value, double* derivative, int64_t* valid);
 
 // Core evaluation (mattes.cu).
 mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double* jac0,

@@ -273,6 +273,7 @@ void free_metric(mi_metric* m) {
     if (m->ws.host_result) cudaFreeHost(m->ws.host_result);
     for (int i = 0; i < 5; ++i)
         if (m->ws.ev[i]) cudaEventDestroy(m->ws.ev[i]);
+    moments_free(m);
     delete m;
 }
 
@@ -404,6 +405,8 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     SamplerParams P;
     mi_status s = fill_params(m, stages, nstage, P);
     if (s != MI_OK) return s;
+    if (m->metric_kind != MI_METRIC_MATTES)
+        return evaluate_moments(m, P, jac0, jacc, nparams, want_derivative, value, derivative, valid);
     const int B = m->bins;
     cudaStream_t st = ctx->stream;
     Workspace& ws = m->ws;
@@ -525,14 +528,19 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     const int storage = options ? options->moving_storage : MI_STORAGE_F32;
     if (storage != MI_STORAGE_F32 && storage != MI_STORAGE_BF16)
         return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "moving_storage must be MI_STORAGE_F32 or MI_STORAGE_BF16");
+    const int metric = options ? options->metric : MI_METRIC_MATTES;
+    if (metric != MI_METRIC_MATTES && metric != MI_METRIC_MEAN_SQUARES && metric != MI_METRIC_CORRELATION)
+        return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "unknown metric kind");
+    const bool mattes = metric == MI_METRIC_MATTES;
+    if (!mattes) bins = 0;  // no histogram
     *out = nullptr;
     if (fixed->ctx != ctx || moving->ctx != ctx || (fixed_mask && fixed_mask->ctx != ctx))
         return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "images belong to another context");
-    if (bins < 2 * PADDING + 1)
+    if (mattes && bins < 2 * PADDING + 1)
         return set_error(ctx, MI_ERR_TOO_FEW_HISTOGRAM_BINS,
                          "need at least " + std::to_string(2 * PADDING + 1) + " histogram bins, got " +
                              std::to_string(bins));
-    if (bins > MI_MAX_BINS)
+    if (mattes && bins > MI_MAX_BINS)
         return set_error(ctx, MI_ERR_TOO_MANY_HISTOGRAM_BINS,
                          "the shared-memory histogram holds at most " + std::to_string(MI_MAX_BINS) + " bins");
     if (fixed_mask)
@@ -553,6 +561,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     mi_metric* m = new (std::nothrow) mi_metric();
     if (!m) return MI_ERR_OUT_OF_MEMORY;
     m->ctx = ctx;
+    m->metric_kind = metric;
     m->fgeo = fixed->geo;
     m->mgeo = moving->geo;
     m->bins = bins;
@@ -589,26 +598,29 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
 
     // Histogram geometry from the sampled fixed values and the masked moving volume
     // (metric.rs:633-640, :913-924; MattesGeometry::new, mattes.rs:152-186).
-    double fmin, fmax, mmin, mmax;
-    bool anyf, anym;
-    s = minmax(ctx, m->fixed, m->samples, nullptr, m->n_samples, &fmin, &fmax, &anyf);
-    if (s != MI_OK) return fail(s);
-    s = minmax(ctx, m->moving, nullptr, m->mmask, mvox, &mmin, &mmax, &anym);
-    if (s != MI_OK) return fail(s);
-    if (fmax - fmin <= DBL_EPSILON) return fail(set_error(ctx, MI_ERR_CONSTANT_FIXED, "constant intensity: fixed"));
-    if (mmax - mmin <= DBL_EPSILON) return fail(set_error(ctx, MI_ERR_CONSTANT_MOVING, "constant intensity: moving"));
-    const double denom = (double)(bins - 2 * PADDING);
+    // Mean squares and correlation have no histogram and refuse no constant image.
+    double fmin = 0.0, fmax = 0.0, mmin = 0.0, mmax = 0.0;
     mi_metric_info& info = m->info;
     info.bins = bins;
     info.n_samples = m->n_samples;
-    info.fixed_min = fmin;
-    info.fixed_max = fmax;
-    info.moving_min = mmin;
-    info.moving_max = mmax;
-    info.fixed_bin_size = (fmax - fmin) / denom;
-    info.moving_bin_size = (mmax - mmin) / denom;
-    info.fixed_normalized_min = fmin / info.fixed_bin_size - (double)PADDING;
-    info.moving_normalized_min = mmin / info.moving_bin_size - (double)PADDING;
+    if (mattes) {
+        bool anyf, anym;
+        s = minmax(ctx, m->fixed, m->samples, nullptr, m->n_samples, &fmin, &fmax, &anyf);
+        if (s != MI_OK) return fail(s);
+        s = minmax(ctx, m->moving, nullptr, m->mmask, mvox, &mmin, &mmax, &anym);
+        if (s != MI_OK) return fail(s);
+        if (fmax - fmin <= DBL_EPSILON) return fail(set_error(ctx, MI_ERR_CONSTANT_FIXED, "constant intensity: fixed"));
+        if (mmax - mmin <= DBL_EPSILON) return fail(set_error(ctx, MI_ERR_CONSTANT_MOVING, "constant intensity: moving"));
+        const double denom = (double)(bins - 2 * PADDING);
+        info.fixed_min = fmin;
+        info.fixed_max = fmax;
+        info.moving_min = mmin;
+        info.moving_max = mmax;
+        info.fixed_bin_size = (fmax - fmin) / denom;
+        info.moving_bin_size = (mmax - mmin) / denom;
+        info.fixed_normalized_min = fmin / info.fixed_bin_size - (double)PADDING;
+        info.moving_normalized_min = mmin / info.moving_bin_size - (double)PADDING;
+    }
 
     SamplerParams& P = m->base;
     std::memset(&P, 0, sizeof(P));
@@ -671,7 +683,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     P.bins = bins;
     P.fixed_bin_size = info.fixed_bin_size;
     P.moving_bin_size = info.moving_bin_size;
-    P.inv_moving_bin_size = 1.0 / info.moving_bin_size;
+    P.inv_moving_bin_size = mattes ? 1.0 / info.moving_bin_size : 0.0;
     P.fixed_nmin = info.fixed_normalized_min;
     P.moving_nmin = info.moving_normalized_min;
     P.moving_min = mmin;
@@ -682,6 +694,14 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         P.xref[r] = P.forigin[r] + f_i2p[r * 3] * mid[0] + f_i2p[r * 3 + 1] * mid[1] + f_i2p[r * 3 + 2] * mid[2];
         P.xb[r] = (float)(P.forigin[r] - P.xref[r]);
         for (int c = 0; c < 3; ++c) P.xA[r * 3 + c] = (float)f_i2p[r * 3 + c];
+    }
+
+    if (!mattes) {
+        s = moments_setup(m);
+        if (s != MI_OK) return fail(s);
+        TRY_CUDA(cudaStreamSynchronize(st));
+        *out = m;
+        return MI_OK;
     }
 
     // The exact fixed bin of every sample (a pure function of the fixed value).
@@ -824,6 +844,8 @@ mi_status mi_metric_timing_enable(mi_metric* m, int enable) {
 
 mi_status mi_metric_set_fused(mi_metric* m, int fused) {
     if (!m) return MI_ERR_INVALID_ARGUMENT;
+    if (m->metric_kind != MI_METRIC_MATTES)
+        return mi::set_error(m->ctx, MI_ERR_INVALID_ARGUMENT, "the launch form is a Mattes-metric setting");
     mi::Workspace& ws = m->ws;
     if (fused && !ws.can_fuse)
         return mi::set_error(m->ctx, MI_ERR_INVALID_ARGUMENT, "a cooperative launch is not available here");
@@ -867,6 +889,8 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
     using namespace mi;
     if (!m) return MI_ERR_INVALID_ARGUMENT;
     mi_context* ctx = m->ctx;
+    if (m->metric_kind != MI_METRIC_MATTES)
+        return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "per-sample Parzen decisions exist for the Mattes metric only");
     if (n < m->n_samples) return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "output arrays shorter than the sample count");
     if (nstage < 0 || nstage > MI_MAX_STAGES) return set_error(ctx, MI_ERR_POINT_MAP_STAGE_COUNT, "too many stages");
     MI_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -162,6 +162,30 @@ __device__ __forceinline__ double exact_value(const SamplerParams& P, const doub
 //    distance from the reference's FP64 value.
 // 5. Range reject and Parzen bin from the FP32 value when dv cannot flip them;
 //    otherwise the reference's value is recomputed exactly (exact_value).
+// The eight corners of the cell whose lowest corner is fl (floor of a continuous
+// index that passed the inside test, so each fl[d] ∈ [−1, size − 1]), corner t at
+// fl + (t & 1, (t >> 1) & 1, t >> 2), from the moving volume's texture (point
+// sampling at voxel centres, clamp addressing = the clamp-to-edge of each corner).
+__device__ __forceinline__ void fetch_corners(const SamplerParams& P, const double* fl, float* v) {
+    float cx[2], cy[2], cz[2];
+    cx[0] = (float)fl[0] + 0.5f;
+    cy[0] = (float)fl[1] + 0.5f;
+    cz[0] = (float)fl[2] + 0.5f;
+    cx[1] = cx[0] + 1.0f;
+    cy[1] = cy[0] + 1.0f;
+    cz[1] = cz[0] + 1.0f;
+    if (P.mbf16) {
+        // BF16 storage: the upper half of an f32, so the widening is exact
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+            v[t] = __uint_as_float((uint32_t)tex3D<unsigned short>(P.mtex, cx[t & 1], cy[(t >> 1) & 1], cz[t >> 2])
+                                   << 16);
+    } else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) v[t] = tex3D<float>(P.mtex, cx[t & 1], cy[(t >> 1) & 1], cz[t >> 2]);
+    }
+}
+
 struct Prep {
     uint32_t flat;
     float fr[3];
@@ -239,25 +263,9 @@ __device__ __forceinline__ void prep(const SamplerParams& P, uint32_t flat, cons
     // sampling at voxel centres returns the stored f32 voxel unchanged, clamp
     // addressing is exactly the reference's clamp-to-edge of each corner index, and
     // the block-linear layout keeps a cell's corners on a few cache lines.
-    float cx[2], cy[2], cz[2];
 #pragma unroll
     for (int d = 0; d < 3; ++d) p.fr[d] = (float)frd[d];
-    cx[0] = (float)fl[0] + 0.5f;
-    cy[0] = (float)fl[1] + 0.5f;
-    cz[0] = (float)fl[2] + 0.5f;
-    cx[1] = cx[0] + 1.0f;
-    cy[1] = cy[0] + 1.0f;
-    cz[1] = cz[0] + 1.0f;
-    if (P.mbf16) {
-        // BF16 storage: the upper half of an f32, so the widening is exact
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-            p.v[t] = __uint_as_float((uint32_t)tex3D<unsigned short>(P.mtex, cx[t & 1], cy[(t >> 1) & 1], cz[t >> 2])
-                                     << 16);
-    } else {
-#pragma unroll
-        for (int t = 0; t < 8; ++t) p.v[t] = tex3D<float>(P.mtex, cx[t & 1], cy[(t >> 1) & 1], cz[t >> 2]);
-    }
+    fetch_corners(P, fl, p.v);
     p.ok = true;
 }
 

@@ -58,6 +58,13 @@ class MiMetricInfo(ctypes.Structure):
                 ("moving_normalized_min", ctypes.c_double)]
 
 
+class MiMetricOptions(ctypes.Structure):
+    _fields_ = [("moving_storage", ctypes.c_int), ("metric", ctypes.c_int)]
+
+
+METRIC_MATTES, METRIC_MEAN_SQUARES, METRIC_CORRELATION = 0, 1, 2
+
+
 class MiError(RuntimeError):
     """A named refusal from the library (mirrors DeviceMetricError / CudaError)."""
 
@@ -101,7 +108,7 @@ def load(path: str | None = None):
     L.mi_image_free.argtypes = [vp]
     L.mi_metric_create.argtypes = [vp, vp, vp, vp, P(ctypes.c_uint8), P(MiSampling), ctypes.c_int, P(vp)]
     L.mi_metric_create_ex.argtypes = [vp, vp, vp, vp, P(ctypes.c_uint8), P(MiSampling), ctypes.c_int,
-                                      P(ctypes.c_int), P(vp)]
+                                      P(MiMetricOptions), P(vp)]
     L.mi_metric_create_ex.restype = ctypes.c_int
     L.mi_metric_info_get.argtypes = [vp, P(MiMetricInfo)]
     L.mi_metric_destroy.argtypes = [vp]

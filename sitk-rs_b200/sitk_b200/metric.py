@@ -179,7 +179,7 @@ class DeviceMattesMetric:
     def from_device_sampled(cls, fixed: DeviceImage, moving: DeviceImage, fixed_mask=None,
                             moving_mask=None, samples=None, bins: int = 50, *,
                             strategy: int | None = None, percentage: float = 1.0, seed: int = 0,
-                            moving_storage: str = "f32"):
+                            moving_storage: str = "f32", _metric: int = _lib.METRIC_MATTES):
         """`samples` is an explicit flat-index list (FixedSamples::selected_indices);
         alternatively `strategy`/`percentage`/`seed` draw on the device exactly as
         draw_samples does (registration/metric.rs:419-437). `moving_storage` "bf16"
@@ -209,7 +209,7 @@ class DeviceMattesMetric:
                 keep.append(fmi)
                 fm_handle = fmi.handle
         h = ctypes.c_void_p()
-        opts = ctypes.c_int(storage)  # mi_metric_options{moving_storage}
+        opts = _lib.MiMetricOptions(storage, int(_metric))
         _lib.check(_lib.load().mi_metric_create_ex(
             ctx.handle, fixed.handle, moving.handle, fm_handle,
             None if mm is None else mm.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
@@ -298,6 +298,42 @@ class DeviceMattesMetric:
             self.close()
         except Exception:
             pass
+
+
+class DeviceMeanSquaresMetric(DeviceMattesMetric):
+    """registration/device.rs:203-365 DeviceMeanSquaresMetric: value = Σ(m − f)²/count
+    and its parameter derivative, over the same sample set, masks and sampler as the
+    Mattes metric (mi_metric_create_ex with MI_METRIC_MEAN_SQUARES)."""
+
+    @classmethod
+    def from_device(cls, fixed: DeviceImage, moving: DeviceImage):
+        return cls.from_device_sampled(fixed, moving)
+
+    @classmethod
+    def from_device_sampled(cls, fixed: DeviceImage, moving: DeviceImage, fixed_mask=None, moving_mask=None,
+                            samples=None, *, strategy: int | None = None, percentage: float = 1.0, seed: int = 0,
+                            moving_storage: str = "f32"):
+        return super().from_device_sampled(fixed, moving, fixed_mask, moving_mask, samples, 0, strategy=strategy,
+                                           percentage=percentage, seed=seed, moving_storage=moving_storage,
+                                           _metric=_lib.METRIC_MEAN_SQUARES)
+
+
+class DeviceCorrelationMetric(DeviceMattesMetric):
+    """registration/device.rs:474-575 DeviceCorrelationMetric: value = −sfm²/(sff·smm)
+    over the mean-subtracted samples, two device passes (means, then moments), and its
+    parameter derivative (mi_metric_create_ex with MI_METRIC_CORRELATION)."""
+
+    @classmethod
+    def from_device(cls, fixed: DeviceImage, moving: DeviceImage):
+        return cls.from_device_sampled(fixed, moving)
+
+    @classmethod
+    def from_device_sampled(cls, fixed: DeviceImage, moving: DeviceImage, fixed_mask=None, moving_mask=None,
+                            samples=None, *, strategy: int | None = None, percentage: float = 1.0, seed: int = 0,
+                            moving_storage: str = "f32"):
+        return super().from_device_sampled(fixed, moving, fixed_mask, moving_mask, samples, 0, strategy=strategy,
+                                           percentage=percentage, seed=seed, moving_storage=moving_storage,
+                                           _metric=_lib.METRIC_CORRELATION)
 
 
 def transform_form(transform: ParametricTransform):
