@@ -309,6 +309,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     m = sb.DeviceImage.upload(pair.moving, ctx=ctx)
     metric = sb.DeviceMattesMetric.from_device_sampled(f, m, bins=BINS, strategy=sb.SAMPLING_RANDOM,
                                                        percentage=PCT, seed=SEED)
+    siblings = None
+    if not args.no_siblings and rank == 0:
+        siblings = {name: cls.from_device_sampled(f, m, strategy=sb.SAMPLING_RANDOM, percentage=PCT, seed=SEED)
+                    for name, cls in (("mean_squares", sb.DeviceMeanSquaresMetric),
+                                      ("correlation", sb.DeviceCorrelationMetric))}
     f.free()
     m.free()
     info = metric.info()
@@ -429,6 +434,24 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                          f"restatement of the reference CPU metric (~{sum(times):.1f} s)"}
 
     clocks = sampler.summary() if sampler else None
+    sib = None
+    if siblings:
+        # the reference's other device metrics on the same samples and pose: value +
+        # derivative, device time per evaluation (events), L2 flushed before each
+        sib = {}
+        for name, sm in siblings.items():
+            for _ in range(3):
+                sm.evaluate(t)
+            enable_timing(sm, True)
+            read_timing(sm)
+            for _ in range(min(args.steps, 50)):
+                l2_flush()
+                sm.evaluate(t)
+            sms, snev = read_timing(sm)
+            enable_timing(sm, False)
+            sib[name] = {"evals_per_s": snev / (sms[0] / 1e3), "ms_per_eval": sms[0] / snev,
+                         "launches_per_eval": 1 if name == "mean_squares" else 2}
+            sm.close()
     reg = None if args.no_registration else time_registration(pair, ctx, dev)
     batch = None if args.no_batch else time_batch(ctx, dev, SEED)
     line = {
@@ -455,6 +478,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "result": {"value": last.value, "valid": last.valid_points},
         "registration": reg,
         "batch": batch,
+        "other_metrics": sib,
     }
     print(json.dumps(line), flush=True)
     if dist:
@@ -624,6 +648,8 @@ def main():
                     help="skip the full three-level registration run reported beside the metric")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the 64-pair batched registration run reported beside the metric")
+    ap.add_argument("--no-siblings", action="store_true",
+                    help="skip the mean-squares and correlation timings reported beside the metric")
     ap.add_argument("--form", default="split", choices=["split", "fused"],
                     help="launch form of an evaluation: two kernels, or one cooperative kernel")
     ap.add_argument("--settle", type=float, default=1.0,
