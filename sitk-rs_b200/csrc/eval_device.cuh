@@ -23,7 +23,14 @@ namespace {
 // corner gathers issued together), and a register cap that keeps HIST_MIN_BLOCKS
 // CTAs of HIST_BLOCK threads resident per SM.
 #ifndef MI_HIST_ILP
-#define MI_HIST_ILP 2
+#define MI_HIST_ILP 1
+#endif
+// Resident CTAs per SM the derivative kernel's register budget is sized for. Every
+// CTA of k_deriv forms the tail itself, so fewer, larger CTAs repeat it less: two per
+// SM measured fastest on the 256³ workload (22.6 µs against 23.5 with three and 26.9
+// with four).
+#ifndef MI_DERIV_MIN_BLOCKS
+#define MI_DERIV_MIN_BLOCKS 2
 #endif
 #ifndef MI_HIST_MIN_BLOCKS
 #define MI_HIST_MIN_BLOCKS 4
@@ -43,6 +50,7 @@ constexpr int HIST_BLOCK = 256;
 constexpr int HIST_MIN_BLOCKS = MI_HIST_MIN_BLOCKS;
 constexpr int HIST_ILP = MI_HIST_ILP;
 constexpr int DERIV_BLOCK = 256;
+constexpr int DERIV_MIN_BLOCKS = MI_DERIV_MIN_BLOCKS;
 constexpr int NMOM = 12;
 
 struct JacobianForm {
@@ -78,7 +86,7 @@ size_t hist_smem(int B) {
 constexpr int TAIL_BLOCK = 256;
 __host__ __device__ inline int tail_groups(int B) { return TAIL_BLOCK / B; }
 __host__ __device__ inline size_t tail_smem(int B) {
-    return ((size_t)B * B + B + (size_t)tail_groups(B) * B + B) * 8 + ((2 * (size_t)B + 7) & ~(size_t)7);
+    return ((size_t)B * B + B + (size_t)tail_groups(B) * B + B) * 8 + ((2 * (size_t)B + 7) & ~(size_t)7) + 8;
 }
 size_t deriv_smem(int B) { return 32 * (size_t)NMOM * sizeof(double) + tail_smem(B) + (size_t)B * B * sizeof(float); }
 // The fused kernel reuses one dynamic allocation for its phases. The derivative
@@ -188,8 +196,11 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
     const uint32_t* __restrict__ samples = a.samples;
     const uint8_t* __restrict__ fbin = a.fbin;
     const float hist_scale = a.hist_scale, fine_scale = a.fine_scale;
-    // Two samples per iteration: both samples' corner gathers are issued (prep) before
-    // either is finished, so each thread keeps two gathers in flight.
+    // With MI_HIST_ILP 2, two samples per iteration: both samples' corner gathers are
+    // issued (prep) before either is finished, so each thread keeps two gathers in
+    // flight. One sample per iteration (the default) measured 5 % faster on the 256³
+    // workload: the two-sample form needs more than the 64 registers that four
+    // resident CTAs allow and spills.
     // The CTA keeps `copies` interleaved copies of the histogram and lane l adds into
     // copy l mod copies: neighbouring lanes, whose sorted samples usually share a bin
     // pair, then add to different addresses instead of replaying on one. The copies
@@ -289,6 +300,7 @@ struct TailSmem {
     unsigned long long* col;   // B
     uint8_t* okm;              // B
     uint8_t* okf;              // B
+    unsigned long long* jmin;  // 1: the least joint count whose joint probability exceeds ε
 };
 __device__ __forceinline__ TailSmem tail_layout(int B, unsigned char* base) {
     TailSmem t;
@@ -297,6 +309,7 @@ __device__ __forceinline__ TailSmem tail_layout(int B, unsigned char* base) {
     t.col = t.part + tail_groups(B) * B;
     t.okm = reinterpret_cast<uint8_t*>(t.col + B);
     t.okf = t.okm + B;
+    t.jmin = reinterpret_cast<unsigned long long*>(t.okm + ((2 * B + 7) & ~7));
     return t;
 }
 
@@ -363,23 +376,44 @@ __device__ TailCtx tail_prepare(int B, double moving_bin_size, const EvalArgs& a
         ts.okm[threadIdx.x] = (double)ts.col[threadIdx.x] / t.dt > DBL_EPSILON;
         ts.okf[threadIdx.x] = (double)cnt[threadIdx.x] / t.joint_sum > DBL_EPSILON;
     }
+    if (threadIdx.x == blockDim.x - 1) {
+        // jp = jv/total > ε is monotone in the integer jv: find its least jv once,
+        // starting next to ε·total, so the table tests an integer instead of dividing
+        unsigned long long c = (unsigned long long)(DBL_EPSILON * t.dt);
+        for (int it = 0; it < 64 && c > 0ull && (double)(c - 1ull) / t.dt > DBL_EPSILON; ++it) --c;
+        for (int it = 0; it < 64 && !((double)c / t.dt > DBL_EPSILON); ++it) ++c;
+        *ts.jmin = c > 0ull ? c : 1ull;
+    }
     __syncthreads();
     return t;
 }
 
+// ln(a/b) for positive a, b in FP32: the quotient by the fast reciprocal (a few ulps)
+// and the accurate logf.
+__device__ __forceinline__ float log_ratio(float a, float b) { return logf(__fdividef(a, b)); }
+
 // pRatio·nFactor of every bin into pr (shared memory, FP32): 0 where the reference
-// skips the bin, else ln(joint/col)·nFactor with the ratio formed in FP64 and the
-// logarithm taken in FP32 (the table is FP32).
+// skips the bin (jp, mm or fm not above ε), else ln(joint/col)·nFactor in FP32 (the
+// table is FP32; the ratio of the two exact integers carries a few units of 2^-24,
+// far below what the derivative's tolerance sees). The entry's (row, column) advance
+// with the thread's stride, so no per-entry division.
 __device__ void pr_table(int B, const TailCtx& t, const TailSmem& ts, float* pr) {
     const int B2 = B * B;
     const float nf = (float)t.n_factor;
+    const unsigned long long jmin = *ts.jmin;
+    int f = (int)threadIdx.x / B, m = (int)threadIdx.x - f * B;
+    const int df = (int)blockDim.x / B, dm = (int)blockDim.x - df * B;
     for (int i = threadIdx.x; i < B2; i += blockDim.x) {
-        const int f = i / B, m = i - f * B;
         const unsigned long long jv = ts.hist[i];
         float r = 0.0f;
-        if (ts.okf[f] && ts.okm[m] && jv && (double)jv / t.dt > DBL_EPSILON)
-            r = logf((float)((double)jv / (double)ts.col[m])) * nf;
+        if (ts.okf[f] && ts.okm[m] && jv >= jmin) r = log_ratio((float)jv, (float)ts.col[m]) * nf;
         pr[i] = r;
+        f += df;
+        m += dm;
+        if (m >= B) {
+            m -= B;
+            ++f;
+        }
     }
 }
 

@@ -80,6 +80,9 @@ struct SamplerParams {
     double fixed_bin_size, moving_bin_size;
     double fixed_nmin, moving_nmin;
     double moving_min, moving_max;
+    // FP32 copies for the fast Parzen decision (the range ends are f32 voxel values,
+    // so exact); cerr_f ≥ cerr
+    float mmin_f, mmax_f, inv_bin_f, nmin_f, rmag_f, bin_hi_f, cerr_f;
     // derivative moments are taken about this point to limit cancellation
     double xref[3];
 };

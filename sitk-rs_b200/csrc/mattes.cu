@@ -103,7 +103,7 @@ k_tail(int B, double moving_bin_size, EvalArgs a) {
 }
 
 // Tail and derivative pass of the split form.
-__global__ void __launch_bounds__(DERIV_BLOCK)
+__global__ void __launch_bounds__(DERIV_BLOCK, DERIV_MIN_BLOCKS)
 k_deriv(SamplerParams P, JacobianForm J, EvalArgs a) {
     extern __shared__ double dsh[];
     const TailCtx t = deriv_phase(P, a, dsh, grid_groups(a));
@@ -688,6 +688,12 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     P.moving_nmin = info.moving_normalized_min;
     P.moving_min = mmin;
     P.moving_max = mmax;
+    P.mmin_f = (float)mmin;
+    P.mmax_f = (float)mmax;
+    P.inv_bin_f = (float)P.inv_moving_bin_size;
+    P.nmin_f = (float)P.moving_nmin;
+    P.rmag_f = std::max(std::fabs(P.mmin_f), std::fabs(P.mmax_f));
+    P.bin_hi_f = (float)(bins - PADDING - 1);
     // x_ref: the fixed grid's physical centre; x − x_ref = M_f·idx + (o_f − x_ref)
     const double mid[3] = {0.5 * (double)(P.fsize0 - 1), 0.5 * (double)(P.fsize1 - 1), 0.5 * (double)(P.fsize2 - 1)};
     for (int r = 0; r < 3; ++r) {

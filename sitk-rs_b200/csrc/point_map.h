@@ -91,6 +91,7 @@ MI_HD inline bool point_map_fill(SamplerParams& P, const double* stages, int nst
     }
     if (!(cmax <= DBL_MAX)) return false;
     P.cerr = mul(mul(0x1p-40, add(1.0, cmax)), (double)(1 + nstage));
+    P.cerr_f = (float)mul(P.cerr, 1.000001);  // rounded to f32 and still ≥ cerr
     P.ilo = add(-0.5, mul(2.0, P.cerr));
     P.olo = sub(-0.5, mul(2.0, P.cerr));
     for (int d = 0; d < 3; ++d) {

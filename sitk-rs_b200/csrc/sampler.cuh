@@ -40,6 +40,11 @@ namespace mi {
 
 constexpr int PADDING = 2;  // registration/mattes.rs:92
 
+// Range and Parzen decisions of the fast path in FP32 (1) or FP64 (0).
+#ifndef MI_PARZEN_F32
+#define MI_PARZEN_F32 1
+#endif
+
 enum : int { SAMPLE_OUTSIDE = 0, SAMPLE_OUT_OF_RANGE = 1, SAMPLE_VALID = 2 };
 
 struct Sample {
@@ -299,10 +304,58 @@ __device__ __forceinline__ int finish(const SamplerParams& P, const Prep& p, con
     // |mv − reference value| ≤ dv: three levels of FP32 lerps add at most 12 units of
     // 2^-24 of the largest corner magnitude (32 allowed), plus the Lipschitz effect
     // (≤ 6·vmax per voxel) of the continuous-index error ce.
-    const double ce = p.exact_c ? 0.0 : P.cerr;
     float vmax = fabsf(v[0]);
 #pragma unroll
     for (int t = 1; t < 8; ++t) vmax = fmaxf(vmax, fabsf(v[t]));
+#if MI_PARZEN_F32
+    // The range and Parzen decisions in FP32 with a bound that covers the value's error
+    // dv and every FP32 rounding on the way: e bounds |mv − v_ref| plus the rounding of
+    // mv ± e (the 2^-20 terms are ≥ 16 ulps of every magnitude involved, the range ends
+    // are f32 voxel values and so exact); dt bounds |term − term_ref| with
+    // term_ref = v_ref/binSize − normMin (inv_bin_f and nmin_f carry 2^-24 relative
+    // error, the FMA one rounding, the reference's FP64 chain ≪ 2^-40) plus the
+    // rounding of term ± dt. Every operation is an explicitly rounded intrinsic, so no
+    // kernel that inlines this contracts it differently: a sample takes the same path
+    // in every kernel.
+    const float cef = p.exact_c ? 0.0f : P.cerr_f;
+    const float dvf = __fmul_rn(vmax, __fmaf_rn(8.0f, cef, 32.0f * 5.9604644775390625e-08f));
+    bool certain = dvf < 1e30f && isfinite(mv);
+    float termf = 0.0f;
+    int mi = 0;
+    if (certain) {
+        const float mag = __fadd_rn(__fadd_rn(fabsf(mv), P.rmag_f), vmax);
+        const float e = __fmaf_rn(dvf, 1.001f, __fmul_rn(mag, 9.5367431640625e-07f));
+        if (__fadd_rn(mv, e) < P.mmin_f || __fsub_rn(mv, e) > P.mmax_f) return SAMPLE_OUT_OF_RANGE;
+        certain = __fsub_rn(mv, e) >= P.mmin_f && __fadd_rn(mv, e) <= P.mmax_f;
+        termf = __fmaf_rn(mv, P.inv_bin_f, -P.nmin_f);
+        const float tmag = __fadd_rn(__fadd_rn(__fadd_rn(fabsf(__fmul_rn(mv, P.inv_bin_f)), fabsf(P.nmin_f)),
+                                               fabsf(termf)), 1.0f);
+        const float dt = __fmaf_rn(__fmul_rn(dvf, P.inv_bin_f), 1.001f, __fmul_rn(tmag, 2.384185791015625e-07f));
+        // truncation then clamp to [2, bins − 3] equals floor then clamp for every
+        // term (anything below 2 clamps to 2)
+        const float lo = fminf(fmaxf(floorf(__fsub_rn(termf, dt)), (float)PADDING), P.bin_hi_f);
+        const float hi = fminf(fmaxf(floorf(__fadd_rn(termf, dt)), (float)PADDING), P.bin_hi_f);
+        certain = certain && lo == hi;
+        mi = (int)lo;
+    }
+    if (!certain) {
+        uint32_t i, j, k;
+        grid_index(P, p.flat, i, j, k);
+        double c[3];
+        exact_index(P, i, j, k, c);
+        o.exact = true;
+        const double mvx = exact_value(P, c, moving);
+        if (mvx < P.moving_min || mvx > P.moving_max) return SAMPLE_OUT_OF_RANGE;
+        const double term = __dsub_rn(__ddiv_rn(mvx, P.moving_bin_size), P.moving_nmin);
+        mi = parzen_bin(term, P.bins);
+        o.f = (float)(term - (double)mi);
+    } else {
+        o.f = __fsub_rn(termf, (float)mi);
+    }
+    o.mi = mi;
+    return SAMPLE_VALID;
+#else
+    const double ce = p.exact_c ? 0.0 : P.cerr;
     const double dv = (double)vmax * (32.0 * 5.9604644775390625e-08 + 8.0 * ce) + 1e-300;
     const double mvd = (double)mv;
     bool certain = true;
@@ -340,6 +393,7 @@ __device__ __forceinline__ int finish(const SamplerParams& P, const Prep& p, con
     o.f = (float)(term - (double)mi);
     o.mi = mi;
     return SAMPLE_VALID;
+#endif
 }
 
 template <bool GRAD>
