@@ -313,6 +313,13 @@ mi_status mi_shrink_geometry(const mi_geometry* in, const int64_t* factors3, mi_
 mi_status mi_image_resample(mi_context* ctx, const mi_image* in, const mi_geometry* grid, double fill,
                             mi_image** out);
 
+/* The same with the nearest-neighbour interpolator (transform/interpolator.rs:36-54:
+ * floor(c + 0.5) per axis, clamped): how the device driver carries a fixed mask onto
+ * a pyramid level (registration/method.rs:3068-3110 level_mask_on_device; nonzero =
+ * inside, fill 0). */
+mi_status mi_image_resample_nearest(mi_context* ctx, const mi_image* in, const mi_geometry* grid, double fill,
+                                    mi_image** out);
+
 /* One level of the multi-resolution schedule as prepare_level builds it without a
  * virtual domain, fixed-initial transform or masks: both images smoothed with
  * `sigma` (physical units when sigma_physical, else voxels scaled by the fixed

@@ -351,6 +351,30 @@ def resample_linear(volume, geo_in, geo_out, fill=0.0):
     return out.reshape(int(geo_out.size[2]), int(geo_out.size[1]), int(geo_out.size[0]))
 
 
+def resample_nearest(volume, geo_in, geo_out, fill=0.0):
+    """ResampleImageFilter through the identity, nearest neighbour (interpolator.rs:36-54)."""
+    L = _pyr_bind()
+    if not hasattr(L.or_resample_nearest, "_typed"):
+        L.or_resample_nearest.argtypes = L.or_resample_linear.argtypes
+        L.or_resample_nearest.restype = ctypes.c_int
+        L.or_resample_nearest._typed = True
+    v = np.ascontiguousarray(volume, dtype=np.float32)
+    n = int(geo_out.size[0] * geo_out.size[1] * geo_out.size[2])
+    out = np.empty(n, dtype=np.float32)
+    st = L.or_resample_nearest(_ptr(v, ctypes.c_float), ctypes.byref(geo_in), ctypes.byref(geo_out), float(fill),
+                               _ptr(out, ctypes.c_float))
+    if st:
+        raise OracleError(st)
+    return out.reshape(int(geo_out.size[2]), int(geo_out.size[1]), int(geo_out.size[0]))
+
+
+def level_mask(mask, geo, level_geo):
+    """level_mask_on_device without virtual domain or fixed-initial transform
+    (registration/method.rs:3068-3110): the user mask resampled nearest-neighbour onto
+    the level's grid, fill 0, nonzero = inside."""
+    return (resample_nearest(np.asarray(mask, dtype=np.float32), geo, level_geo, 0.0) != 0).astype(np.uint8)
+
+
 def pyramid_level(fixed, fgeo, moving, mgeo, sigma, factors, sigma_physical=True):
     """prepare_level (registration/method.rs:2416) without virtual domain, fixed-initial
     transform or masks: returns (fixed_level, fixed_level_geo, moving_level)."""

@@ -166,8 +166,26 @@ int or_shrink_geometry(const or_pgeometry* in, const int64_t* factors, or_pgeome
 int or_invert3(const double* m, double* inv);  // mattes_oracle.cpp (core/matrix.rs Gauss–Jordan)
 
 // ResampleImageFilter::execute through the identity, linear interpolator.
+static int resample(const float* in, const or_pgeometry* gin, const or_pgeometry* gout, double fill, bool linear,
+                    float* out);
+
+// ResampleImageFilter through the identity with the linear interpolator
+// (transform/resample.rs:226-290, transform/interpolator.rs:103-152).
 int or_resample_linear(const float* in, const or_pgeometry* gin, const or_pgeometry* gout, double fill,
                        float* out) {
+    return resample(in, gin, gout, fill, true, out);
+}
+
+// The same with the nearest-neighbour interpolator (interpolator.rs:36-54): inside
+// test, then floor(c + 0.5) per axis clamped to the grid; the level mask of the
+// device driver (registration/method.rs:3068-3110 level_mask_on_device).
+int or_resample_nearest(const float* in, const or_pgeometry* gin, const or_pgeometry* gout, double fill,
+                        float* out) {
+    return resample(in, gin, gout, fill, false, out);
+}
+
+static int resample(const float* in, const or_pgeometry* gin, const or_pgeometry* gout, double fill, bool linear,
+                    float* out) {
     double m_in[9], inv[9], m_out[9];
     for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c) {
@@ -203,7 +221,15 @@ int or_resample_linear(const float* in, const or_pgeometry* gin, const or_pgeome
         bool inside = true;
         for (int d = 0; d < 3; ++d) inside = inside && ci[d] >= -0.5 && ci[d] < (double)gin->size[d] - 0.5;
         double v = fill;
-        if (inside) {
+        if (inside && !linear) {
+            int64_t off = 0;
+            for (int d = 0; d < 3; ++d) {
+                int64_t i = (int64_t)std::floor(ci[d] + 0.5);
+                i = std::min<int64_t>(std::max<int64_t>(i, 0), gin->size[d] - 1);
+                off += i * istr[d];
+            }
+            v = (double)in[off];
+        } else if (inside) {
             int64_t base[3];
             double frac[3];
             for (int d = 0; d < 3; ++d) {

@@ -206,8 +206,11 @@ struct ResampleGeo {
     double ip2i[9], iorg[3];  // input physical → index
 };
 
-__global__ void k_resample_linear(const float* __restrict__ in, float* __restrict__ out, ResampleGeo G,
-                                  double fill) {
+// LINEAR: the linear interpolator (transform/interpolator.rs:103-152); otherwise the
+// nearest-neighbour one (interpolator.rs:36-54: floor(c + 0.5), clamped), both behind
+// the same inside test and the same index arithmetic.
+template <bool LINEAR>
+__global__ void k_resample(const float* __restrict__ in, float* __restrict__ out, ResampleGeo G, double fill) {
     const int64_t n = G.osz[0] * G.osz[1] * G.osz[2];
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
         const double idx[3] = {(double)(q % G.osz[0]), (double)((q / G.osz[0]) % G.osz[1]),
@@ -239,7 +242,17 @@ __global__ void k_resample_linear(const float* __restrict__ in, float* __restric
             inside = inside && c[r] >= -0.5 && c[r] < (double)G.isz[r] - 0.5;
         }
         double v = fill;
-        if (inside) {
+        if (inside && !LINEAR) {
+            int64_t off = 0, mul = 1;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                int64_t i = (int64_t)floor(__dadd_rn(c[d], 0.5));  // round half up
+                i = i < 0 ? 0 : (i > G.isz[d] - 1 ? G.isz[d] - 1 : i);
+                off += i * mul;
+                mul *= G.isz[d];
+            }
+            v = (double)__ldg(in + off);
+        } else if (inside) {
             double fr[3];
             int64_t b0[3], b1[3];
 #pragma unroll
@@ -375,8 +388,8 @@ mi_status mi_shrink_geometry(const mi_geometry* in, const int64_t* factors3, mi_
     return MI_OK;
 }
 
-mi_status mi_image_resample(mi_context* ctx, const mi_image* in, const mi_geometry* grid, double fill,
-                            mi_image** out) {
+static mi_status resample(mi_context* ctx, const mi_image* in, const mi_geometry* grid, double fill, bool linear,
+                          mi_image** out) {
     if (!ctx || !in || !grid || !out) return MI_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     if (!geo_valid(grid)) return mi::set_error(ctx, MI_ERR_INVALID_ARGUMENT, "bad output geometry");
@@ -396,15 +409,28 @@ mi_status mi_image_resample(mi_context* ctx, const mi_image* in, const mi_geomet
     mi_status s = new_image(ctx, *grid, &res);
     if (s != MI_OK) return s;
     const int64_t n = res->n;
-    k_resample_linear<<<grid_of(n, ctx->num_sms), 256, 0, ctx->stream>>>(in->data, res->data, G, fill);
+    if (linear)
+        k_resample<true><<<grid_of(n, ctx->num_sms), 256, 0, ctx->stream>>>(in->data, res->data, G, fill);
+    else
+        k_resample<false><<<grid_of(n, ctx->num_sms), 256, 0, ctx->stream>>>(in->data, res->data, G, fill);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
         mi_image_free(res);
-        return mi::cuda_status(ctx, e, "mi_image_resample");
+        return mi::cuda_status(ctx, e, linear ? "mi_image_resample" : "mi_image_resample_nearest");
     }
     *out = res;
     return MI_OK;
+}
+
+mi_status mi_image_resample(mi_context* ctx, const mi_image* in, const mi_geometry* grid, double fill,
+                            mi_image** out) {
+    return resample(ctx, in, grid, fill, true, out);
+}
+
+mi_status mi_image_resample_nearest(mi_context* ctx, const mi_image* in, const mi_geometry* grid, double fill,
+                                    mi_image** out) {
+    return resample(ctx, in, grid, fill, false, out);
 }
 
 mi_status mi_pyramid_level(mi_context* ctx, const mi_image* fixed, const mi_image* moving, double sigma,

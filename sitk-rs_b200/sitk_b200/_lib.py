@@ -34,7 +34,7 @@ EXPORTED = [
     "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level", "mi_batch_create", "mi_batch_register",
     "mi_batch_shape", "mi_batch_destroy", "mi_synth_pair", "mi_gemm_bf16_tn", "mi_initnet_create",
     "mi_initnet_destroy", "mi_initnet_get", "mi_initnet_set", "mi_initnet_forward", "mi_initnet_train_step",
-    "mi_initnet_prepare", "mi_metric_create_ex",
+    "mi_initnet_prepare", "mi_metric_create_ex", "mi_image_resample_nearest",
 ]
 
 
@@ -129,6 +129,8 @@ def load(path: str | None = None):
     L.mi_image_smooth.argtypes = [vp, vp, dp, P(vp)]
     L.mi_shrink_geometry.argtypes = [P(MiGeometry), i64p, P(MiGeometry)]
     L.mi_image_resample.argtypes = [vp, vp, P(MiGeometry), ctypes.c_double, P(vp)]
+    L.mi_image_resample_nearest.argtypes = [vp, vp, P(MiGeometry), ctypes.c_double, P(vp)]
+    L.mi_image_resample_nearest.restype = ctypes.c_int
     L.mi_pyramid_level.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int, i64p, P(vp), P(vp)]
     L.mi_metric_get_fused.argtypes = [vp, P(ctypes.c_int)]
     for name in ["mi_image_smooth", "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level",

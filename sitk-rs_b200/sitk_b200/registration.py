@@ -108,23 +108,30 @@ class MultiLevelResult:
 def register_multilevel(fixed: DeviceImage, moving: DeviceImage, transform: ParametricTransform,
                         shrink_factors=(4, 2, 1), smoothing_sigmas=(2.0, 1.0, 0.0), sigmas_physical: bool = True,
                         bins: int = 32, strategy: int | None = 2, percentage: float = 0.1, seed: int = 0,
-                        iterations: int = 200, **rsgd) -> MultiLevelResult:
+                        iterations: int = 200, fixed_mask: DeviceImage | None = None, **rsgd) -> MultiLevelResult:
     """The device registration loop of ImageRegistrationMethod::execute_on_device
     (registration/method.rs:2698-2880) for the Mattes metric: per level, the
     pyramid level (prepare_level: smoothed fixed resampled onto its shrunk grid,
-    smoothed moving), the level's sample draw (same strategy, percentage and seed,
-    over the level's fixed grid), then one regular-step gradient descent run from
-    the previous level's parameters. `transform` is updated in place."""
+    smoothed moving), the level's fixed mask (level_mask_on_device, method.rs:3068-
+    3110: the user mask resampled nearest-neighbour onto the level's grid, fill 0),
+    the level's sample draw (same strategy, percentage and seed, over the level's
+    fixed grid, then gated by the mask), then one regular-step gradient descent run
+    from the previous level's parameters. `transform` is updated in place."""
     from .metric import pyramid_level
     if len(shrink_factors) != len(smoothing_sigmas):
         raise ValueError("PyramidScheduleLength: shrink and smoothing schedules differ in length")
+    if fixed_mask is not None and tuple(fixed_mask.size) != tuple(fixed.size):
+        raise ValueError("MaskSizeMismatch: the fixed mask must lie on the fixed image's grid")
     records = []
     for f, s in zip(shrink_factors, smoothing_sigmas):
         fl, ml = pyramid_level(fixed, moving, s, f, sigmas_physical)
-        metric = DeviceMattesMetric.from_device_sampled(fl, ml, bins=bins, strategy=strategy, percentage=percentage,
-                                                        seed=seed)
+        lm = None if fixed_mask is None else fixed_mask.resample_nearest(fl.geo, 0.0)
+        metric = DeviceMattesMetric.from_device_sampled(fl, ml, fixed_mask=lm, bins=bins, strategy=strategy,
+                                                        percentage=percentage, seed=seed)
         fl.free()
         ml.free()
+        if lm is not None:
+            lm.free()
         records.append(register_rsgd(metric, transform, iterations=iterations, **rsgd))
         metric.close()
     return MultiLevelResult(np.array(transform.params, dtype=np.float64), records)

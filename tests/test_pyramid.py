@@ -166,3 +166,24 @@ def test_device_pyramid_levels_are_the_oracle_bit_for_bit(oracle_lib):
             assert fl.geo.origin[i] == ogeo.origin[i] and fl.geo.spacing[i] == ogeo.spacing[i]
         np.testing.assert_array_equal(fl.to_host(), ofl)
         np.testing.assert_array_equal(ml.to_host(), oml)
+
+
+@pytest.mark.gpu
+def test_nearest_resample_matches_the_oracle_bitwise(oracle_lib):
+    """transform/interpolator.rs:36-54 through the identity (the level-mask resample of
+    registration/method.rs:3068-3110), on a shrunk grid of a non-unit geometry."""
+    import sitk_b200 as sb
+    from sitk_b200.metric import shrink_geometry
+    import oracle
+    rng = np.random.default_rng(2)
+    vol = (rng.random((30, 26, 22)) * 100).astype(np.float32)
+    sp, org = (0.9, 1.2, 1.05), (-4.0, 3.0, 1.5)
+    img = sb.DeviceImage.upload(vol, sp, org)
+    for factors in ((2, 2, 2), (3, 1, 2), (1, 1, 1)):
+        grid = shrink_geometry(img.geo, factors)
+        out = img.resample_nearest(grid, 0.0).to_host()
+        gi = oracle.make_geometry((22, 26, 30), sp, org)
+        go = oracle.shrink_geometry(gi, factors)
+        ref = oracle.resample_nearest(vol, gi, go, 0.0)
+        assert out.shape == ref.shape
+        assert np.array_equal(out.view(np.uint32), ref.view(np.uint32)), factors

@@ -208,3 +208,40 @@ def test_multilevel_registration_matches_the_oracle_level_by_level(oracle_lib):
         p = ref["params"]
     assert np.max(np.abs(res.params - p)) < 1e-3, (res.params, p)
     assert np.max(np.abs(res.params)) > 0.5
+
+
+@pytest.mark.gpu
+def test_masked_multilevel_registration_matches_the_oracle_level_by_level(oracle_lib):
+    # the level loop with a fixed mask: per level the mask is resampled nearest-neighbour
+    # onto the level's grid (level_mask_on_device, method.rs:3068-3110) and gates the
+    # level's samples
+    import sitk_b200 as sb
+    from sitk_b200 import registration
+    n = 40
+    sp, org = (1.0, 0.9, 1.1), (2.0, -1.0, 0.5)
+    fixed = _analytic_volume(n, (0.0, 0.0, 0.0))
+    moving = _analytic_volume(n, (1.5, -1.0, 0.5))
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    mask = (((x - 20) ** 2 + (y - 18) ** 2 + (z - 21) ** 2) < 15 ** 2).astype(np.float32)
+    f = sb.DeviceImage.upload(fixed, sp, org)
+    m = sb.DeviceImage.upload(moving, sp, org)
+    fm = sb.DeviceImage.upload(mask, sp, org)
+    t = sb.TranslationTransform((0.0, 0.0, 0.0))
+    schedule = ((2, 1.0), (1, 0.0))
+    res = registration.register_multilevel(f, m, t, shrink_factors=[s[0] for s in schedule],
+                                           smoothing_sigmas=[s[1] for s in schedule], bins=40, strategy=None,
+                                           iterations=200, minimum_step=0.01, gradient_tolerance=1e-6,
+                                           fixed_mask=fm)
+    g = oracle_lib.make_geometry((n, n, n), sp, org)
+    p = np.zeros(3)
+    for (factor, sigma), level in zip(schedule, res.levels):
+        ofl, ogeo, oml = oracle_lib.pyramid_level(fixed, g, moving, g, sigma, (factor,) * 3)
+        lmask = oracle_lib.level_mask(mask, g, ogeo)
+        ref = oracle_lib.register(ofl, ogeo, oml, g, 40, 3, p, None, fmask=lmask, iterations=200,
+                                  minimum_step=0.01, gradient_tolerance=1e-6, nthreads=8)
+        assert level.valid_points <= int(lmask.sum())
+        assert level.iterations == ref["iterations"], (factor, level, ref)
+        assert abs(level.value - ref["value"]) <= 1e-3 * abs(ref["value"])
+        p = ref["params"]
+    assert np.max(np.abs(res.params - p)) < 1e-3, (res.params, p)
+    assert np.max(np.abs(res.params)) > 0.5
