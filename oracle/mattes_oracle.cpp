@@ -521,7 +521,8 @@ struct Accum {
 
 // The per-sample body of evaluate_global_support (mattes.rs:536-588), or of
 // build_histogram (mattes.rs:451-483) when want_deriv is false.
-inline void sample_body(const Problem& P, const Geometry& G, const Transform& T, int64_t s,
+template <class TransformT>
+inline void sample_body(const Problem& P, const Geometry& G, const TransformT& T, int64_t s,
                         bool want_deriv, Accum& A, int8_t* status, int32_t* fi_out,
                         int32_t* mi_out) {
     const int bins = G.bins;
@@ -898,6 +899,252 @@ double or_kahan_sum(const double* v, int64_t n) { return kahan_sum(v, (size_t)n)
 int64_t or_round_half_integer_up(double x) { return (int64_t)std::floor(x + 0.5); }
 
 int or_invert3(const double* m, double* inv) { return invert3(m, inv) ? OR_OK : OR_SINGULAR_DIRECTION; }
+
+}  // extern "C"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// The cubic B-spline transform (transform/bspline.rs), 3-D, order 3.
+// ---------------------------------------------------------------------------
+
+// bspline.rs:94-106 (the deformation kernel; same basis as the Parzen window, its own
+// expression order)
+double bs_cubic(double u) {
+    double a = std::fabs(u);
+    if (a < 1.0) {
+        double sq = a * a;
+        return (4.0 - 6.0 * sq + 3.0 * sq * a) / 6.0;
+    } else if (a < 2.0) {
+        double sq = a * a;
+        return (8.0 - 12.0 * a + 6.0 * sq - sq * a) / 6.0;
+    }
+    return 0.0;
+}
+
+struct BSpline {
+    int64_t gsize[3];
+    double gorigin[3], gspacing[3], gdir[9], p2i[9];
+    int64_t gstride[3];
+    int64_t nper = 0;
+    const double* coef = nullptr;
+
+    // set_fixed_parameters / from_grid_geometry (bspline.rs:275-321, :638-656):
+    // [gridSize(3), gridOrigin(3), gridSpacing(3), gridDirection(9)]
+    bool init(const double* fp, const double* c, int64_t ncoef) {
+        for (int d = 0; d < 3; ++d) {
+            gsize[d] = fp[d] >= 1.0 ? (int64_t)fp[d] : 0;
+            if (gsize[d] == 0) return false;
+            gorigin[d] = fp[3 + d];
+            gspacing[d] = fp[6 + d];
+        }
+        for (int i = 0; i < 9; ++i) gdir[i] = fp[9 + i];
+        double m[9];
+        for (int r = 0; r < 3; ++r)
+            for (int cc = 0; cc < 3; ++cc) m[r * 3 + cc] = gdir[r * 3 + cc] * gspacing[cc];
+        if (!invert3(m, p2i)) return false;
+        gstride[0] = 1;
+        gstride[1] = gsize[0];
+        gstride[2] = gsize[0] * gsize[1];
+        nper = gsize[0] * gsize[1] * gsize[2];
+        if (ncoef != 3 * nper) return false;
+        coef = c;
+        return true;
+    }
+
+    // bspline.rs:488-499
+    void continuous_index(const double* p, double* idx) const {
+        for (int r = 0; r < 3; ++r) {
+            double acc = -0.0;
+            for (int cc = 0; cc < 3; ++cc) acc += p2i[r * 3 + cc] * (p[cc] - gorigin[cc]);
+            idx[r] = acc;
+        }
+    }
+
+    // bspline.rs:504-520 (the far limit snapped inward)
+    bool inside_valid_region(double* idx) const {
+        const double min_limit = 0.5 * (3.0 - 1.0);
+        for (int d = 0; d < 3; ++d) {
+            const double max_limit = (double)gsize[d] - 0.5 * (3.0 - 1.0) - 1.0;
+            const double ulp = 4.0 * DBL_EPSILON * std::max(std::fabs(max_limit), 1.0);
+            if (std::fabs(idx[d] - max_limit) <= ulp)
+                idx[d] = max_limit - 6.0 * DBL_EPSILON * std::max(std::fabs(max_limit), 1.0);
+            else if (idx[d] >= max_limit || idx[d] < min_limit)
+                return false;
+        }
+        return true;
+    }
+
+    // bspline.rs:525-557: 64 weights, first axis fastest, and the support start
+    void weights(const double* idx, double* w, int64_t* start) const {
+        double w1[3][4];
+        for (int d = 0; d < 3; ++d) {
+            start[d] = (int64_t)std::floor(idx[d] + 0.5 - 3.0 / 2.0);
+            double x = idx[d] - (double)start[d];
+            for (int t = 0; t < 4; ++t) {
+                w1[d][t] = bs_cubic(x);
+                x -= 1.0;
+            }
+        }
+        for (int k = 0; k < 64; ++k) {
+            double prod = 1.0;
+            int rem = k;
+            for (int d = 0; d < 3; ++d) {
+                prod *= w1[d][rem % 4];
+                rem /= 4;
+            }
+            w[k] = prod;
+        }
+    }
+
+    int64_t support_flat(const int64_t* start, int k) const {
+        int rem = k;
+        int64_t flat = 0;
+        for (int d = 0; d < 3; ++d) {
+            flat += (start[d] + rem % 4) * gstride[d];
+            rem /= 4;
+        }
+        return flat;
+    }
+
+    // bspline.rs:561-585
+    void transform_point(const double* x, double* y) const {
+        double idx[3];
+        continuous_index(x, idx);
+        if (!inside_valid_region(idx)) {
+            for (int d = 0; d < 3; ++d) y[d] = x[d];
+            return;
+        }
+        double w[64];
+        int64_t start[3];
+        weights(idx, w, start);
+        double disp[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < 64; ++k) {
+            const int64_t flat = support_flat(start, k);
+            for (int d = 0; d < 3; ++d) disp[d] += w[k] * coef[d * nper + flat];
+        }
+        for (int d = 0; d < 3; ++d) y[d] = x[d] + disp[d];
+    }
+
+    static constexpr int nparams = 0;  // the sparse path never asks for a dense Jacobian
+    void jacobian(const double*, double*) const {}
+};
+
+// mattes_tail's pRatio table (mattes.rs:273-328) beside the value: pratio[f·B + m] =
+// ln(jp/mm)·nFactor where both are above ε, else 0. Returns false when degenerate.
+bool tail_with_pratio(const Geometry& G, Accum& A, double* value, std::vector<double>& pratio) {
+    const int bins = G.bins;
+    pratio.assign((size_t)bins * bins, 0.0);
+    if (A.valid == 0) return false;
+    double joint_sum = kahan_sum(A.joint.data(), A.joint.size());
+    if (joint_sum < DBL_EPSILON) return false;
+    double n_factor = 1.0 / (G.moving_bin_size * (double)A.valid);
+    double inv_sum = 1.0 / joint_sum;
+    for (auto& p : A.joint) p *= inv_sum;
+    for (auto& p : A.fixed_marginal) p *= inv_sum;
+    std::vector<double> mm(bins, 0.0);
+    for (int f = 0; f < bins; ++f)
+        for (int m = 0; m < bins; ++m) mm[m] += A.joint[(size_t)f * bins + m];
+    double sum = 0.0;
+    for (int f = 0; f < bins; ++f) {
+        double fm = A.fixed_marginal[f];
+        if (fm <= DBL_EPSILON) continue;
+        double log_fm = std::log(fm);
+        for (int m = 0; m < bins; ++m) {
+            double mmv = mm[m], jp = A.joint[(size_t)f * bins + m];
+            if (mmv > DBL_EPSILON && jp > DBL_EPSILON) {
+                double pr = std::log(jp / mmv);
+                sum += jp * (pr - log_fm);
+                pratio[(size_t)f * bins + m] = pr * n_factor;
+            }
+        }
+    }
+    *value = -sum;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// A point through the B-spline transform (bspline.rs:561-585); for tests.
+int or_bspline_transform_point(const double* fixed18, const double* coef, int64_t ncoef, const double* x,
+                               double* y) {
+    BSpline T;
+    if (!T.init(fixed18, coef, ncoef)) return OR_BAD_ARGUMENT;
+    T.transform_point(x, y);
+    return OR_OK;
+}
+
+// The Mattes metric through a B-spline transform: evaluate_sparse_support
+// (mattes.rs:722-796). Pass 1 is build_histogram (the same per-sample body as the
+// global-support path, through the B-spline point map); the value and pRatio come
+// from mattes_tail; pass 2 re-walks the samples and, for every valid sample inside the
+// transform's valid region, adds inner·acc to each of its 64·3 coefficients in
+// support order (k, then d), with inner = weight·∇M[d] and acc = Σ_taps B₃′·pRatio.
+// Per-sample status / bins as or_mattes_evaluate.
+int or_bspline_mattes_evaluate(const float* fixed, const or_geometry* fg, const float* moving,
+                               const or_geometry* mg, const uint8_t* fmask, const uint8_t* mmask,
+                               const int64_t* draw, int64_t ndraw, int bins, const double* fixed18,
+                               const double* coef, int64_t ncoef, int want_derivative, double* value,
+                               double* deriv, int64_t* valid, int8_t* status, int32_t* fi_out, int32_t* mi_out) {
+    Problem P;
+    int st = prepare(fixed, fg, moving, mg, fmask, mmask, draw, ndraw, P);
+    if (st) return st;
+    double fmin, fmax, mmin, mmax;
+    ranges(P, &fmin, &fmax, &mmin, &mmax);
+    Geometry G;
+    st = make_geometry(fmin, fmax, mmin, mmax, bins, G);
+    if (st) return st;
+    BSpline T;
+    if (!T.init(fixed18, coef, ncoef)) return OR_BAD_ARGUMENT;
+    Accum A;
+    A.joint.assign((size_t)bins * bins, 0.0);
+    A.fixed_marginal.assign(bins, 0.0);
+    for (int64_t s = 0; s < P.n; ++s) sample_body(P, G, T, s, false, A, status, fi_out, mi_out);
+    if (want_derivative)
+        for (int64_t k = 0; k < ncoef; ++k) deriv[k] = 0.0;
+    *valid = A.valid;
+    std::vector<double> pratio;
+    if (!tail_with_pratio(G, A, value, pratio)) {
+        *value = DBL_MAX;
+        return OR_OK;
+    }
+    if (!want_derivative) return OR_OK;
+    for (int64_t s = 0; s < P.n; ++s) {
+        const int64_t flat = sample_flat(P, s);
+        double fp[3], mp[3], mv, g[3];
+        grid_point(P, flat, fp);
+        const double fv = (double)P.fixed[flat];
+        T.transform_point(fp, mp);
+        if (!moving_value_grad(P, mp, &mv, g, true)) continue;
+        if (mv < G.moving_true_min || mv > G.moving_true_max) continue;
+        double idx[3];
+        T.continuous_index(fp, idx);
+        if (!T.inside_valid_region(idx)) continue;  // empty sparse Jacobian
+        double w[64];
+        int64_t start[3];
+        T.weights(idx, w, start);
+        const double moving_term = mv / G.moving_bin_size - G.moving_normalized_min;
+        const int mi = parzen_index(mv, G.moving_bin_size, G.moving_normalized_min, bins);
+        const int fi = parzen_index(fv, G.fixed_bin_size, G.fixed_normalized_min, bins);
+        for (int k = 0; k < 64; ++k) {
+            const int64_t cp = T.support_flat(start, k);
+            for (int d = 0; d < 3; ++d) {
+                // inner = Σ_e col[e]·∇M[e] with col = w·e_d
+                double inner = -0.0;
+                for (int e = 0; e < 3; ++e) inner += (e == d ? w[k] : 0.0) * g[e];
+                double acc = 0.0;
+                for (int m = mi - 1; m < mi + 3; ++m) {
+                    const double arg = (double)m - moving_term;
+                    acc += cubic_bspline_derivative(arg) * pratio[(size_t)fi * bins + m];
+                }
+                deriv[d * T.nper + cp] += inner * acc;
+            }
+        }
+    }
+    return OR_OK;
+}
 
 // ---------------------------------------------------------------------------
 // The shared-sampler siblings of the Mattes metric, over the same Problem (sample

@@ -221,6 +221,70 @@ def correlation(fixed, fgeo, moving, mgeo, kind, params, fixed_params=None, fmas
                            mmask, draw, derivative)
 
 
+def _bs_bind():
+    L = lib()
+    if not hasattr(L.or_bspline_mattes_evaluate, "_typed"):
+        P = ctypes.POINTER
+        dp, fp, i64p = P(ctypes.c_double), P(ctypes.c_float), P(ctypes.c_int64)
+        L.or_bspline_transform_point.argtypes = [dp, dp, ctypes.c_int64, dp, dp]
+        L.or_bspline_transform_point.restype = ctypes.c_int
+        L.or_bspline_mattes_evaluate.argtypes = [fp, P(OrGeometry), fp, P(OrGeometry), P(ctypes.c_uint8),
+                                                 P(ctypes.c_uint8), i64p, ctypes.c_int64, ctypes.c_int, dp, dp,
+                                                 ctypes.c_int64, ctypes.c_int, dp, dp, i64p, P(ctypes.c_int8),
+                                                 P(ctypes.c_int32), P(ctypes.c_int32)]
+        L.or_bspline_mattes_evaluate.restype = ctypes.c_int
+        L.or_bspline_mattes_evaluate._typed = True
+    return L
+
+
+def bspline_transform_point(fixed18, coef, point):
+    """BSplineTransform::transform_point (transform/bspline.rs:561-585)."""
+    f = np.ascontiguousarray(fixed18, dtype=np.float64)
+    c = np.ascontiguousarray(coef, dtype=np.float64)
+    x = np.ascontiguousarray(point, dtype=np.float64)
+    y = np.zeros(3)
+    st = _bs_bind().or_bspline_transform_point(_ptr(f, ctypes.c_double), _ptr(c, ctypes.c_double), c.size,
+                                               _ptr(x, ctypes.c_double), _ptr(y, ctypes.c_double))
+    if st:
+        raise OracleError(st)
+    return y
+
+
+def bspline_mattes(fixed, fgeo, moving, mgeo, bins, fixed18, coef, fmask=None, mmask=None, draw=None,
+                   derivative=True, per_sample=False):
+    """Mattes value and derivative through a B-spline transform: evaluate_sparse_support
+    (registration/mattes.rs:722-796)."""
+    fixed = np.ascontiguousarray(fixed, dtype=np.float32)
+    moving = np.ascontiguousarray(moving, dtype=np.float32)
+    fm = None if fmask is None else np.ascontiguousarray(np.asarray(fmask) != 0, dtype=np.uint8)
+    mm = None if mmask is None else np.ascontiguousarray(np.asarray(mmask) != 0, dtype=np.uint8)
+    dr = None if draw is None else np.ascontiguousarray(draw, dtype=np.int64)
+    f18 = np.ascontiguousarray(fixed18, dtype=np.float64)
+    c = np.ascontiguousarray(coef, dtype=np.float64)
+    deriv = np.zeros(c.size)
+    value = ctypes.c_double(0.0)
+    valid = ctypes.c_int64(0)
+    status = fi = mi = None
+    if per_sample:
+        nvox = int(np.prod([fgeo.size[i] for i in range(3)]))
+        n = nvox if dr is None else len(dr)
+        status = np.full(n, -1, dtype=np.int8)
+        fi = np.full(n, -1, dtype=np.int32)
+        mi = np.full(n, -1, dtype=np.int32)
+    st = _bs_bind().or_bspline_mattes_evaluate(
+        _ptr(fixed, ctypes.c_float), ctypes.byref(fgeo), _ptr(moving, ctypes.c_float), ctypes.byref(mgeo),
+        _ptr(fm, ctypes.c_uint8), _ptr(mm, ctypes.c_uint8), _ptr(dr, ctypes.c_int64), 0 if dr is None else len(dr),
+        bins, _ptr(f18, ctypes.c_double), _ptr(c, ctypes.c_double), c.size, 1 if derivative else 0,
+        ctypes.byref(value), _ptr(deriv, ctypes.c_double), ctypes.byref(valid), _ptr(status, ctypes.c_int8),
+        _ptr(fi, ctypes.c_int32), _ptr(mi, ctypes.c_int32))
+    if st:
+        raise OracleError(st)
+    out = {"value": value.value, "derivative": deriv, "valid": valid.value}
+    if per_sample:
+        out.update(status=status, fi=fi, mi=mi)
+    return out
+
+
 def transform(kind, params, fixed_params=None, point=None):
     params = np.ascontiguousarray(params, dtype=np.float64)
     fpar = None if fixed_params is None else np.ascontiguousarray(fixed_params, dtype=np.float64)

@@ -88,3 +88,54 @@ class TranslationTransform(ParametricTransform):
 
     def __init__(self, translation=(0.0, 0.0, 0.0)):
         super().__init__(translation, [])
+
+
+class BSplineTransform:
+    """Cubic B-spline free-form deformation (transform/bspline.rs): a control-point grid
+    (size = mesh + 3 per axis) with one coefficient per control point and dimension;
+    x ↦ x + Σ_k w_k(x)·c_k over the 4³ control points whose support covers x, identity
+    outside the grid's valid region. Parameters are the coefficients, dimension-major
+    ([all x][all y][all z], each grid x-fastest); fixed parameters are the grid's
+    [size(3), origin(3), spacing(3), direction(9)], as ITK lays them out."""
+
+    BSPLINE = 4  # no affine form: evaluated through its own device path
+
+    def __init__(self, domain_origin, domain_physical_dimensions, domain_direction, mesh_size):
+        """BSplineTransform::new (bspline.rs:229-272)."""
+        mesh = [int(m) for m in mesh_size]
+        if len(mesh) != 3 or min(mesh) < 1:
+            raise ValueError("InvalidBSplineDomain: three positive mesh sizes")
+        d = [float(v) for v in np.asarray(domain_direction, dtype=np.float64).ravel()]
+        size = [m + 3 for m in mesh]
+        spacing = [float(domain_physical_dimensions[i]) / float(mesh[i]) for i in range(3)]
+        shift = [-0.5 * spacing[i] * (3.0 - 1.0) for i in range(3)]
+        rotated = []
+        for r in range(3):  # core/matrix.rs mat_vec: from 0.0, columns in order
+            acc = 0.0
+            for c in range(3):
+                acc += d[r * 3 + c] * shift[c]
+            rotated.append(acc)
+        origin = [float(domain_origin[i]) + rotated[i] for i in range(3)]
+        self.fixed_params = np.array([float(v) for v in size] + origin + spacing + d, dtype=np.float64)
+        self.grid_size = tuple(size)
+        self.params = np.zeros(3 * size[0] * size[1] * size[2])
+        self.nparams = self.params.size
+
+    @classmethod
+    def from_image_domain(cls, geo, mesh_size):
+        """BSplineTransform::from_image_domain (bspline.rs:324-336): the domain is the
+        image's origin, direction and size·spacing."""
+        phys = [float(geo.size[i]) * float(geo.spacing[i]) for i in range(3)]
+        return cls([geo.origin[i] for i in range(3)], phys, [geo.direction[i] for i in range(9)], mesh_size)
+
+    def number_of_parameters(self) -> int:
+        return self.nparams
+
+    def parameters(self) -> np.ndarray:
+        return self.params.copy()
+
+    def set_parameters(self, p) -> None:
+        p = np.asarray(p, dtype=np.float64)
+        if p.size != self.nparams:
+            raise ValueError("parameter count mismatch")
+        self.params = p.ravel().copy()
