@@ -177,6 +177,22 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
                               const mi_sampling* sampling, int bins, const mi_metric_options* options,
                               mi_metric** out);
 mi_status mi_metric_info_get(const mi_metric* m, mi_metric_info* out);
+
+/* The Mattes value and derivative through a cubic B-spline free-form deformation
+ * (transform/bspline.rs BSplineTransform; registration/mattes.rs:722-796
+ * evaluate_sparse_support), on a Mattes metric handle. fixed18: the control-point
+ * grid as ITK's fixed parameters [size(3), origin(3), spacing(3), direction(9,
+ * row-major)]; coef: the 3·Π size coefficients, dimension-major, each grid x-fastest.
+ * Every sample takes the reference's exact FP64 chain, so validity and both Parzen
+ * bins are the reference's; derivative (may be NULL for the value alone) receives
+ * ∂value/∂coef, summed with atomics (its last bits may vary between runs). */
+mi_status mi_metric_value_and_derivative_bspline(mi_metric* m, const double* fixed18, const double* coef,
+                                                 int64_t ncoef, double* value, double* derivative, int64_t* valid);
+/* Test hook (no reference counterpart): each sample's outcome on the B-spline path in
+ * the metric's sample order (ascending voxel): moving bin | fixed bin << 8 when valid,
+ * else 0. n ≥ the sample count. */
+mi_status mi_metric_bspline_records(mi_metric* m, const double* fixed18, const double* coef, int64_t ncoef,
+                                    uint16_t* records, int64_t n);
 mi_status mi_metric_destroy(mi_metric* m);
 
 /* DeviceMattesMetric::value (device.rs:734-737): value = −MI at the point map given

@@ -1,0 +1,423 @@
+// The Mattes metric through a cubic B-spline free-form deformation: the reference's
+// sparse-support path (registration/mattes.rs:722-796 evaluate_sparse_support) with its
+// BSplineTransform (transform/bspline.rs), on the metric's own samples, masks, ranges
+// and histogram geometry.
+//
+// A B-spline transform has no affine form, so the fast composite map of the affine
+// families does not apply: every sample takes the reference's exact FP64 chain —
+// fixed point (origin-seeded), the control-point grid index, the valid-region test
+// with its far-limit snap, the 4³ cubic weights, the displacement summed in support
+// order, the moving continuous index, mask, inside test, trilinear value — each
+// operation separately rounded in the reference's order, so every sample's validity
+// and both Parzen bins are the reference's exactly.
+//
+//   k_bs_hist   pass 1: the joint histogram (FP64 Parzen taps quantised at the metric's
+//               fine unit 2^-kf, u64 shared-memory copies flushed with u64 atomics) and
+//               a record per sample (bins, Parzen fraction, moving gradient).
+//   k_bs_deriv  every CTA forms the tail from the integer histogram (as the affine
+//               path's k_deriv does), then re-walks the samples: each valid sample
+//               inside the transform's valid region adds weight_k·∇M[d]·Σ_taps B₃′·pRatio
+//               to coefficient (d, support point k) of its 4³·3. Lanes of a warp whose
+//               samples share a support start are summed with a segmented shuffle scan
+//               first, and the run's last lane adds the sum with an FP64 atomic. The
+//               last CTA folds the value slices.
+//
+// The derivative is summed with atomics, so its last bits can differ from run to run;
+// the value, the valid count and the histogram are integer-exact and repeat bitwise.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "internal.h"
+#include "sampler.cuh"
+#include "eval_device.cuh"
+
+namespace mi {
+
+bool invert3(const double* m, double* inv);
+
+namespace {
+
+constexpr int BS_BLOCK = 256;
+
+// The control-point grid (bspline.rs:209-218) and its valid-region limits, formed on
+// the host once per call with the reference's expressions.
+struct BSplineDev {
+    int64_t gsize[3], gstride[3], nper;
+    double gorigin[3], p2i[9];
+    double max_limit[3], snap_ulp[3], snap_to[3];
+};
+
+// bspline.rs:94-106, every operation separately rounded in the reference's order
+__device__ __forceinline__ double bs_cubic(double u) {
+    const double a = fabs(u);
+    if (a < 1.0) {
+        const double sq = __dmul_rn(a, a);
+        return __ddiv_rn(__dadd_rn(__dsub_rn(4.0, __dmul_rn(6.0, sq)), __dmul_rn(__dmul_rn(3.0, sq), a)), 6.0);
+    } else if (a < 2.0) {
+        const double sq = __dmul_rn(a, a);
+        return __ddiv_rn(__dsub_rn(__dadd_rn(__dsub_rn(8.0, __dmul_rn(12.0, a)), __dmul_rn(6.0, sq)), __dmul_rn(sq, a)),
+                         6.0);
+    }
+    return 0.0;
+}
+
+// The fixed grid point, origin-seeded (registration/scales.rs:259-271)
+__device__ __forceinline__ void fixed_point(const SamplerParams& P, uint32_t i, uint32_t j, uint32_t k, double* x) {
+    const double di = (double)i, dj = (double)j, dk = (double)k;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        double acc = P.forigin[r];
+        acc = __dadd_rn(acc, __dmul_rn(P.fi2p[r * 3 + 0], di));
+        acc = __dadd_rn(acc, __dmul_rn(P.fi2p[r * 3 + 1], dj));
+        acc = __dadd_rn(acc, __dmul_rn(P.fi2p[r * 3 + 2], dk));
+        x[r] = acc;
+    }
+}
+
+// The grid index of x (bspline.rs:488-499), the valid-region test with the far-limit
+// snap (:504-520), and the 1-D weights and support start (:525-557). False outside.
+__device__ __forceinline__ bool bs_locate(const BSplineDev& S, const double* x, double (*w1)[4], int64_t* start) {
+    double idx[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        double acc = -0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc = __dadd_rn(acc, __dmul_rn(S.p2i[r * 3 + c], __dsub_rn(x[c], S.gorigin[c])));
+        idx[r] = acc;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (fabs(__dsub_rn(idx[d], S.max_limit[d])) <= S.snap_ulp[d])
+            idx[d] = S.snap_to[d];
+        else if (idx[d] >= S.max_limit[d] || idx[d] < 1.0)
+            return false;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double s = floor(__dsub_rn(__dadd_rn(idx[d], 0.5), 1.5));
+        start[d] = (int64_t)s;
+        double u = __dsub_rn(idx[d], s);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            w1[d][t] = bs_cubic(u);
+            u = __dsub_rn(u, 1.0);
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ double bs_weight(const double (*w1)[4], int k) {
+    return __dmul_rn(__dmul_rn(__dmul_rn(1.0, w1[0][k & 3]), w1[1][(k >> 2) & 3]), w1[2][k >> 4]);
+}
+
+__device__ __forceinline__ int64_t bs_flat(const BSplineDev& S, const int64_t* start, int k) {
+    return (start[0] + (k & 3)) * S.gstride[0] + (start[1] + ((k >> 2) & 3)) * S.gstride[1] +
+           (start[2] + (k >> 4)) * S.gstride[2];
+}
+
+enum { BS_OUTSIDE = 0, BS_OUT_OF_RANGE = 1, BS_VALID = 2 };
+
+// One sample through the B-spline transform and the moving image: status, and for a
+// valid sample the moving Parzen term and bin and the moving physical gradient.
+__device__ int bs_sample(const SamplerParams& P, const BSplineDev& S, const double* __restrict__ coef, uint32_t flat,
+                         const float* __restrict__ moving, const uint8_t* __restrict__ mmask, double& term, int& mi,
+                         double* g) {
+    uint32_t i, j, k;
+    grid_index(P, flat, i, j, k);
+    double x[3], y[3];
+    fixed_point(P, i, j, k, x);
+    double w1[3][4];
+    int64_t start[3];
+    if (bs_locate(S, x, w1, start)) {
+        // bspline.rs:561-585: displacement summed over the 4³ support in order
+        double disp[3] = {0.0, 0.0, 0.0};
+        for (int q = 0; q < 64; ++q) {
+            const double w = bs_weight(w1, q);
+            const int64_t cp = bs_flat(S, start, q);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) disp[d] = __dadd_rn(disp[d], __dmul_rn(w, __ldg(coef + d * S.nper + cp)));
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) y[d] = __dadd_rn(x[d], disp[d]);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) y[d] = x[d];
+    }
+    // the moving continuous index (registration/metric.rs:795-806)
+    const double e0 = __dsub_rn(y[0], P.morigin[0]);
+    const double e1 = __dsub_rn(y[1], P.morigin[1]);
+    const double e2 = __dsub_rn(y[2], P.morigin[2]);
+    double c[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        double acc = __dmul_rn(P.mp2i[r * 3 + 0], e0);
+        acc = __dadd_rn(acc, __dmul_rn(P.mp2i[r * 3 + 1], e1));
+        acc = __dadd_rn(acc, __dmul_rn(P.mp2i[r * 3 + 2], e2));
+        c[r] = acc;
+    }
+    if (P.has_mmask) {
+        uint32_t mflat = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double r = floor(__dadd_rn(c[d], 0.5));
+            if (!(r >= 0.0 && r < (double)P.msz[d])) return BS_OUTSIDE;
+            const uint32_t ri = (uint32_t)r;
+            mflat += d == 0 ? ri : (d == 1 ? ri * P.ms1 : ri * P.ms2);
+        }
+        if (!__ldg(mmask + mflat)) return BS_OUTSIDE;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        if (!(c[d] >= -0.5 && c[d] < P.mhi[d])) return BS_OUTSIDE;
+    const double mv = exact_value(P, c, moving);
+    // the interpolant's exact gradient on the same cell, in FP64 (a continuous weight)
+    double fl[3], fr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        fl[d] = floor(c[d]);
+        fr[d] = c[d] - fl[d];
+    }
+    float v[8];
+    fetch_corners(P, fl, v);
+    double gi[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int b0 = t & 1, b1 = (t >> 1) & 1, b2 = t >> 2;
+        const double w0 = b0 ? fr[0] : 1.0 - fr[0], wy = b1 ? fr[1] : 1.0 - fr[1], wz = b2 ? fr[2] : 1.0 - fr[2];
+        const double b = (double)v[t];
+        gi[0] += (b0 ? 1.0 : -1.0) * (wy * wz) * b;
+        gi[1] += (b1 ? 1.0 : -1.0) * (w0 * wz) * b;
+        gi[2] += (b2 ? 1.0 : -1.0) * (w0 * wy) * b;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) g[d] = gi[0] * P.mp2i[0 * 3 + d] + gi[1] * P.mp2i[1 * 3 + d] + gi[2] * P.mp2i[2 * 3 + d];
+    if (mv < P.moving_min || mv > P.moving_max) return BS_OUT_OF_RANGE;
+    term = __dsub_rn(__ddiv_rn(mv, P.moving_bin_size), P.moving_nmin);
+    mi = parzen_bin(term, P.bins);
+    return BS_VALID;
+}
+
+// Pass 1: histogram and records. The taps are the cubic B-spline of the FP64 fraction
+// f = term − bin (the same polynomial pieces as the affine path), rounded to the fine
+// unit 2^-kf of the metric's global histogram.
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(const SamplerParams P, const BSplineDev S,
+                                                       const double* __restrict__ coef, const EvalArgs a,
+                                                       double fscale) {
+    extern __shared__ __align__(16) unsigned long long bh[];
+    const int B = P.bins, nb = B * B + B;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) bh[q] = 0ull;
+    __syncthreads();
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
+        const uint32_t flat = a.samples ? __ldg(a.samples + s) : s;
+        double term, g[3];
+        int mi = 0;
+        const int st = bs_sample(P, S, coef, flat, a.moving, a.mmask, term, mi, g);
+        if (st != BS_VALID) {
+            a.rec_bins[s] = 0;
+            continue;
+        }
+        const int fi = __ldg(a.fbin + s);
+        const double f = term - (double)mi, h = 1.0 - f, f2 = f * f, f3 = f2 * f;
+        const double w[4] = {h * h * h / 6.0, (3.0 * f3 - 6.0 * f2 + 4.0) / 6.0,
+                             (-3.0 * f3 + 3.0 * f2 + 3.0 * f + 1.0) / 6.0, f3 / 6.0};
+        unsigned long long* row = bh + fi * B + (mi - 1);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) atomicAdd(row + t, __double2ull_rn(w[t] * fscale));
+        atomicAdd(bh + B * B + fi, 1ull);
+        a.rec_bins[s] = (uint16_t)(mi | (fi << 8));
+        a.rec_f[s] = (float)f;
+        a.rec_g[s] = (float)g[0];
+        a.rec_g[(size_t)a.npad + s] = (float)g[1];
+        a.rec_g[2 * (size_t)a.npad + s] = (float)g[2];
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nb; q += blockDim.x)
+        if (bh[q]) atomicAdd(a.ghist + q, bh[q]);
+}
+
+// Pass 2: the tail in every CTA, then the sparse scatter of the derivative.
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_deriv(const SamplerParams P, const BSplineDev S, const EvalArgs a,
+                                                        double* __restrict__ deriv) {
+    extern __shared__ __align__(16) unsigned char bsh[];
+    const int B = P.bins;
+    const TailSmem ts = tail_layout(B, bsh);
+    float* pr = reinterpret_cast<float*>(bsh + tail_smem(B));
+    const TailCtx t = tail_prepare(B, P.moving_bin_size, a, ts);
+    if (!t.degenerate) {
+        pr_table(B, t, ts, pr);
+        value_slices_share(B, a, t, ts, blockIdx.x, gridDim.x);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    if (deriv && !t.degenerate) {
+        const uint32_t stride = gridDim.x * blockDim.x;
+        // whole warps walk contiguous samples together (the loop bound is the warp's)
+        for (uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < a.n; b += stride) {
+            const uint32_t s = b + lane;
+            bool ok = false;
+            double w1[3][4], G[3] = {0.0, 0.0, 0.0};
+            int64_t start[3] = {0, 0, 0};
+            if (s < a.n) {
+                const uint16_t bins = a.rec_bins[s];
+                if (bins) {
+                    const uint32_t flat = a.samples ? __ldg(a.samples + s) : s;
+                    uint32_t i, j, k;
+                    grid_index(P, flat, i, j, k);
+                    double x[3];
+                    fixed_point(P, i, j, k, x);
+                    ok = bs_locate(S, x, w1, start);  // outside the valid region: no derivative
+                    if (ok) {
+                        const int mi = bins & 0xff, fi = bins >> 8;
+                        float dw[4];
+                        bspline3_deriv_taps(a.rec_f[s], dw);
+                        const float* rowp = pr + fi * B + (mi - 1);
+                        const double ws = (double)fmaf(dw[3], rowp[3], fmaf(dw[2], rowp[2], fmaf(dw[1], rowp[1],
+                                                                                               dw[0] * rowp[0])));
+                        G[0] = ws * (double)a.rec_g[s];
+                        G[1] = ws * (double)a.rec_g[(size_t)a.npad + s];
+                        G[2] = ws * (double)a.rec_g[2 * (size_t)a.npad + s];
+                    }
+                }
+            }
+            // runs of consecutive lanes with the same support start (sorted samples make
+            // them long); invalid lanes are runs of their own
+            const long long key = ok ? (long long)(start[0] + S.gsize[0] * (start[1] + S.gsize[1] * start[2]))
+                                     : -1 - (long long)lane;
+            const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+            const bool head = lane == 0 || prev != key;
+            const unsigned int heads = __ballot_sync(0xffffffffu, head);
+            const int run_start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+            const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+            for (int q = 0; q < 64; ++q) {
+                const double wq = ok ? bs_weight(w1, q) : 0.0;
+                const int64_t cp = ok ? bs_flat(S, start, q) : 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    double v = wq * G[d];
+#pragma unroll
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const double u = __shfl_up_sync(0xffffffffu, v, off);
+                        if (lane - off >= run_start) v += u;
+                    }
+                    if (tail && ok) atomicAdd(deriv + d * S.nper + cp, v);
+                }
+            }
+        }
+    }
+    if (!last_to_arrive(a.sync)) return;
+    if (threadIdx.x < 32) fold_value(B, a, t);
+    if (threadIdx.x == 0) a.sync[0] = 0u;
+    for (int q = threadIdx.x; q < B * B + B; q += blockDim.x) a.ghist[q] = 0ull;
+}
+
+}  // namespace
+
+// Host side of the B-spline evaluation (see the entry point below).
+mi_status evaluate_bspline(mi_metric* m, const double* fixed18, const double* coef, int64_t ncoef, double* value,
+                           double* derivative, int64_t* valid, uint16_t* records = nullptr) {
+    mi_context* ctx = m->ctx;
+    if (m->metric_kind != MI_METRIC_MATTES)
+        return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "the B-spline path is a Mattes-metric evaluation");
+    BSplineDev S;
+    double mdir[9];
+    for (int d = 0; d < 3; ++d) {
+        const double sz = fixed18[d];
+        S.gsize[d] = sz >= 1.0 ? (int64_t)sz : 0;  // static_cast<SizeValueType>, as ITK truncates
+        if (S.gsize[d] == 0) return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "InvalidBSplineDomain: a zero grid size");
+        S.gorigin[d] = fixed18[3 + d];
+    }
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) mdir[r * 3 + c] = fixed18[9 + r * 3 + c] * fixed18[6 + c];
+    if (!invert3(mdir, S.p2i)) return set_error(ctx, MI_ERR_SINGULAR_DIRECTION, "singular B-spline grid direction");
+    S.gstride[0] = 1;
+    S.gstride[1] = S.gsize[0];
+    S.gstride[2] = S.gsize[0] * S.gsize[1];
+    S.nper = S.gsize[0] * S.gsize[1] * S.gsize[2];
+    if (ncoef != 3 * S.nper)
+        return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "coefficient count is not 3 × the control-point count");
+    for (int d = 0; d < 3; ++d) {
+        // bspline.rs:504-520
+        const double max_limit = (double)S.gsize[d] - 0.5 * (3.0 - 1.0) - 1.0;
+        const double scale = std::fabs(max_limit) > 1.0 ? std::fabs(max_limit) : 1.0;
+        S.max_limit[d] = max_limit;
+        S.snap_ulp[d] = 4.0 * DBL_EPSILON * scale;
+        S.snap_to[d] = max_limit - 6.0 * DBL_EPSILON * scale;
+    }
+    MI_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if ((size_t)ncoef > m->bs_cap) {
+        cudaFree(m->bs_coef);
+        cudaFree(m->bs_deriv);
+        m->bs_coef = m->bs_deriv = nullptr;
+        m->bs_cap = 0;
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->bs_coef, (size_t)ncoef * sizeof(double)));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->bs_deriv, (size_t)ncoef * sizeof(double)));
+        m->bs_cap = (size_t)ncoef;
+    }
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->bs_coef, coef, (size_t)ncoef * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (derivative) MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->bs_deriv, 0, (size_t)ncoef * sizeof(double), st));
+    Workspace& ws = m->ws;
+    const int B = m->bins;
+    const uint32_t n = (uint32_t)m->n_samples;
+    SamplerParams P = m->base;
+    EvalArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.moving = m->moving;
+    a.mmask = m->mmask;
+    a.samples = m->samples;
+    a.fbin = m->fbin;
+    a.n = n;
+    a.npad = (n + 3u) & ~3u;
+    a.hist_inv = std::ldexp(1.0, -ws.fine_scale_log2);
+    a.ghist = ws.hist;
+    a.rec_bins = ws.rec_bins;
+    a.rec_f = ws.rec_f;
+    a.rec_g = ws.rec_g;
+    a.vsum = ws.vsum;
+    a.sync = ws.done_counter;
+    a.result = ws.result;
+    const size_t hsm = (size_t)(B * B + B) * sizeof(unsigned long long);
+    const size_t dsm = tail_smem(B) + (size_t)B * B * sizeof(float);
+    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_bs_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_bs_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    const int64_t want = ((int64_t)n + BS_BLOCK - 1) / BS_BLOCK;
+    const int ghist = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 4));
+    const int gderiv = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 2));
+    k_bs_hist<<<ghist, BS_BLOCK, hsm, st>>>(P, S, m->bs_coef, a, std::ldexp(1.0, ws.fine_scale_log2));
+    k_bs_deriv<<<gderiv, BS_BLOCK, dsm, st>>>(P, S, a, derivative ? m->bs_deriv : nullptr);
+    MI_CHECK_CUDA(ctx, cudaGetLastError());
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(ws.host_result, ws.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (derivative)
+        MI_CHECK_CUDA(ctx, cudaMemcpyAsync(derivative, m->bs_deriv, (size_t)ncoef * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st));
+    if (records)
+        MI_CHECK_CUDA(ctx, cudaMemcpyAsync(records, ws.rec_bins, (size_t)n * sizeof(uint16_t), cudaMemcpyDeviceToHost,
+                                           st));
+    MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+    if (value) *value = ws.host_result[0];
+    if (valid) *valid = (int64_t)ws.host_result[1];
+    return MI_OK;
+}
+
+}  // namespace mi
+
+extern "C" mi_status mi_metric_value_and_derivative_bspline(mi_metric* m, const double* fixed18, const double* coef,
+                                                            int64_t ncoef, double* value, double* derivative,
+                                                            int64_t* valid) {
+    if (!m || !fixed18 || !coef || !value || ncoef < 1) return MI_ERR_INVALID_ARGUMENT;
+    return mi::evaluate_bspline(m, fixed18, coef, ncoef, value, derivative, valid);
+}
+
+// Per-sample outcome of the B-spline path in the metric's sample order (ascending
+// voxel): moving bin | fixed bin << 8 for a valid sample, 0 otherwise. For the
+// exactness tests.
+extern "C" mi_status mi_metric_bspline_records(mi_metric* m, const double* fixed18, const double* coef,
+                                               int64_t ncoef, uint16_t* records, int64_t n) {
+    if (!m || !fixed18 || !coef || !records || ncoef < 1) return MI_ERR_INVALID_ARGUMENT;
+    if (n < m->n_samples)
+        return mi::set_error(m->ctx, MI_ERR_INVALID_ARGUMENT, "output array shorter than the sample count");
+    double v = 0.0;
+    return mi::evaluate_bspline(m, fixed18, coef, ncoef, &v, nullptr, nullptr, records);
+}

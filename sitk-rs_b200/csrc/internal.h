@@ -146,6 +146,9 @@ struct mi_metric {
     mi::SamplerParams base{};     // everything except the stages
     mi::Workspace ws;
     mi::MomentsWs mom;
+    double* bs_coef = nullptr;    // B-spline coefficients of the last call (bspline.cu)
+    double* bs_deriv = nullptr;   // its derivative
+    size_t bs_cap = 0;            // capacity of both, in doubles
 };
 
 namespace mi {

@@ -274,6 +274,8 @@ void free_metric(mi_metric* m) {
     for (int i = 0; i < 5; ++i)
         if (m->ws.ev[i]) cudaEventDestroy(m->ws.ev[i]);
     moments_free(m);
+    cudaFree(m->bs_coef);
+    cudaFree(m->bs_deriv);
     delete m;
 }
 

@@ -35,6 +35,7 @@ EXPORTED = [
     "mi_batch_shape", "mi_batch_destroy", "mi_synth_pair", "mi_gemm_bf16_tn", "mi_initnet_create",
     "mi_initnet_destroy", "mi_initnet_get", "mi_initnet_set", "mi_initnet_forward", "mi_initnet_train_step",
     "mi_initnet_prepare", "mi_metric_create_ex", "mi_image_resample_nearest",
+    "mi_metric_value_and_derivative_bspline", "mi_metric_bspline_records",
 ]
 
 
@@ -131,6 +132,10 @@ def load(path: str | None = None):
     L.mi_image_resample.argtypes = [vp, vp, P(MiGeometry), ctypes.c_double, P(vp)]
     L.mi_image_resample_nearest.argtypes = [vp, vp, P(MiGeometry), ctypes.c_double, P(vp)]
     L.mi_image_resample_nearest.restype = ctypes.c_int
+    L.mi_metric_value_and_derivative_bspline.argtypes = [vp, dp, dp, ctypes.c_int64, dp, dp, i64p]
+    L.mi_metric_value_and_derivative_bspline.restype = ctypes.c_int
+    L.mi_metric_bspline_records.argtypes = [vp, dp, dp, ctypes.c_int64, P(ctypes.c_uint16), ctypes.c_int64]
+    L.mi_metric_bspline_records.restype = ctypes.c_int
     L.mi_pyramid_level.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int, i64p, P(vp), P(vp)]
     L.mi_metric_get_fused.argtypes = [vp, P(ctypes.c_int)]
     for name in ["mi_image_smooth", "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level",

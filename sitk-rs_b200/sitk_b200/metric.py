@@ -244,6 +244,8 @@ class DeviceMattesMetric:
         return int(self.info()["n_samples"])
 
     def value(self, transform: ParametricTransform) -> float:
+        if getattr(transform, "BSPLINE", None):
+            return self._bspline(transform, False).value
         st = self.stages(transform)
         v = ctypes.c_double()
         _lib.check(_lib.load().mi_metric_value(self.handle, st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
@@ -258,7 +260,21 @@ class DeviceMattesMetric:
                                                st.size // 12, ctypes.byref(v), ctypes.byref(n)), self.ctx.handle)
         return v.value, n.value
 
+    def _bspline(self, transform, derivative: bool):
+        fp = np.ascontiguousarray(transform.fixed_params, dtype=np.float64)
+        c = np.ascontiguousarray(transform.params, dtype=np.float64)
+        d = np.zeros(c.size) if derivative else None
+        v = ctypes.c_double()
+        n = ctypes.c_int64()
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.check(_lib.load().mi_metric_value_and_derivative_bspline(
+            self.handle, fp.ctypes.data_as(dp), c.ctypes.data_as(dp), c.size, ctypes.byref(v),
+            d.ctypes.data_as(dp) if derivative else None, ctypes.byref(n)), self.ctx.handle)
+        return MetricValue(v.value, d, n.value)
+
     def evaluate(self, transform: ParametricTransform) -> MetricValue:
+        if getattr(transform, "BSPLINE", None):
+            return self._bspline(transform, True)
         params = transform.params.tolist()
         fixed = transform.fixed_params.tolist()
         n, nf = len(params), len(fixed)
