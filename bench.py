@@ -452,6 +452,26 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             sib[name] = {"evals_per_s": snev / (sms[0] / 1e3), "ms_per_eval": sms[0] / snev,
                          "launches_per_eval": 1 if name == "mean_squares" else 2}
             sm.close()
+        # the same metric through a cubic B-spline transform (mesh 8³ over the fixed
+        # image, coefficients N(0, 1 mm), seeded): value + derivative of all 3·11³
+        # coefficients, timed end to end on the stream (torch events around the call)
+        from sitk_b200.transforms import BSplineTransform
+        from sitk_b200.metric import geometry
+        bst = BSplineTransform.from_image_domain(geometry((N, N, N)), (8, 8, 8))
+        bst.set_parameters(np.random.default_rng(SEED).standard_normal(bst.nparams))
+        for _ in range(3):
+            metric.evaluate(bst)
+        bs_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(20)]
+        for e0, e1 in bs_ev:
+            l2_flush()
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            metric.evaluate(bst)
+            e1.record(stream)
+        torch.cuda.synchronize(dev)
+        bms = sum(a.elapsed_time(b) for a, b in bs_ev) / len(bs_ev)
+        sib["mattes_bspline_8x8x8"] = {"evals_per_s": 1e3 / bms, "ms_per_eval": bms, "parameters": bst.nparams,
+                                       "timing": "end to end per call (events around the synchronous call)"}
     reg = None if args.no_registration else time_registration(pair, ctx, dev)
     batch = None if args.no_batch else time_batch(ctx, dev, SEED)
     line = {

@@ -14,16 +14,19 @@
 //   k_bs_hist   pass 1: the joint histogram (FP64 Parzen taps quantised at the metric's
 //               fine unit 2^-kf, u64 shared-memory copies flushed with u64 atomics) and
 //               a record per sample (bins, Parzen fraction, moving gradient).
-//   k_bs_deriv  every CTA forms the tail from the integer histogram (as the affine
-//               path's k_deriv does), then re-walks the samples: each valid sample
-//               inside the transform's valid region adds weight_k·∇M[d]·Σ_taps B₃′·pRatio
-//               to coefficient (d, support point k) of its 4³·3. Lanes of a warp whose
-//               samples share a support start are summed with a segmented shuffle scan
-//               first, and the run's last lane adds the sum with an FP64 atomic. The
-//               last CTA folds the value slices.
+//   k_bs_tail   one CTA: the tail from the integer histogram (value, and the
+//               pRatio·nFactor table into global memory).
+//   k_bs_cell_deriv  one CTA per support cell of the grid (the samples grouped by cell
+//               once per grid, k_bs_cell_of + a stable radix sort): each valid sample of
+//               the cell adds weight_k·∇M[d]·Σ_taps B₃′·pRatio to coefficient (d, support
+//               point k) of the cell's 4³·3; the CTA sums them and adds each sum once.
 //
-// The derivative is summed with atomics, so its last bits can differ from run to run;
-// the value, the valid count and the histogram are integer-exact and repeat bitwise.
+// Each coefficient receives the sums of the (up to 64) cells that share it through
+// FP64 atomics, so the derivative's last bits can differ from run to run; the value,
+// the valid count and the histogram are integer-exact and repeat bitwise.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -47,6 +50,7 @@ struct BSplineDev {
     int64_t gsize[3], gstride[3], nper;
     double gorigin[3], p2i[9];
     double max_limit[3], snap_ulp[3], snap_to[3];
+    int smem_coef;  // pass 1 stages the coefficients in shared memory
 };
 
 // bspline.rs:94-106, every operation separately rounded in the reference's order
@@ -121,7 +125,7 @@ enum { BS_OUTSIDE = 0, BS_OUT_OF_RANGE = 1, BS_VALID = 2 };
 
 // One sample through the B-spline transform and the moving image: status, and for a
 // valid sample the moving Parzen term and bin and the moving physical gradient.
-__device__ int bs_sample(const SamplerParams& P, const BSplineDev& S, const double* __restrict__ coef, uint32_t flat,
+__device__ int bs_sample(const SamplerParams& P, const BSplineDev& S, const double* coef, uint32_t flat,
                          const float* __restrict__ moving, const uint8_t* __restrict__ mmask, double& term, int& mi,
                          double* g) {
     uint32_t i, j, k;
@@ -132,12 +136,22 @@ __device__ int bs_sample(const SamplerParams& P, const BSplineDev& S, const doub
     int64_t start[3];
     if (bs_locate(S, x, w1, start)) {
         // bspline.rs:561-585: displacement summed over the 4³ support in order
-        double disp[3] = {0.0, 0.0, 0.0};
-        for (int q = 0; q < 64; ++q) {
-            const double w = bs_weight(w1, q);
-            const int64_t cp = bs_flat(S, start, q);
+        // weight q = ((1·wx)·wy)·wz as the reference forms it: the 16 (1·wx)·wy
+        // products once, then one product per support point
+        double wxy[16];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) disp[d] = __dadd_rn(disp[d], __dmul_rn(w, __ldg(coef + d * S.nper + cp)));
+        for (int q = 0; q < 16; ++q) wxy[q] = __dmul_rn(__dmul_rn(1.0, w1[0][q & 3]), w1[1][q >> 2]);
+        double disp[3] = {0.0, 0.0, 0.0};
+        const int64_t base = start[0] * S.gstride[0] + start[1] * S.gstride[1] + start[2] * S.gstride[2];
+#pragma unroll
+        for (int tz = 0; tz < 4; ++tz) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const double w = __dmul_rn(wxy[q], w1[2][tz]);
+                const int64_t cp = base + (q & 3) + (q >> 2) * S.gstride[1] + tz * S.gstride[2];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) disp[d] = __dadd_rn(disp[d], __dmul_rn(w, coef[d * S.nper + cp]));
+            }
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) y[d] = __dadd_rn(x[d], disp[d]);
@@ -208,12 +222,19 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(const SamplerParams P, con
     extern __shared__ __align__(16) unsigned long long bh[];
     const int B = P.bins, nb = B * B + B;
     for (int q = threadIdx.x; q < nb; q += blockDim.x) bh[q] = 0ull;
+    // the coefficients in shared memory when they fit (the launch sized it), else global
+    const double* cf = coef;
+    if (S.smem_coef) {
+        double* sc = reinterpret_cast<double*>(bh + ((nb + 1) & ~1));
+        for (int64_t q = threadIdx.x; q < 3 * S.nper; q += blockDim.x) sc[q] = __ldg(coef + q);
+        cf = sc;
+    }
     __syncthreads();
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
         const uint32_t flat = a.samples ? __ldg(a.samples + s) : s;
         double term, g[3];
         int mi = 0;
-        const int st = bs_sample(P, S, coef, flat, a.moving, a.mmask, term, mi, g);
+        const int st = bs_sample(P, S, cf, flat, a.moving, a.mmask, term, mi, g);
         if (st != BS_VALID) {
             a.rec_bins[s] = 0;
             continue;
@@ -237,9 +258,34 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(const SamplerParams P, con
         if (bh[q]) atomicAdd(a.ghist + q, bh[q]);
 }
 
-// Pass 2: the tail in every CTA, then the sparse scatter of the derivative.
-__global__ void __launch_bounds__(BS_BLOCK) k_bs_deriv(const SamplerParams P, const BSplineDev S, const EvalArgs a,
-                                                        double* __restrict__ deriv) {
+// The support cell of every sample: its grid start (exact, as pass 1 forms it) as one
+// index over the (gsize − 3)³ cells, or NO_CELL outside the transform's valid region.
+// Depends on the fixed points and the grid only, so it is formed once per grid.
+constexpr uint32_t NO_CELL = 0xffffffffu;
+__global__ void k_bs_cell_of(const SamplerParams P, const BSplineDev S, const uint32_t* __restrict__ samples,
+                             uint32_t n, uint32_t* __restrict__ cell, uint32_t* __restrict__ idx,
+                             uint32_t* __restrict__ count) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const uint32_t flat = samples ? __ldg(samples + s) : s;
+        uint32_t i, j, k;
+        grid_index(P, flat, i, j, k);
+        double x[3], w1[3][4];
+        int64_t st[3];
+        fixed_point(P, i, j, k, x);
+        uint32_t c = NO_CELL;
+        if (bs_locate(S, x, w1, st)) {
+            c = (uint32_t)(st[0] + (S.gsize[0] - 3) * (st[1] + (S.gsize[1] - 3) * st[2]));
+            atomicAdd(count + c, 1u);
+        }
+        cell[s] = c;
+        idx[s] = s;
+    }
+}
+
+// The tail once (one CTA): value slices folded into the result, the pRatio·nFactor
+// table into global memory for the cells, the global histogram re-zeroed.
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_tail(const SamplerParams P, const EvalArgs a,
+                                                       float* __restrict__ pr_out) {
     extern __shared__ __align__(16) unsigned char bsh[];
     const int B = P.bins;
     const TailSmem ts = tail_layout(B, bsh);
@@ -247,69 +293,119 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_deriv(const SamplerParams P, co
     const TailCtx t = tail_prepare(B, P.moving_bin_size, a, ts);
     if (!t.degenerate) {
         pr_table(B, t, ts, pr);
-        value_slices_share(B, a, t, ts, blockIdx.x, gridDim.x);
+        value_slices_share(B, a, t, ts, 0, 1);
+    } else {
+        for (int q = threadIdx.x; q < B * B; q += blockDim.x) pr[q] = 0.0f;
     }
+    __threadfence_block();
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    if (deriv && !t.degenerate) {
-        const uint32_t stride = gridDim.x * blockDim.x;
-        // whole warps walk contiguous samples together (the loop bound is the warp's)
-        for (uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); b < a.n; b += stride) {
-            const uint32_t s = b + lane;
-            bool ok = false;
-            double w1[3][4], G[3] = {0.0, 0.0, 0.0};
-            int64_t start[3] = {0, 0, 0};
-            if (s < a.n) {
-                const uint16_t bins = a.rec_bins[s];
-                if (bins) {
-                    const uint32_t flat = a.samples ? __ldg(a.samples + s) : s;
-                    uint32_t i, j, k;
-                    grid_index(P, flat, i, j, k);
-                    double x[3];
-                    fixed_point(P, i, j, k, x);
-                    ok = bs_locate(S, x, w1, start);  // outside the valid region: no derivative
-                    if (ok) {
-                        const int mi = bins & 0xff, fi = bins >> 8;
-                        float dw[4];
-                        bspline3_deriv_taps(a.rec_f[s], dw);
-                        const float* rowp = pr + fi * B + (mi - 1);
-                        const double ws = (double)fmaf(dw[3], rowp[3], fmaf(dw[2], rowp[2], fmaf(dw[1], rowp[1],
-                                                                                               dw[0] * rowp[0])));
-                        G[0] = ws * (double)a.rec_g[s];
-                        G[1] = ws * (double)a.rec_g[(size_t)a.npad + s];
-                        G[2] = ws * (double)a.rec_g[2 * (size_t)a.npad + s];
-                    }
-                }
-            }
-            // runs of consecutive lanes with the same support start (sorted samples make
-            // them long); invalid lanes are runs of their own
-            const long long key = ok ? (long long)(start[0] + S.gsize[0] * (start[1] + S.gsize[1] * start[2]))
-                                     : -1 - (long long)lane;
-            const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
-            const bool head = lane == 0 || prev != key;
-            const unsigned int heads = __ballot_sync(0xffffffffu, head);
-            const int run_start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
-            const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
-            for (int q = 0; q < 64; ++q) {
-                const double wq = ok ? bs_weight(w1, q) : 0.0;
-                const int64_t cp = ok ? bs_flat(S, start, q) : 0;
+    for (int q = threadIdx.x; q < B * B; q += blockDim.x) pr_out[q] = pr[q];
+    if (threadIdx.x < 32) fold_value(B, a, t);
+    for (int q = threadIdx.x; q < B * B + B; q += blockDim.x) a.ghist[q] = 0ull;
+}
+
+// One CTA per support cell: the derivative of the 4³·3 coefficients over the cell's
+// samples (sorted by cell), summed in the CTA and added once per coefficient. Thread t
+// owns the four support points of column (kx, ky) = t mod 16 for the samples
+// j ≡ ⌊t/16⌋ (mod 16) of each staged group; the sixteen partial sums are then combined
+// in order. The support weights are continuous factors of the derivative, formed in
+// FP32 from the FP64 grid index; the sums are FP64.
+__global__ void __launch_bounds__(BS_BLOCK) k_bs_cell_deriv(const SamplerParams P, const BSplineDev S,
+                                                             const EvalArgs a, const float* __restrict__ pr_g,
+                                                             const uint32_t* __restrict__ order,
+                                                             const uint32_t* __restrict__ off,
+                                                             double* __restrict__ deriv) {
+    extern __shared__ __align__(16) unsigned char csh[];
+    const int B = P.bins;
+    float* pr = reinterpret_cast<float*>(csh);                  // B²
+    float* sg = pr + ((B * B + 3) & ~3);                        // [3][BS_BLOCK] weighted gradient
+    float* sw = sg + 3 * BS_BLOCK;                              // [12][BS_BLOCK] 1-D weights
+    __shared__ double red[3][BS_BLOCK];
+    const uint32_t c = blockIdx.x;
+    const uint32_t beg = off[c], end = off[c + 1];
+    if (beg == end) return;
+    for (int q = threadIdx.x; q < B * B; q += blockDim.x) pr[q] = __ldg(pr_g + q);
+    const int64_t ncx = S.gsize[0] - 3, ncy = S.gsize[1] - 3;
+    const int64_t st[3] = {(int64_t)(c % ncx), (int64_t)((c / ncx) % ncy), (int64_t)(c / (ncx * ncy))};
+    // thread t: support column (kx, ky) = t & 15 for all four kz, samples j ≡ t >> 4 (mod 16)
+    const int t = threadIdx.x, kxy = t & 15, phase = t >> 4;
+    const int kx = kxy & 3, ky = kxy >> 2;
+    double acc[4][3] = {};
+    __syncthreads();
+    for (uint32_t base = beg; base < end; base += BS_BLOCK) {
+        const uint32_t j = base + t;
+        float G[3] = {0.0f, 0.0f, 0.0f}, W[12];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    double v = wq * G[d];
+        for (int q = 0; q < 12; ++q) W[q] = 0.0f;
+        if (j < end) {
+            const uint32_t s = __ldg(order + j);
+            const uint16_t bins = a.rec_bins[s];
+            if (bins) {
+                const int mi = bins & 0xff, fi = bins >> 8;
+                float dw[4];
+                bspline3_deriv_taps(a.rec_f[s], dw);
+                const float* row = pr + fi * B + (mi - 1);
+                const float ws = fmaf(dw[3], row[3], fmaf(dw[2], row[2], fmaf(dw[1], row[1], dw[0] * row[0])));
+                G[0] = ws * a.rec_g[s];
+                G[1] = ws * a.rec_g[(size_t)a.npad + s];
+                G[2] = ws * a.rec_g[2 * (size_t)a.npad + s];
+                const uint32_t flat = a.samples ? __ldg(a.samples + s) : s;
+                uint32_t i, jj, kk;
+                grid_index(P, flat, i, jj, kk);
+                double x[3];
+                fixed_point(P, i, jj, kk, x);
 #pragma unroll
-                    for (int off = 1; off < 32; off <<= 1) {
-                        const double u = __shfl_up_sync(0xffffffffu, v, off);
-                        if (lane - off >= run_start) v += u;
+                for (int r = 0; r < 3; ++r) {
+                    double g = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) g += S.p2i[r * 3 + q] * (x[q] - S.gorigin[q]);
+                    float u = (float)(g - (double)st[r]);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float au = fabsf(u), sq = au * au;
+                        W[r * 4 + q] = au < 1.0f ? (4.0f - 6.0f * sq + 3.0f * sq * au) * (1.0f / 6.0f)
+                                                 : (au < 2.0f ? (2.0f - au) * (2.0f - au) * (2.0f - au) * (1.0f / 6.0f)
+                                                              : 0.0f);
+                        u -= 1.0f;
                     }
-                    if (tail && ok) atomicAdd(deriv + d * S.nper + cp, v);
                 }
             }
         }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sg[d * BS_BLOCK + t] = G[d];
+#pragma unroll
+        for (int q = 0; q < 12; ++q) sw[q * BS_BLOCK + t] = W[q];
+        __syncthreads();
+        const int cnt = (int)min((uint32_t)BS_BLOCK, end - base);
+        for (int jj = phase; jj < cnt; jj += 16) {
+            const float wxy = sw[kx * BS_BLOCK + jj] * sw[(4 + ky) * BS_BLOCK + jj];
+            const double g0 = (double)sg[jj], g1 = (double)sg[BS_BLOCK + jj], g2 = (double)sg[2 * BS_BLOCK + jj];
+#pragma unroll
+            for (int kz = 0; kz < 4; ++kz) {
+                const double w = (double)(wxy * sw[(8 + kz) * BS_BLOCK + jj]);
+                acc[kz][0] += w * g0;
+                acc[kz][1] += w * g1;
+                acc[kz][2] += w * g2;
+            }
+        }
+        __syncthreads();
     }
-    if (!last_to_arrive(a.sync)) return;
-    if (threadIdx.x < 32) fold_value(B, a, t);
-    if (threadIdx.x == 0) a.sync[0] = 0u;
-    for (int q = threadIdx.x; q < B * B + B; q += blockDim.x) a.ghist[q] = 0ull;
+    // the 16 phases of each column, summed in phase order
+    for (int kz = 0; kz < 4; ++kz) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) red[d][t] = acc[kz][d];
+        __syncthreads();
+        if (t < 16) {
+            const int64_t cp = (st[0] + kx) * S.gstride[0] + (st[1] + ky) * S.gstride[1] + (st[2] + kz) * S.gstride[2];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double v = 0.0;
+                for (int ph = 0; ph < 16; ++ph) v += red[d][t + 16 * ph];
+                if (v != 0.0) atomicAdd(deriv + d * S.nper + cp, v);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 }  // namespace
@@ -321,6 +417,7 @@ mi_status evaluate_bspline(mi_metric* m, const double* fixed18, const double* co
     if (m->metric_kind != MI_METRIC_MATTES)
         return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "the B-spline path is a Mattes-metric evaluation");
     BSplineDev S;
+    S.smem_coef = 0;
     double mdir[9];
     for (int d = 0; d < 3; ++d) {
         const double sz = fixed18[d];
@@ -378,15 +475,73 @@ mi_status evaluate_bspline(mi_metric* m, const double* fixed18, const double* co
     a.vsum = ws.vsum;
     a.sync = ws.done_counter;
     a.result = ws.result;
-    const size_t hsm = (size_t)(B * B + B) * sizeof(unsigned long long);
-    const size_t dsm = tail_smem(B) + (size_t)B * B * sizeof(float);
-    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_bs_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
-    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_bs_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
     const int64_t want = ((int64_t)n + BS_BLOCK - 1) / BS_BLOCK;
+    // the samples grouped by support cell: formed once per grid (the cell of a sample
+    // depends on the fixed point and the grid only)
+    if (derivative && (!m->bs_have_key || std::memcmp(m->bs_key, fixed18, sizeof(m->bs_key)) != 0)) {
+        m->bs_have_key = false;
+        cudaFree(m->bs_order);
+        cudaFree(m->bs_off);
+        m->bs_order = nullptr;
+        m->bs_off = nullptr;
+        const bool any = S.gsize[0] > 3 && S.gsize[1] > 3 && S.gsize[2] > 3;
+        const int64_t ncells = any ? (S.gsize[0] - 3) * (S.gsize[1] - 3) * (S.gsize[2] - 3) : 0;
+        if (ncells >= (int64_t)0xffffffffu)
+            return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "B-spline grid too large (≥ 2^32 support cells)");
+        m->bs_ncells = ncells;
+        if (ncells > 0 && n > 0) {
+            uint32_t *cell = nullptr, *idx = nullptr, *cell_sorted = nullptr, *count = nullptr;
+            void* tmp = nullptr;
+            size_t sort_bytes = 0, scan_bytes = 0;
+            cudaError_t e = cudaMalloc(&cell, (size_t)n * 4);
+            if (e == cudaSuccess) e = cudaMalloc(&idx, (size_t)n * 4);
+            if (e == cudaSuccess) e = cudaMalloc(&cell_sorted, (size_t)n * 4);
+            if (e == cudaSuccess) e = cudaMalloc(&count, (size_t)(ncells + 1) * 4);
+            if (e == cudaSuccess) e = cudaMalloc(&m->bs_order, (size_t)n * 4);
+            if (e == cudaSuccess) e = cudaMalloc(&m->bs_off, (size_t)(ncells + 1) * 4);
+            if (e == cudaSuccess) e = cudaMemsetAsync(count, 0, (size_t)(ncells + 1) * 4, st);
+            if (e == cudaSuccess) {
+                const int g = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 8));
+                k_bs_cell_of<<<g, BS_BLOCK, 0, st>>>(P, S, m->samples, n, cell, idx, count);
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess)
+                e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, cell, cell_sorted, idx, m->bs_order, (int)n, 0,
+                                                    32, st);
+            if (e == cudaSuccess)
+                e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, count, m->bs_off, (int)(ncells + 1), st);
+            if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max(sort_bytes, scan_bytes));
+            if (e == cudaSuccess)
+                e = cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, cell, cell_sorted, idx, m->bs_order, (int)n, 0, 32,
+                                                    st);
+            if (e == cudaSuccess)
+                e = cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, count, m->bs_off, (int)(ncells + 1), st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            cudaFree(tmp);
+            cudaFree(cell);
+            cudaFree(idx);
+            cudaFree(cell_sorted);
+            cudaFree(count);
+            if (e != cudaSuccess) return cuda_status(ctx, e, "B-spline support cells");
+        }
+        std::memcpy(m->bs_key, fixed18, sizeof(m->bs_key));
+        m->bs_have_key = true;
+    }
+    if (!m->bs_pr) MI_CHECK_CUDA(ctx, cudaMalloc(&m->bs_pr, (size_t)B * B * sizeof(float)));
+    size_t hsm = (size_t)(((B * B + B) + 1) & ~1) * sizeof(unsigned long long);
+    S.smem_coef = hsm + (size_t)ncoef * sizeof(double) <= 96 * 1024 ? 1 : 0;
+    if (S.smem_coef) hsm += (size_t)ncoef * sizeof(double);
+    const size_t tsm = tail_smem(B) + (size_t)B * B * sizeof(float);
+    const size_t csm = (size_t)((B * B + 3) & ~3) * sizeof(float) + (size_t)15 * BS_BLOCK * sizeof(float);
+    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_bs_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm));
+    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_bs_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_bs_cell_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
     const int ghist = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 4));
-    const int gderiv = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->num_sms * 2));
     k_bs_hist<<<ghist, BS_BLOCK, hsm, st>>>(P, S, m->bs_coef, a, std::ldexp(1.0, ws.fine_scale_log2));
-    k_bs_deriv<<<gderiv, BS_BLOCK, dsm, st>>>(P, S, a, derivative ? m->bs_deriv : nullptr);
+    k_bs_tail<<<1, BS_BLOCK, tsm, st>>>(P, a, m->bs_pr);
+    if (derivative && m->bs_ncells > 0 && n > 0)
+        k_bs_cell_deriv<<<(unsigned)m->bs_ncells, BS_BLOCK, csm, st>>>(P, S, a, m->bs_pr, m->bs_order, m->bs_off,
+                                                                        m->bs_deriv);
     MI_CHECK_CUDA(ctx, cudaGetLastError());
     MI_CHECK_CUDA(ctx, cudaMemcpyAsync(ws.host_result, ws.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (derivative)

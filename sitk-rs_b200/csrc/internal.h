@@ -149,6 +149,13 @@ struct mi_metric {
     double* bs_coef = nullptr;    // B-spline coefficients of the last call (bspline.cu)
     double* bs_deriv = nullptr;   // its derivative
     size_t bs_cap = 0;            // capacity of both, in doubles
+    // the samples grouped by B-spline support cell, for the grid in bs_key
+    double bs_key[18] = {};
+    bool bs_have_key = false;
+    uint32_t* bs_order = nullptr;  // sample indices sorted by cell (valid-region samples first)
+    uint32_t* bs_off = nullptr;    // [cells + 1] offsets into bs_order
+    int64_t bs_ncells = 0;
+    float* bs_pr = nullptr;        // the pRatio·nFactor table of the last evaluation
 };
 
 namespace mi {

@@ -276,6 +276,9 @@ void free_metric(mi_metric* m) {
     moments_free(m);
     cudaFree(m->bs_coef);
     cudaFree(m->bs_deriv);
+    cudaFree(m->bs_order);
+    cudaFree(m->bs_off);
+    cudaFree(m->bs_pr);
     delete m;
 }
 
