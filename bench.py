@@ -115,10 +115,18 @@ def _peaks():
 
 
 def _kernel_source_hash() -> str:
+    """Hash of the device code of the evaluation kernels: sampler.cuh, eval_device.cuh
+    and the kernel section of mattes.cu (host code there does not change the traffic)."""
     h = hashlib.sha256()
-    for name in ("sampler.cuh", "eval_device.cuh", "mattes.cu"):
-        with open(os.path.join(ROOT, "sitk-rs_b200", "csrc", name), "rb") as f:
+    csrc = os.path.join(ROOT, "sitk-rs_b200", "csrc")
+    for name in ("sampler.cuh", "eval_device.cuh"):
+        with open(os.path.join(csrc, name), "rb") as f:
             h.update(f.read())
+    with open(os.path.join(csrc, "mattes.cu"), encoding="utf-8") as f:
+        text = f.read()
+    a = text.index("// Kernels. The fused evaluation")
+    b = text.index("// Set-up kernels:")
+    h.update(text[a:b].encode())
     return h.hexdigest()[:16]
 
 
