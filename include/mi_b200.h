@@ -130,6 +130,20 @@ mi_status mi_image_geometry(const mi_image* img, mi_geometry* out);
 const float* mi_image_device_ptr(const mi_image* img);
 mi_status mi_image_free(mi_image* img);
 
+/* MetaImage (.mha, or .mhd beside its raw file) reader for 3-D scalar volumes
+ * (io/meta_image.rs read): the header's geometry (ElementSpacing; Offset / Position /
+ * Origin and Orientation / Rotation / TransformMatrix in MetaIO's fixed precedence;
+ * the last value of a repeated key), any of the ten scalar ElementTypes in either
+ * byte order, pixels LOCAL or in a named file, zlib/gzip compressed or not; uploaded
+ * with mi_image_upload's casts. Refused with MI_ERR_INVALID_ARGUMENT (detail in
+ * mi_last_error): other dimensions than 3, more than one channel, ElementDataFile =
+ * LIST, a LOCAL compressed header without CompressedDataSize, truncated data. */
+mi_status mi_image_read_meta(mi_context* ctx, const char* path, mi_image** out);
+/* The same on the host only: the geometry, and (when dst is not NULL) the voxels cast
+ * to f32 as the upload casts them into dst (n_elements ≥ the voxel count). Needs no
+ * device. */
+mi_status mi_image_read_meta_host(const char* path, mi_geometry* geometry, float* dst, size_t n_elements);
+
 /* ---- metric (registration/device.rs:632-800 DeviceMattesMetric) ----------- */
 
 /* from_device / from_device_sampled (device.rs:644-696). The metric copies both

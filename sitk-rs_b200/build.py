@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmi_b200.so")
 
 CU_SOURCES = ["context.cu", "mattes.cu", "noalloc.cu", "pyramid.cu", "batch.cu", "synth.cu", "initnet.cu", "moments.cu", "bspline.cu"]
-CPP_SOURCES = ["transforms.cpp", "geometry.cpp", "register.cpp"]
+CPP_SOURCES = ["transforms.cpp", "geometry.cpp", "register.cpp", "io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -78,7 +78,7 @@ def build(verbose: bool = False, force: bool = False, defines: dict | None = Non
             _run(cmd)
         objs.append(o)
     if force or _stale(lib, objs):
-        _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", lib, *objs])
+        _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", lib, *objs, "-lz"])
     return lib
 
 

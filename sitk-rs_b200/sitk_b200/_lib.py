@@ -35,7 +35,8 @@ EXPORTED = [
     "mi_batch_shape", "mi_batch_destroy", "mi_synth_pair", "mi_gemm_bf16_tn", "mi_initnet_create",
     "mi_initnet_destroy", "mi_initnet_get", "mi_initnet_set", "mi_initnet_forward", "mi_initnet_train_step",
     "mi_initnet_prepare", "mi_metric_create_ex", "mi_image_resample_nearest",
-    "mi_metric_value_and_derivative_bspline", "mi_metric_bspline_records",
+    "mi_metric_value_and_derivative_bspline", "mi_metric_bspline_records", "mi_image_read_meta",
+    "mi_image_read_meta_host",
 ]
 
 
@@ -136,6 +137,10 @@ def load(path: str | None = None):
     L.mi_metric_value_and_derivative_bspline.restype = ctypes.c_int
     L.mi_metric_bspline_records.argtypes = [vp, dp, dp, ctypes.c_int64, P(ctypes.c_uint16), ctypes.c_int64]
     L.mi_metric_bspline_records.restype = ctypes.c_int
+    L.mi_image_read_meta.argtypes = [vp, ctypes.c_char_p, P(vp)]
+    L.mi_image_read_meta.restype = ctypes.c_int
+    L.mi_image_read_meta_host.argtypes = [ctypes.c_char_p, P(MiGeometry), P(ctypes.c_float), ctypes.c_size_t]
+    L.mi_image_read_meta_host.restype = ctypes.c_int
     L.mi_pyramid_level.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int, i64p, P(vp), P(vp)]
     L.mi_metric_get_fused.argtypes = [vp, P(ctypes.c_int)]
     for name in ["mi_image_smooth", "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level",

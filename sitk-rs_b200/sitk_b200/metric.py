@@ -9,6 +9,7 @@ the C ABI of libmi_b200.so; there is no other compute path.
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -101,6 +102,16 @@ class DeviceImage:
         h = ctypes.c_void_p()
         _lib.check(_lib.load().mi_image_upload(ctx.handle, a.ctypes.data_as(ctypes.c_void_p), code,
                                                ctypes.byref(geo), ctypes.byref(h)), ctx.handle)
+        return cls(h, ctx, geo)
+
+    @classmethod
+    def read(cls, path: str, ctx: "Context | None" = None) -> "DeviceImage":
+        """A MetaImage file (.mha / .mhd) read and uploaded (mi_image_read_meta)."""
+        ctx = ctx or default_context()
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().mi_image_read_meta(ctx.handle, os.fsencode(path), ctypes.byref(h)), ctx.handle)
+        geo = _lib.MiGeometry()
+        _lib.check(_lib.load().mi_image_geometry(h, ctypes.byref(geo)))
         return cls(h, ctx, geo)
 
     @classmethod
@@ -453,3 +464,17 @@ def pyramid_level(fixed: DeviceImage, moving: DeviceImage, sigma: float, factors
     _lib.check(L.mi_image_geometry(hf, ctypes.byref(gf)))
     _lib.check(L.mi_image_geometry(hm, ctypes.byref(gm)))
     return DeviceImage(hf, fixed.ctx, gf), DeviceImage(hm, moving.ctx, gm)
+
+
+def read_meta_host(path: str):
+    """A MetaImage file read on the host alone (mi_image_read_meta_host): (voxels as a
+    float32 [z, y, x] array cast as the upload casts them, geometry)."""
+    L = _lib.load()
+    geo = _lib.MiGeometry()
+    p = os.fsencode(path)
+    _lib.check(L.mi_image_read_meta_host(p, ctypes.byref(geo), None, 0))
+    nx, ny, nz = (int(geo.size[i]) for i in range(3))
+    out = np.empty((nz, ny, nx), dtype=np.float32)
+    _lib.check(L.mi_image_read_meta_host(p, ctypes.byref(geo), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                         out.size))
+    return out, geo
