@@ -40,10 +40,6 @@ namespace mi {
 
 constexpr int PADDING = 2;  // registration/mattes.rs:92
 
-// Range and Parzen decisions of the fast path in FP32 (1) or FP64 (0).
-#ifndef MI_PARZEN_F32
-#define MI_PARZEN_F32 1
-#endif
 
 enum : int { SAMPLE_OUTSIDE = 0, SAMPLE_OUT_OF_RANGE = 1, SAMPLE_VALID = 2 };
 
@@ -307,7 +303,6 @@ __device__ __forceinline__ int finish(const SamplerParams& P, const Prep& p, con
     float vmax = fabsf(v[0]);
 #pragma unroll
     for (int t = 1; t < 8; ++t) vmax = fmaxf(vmax, fabsf(v[t]));
-#if MI_PARZEN_F32
     // The range and Parzen decisions in FP32 with a bound that covers the value's error
     // dv and every FP32 rounding on the way: e bounds |mv − v_ref| plus the rounding of
     // mv ± e (the 2^-20 terms are ≥ 16 ulps of every magnitude involved, the range ends
@@ -354,46 +349,6 @@ __device__ __forceinline__ int finish(const SamplerParams& P, const Prep& p, con
     }
     o.mi = mi;
     return SAMPLE_VALID;
-#else
-    const double ce = p.exact_c ? 0.0 : P.cerr;
-    const double dv = (double)vmax * (32.0 * 5.9604644775390625e-08 + 8.0 * ce) + 1e-300;
-    const double mvd = (double)mv;
-    bool certain = true;
-    double term = 0.0;
-    int mi = 0;
-    if (!(dv < 1e300) || !isfinite(mvd)) {
-        certain = false;
-    } else if (mvd + dv < P.moving_min || mvd - dv > P.moving_max) {
-        return SAMPLE_OUT_OF_RANGE;
-    } else if (!(mvd - dv >= P.moving_min && mvd + dv <= P.moving_max)) {
-        certain = false;
-    }
-    if (certain) {
-        // truncation then clamp to [2, bins − 3] equals floor then clamp for every
-        // term (anything below 2 clamps to 2)
-        term = fma(mvd, P.inv_moving_bin_size, -P.moving_nmin);
-        const double dt = dv * P.inv_moving_bin_size * 1.0000001 +
-                          (fabs(term) + fabs(mvd * P.inv_moving_bin_size) + 1.0) * 1e-13;
-        const double lo = fmin(fmax(floor(term - dt), (double)PADDING), P.bin_hi);
-        const double hi = fmin(fmax(floor(term + dt), (double)PADDING), P.bin_hi);
-        if (lo != hi) certain = false;
-        else mi = (int)lo;
-    }
-    if (!certain) {
-        uint32_t i, j, k;
-        grid_index(P, p.flat, i, j, k);
-        double c[3];
-        exact_index(P, i, j, k, c);
-        o.exact = true;
-        const double mvx = exact_value(P, c, moving);
-        if (mvx < P.moving_min || mvx > P.moving_max) return SAMPLE_OUT_OF_RANGE;
-        term = __dsub_rn(__ddiv_rn(mvx, P.moving_bin_size), P.moving_nmin);
-        mi = parzen_bin(term, P.bins);
-    }
-    o.f = (float)(term - (double)mi);
-    o.mi = mi;
-    return SAMPLE_VALID;
-#endif
 }
 
 template <bool GRAD>
