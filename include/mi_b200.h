@@ -192,6 +192,14 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
                               mi_metric** out);
 mi_status mi_metric_info_get(const mi_metric* m, mi_metric_info* out);
 
+/* The flat fixed-grid index of every sample, in the order the device walks them
+ * (n ≥ info.n_samples entries). The set is the sampling strategy's draw gated by the
+ * fixed mask (metric.rs:101-122, 494-581); the order is 8³ bricks of the fixed grid,
+ * bricks and the voxels inside each x-fastest (the whole grid without a mask is
+ * walked plainly x-fastest). Per-sample outputs (the records hooks) come in this
+ * order. */
+mi_status mi_metric_sample_order(mi_metric* m, uint32_t* out, int64_t n);
+
 /* The Mattes value and derivative through a cubic B-spline free-form deformation
  * (transform/bspline.rs BSplineTransform; registration/mattes.rs:722-796
  * evaluate_sparse_support), on a Mattes metric handle. fixed18: the control-point

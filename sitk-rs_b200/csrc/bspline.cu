@@ -565,9 +565,9 @@ extern "C" mi_status mi_metric_value_and_derivative_bspline(mi_metric* m, const 
     return mi::evaluate_bspline(m, fixed18, coef, ncoef, value, derivative, valid);
 }
 
-// Per-sample outcome of the B-spline path in the metric's sample order (ascending
-// voxel): moving bin | fixed bin << 8 for a valid sample, 0 otherwise. For the
-// exactness tests.
+// Per-sample outcome of the B-spline path in the metric's sample order
+// (mi_metric_sample_order): moving bin | fixed bin << 8 for a valid sample, 0
+// otherwise. For the exactness tests.
 extern "C" mi_status mi_metric_bspline_records(mi_metric* m, const double* fixed18, const double* coef,
                                                int64_t ncoef, uint16_t* records, int64_t n) {
     if (!m || !fixed18 || !coef || !records || ncoef < 1) return MI_ERR_INVALID_ARGUMENT;

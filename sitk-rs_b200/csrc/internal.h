@@ -94,7 +94,8 @@ struct Workspace {
     double* vsum = nullptr;              // value slice sums
     double* result = nullptr;            // [2 + MI_MAX_PARAMS]: value, valid, derivative
     unsigned int* done_counter = nullptr;
-    double* host_result = nullptr;       // pinned mirror of result
+    double* host_result = nullptr;       // pinned mirror of result (mapped)
+    double* host_result_dev = nullptr;   // the mirror's device address
     // per-sample records pass 1 hands pass 2 (struct of arrays, sample order):
     // moving bin (0 = not a valid sample), Parzen fraction, moving gradient
     uint16_t* rec_bins = nullptr;

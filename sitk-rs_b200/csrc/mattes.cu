@@ -87,6 +87,7 @@ template <bool RECORD>
 __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
 k_hist(SamplerParams P, EvalArgs a) {
     extern __shared__ unsigned int sh[];
+    pdl_launch_dependents();
     hist_phase<RECORD>(P, a, sh, grid_samples(a.n));
 }
 
@@ -94,24 +95,28 @@ k_hist(SamplerParams P, EvalArgs a) {
 __global__ void __launch_bounds__(TAIL_BLOCK)
 k_tail(int B, double moving_bin_size, EvalArgs a) {
     extern __shared__ __align__(16) unsigned char tsh[];
+    pdl_wait();
     const TailSmem ts = tail_layout(B, tsh);
     const TailCtx t = tail_prepare(B, moving_bin_size, a, ts);
     if (!t.degenerate) value_slices_share(B, a, t, ts, (int)blockIdx.x, (int)gridDim.x);
     __syncthreads();
     if (threadIdx.x < 32) fold_value(B, a, t);
     for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) a.ghist[i] = 0ull;
+    publish_result(a);
 }
 
 // Tail and derivative pass of the split form.
 __global__ void __launch_bounds__(DERIV_BLOCK, DERIV_MIN_BLOCKS)
 k_deriv(SamplerParams P, JacobianForm J, EvalArgs a) {
     extern __shared__ double dsh[];
+    pdl_wait();
     const TailCtx t = deriv_phase(P, a, dsh, grid_groups(a));
     if (!last_to_arrive(a.sync)) return;
     deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
     if (threadIdx.x < 32) fold_value(P.bins, a, t);
     if (threadIdx.x == 0) a.sync[0] = 0u;
     for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
+    publish_result(a);
 }
 
 // Per-sample decisions of the same sampler the kernels use, for the exactness tests.
@@ -147,6 +152,21 @@ __global__ void k_draw_random(uint64_t seed, uint64_t voxels, int64_t count, uin
         z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
         z ^= z >> 31;
         out[i] = (uint32_t)(z % voxels);
+    }
+}
+
+// Sort key of a voxel in brick order: the fixed grid cut into bricks of 2^lb voxels
+// per axis, bricks x-fastest, voxels inside a brick x-fastest.
+__global__ void k_brick_key(const uint32_t* __restrict__ idx, int64_t count, int64_t nx, int64_t ny, int lb,
+                            int64_t nbx, int64_t nby, unsigned long long* __restrict__ key) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = idx[t];
+        const int64_t x = v % nx, row = v / nx;
+        const int64_t y = row % ny, z = row / ny;
+        const int64_t m = ((int64_t)1 << lb) - 1;
+        const int64_t brick = ((z >> lb) * nby + (y >> lb)) * nbx + (x >> lb);
+        key[t] = ((unsigned long long)brick << (3 * lb)) |
+                 (unsigned long long)((((z & m) << lb | (y & m)) << lb) | (x & m));
     }
 }
 
@@ -282,9 +302,9 @@ void free_metric(mi_metric* m) {
     delete m;
 }
 
-// Build the sample list: the strategy's draw, gated by the fixed mask, sorted
-// ascending. The histogram is a sum of exact integers and so does not depend on the
-// order; sorting only buys locality.
+// Build the sample list: the strategy's draw, gated by the fixed mask, sorted into
+// brick order (SAMPLE_BRICK_LOG2). The histogram is a sum of exact integers and so
+// does not depend on the order; sorting only buys locality.
 mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mask, const mi_sampling* smp,
                         int64_t nvox) {
     const int strategy = smp ? smp->strategy : MI_SAMPLING_NONE;
@@ -368,7 +388,34 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
         kept = out;
         nkept = h;
     }
-    if (nkept > 1) {
+    if (nkept > 1 && SAMPLE_BRICK_LOG2 > 0) {
+        const int lb = SAMPLE_BRICK_LOG2;
+        const int64_t nx = m->fgeo.size[0], ny = m->fgeo.size[1], nz = m->fgeo.size[2];
+        const int64_t nbx = (nx + (1 << lb) - 1) >> lb, nby = (ny + (1 << lb) - 1) >> lb;
+        const int64_t nbz = (nz + (1 << lb) - 1) >> lb;
+        const uint64_t kmax = (uint64_t)(nbx * nby * nbz) << (3 * lb);
+        int bits = 1;
+        while (bits < 64 && ((uint64_t)1 << bits) < kmax) ++bits;
+        unsigned long long *keys = nullptr, *keys_out = nullptr;
+        uint32_t* sorted = nullptr;
+        MI_CHECK_CUDA(ctx, cudaMalloc(&keys, (size_t)nkept * 8));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&keys_out, (size_t)nkept * 8));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&sorted, pad4(nkept) * 4));
+        k_brick_key<<<grid_for(nkept, block, ctx->num_sms * 8), block, 0, st>>>(kept, nkept, nx, ny, lb, nbx, nby, keys);
+        MI_CHECK_CUDA(ctx, cudaGetLastError());
+        tmp_bytes = 0;
+        MI_CHECK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys_out, kept, sorted,
+                                                           (int)nkept, 0, bits, st));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&tmp, tmp_bytes));
+        MI_CHECK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_out, kept, sorted, (int)nkept,
+                                                           0, bits, st));
+        MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+        cudaFree(tmp);
+        cudaFree(keys);
+        cudaFree(keys_out);
+        cudaFree(kept);
+        kept = sorted;
+    } else if (nkept > 1) {
         uint32_t* sorted = nullptr;
         MI_CHECK_CUDA(ctx, cudaMalloc(&sorted, pad4(nkept) * 4));
         int bits = 1;
@@ -439,6 +486,9 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.vsum = ws.vsum;
     a.sync = ws.done_counter;
     a.result = ws.result;
+    // the split form's last kernel copies the result into the mapped mirror; the
+    // fused form, whose CTAs may leave early on a barrier timeout, is copied back
+    a.result_host = ws.fused ? nullptr : ws.host_result_dev;
     JacobianForm J;
     J.nparams = want_derivative ? nparams : 0;
     for (int i = 0; i < 3 * J.nparams; ++i) {
@@ -469,18 +519,35 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         else
             k_hist<false><<<ws.grid_hist, HIST_BLOCK, hist_smem(B), st>>>(P, a);
         if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
-        if (want_derivative)
-            k_deriv<<<ws.grid_deriv, DERIV_BLOCK, deriv_smem(B), st>>>(P, J, a);
-        else
-            k_tail<<<1, TAIL_BLOCK, tail_smem(B), st>>>(B, P.moving_bin_size, a);
+        // the second kernel is launched as a programmatic dependent of k_hist (no
+        // event between them), so its launch overlaps k_hist's last CTAs
+        cudaLaunchConfig_t cfg = {};
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = per_kernel ? 0 : 1;
+        if (want_derivative) {
+            cfg.gridDim = dim3((unsigned)ws.grid_deriv);
+            cfg.blockDim = dim3(DERIV_BLOCK);
+            cfg.dynamicSmemBytes = deriv_smem(B);
+            MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_deriv, P, J, a));
+        } else {
+            cfg.gridDim = dim3(1);
+            cfg.blockDim = dim3(TAIL_BLOCK);
+            cfg.dynamicSmemBytes = tail_smem(B);
+            MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_tail, B, P.moving_bin_size, a));
+        }
         if (per_kernel) {
             MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[2], st));
             MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[3], st));
         }
     }
     MI_CHECK_CUDA(ctx, cudaGetLastError());
-    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(ws.host_result, ws.result, RESULT_DOUBLES * sizeof(double),
-                                       cudaMemcpyDeviceToHost, st));
+    if (!a.result_host)
+        MI_CHECK_CUDA(ctx, cudaMemcpyAsync(ws.host_result, ws.result, RESULT_DOUBLES * sizeof(double),
+                                           cudaMemcpyDeviceToHost, st));
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[4], st));
     MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
     unsigned int err = 0;
@@ -795,7 +862,8 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     TRY_CUDA(cudaMalloc(&ws.done_counter, 4 * sizeof(unsigned int)));
     TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));
     TRY_CUDA(cudaMemsetAsync(ws.result, 0, RESULT_DOUBLES * 8, st));
-    TRY_CUDA(cudaMallocHost(&ws.host_result, RESULT_DOUBLES * 8));
+    TRY_CUDA(cudaHostAlloc(&ws.host_result, RESULT_DOUBLES * 8, cudaHostAllocMapped));
+    TRY_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ws.host_result_dev), ws.host_result, 0));
     TRY_CUDA(cudaStreamSynchronize(st));
 #undef TRY_CUDA
     *out = m;
@@ -805,6 +873,22 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
 mi_status mi_metric_info_get(const mi_metric* m, mi_metric_info* out) {
     if (!m || !out) return MI_ERR_INVALID_ARGUMENT;
     *out = m->info;
+    return MI_OK;
+}
+
+mi_status mi_metric_sample_order(mi_metric* m, uint32_t* out, int64_t n) {
+    if (!m || (!out && m->n_samples > 0)) return MI_ERR_INVALID_ARGUMENT;
+    mi_context* ctx = m->ctx;
+    if (n < m->n_samples)
+        return mi::set_error(ctx, MI_ERR_INVALID_ARGUMENT, "output array shorter than the sample count");
+    if (!m->samples) {
+        for (int64_t i = 0; i < m->n_samples; ++i) out[i] = (uint32_t)i;
+        return MI_OK;
+    }
+    MI_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(out, m->samples, (size_t)m->n_samples * 4, cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    MI_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return MI_OK;
 }
 

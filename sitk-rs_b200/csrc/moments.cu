@@ -49,7 +49,7 @@ __host__ __device__ constexpr int slots() {
 struct MomArgs {
     const float* fixed;        // the fixed volume (the sample's value is fixed[flat])
     const uint8_t* mmask;
-    const uint32_t* samples;   // sorted flat indices, or null for the whole grid
+    const uint32_t* samples;   // flat indices in brick order, or null for the whole grid
     uint32_t n;
     double* partials;          // [grid][slots]
     unsigned int* counter;     // arrivals of the current launch (reset by the last CTA)

@@ -26,7 +26,7 @@ EXPORTED = [
     "mi_status_string", "mi_context_create", "mi_context_destroy", "mi_context_sync",
     "mi_last_error", "mi_context_stream", "mi_image_upload", "mi_image_from_device",
     "mi_image_to_host", "mi_image_geometry", "mi_image_device_ptr", "mi_image_free",
-    "mi_metric_create", "mi_metric_info_get", "mi_metric_destroy", "mi_metric_value",
+    "mi_metric_create", "mi_metric_info_get", "mi_metric_sample_order", "mi_metric_destroy", "mi_metric_value",
     "mi_metric_value_and_derivative", "mi_metric_value_and_derivative_stages",
     "mi_metric_sample_decisions", "mi_transform_form", "mi_metric_timing_enable",
     "mi_metric_timing_read", "mi_metric_value_noalloc", "mi_register_rsgd",
@@ -113,6 +113,8 @@ def load(path: str | None = None):
                                       P(MiMetricOptions), P(vp)]
     L.mi_metric_create_ex.restype = ctypes.c_int
     L.mi_metric_info_get.argtypes = [vp, P(MiMetricInfo)]
+    L.mi_metric_sample_order.argtypes = [vp, P(ctypes.c_uint32), ctypes.c_int64]
+    L.mi_metric_sample_order.restype = ctypes.c_int
     L.mi_metric_destroy.argtypes = [vp]
     L.mi_metric_value.argtypes = [vp, dp, ctypes.c_int, dp, i64p]
     L.mi_metric_value_and_derivative.argtypes = [vp, ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int,

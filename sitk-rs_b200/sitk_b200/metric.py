@@ -254,6 +254,15 @@ class DeviceMattesMetric:
     def sample_count(self) -> int:
         return int(self.info()["n_samples"])
 
+    def sample_order(self) -> np.ndarray:
+        """Flat fixed-grid index of every sample in the order the device walks them
+        (the order of per-sample outputs)."""
+        n = self.sample_count()
+        out = np.zeros(max(n, 1), dtype=np.uint32)
+        _lib.check(_lib.load().mi_metric_sample_order(self.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                                      n), self.ctx.handle)
+        return out[:n]
+
     def value(self, transform: ParametricTransform) -> float:
         if getattr(transform, "BSPLINE", None):
             return self._bspline(transform, False).value

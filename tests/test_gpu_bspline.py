@@ -48,11 +48,17 @@ def _records(metric, t):
 def _compare(oracle, p, metric, t, g, draw, n, fmask=None, mmask=None):
     ref = oracle.bspline_mattes(p.fixed, g, p.moving, g, 32, t.fixed_params, t.params, fmask=fmask, mmask=mmask,
                                 draw=draw, per_sample=True)
-    # per-sample decisions, in the device's sorted sample order
+    # per-sample decisions, in the device's sample order: the same multiset of voxels,
+    # matched voxel for voxel (repeated draws of one voxel have identical outcomes)
     oflat = np.arange(n ** 3) if draw is None else np.asarray(draw)
     if fmask is not None:
         oflat = oflat[np.asarray(fmask).ravel()[oflat] != 0]
-    order = np.argsort(oflat, kind="stable")
+    dev = metric.sample_order().astype(np.int64)
+    o_ord = np.argsort(oflat, kind="stable")
+    d_ord = np.argsort(dev, kind="stable")
+    np.testing.assert_array_equal(oflat[o_ord], dev[d_ord])
+    order = np.empty_like(o_ord)
+    order[d_ord] = o_ord
     rec = _records(metric, t)
     st = ref["status"][order]
     np.testing.assert_array_equal(rec != 0, st == 2)

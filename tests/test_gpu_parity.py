@@ -68,8 +68,8 @@ def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0
         assert info[k] == ginfo[k], k
     assert info["n_samples"] == ginfo["nsamples"]
 
-    # exact per-sample decisions (device order is sorted by voxel; compare as multisets
-    # keyed by voxel — equal voxels give equal decisions)
+    # exact per-sample decisions, in the device's sample order (the same multiset of
+    # voxels; matched voxel for voxel, since equal voxels give equal decisions)
     st = sb.transform_stage(transform)
     dec = metric.sample_decisions(st)
     if draw is None and fmask is None:
@@ -78,8 +78,13 @@ def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0
         oflat = np.arange(n ** 3) if draw is None else draw
         if fmask is not None:
             oflat = oflat[np.asarray(fmask).ravel()[oflat] != 0]
-    order = np.argsort(oflat, kind="stable")
-    np.testing.assert_array_equal(dec["flat"], oflat[order])
+    dev = np.asarray(dec["flat"], dtype=np.int64)
+    np.testing.assert_array_equal(dev, metric.sample_order())
+    o_ord = np.argsort(oflat, kind="stable")
+    d_ord = np.argsort(dev, kind="stable")
+    np.testing.assert_array_equal(dev[d_ord], oflat[o_ord])
+    order = np.empty_like(o_ord)
+    order[d_ord] = o_ord
     o_status = ref["status"][order]
     np.testing.assert_array_equal(dec["status"], o_status)
     np.testing.assert_array_equal(dec["fi"], np.where(o_status == 2, ref["fi"][order], -1))
@@ -280,3 +285,25 @@ def test_bf16_moving_storage_euler_64_bins(oracle_lib):
     assert abs(mv.value - ref_f["value"]) <= 1e-2 * abs(ref_f["value"])
     scale = np.max(np.abs(ref_f["derivative"]))
     assert np.max(np.abs(mv.derivative - ref_f["derivative"])) <= 0.1 * scale
+
+
+def test_sample_order_is_the_gated_draw_in_brick_order(oracle_lib):
+    # The device walks the strategy's draw gated by the fixed mask, as the same multiset,
+    # in 8³-brick order (grid sizes that are not multiples of 8 leave partial bricks)
+    sb = _sb()
+    rng = np.random.default_rng(3)
+    nz, ny, nx = 21, 29, 37
+    vol = rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    fmask = (rng.random(vol.shape) > 0.4).astype(np.float32)
+    f, m = sb.DeviceImage.upload(vol), sb.DeviceImage.upload(vol)
+    for strategy, pct in ((sb.SAMPLING_RANDOM, 0.5), (sb.SAMPLING_REGULAR, 0.25)):
+        metric = sb.DeviceMattesMetric.from_device_sampled(f, m, fixed_mask=fmask, bins=32, strategy=strategy,
+                                                           percentage=pct, seed=11)
+        order = metric.sample_order().astype(np.int64)
+        draw = np.asarray(oracle_lib.draw_samples(vol.size, strategy, pct, 11))
+        draw = draw[fmask.ravel()[draw] != 0]
+        np.testing.assert_array_equal(np.sort(order), np.sort(draw))
+        x, y, z = order % nx, (order // nx) % ny, order // (nx * ny)
+        nbx, nby = -(-nx // 8), -(-ny // 8)
+        key = (((z >> 3) * nby + (y >> 3)) * nbx + (x >> 3)) * 512 + (z & 7) * 64 + (y & 7) * 8 + (x & 7)
+        assert np.all(np.diff(key) >= 0)
