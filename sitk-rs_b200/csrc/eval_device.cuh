@@ -33,7 +33,7 @@ namespace {
 #define MI_DERIV_MIN_BLOCKS 2
 #endif
 #ifndef MI_HIST_MIN_BLOCKS
-#define MI_HIST_MIN_BLOCKS 4
+#define MI_HIST_MIN_BLOCKS 2
 #endif
 // Histogram copies per CTA (coarse and fine parts) and the fine part's threshold
 // 2^-MI_HIST_FINE_T (see k_hist).
@@ -54,7 +54,13 @@ namespace {
 #define MI_SAMPLE_BRICK_LOG2 3
 #endif
 constexpr int SAMPLE_BRICK_LOG2 = MI_SAMPLE_BRICK_LOG2;
-constexpr int HIST_BLOCK = 256;
+// Threads per histogram CTA: 512 (two resident per SM) measured 0.8 µs per
+// evaluation faster than 256 (four per SM) on the 256³ workload: half as many CTAs
+// zero, flush and retire their histograms.
+#ifndef MI_HIST_BLOCK
+#define MI_HIST_BLOCK 512
+#endif
+constexpr int HIST_BLOCK = MI_HIST_BLOCK;
 constexpr int HIST_MIN_BLOCKS = MI_HIST_MIN_BLOCKS;
 constexpr int HIST_ILP = MI_HIST_ILP;
 // Threads per derivative CTA (at least TAIL_BLOCK: the tail's column sums use
@@ -84,16 +90,19 @@ int hist_copies(int B) {
 // The fine histogram (B² u32 counters per copy) that takes the small outer taps.
 __host__ __device__ inline int hist_fine_stride(int B) { return ((B * B + 31) & ~31) + 4; }
 // Fine copies: up to MI_HIST_FINE_COPIES, fewer if the two parts together pass
-// 52 KB (four 256-thread CTAs resident per SM at 32 bins).
+// 52 KB (so that even four CTAs fit in an SM's shared memory at 32 bins).
 int hist_fine_copies(int B) {
     const size_t coarse = (size_t)hist_copies(B) * hist_copy_stride(B) * sizeof(unsigned int);
     int c = MI_HIST_FINE_COPIES;
     while (c > 1 && coarse + (size_t)c * hist_fine_stride(B) * sizeof(unsigned int) > 52 * 1024) c >>= 1;
     return c;
 }
+// The copies, then B u64 column sums of the CTA's histogram (used when the launch
+// flushes column marginals, EvalArgs::gcols).
 size_t hist_smem(int B) {
     return ((size_t)hist_copies(B) * hist_copy_stride(B) + (size_t)hist_fine_copies(B) * hist_fine_stride(B)) *
-           sizeof(unsigned int);
+               sizeof(unsigned int) +
+           (size_t)B * sizeof(unsigned long long);
 }
 // Shared memory of the tail (see TailSmem).
 constexpr int TAIL_BLOCK = 256;
@@ -149,6 +158,7 @@ struct EvalArgs {
     int fine_shift, copies, fine_copies;
     double hist_inv;
     unsigned long long* ghist;
+    unsigned long long* gcols = nullptr;  // B column sums of the joint part, flushed with it (or null)
     uint16_t* rec_bins;  // per sample: moving bin | fixed bin << 8 (0 = not valid)
     float* rec_f;
     float* rec_g;
@@ -156,21 +166,16 @@ struct EvalArgs {
     double* vsum;  // value slice sums (value_slices(B))
     unsigned int* sync;
     double* result;
-    double* result_host = nullptr;  // mapped pinned mirror the last CTA copies result into, or null
+    // mapped pinned mirror of result (or null): the split form's last kernel writes value,
+    // valid, derivative and a zero error word there as well, so the host reads them
+    // once the stream completes (the kernel's completion makes the stores visible) with
+    // no device-to-host copy
+    double* result_host = nullptr;
 };
 constexpr int RESULT_ERR = 2 + MI_MAX_PARAMS;  // result slot holding the error word
 constexpr int RESULT_DOUBLES = RESULT_ERR + 2;
 __device__ __forceinline__ unsigned int* error_word(const EvalArgs& a) {
     return reinterpret_cast<unsigned int*>(a.result + RESULT_ERR);
-}
-
-// Run by the whole CTA that wrote the result: copies it into the host's mapped
-// mirror, so the host reads it after the stream completes with no copy of its own.
-__device__ __forceinline__ void publish_result(const EvalArgs& a) {
-    if (!a.result_host) return;
-    __syncthreads();
-    if (threadIdx.x < RESULT_DOUBLES) a.result_host[threadIdx.x] = __ldcg(a.result + threadIdx.x);
-    __threadfence_system();
 }
 
 // Programmatic dependent launch: the histogram pass lets the launch that follows it
@@ -217,6 +222,11 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
     const int fstride = hist_fine_stride(B);
     unsigned int* sh_fine = sh + copies * cstride;
     for (int i = threadIdx.x; i < copies * cstride + fine_copies * fstride; i += blockDim.x) sh[i] = 0u;
+    // the CTA's column sums follow the copies (copies·cstride + fine_copies·fstride is a
+    // multiple of four words, so they are 16-byte aligned)
+    unsigned long long* colacc = reinterpret_cast<unsigned long long*>(sh + copies * cstride + fine_copies * fstride);
+    if (a.gcols)
+        for (int i = threadIdx.x; i < B; i += blockDim.x) colacc[i] = 0ull;
     __syncthreads();
     unsigned int* sh_joint = sh;
     unsigned int* sh_fixed = sh + B * B;
@@ -305,8 +315,15 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
             unsigned long long f = 0ull;
             for (int c = 0; c < fine_copies; ++c) f += sh_fine[c * fstride + i];
             v = (v << a.fine_shift) + f;
+            if (a.gcols && v) atomicAdd(&colacc[i % B], v);
         }
         if (v) atomicAdd(&a.ghist[i], v);
+    }
+    if (a.gcols) {
+        // column marginals of the joint part, exact integer sums like the bins
+        __syncthreads();
+        for (int m = threadIdx.x; m < B; m += blockDim.x)
+            if (colacc[m]) atomicAdd(&a.gcols[m], colacc[m]);
     }
 }
 
@@ -357,37 +374,51 @@ struct TailCtx {
 // the marginals from the copy: column m's sum in tail_groups(B) row groups, then over
 // the groups; counts are read in place. Integer sums, so any order gives the same
 // bits.
-__device__ TailCtx tail_prepare(int B, double moving_bin_size, const EvalArgs& a, const TailSmem& ts) {
+// The fetch: the histogram (and, when the launch flushed them, the column sums) into
+// shared memory.
+__device__ void tail_fetch(int B, const EvalArgs& a, const TailSmem& ts) {
     const int B2 = B * B, nb = B2 + B;
+    const int nl = a.gcols ? nb + B : nb;  // the column sums follow the counts
     const unsigned long long* __restrict__ gh = a.ghist;
-    for (int i0 = threadIdx.x; i0 < nb; i0 += 8 * blockDim.x) {
+    const unsigned long long* __restrict__ gc = a.gcols;
+    for (int i0 = threadIdx.x; i0 < nl; i0 += 8 * blockDim.x) {
         unsigned long long v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int i = i0 + u * blockDim.x;
-            v[u] = i < nb ? __ldcg(gh + i) : 0ull;
+            v[u] = i < nb ? __ldcg(gh + i) : (i < nl ? __ldcg(gc + (i - nb)) : 0ull);
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int i = i0 + u * blockDim.x;
-            if (i < nb) ts.hist[i] = v[u];
+            if (i < nb)
+                ts.hist[i] = v[u];
+            else if (i < nl)
+                ts.col[i - nb] = v[u];
         }
     }
     __syncthreads();
-    const int G = tail_groups(B);
-    if ((int)threadIdx.x < G * B) {
-        const int m = threadIdx.x % B, g = threadIdx.x / B;
-        unsigned long long v = 0ull;
-        for (int f = g; f < B; f += G) v += ts.hist[f * B + m];
-        ts.part[g * B + m] = v;
+}
+
+// The rest of the tail on the fetched histogram.
+__device__ TailCtx tail_finish(int B, double moving_bin_size, const EvalArgs& a, const TailSmem& ts) {
+    const int B2 = B * B;
+    if (!a.gcols) {
+        const int G = tail_groups(B);
+        if ((int)threadIdx.x < G * B) {
+            const int m = threadIdx.x % B, g = threadIdx.x / B;
+            unsigned long long v = 0ull;
+            for (int f = g; f < B; f += G) v += ts.hist[f * B + m];
+            ts.part[g * B + m] = v;
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < B) {
+            unsigned long long v = 0ull;
+            for (int g = 0; g < G; ++g) v += ts.part[g * B + threadIdx.x];
+            ts.col[threadIdx.x] = v;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    if ((int)threadIdx.x < B) {
-        unsigned long long v = 0ull;
-        for (int g = 0; g < G; ++g) v += ts.part[g * B + threadIdx.x];
-        ts.col[threadIdx.x] = v;
-    }
-    __syncthreads();
     const unsigned long long* cnt = ts.hist + B2;
     const int lane = threadIdx.x & 31;
     TailCtx t;
@@ -417,6 +448,11 @@ __device__ TailCtx tail_prepare(int B, double moving_bin_size, const EvalArgs& a
     }
     __syncthreads();
     return t;
+}
+
+__device__ TailCtx tail_prepare(int B, double moving_bin_size, const EvalArgs& a, const TailSmem& ts) {
+    tail_fetch(B, a, ts);
+    return tail_finish(B, moving_bin_size, a, ts);
 }
 
 // ln(a/b) for positive a, b in FP32: the quotient by the fast reciprocal (a few ulps)
@@ -473,13 +509,15 @@ __device__ double value_slice(int B, const TailCtx& t, const TailSmem& ts, int s
 }
 
 // This CTA's share of the value slices: with the CTAs numbered 0..units−1 (this one
-// `unit`), global warp w takes slices w, w + W, …; the sums go to a.vsum.
+// `unit`), warp w of CTA u takes slices w·units + u, then W further on (W = all
+// warps), so a launch of many CTAs gives at most one slice to a warp and the slices
+// land on different CTAs; the sums go to a.vsum.
 __device__ void value_slices_share(int B, const EvalArgs& a, const TailCtx& t, const TailSmem& ts, int unit,
                                    int units) {
     const int lane = threadIdx.x & 31;
     const int nw = blockDim.x >> 5;
     const int ns = value_slices(B);
-    for (int s = unit * nw + (threadIdx.x >> 5); s < ns; s += units * nw) {
+    for (int s = (threadIdx.x >> 5) * units + unit; s < ns; s += units * nw) {
         const double v = value_slice(B, t, ts, s);
         if (lane == 0) a.vsum[s] = v;
     }
@@ -494,8 +532,14 @@ __device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
 #pragma unroll
     for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     if (lane == 0) {
-        a.result[0] = t.degenerate ? DBL_MAX : -v;
-        a.result[1] = (double)t.valid;
+        const double r0 = t.degenerate ? DBL_MAX : -v, r1 = (double)t.valid;
+        a.result[0] = r0;
+        a.result[1] = r1;
+        if (a.result_host) {
+            a.result_host[0] = r0;
+            a.result_host[1] = r1;
+            a.result_host[RESULT_ERR] = 0.0;  // the split form has no barrier to time out
+        }
     }
 }
 
@@ -549,6 +593,29 @@ __device__ __forceinline__ GroupWork grid_groups(const EvalArgs& a) {
                      a.partials + blockIdx.x, (int64_t)gridDim.x, (int)blockIdx.x, (int)gridDim.x};
 }
 
+// The CTA's moments, reduced in a fixed order (shuffles within a warp, then over
+// warps in FP64), stored into partials slot-major, [slot][CTA], so the fold reads
+// them coalesced.
+__device__ __forceinline__ void store_moments(const float* acc, double* red, double* part, int64_t part_stride) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double accd[NMOM];
+#pragma unroll
+    for (int i = 0; i < NMOM; ++i) {
+        double v = (double)acc[i];
+#pragma unroll
+        for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        accd[i] = v;
+    }
+    if (lane == 0)
+        for (int i = 0; i < NMOM; ++i) red[warp * NMOM + i] = accd[i];
+    __syncthreads();
+    if (threadIdx.x < NMOM) {
+        double v = 0.0;
+        for (int k = 0; k < nw; ++k) v += red[k * NMOM + threadIdx.x];
+        part[(int64_t)threadIdx.x * part_stride] = v;
+    }
+}
+
 __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double* dsh, const GroupWork w) {
     const int B = P.bins;
     double* red = dsh;  // 32 * NMOM
@@ -586,13 +653,15 @@ __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double
     };
     uint32_t q = w.begin + w.first;
     Group cur;
+    // the histogram's loads go out first (every CTA waits on them); the first record
+    // group's loads then overlap the rest of the tail
+    tail_fetch(B, a, ts);
     if (q < ngroups) load(q, cur);
-    const TailCtx t = tail_prepare(B, P.moving_bin_size, a, ts);
-    if (!t.degenerate) {
-        pr_table(B, t, ts, pr);
-        value_slices_share(B, a, t, ts, w.unit, w.units);
-    }
+    const TailCtx t = tail_finish(B, P.moving_bin_size, a, ts);
+    if (!t.degenerate) pr_table(B, t, ts, pr);
     __syncthreads();
+    // a warp with a value slice sums it before its share of the records
+    if (!t.degenerate) value_slices_share(B, a, t, ts, w.unit, w.units);
     if (!t.degenerate) {
         while (q < ngroups) {
             const uint32_t qn = q + stride;
@@ -606,25 +675,7 @@ __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double
             q = qn;
         }
     }
-    // CTA reduction in a fixed order: shuffles within a warp, then over warps.
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    double accd[NMOM];
-#pragma unroll
-    for (int i = 0; i < NMOM; ++i) {
-        double v = (double)acc[i];
-#pragma unroll
-        for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        accd[i] = v;
-    }
-    if (lane == 0)
-        for (int i = 0; i < NMOM; ++i) red[warp * NMOM + i] = accd[i];
-    __syncthreads();
-    // partials are stored slot-major, [slot][CTA], so the fold reads them coalesced
-    if (threadIdx.x < NMOM) {
-        double v = 0.0;
-        for (int k = 0; k < nw; ++k) v += red[k * NMOM + threadIdx.x];
-        w.part[(int64_t)threadIdx.x * w.part_stride] = v;
-    }
+    store_moments(acc, red, w.part, w.part_stride);
     return t;
 }
 
@@ -672,6 +723,7 @@ __device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const 
             }
         }
         a.result[2 + k] = dk;
+        if (a.result_host) a.result_host[2 + k] = dk;
     }
 }
 

@@ -81,6 +81,8 @@ k_eval(SamplerParams P, JacobianForm J, EvalArgs a) {
         a.sync[2] = 0u;
     }
     for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) a.ghist[i] = 0ull;
+    if (a.gcols)
+        for (int i = threadIdx.x; i < B; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
 template <bool RECORD>
@@ -102,7 +104,8 @@ k_tail(int B, double moving_bin_size, EvalArgs a) {
     __syncthreads();
     if (threadIdx.x < 32) fold_value(B, a, t);
     for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) a.ghist[i] = 0ull;
-    publish_result(a);
+    if (a.gcols)
+        for (int i = threadIdx.x; i < B; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
 // Tail and derivative pass of the split form.
@@ -116,7 +119,8 @@ k_deriv(SamplerParams P, JacobianForm J, EvalArgs a) {
     if (threadIdx.x < 32) fold_value(P.bins, a, t);
     if (threadIdx.x == 0) a.sync[0] = 0u;
     for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
-    publish_result(a);
+    if (a.gcols)
+        for (int i = threadIdx.x; i < P.bins; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
 // Per-sample decisions of the same sampler the kernels use, for the exactness tests.
@@ -479,6 +483,7 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.fine_copies = hist_fine_copies(B);
     a.hist_inv = std::ldexp(1.0, -ws.fine_scale_log2);
     a.ghist = ws.hist;
+    a.gcols = ws.hist + B * B + B;
     a.rec_bins = want_derivative ? ws.rec_bins : nullptr;
     a.rec_f = want_derivative ? ws.rec_f : nullptr;
     a.rec_g = want_derivative ? ws.rec_g : nullptr;
@@ -556,7 +561,7 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         // a barrier gave up: clear the counters, the error word and the histogram
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.result, 0, RESULT_DOUBLES * sizeof(double), st));
-        MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + B) * 8, st));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + 2 * B) * 8, st));
         MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
         return set_error(ctx, MI_ERR_TIMEOUT, "a grid barrier of the fused evaluation timed out");
     }
@@ -846,8 +851,9 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         TRY_CUDA(cudaMalloc(&ws.rec_f, ns * sizeof(float)));
         TRY_CUDA(cudaMalloc(&ws.rec_g, 3 * ns * sizeof(float)));
     }
-    TRY_CUDA(cudaMalloc(&ws.hist, (size_t)(B * B + B) * 8));
-    TRY_CUDA(cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + B) * 8, st));
+    // joint B², fixed counts B, then the joint part's B column sums
+    TRY_CUDA(cudaMalloc(&ws.hist, (size_t)(B * B + 2 * B) * 8));
+    TRY_CUDA(cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + 2 * B) * 8, st));
     // partials serve both forms: the split form's k_deriv grid and, should the form
     // be switched, the fused grid
     {

@@ -99,7 +99,9 @@ def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0
     v = metric.value(transform)
     assert v == mv.value
     # the split launch form (two kernels) computes the same histogram and tail, so
-    # the same value bits; its derivative partials are folded over another grid
+    # the same value bits; its derivative sums the moments over another partition of
+    # the samples (FP32 within a thread, FP64 from the warp on), so the two forms agree
+    # to FP32 accumulation error
     from sitk_b200.metric import get_fused, set_fused
     fused = get_fused(metric)
     set_fused(metric, not fused)
@@ -107,7 +109,7 @@ def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0
     assert metric.value(transform) == mv.value
     set_fused(metric, fused)
     assert other.value == mv.value and other.valid_points == mv.valid_points
-    np.testing.assert_allclose(other.derivative, mv.derivative, rtol=0, atol=1e-12 * max(scale, 1e-300))
+    np.testing.assert_allclose(other.derivative, mv.derivative, rtol=0, atol=1e-6 * max(scale, 1e-300))
     return metric, mv, ref, dec
 
 
