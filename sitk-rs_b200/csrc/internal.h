@@ -126,7 +126,8 @@ struct MomentsWs {
     double* partials = nullptr;      // [grid][slots]
     double* result = nullptr;        // [2][28]: the folded moments, then correlation's pass-1 sums
     unsigned int* counter = nullptr; // [2] arrival counters
-    double* host = nullptr;          // pinned copy of the folded moments
+    double* host = nullptr;          // pinned, mapped mirror of the folded moments
+    double* host_dev = nullptr;      // the mirror's device address
 };
 }  // namespace mi
 
@@ -139,7 +140,7 @@ struct mi_metric {
     uint8_t* mmask = nullptr;     // device moving mask or null
     cudaArray_t marray = nullptr; // the moving volume in a block-linear 3-D array
     cudaTextureObject_t mtex = 0; // point-sampling, clamp-to-edge texture over marray
-    uint32_t* samples = nullptr;  // device flat indices (sorted); null = the whole grid
+    uint32_t* samples = nullptr;  // device flat indices (8³-brick order); null = the whole grid
     uint8_t* fbin = nullptr;      // device fixed Parzen bin of every sample (exact, set-up time)
     int64_t n_samples = 0;
     int bins = 0;

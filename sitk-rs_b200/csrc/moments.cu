@@ -54,6 +54,7 @@ struct MomArgs {
     double* partials;          // [grid][slots]
     unsigned int* counter;     // arrivals of the current launch (reset by the last CTA)
     double* result;            // [slots] folded by the last CTA
+    double* result_host;       // mapped host mirror the last CTA also writes (or null)
     const double* means;       // pass 2: pass 1's result (Σf, Σm, count)
 };
 
@@ -150,6 +151,10 @@ template <int MODE, bool GRAD>
 __global__ void __launch_bounds__(MOM_BLOCK) k_moments(const SamplerParams P, const MomArgs a) {
     constexpr int NS = slots<MODE, GRAD>();
     constexpr bool WANT_G = GRAD && MODE != MODE_NCC1;
+    // correlation's pass 2 is a programmatic dependent of pass 1: it waits here for
+    // pass 1's sums (and its use of the partials) before reading anything
+    if (MODE == MODE_NCC1) pdl_launch_dependents();
+    if (MODE == MODE_NCC2) pdl_wait();
     double acc[NS];
 #pragma unroll
     for (int q = 0; q < NS; ++q) acc[q] = 0.0;
@@ -212,10 +217,32 @@ __global__ void __launch_bounds__(MOM_BLOCK) k_moments(const SamplerParams P, co
         if (threadIdx.x == 0) a.partials[(size_t)blockIdx.x * NS + q] = v;
     }
     if (last_to_arrive(a.counter)) {
-        for (int q = threadIdx.x; q < NS; q += blockDim.x) {
+        // fold in a fixed order: lane l of slot q sums the partials of CTAs l, l + L, …
+        // (L = MOM_BLOCK / NS lanes per slot), sixteen loads issued together, then the
+        // L lane sums in lane order
+        constexpr int L = MOM_BLOCK / NS;
+        __shared__ double fold[MOM_BLOCK];
+        const int q = threadIdx.x / L, l = threadIdx.x - q * L;
+        if (q < NS) {
+            double v = 0.0;
+            for (unsigned int b0 = l; b0 < gridDim.x; b0 += 16 * L) {
+                double t[16];
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    const unsigned int b = b0 + u * L;
+                    t[u] = b < gridDim.x ? __ldcg(a.partials + (size_t)b * NS + q) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 16; ++u) v += t[u];
+            }
+            fold[q * L + l] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < NS) {
             double t = 0.0;
-            for (unsigned int b = 0; b < gridDim.x; ++b) t += __ldcg(a.partials + (size_t)b * NS + q);
-            a.result[q] = t;
+            for (int k = 0; k < L; ++k) t += fold[threadIdx.x * L + k];
+            a.result[threadIdx.x] = t;
+            if (a.result_host) a.result_host[threadIdx.x] = t;
         }
         if (threadIdx.x == 0) *a.counter = 0u;
     }
@@ -243,7 +270,8 @@ mi_status moments_setup(mi_metric* m) {
     MI_CHECK_CUDA(ctx, cudaMalloc(&w.counter, 2 * sizeof(unsigned int)));
     MI_CHECK_CUDA(ctx, cudaMemsetAsync(w.counter, 0, 2 * sizeof(unsigned int), st));
     MI_CHECK_CUDA(ctx, cudaMemsetAsync(w.result, 0, 2 * NCC2_SLOTS * sizeof(double), st));
-    MI_CHECK_CUDA(ctx, cudaMallocHost(&w.host, NCC2_SLOTS * sizeof(double)));
+    MI_CHECK_CUDA(ctx, cudaHostAlloc(&w.host, NCC2_SLOTS * sizeof(double), cudaHostAllocMapped));
+    MI_CHECK_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&w.host_dev), w.host, 0));
     return MI_OK;
 }
 
@@ -271,6 +299,7 @@ mi_status evaluate_moments(mi_metric* m, const SamplerParams& P, const double* j
     a.partials = w.partials;
     a.counter = w.counter;
     a.result = w.result;
+    a.result_host = w.host_dev;  // the final pass writes the host mirror: no copy back
     a.means = nullptr;
     const bool ncc = m->metric_kind == MI_METRIC_CORRELATION;
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[0], st));
@@ -285,17 +314,27 @@ mi_status evaluate_moments(mi_metric* m, const SamplerParams& P, const double* j
         // pass 1 folds its sums into result[NCC2_SLOTS..]; pass 2 reads them there
         MomArgs a1 = a;
         a1.result = w.result + NCC2_SLOTS;
+        a1.result_host = nullptr;
         a1.counter = w.counter + 1;
         k_moments<MODE_NCC1, false><<<w.grid, MOM_BLOCK, 0, st>>>(P, a1);
         a.means = a1.result;
         ns = want_derivative ? slots<MODE_NCC2, true>() : slots<MODE_NCC2, false>();
+        // pass 2 as a programmatic dependent of pass 1 (it waits for pass 1 on entry)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)w.grid);
+        cfg.blockDim = dim3(MOM_BLOCK);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
         if (want_derivative)
-            k_moments<MODE_NCC2, true><<<w.grid, MOM_BLOCK, 0, st>>>(P, a);
+            MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_moments<MODE_NCC2, true>, P, a));
         else
-            k_moments<MODE_NCC2, false><<<w.grid, MOM_BLOCK, 0, st>>>(P, a);
+            MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_moments<MODE_NCC2, false>, P, a));
     }
     MI_CHECK_CUDA(ctx, cudaGetLastError());
-    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(w.host, w.result, (size_t)ns * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[4], st));
     MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
     if (timing) {
