@@ -230,16 +230,23 @@ __global__ void __launch_bounds__(BS_BLOCK) k_bs_hist(const SamplerParams P, con
         cf = sc;
     }
     __syncthreads();
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
-        const uint32_t flat = a.samples ? __ldg(a.samples + s) : s;
+    // the next sample's index and this sample's fixed bin are requested before the
+    // sample is evaluated, so those loads overlap it
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t flat = s < a.n ? (a.samples ? __ldg(a.samples + s) : s) : 0u;
+    for (; s < a.n; s += stride) {
+        const uint32_t sn = s + stride;
+        const uint32_t cur = flat;
+        flat = sn < a.n ? (a.samples ? __ldg(a.samples + sn) : sn) : 0u;
+        const int fi = __ldg(a.fbin + s);
         double term, g[3];
         int mi = 0;
-        const int st = bs_sample(P, S, cf, flat, a.moving, a.mmask, term, mi, g);
+        const int st = bs_sample(P, S, cf, cur, a.moving, a.mmask, term, mi, g);
         if (st != BS_VALID) {
             a.rec_bins[s] = 0;
             continue;
         }
-        const int fi = __ldg(a.fbin + s);
         const double f = term - (double)mi, h = 1.0 - f, f2 = f * f, f3 = f2 * f;
         const double w[4] = {h * h * h / 6.0, (3.0 * f3 - 6.0 * f2 + 4.0) / 6.0,
                              (-3.0 * f3 + 3.0 * f2 + 3.0 * f + 1.0) / 6.0, f3 / 6.0};

@@ -63,6 +63,11 @@ constexpr int SAMPLE_BRICK_LOG2 = MI_SAMPLE_BRICK_LOG2;
 constexpr int HIST_BLOCK = MI_HIST_BLOCK;
 constexpr int HIST_MIN_BLOCKS = MI_HIST_MIN_BLOCKS;
 constexpr int HIST_ILP = MI_HIST_ILP;
+// With one sample per thread, prefetch the next sample's index (see hist_phase).
+#ifndef MI_HIST_PREFETCH
+#define MI_HIST_PREFETCH 1
+#endif
+constexpr bool HIST_PREFETCH = MI_HIST_PREFETCH != 0;
 // Threads per derivative CTA (at least TAIL_BLOCK: the tail's column sums use
 // TAIL_BLOCK threads).
 #ifndef MI_DERIV_BLOCK
@@ -250,7 +255,7 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
     unsigned int* my_joint = sh_joint + (lane & (copies - 1)) * cstride;
     unsigned int* my_fixed = sh_fixed + (lane & (copies - 1)) * cstride;
     unsigned int* my_fine = sh_fine + (lane & (fine_copies - 1)) * fstride;
-    auto account = [&](const Prep& p, uint32_t s, bool real) {
+    auto account = [&](const Prep& p, uint32_t s, bool real, int fi) {
         if (!real) return;
         Sample o;
         o.exact = false;
@@ -259,7 +264,6 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
             if (RECORD) a.rec_bins[s] = 0;
             return;
         }
-        const int fi = __ldg(fbin + s);
         float w[4];
         bspline3_taps(o.f, w);
         const int off = fi * B + (o.mi - 1);
@@ -292,19 +296,38 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
             const bool one = s < n, two = s2 < n;
             const uint32_t fa = one ? (samples ? __ldg(samples + s) : s) : 0u;
             const uint32_t fb = two ? (samples ? __ldg(samples + s2) : s2) : fa;
+            const int fia = one ? (int)__ldg(fbin + s) : 0, fib = two ? (int)__ldg(fbin + s2) : 0;
             Prep pa, pb;
             prep<RECORD>(P, fa, moving, mmask, pa);
             prep<RECORD>(P, fb, moving, mmask, pb);
-            account(pa, s, one);
-            account(pb, s2, two);
+            account(pa, s, one, fia);
+            account(pb, s2, two, fib);
+        }
+    } else if (HIST_PREFETCH) {
+        // the next sample's index and this sample's fixed bin are requested at the top
+        // of the iteration, so their loads overlap this sample's corner gathers instead
+        // of adding two memory round trips per sample
+        uint32_t s = wbase + lane;
+        uint32_t flat = s < n ? (samples ? __ldg(samples + s) : s) : 0u;
+        for (uint32_t b = wbase; b < n; b += stride) {
+            const bool one = s < n;
+            const int fi = one ? (int)__ldg(fbin + s) : 0;
+            const uint32_t sn = s + stride;
+            const uint32_t flat_next = sn < n ? (samples ? __ldg(samples + sn) : sn) : 0u;
+            Prep pa;
+            prep<RECORD>(P, flat, moving, mmask, pa);
+            account(pa, s, one, fi);
+            s = sn;
+            flat = flat_next;
         }
     } else {
         for (uint32_t b = wbase; b < n; b += stride) {
             const uint32_t s = b + lane;
             const bool one = s < n;
+            const int fi = one ? (int)__ldg(fbin + s) : 0;
             Prep pa;
             prep<RECORD>(P, one ? (samples ? __ldg(samples + s) : s) : 0u, moving, mmask, pa);
-            account(pa, s, one);
+            account(pa, s, one, fi);
         }
     }
     __syncthreads();

@@ -167,11 +167,17 @@ __global__ void __launch_bounds__(MOM_BLOCK) k_moments(const SamplerParams P, co
         }
     }
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += stride) {
-        const uint32_t flat = a.samples ? __ldg(a.samples + s) : s;
+    // the next sample's index and this sample's fixed value are requested before the
+    // sampler runs, so those loads overlap its corner gathers
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t flat = s < a.n ? (a.samples ? __ldg(a.samples + s) : s) : 0u;
+    for (; s < a.n; s += stride) {
+        const uint32_t sn = s + stride;
+        const uint32_t cur = flat;
+        flat = sn < a.n ? (a.samples ? __ldg(a.samples + sn) : sn) : 0u;
+        const double fv = (double)__ldg(a.fixed + cur);
         double mv, g[3], x[3];
-        if (!sample64<WANT_G>(P, flat, a.mmask, mv, g, x)) continue;
-        const double fv = (double)__ldg(a.fixed + flat);
+        if (!sample64<WANT_G>(P, cur, a.mmask, mv, g, x)) continue;
         if (MODE == MODE_MS) {
             const double diff = mv - fv;
             acc[0] += diff * diff;
