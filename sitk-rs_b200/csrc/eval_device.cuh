@@ -291,17 +291,25 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
     // whole warps iterate together: the loop bound is the warp's first sample
     const uint32_t wbase = r.begin + r.warp_first;
     if (HIST_ILP == 2) {
+        // two samples per iteration, the next pair's indices requested a pair ahead
+        uint32_t s = wbase + lane;
+        uint32_t fa = s < n ? (samples ? __ldg(samples + s) : s) : 0u;
+        uint32_t fb = s + stride < n ? (samples ? __ldg(samples + s + stride) : s + stride) : fa;
         for (uint32_t b = wbase; b < n; b += 2 * stride) {
-            const uint32_t s = b + lane, s2 = s + stride;
+            const uint32_t s2 = s + stride;
             const bool one = s < n, two = s2 < n;
-            const uint32_t fa = one ? (samples ? __ldg(samples + s) : s) : 0u;
-            const uint32_t fb = two ? (samples ? __ldg(samples + s2) : s2) : fa;
             const int fia = one ? (int)__ldg(fbin + s) : 0, fib = two ? (int)__ldg(fbin + s2) : 0;
+            const uint32_t sn = s + 2 * stride, sn2 = sn + stride;
+            const uint32_t fna = sn < n ? (samples ? __ldg(samples + sn) : sn) : 0u;
+            const uint32_t fnb = sn2 < n ? (samples ? __ldg(samples + sn2) : sn2) : fna;
             Prep pa, pb;
             prep<RECORD>(P, fa, moving, mmask, pa);
             prep<RECORD>(P, fb, moving, mmask, pb);
             account(pa, s, one, fia);
             account(pb, s2, two, fib);
+            s = sn;
+            fa = fna;
+            fb = fnb;
         }
     } else if (HIST_PREFETCH) {
         // the next sample's index and this sample's fixed bin are requested at the top
