@@ -54,6 +54,13 @@ namespace {
 #define MI_SAMPLE_BRICK_LOG2 3
 #endif
 constexpr int SAMPLE_BRICK_LOG2 = MI_SAMPLE_BRICK_LOG2;
+// The moving volume's texture: 1 stores it 2-D layered (one layer per z slice, a cell's
+// corners in two gathers) wherever the volume fits the layered limits, 0 always 3-D
+// (eight point fetches).
+#ifndef MI_MOVING_LAYERED
+#define MI_MOVING_LAYERED 1
+#endif
+constexpr bool MOVING_LAYERED = MI_MOVING_LAYERED != 0;
 // Threads per histogram CTA: 512 (two resident per SM) measured 0.8 µs per
 // evaluation faster than 256 (four per SM) on the 256³ workload: half as many CTAs
 // zero, flush and retire their histograms.

@@ -62,8 +62,9 @@ struct SamplerParams {
     float mp2if[9];  // physical→index matrix in FP32 (gradient only)
     int msz[3];      // moving size, 32-bit (the volume is below 2^32 voxels)
     uint32_t ms1, ms2;  // moving strides, 32-bit
-    cudaTextureObject_t mtex;  // the moving volume as a 3-D texture (point, clamp, unnormalised)
+    cudaTextureObject_t mtex;  // the moving volume as a texture (point, clamp, unnormalised)
     int mbf16;                 // the texture holds BF16 bits (u16), widened exactly on fetch
+    int mlayered;              // mtex is 2-D layered (one layer per z slice, gathered), else 3-D
     double inv_moving_bin_size;
     // point map stages (matrix_offset.rs:102-109)
     int nstage;

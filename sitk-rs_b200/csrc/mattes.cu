@@ -724,14 +724,23 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     P.ms1 = (uint32_t)P.mstride1;
     P.ms2 = (uint32_t)P.mstride2;
     {
-        // the moving volume as a block-linear 3-D array behind a point-sampling,
-        // clamp-to-edge, unnormalised-coordinate texture (the fast path's corner fetch)
+        // the moving volume behind a point-sampling, clamp-to-edge, unnormalised-coordinate
+        // texture (the fast path's corner fetch): a 2-D layered array, one layer per z
+        // slice, whose cell corners come in two gathers, when the volume fits the
+        // layered limits; else a block-linear 3-D array read by eight point fetches
         const bool b16 = storage == MI_STORAGE_BF16;
         const cudaChannelFormatDesc fmt = b16 ? cudaCreateChannelDesc<unsigned short>() : cudaCreateChannelDesc<float>();
         const size_t esize = b16 ? 2 : 4;
         const cudaExtent ext = make_cudaExtent((size_t)moving->geo.size[0], (size_t)moving->geo.size[1],
                                                (size_t)moving->geo.size[2]);
-        TRY_CUDA(cudaMalloc3DArray(&m->marray, &fmt, ext));
+        int lw = 0, lh = 0, ll = 0;
+        TRY_CUDA(cudaDeviceGetAttribute(&lw, cudaDevAttrMaxTexture2DLayeredWidth, ctx->device));
+        TRY_CUDA(cudaDeviceGetAttribute(&lh, cudaDevAttrMaxTexture2DLayeredHeight, ctx->device));
+        TRY_CUDA(cudaDeviceGetAttribute(&ll, cudaDevAttrMaxTexture2DLayeredLayers, ctx->device));
+        const bool layered = moving->geo.size[0] <= lw && moving->geo.size[1] <= lh && moving->geo.size[2] <= ll &&
+                             MOVING_LAYERED;
+        TRY_CUDA(cudaMalloc3DArray(&m->marray, &fmt, ext, layered ? cudaArrayLayered : 0));
+        P.mlayered = layered ? 1 : 0;
         cudaMemcpy3DParms cp = {};
         cp.srcPtr = make_cudaPitchedPtr(b16 ? (void*)mbits : (void*)m->moving, (size_t)moving->geo.size[0] * esize,
                                         (size_t)moving->geo.size[0], (size_t)moving->geo.size[1]);

@@ -167,7 +167,54 @@ __device__ __forceinline__ double exact_value(const SamplerParams& P, const doub
 // index that passed the inside test, so each fl[d] ∈ [−1, size − 1]), corner t at
 // fl + (t & 1, (t >> 1) & 1, t >> 2), from the moving volume's texture (point
 // sampling at voxel centres, clamp addressing = the clamp-to-edge of each corner).
+// Layered form: tld4 on the 2-D layered texture returns the 2×2 texels of one z slice
+// whose bilinear footprint covers (x, y), each clamped to the slice's edge, in the
+// order (x0, y1), (x1, y1), (x1, y0), (x0, y0); at (x, y) = fl + 1 the footprint is
+// exactly the cell's x0 = fl_x, y0 = fl_y. Two gathers (slices fl_z and fl_z + 1,
+// clamped to the volume) replace eight point fetches.
+__device__ __forceinline__ void gather_f32(cudaTextureObject_t t, int layer, float x, float y, float* g) {
+    asm volatile("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
+                 : "=f"(g[0]), "=f"(g[1]), "=f"(g[2]), "=f"(g[3])
+                 : "l"(t), "r"(layer), "f"(x), "f"(y), "f"(0.0f));
+}
+__device__ __forceinline__ void gather_u32(cudaTextureObject_t t, int layer, float x, float y, uint32_t* g) {
+    asm volatile("tld4.r.a2d.v4.u32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
+                 : "=r"(g[0]), "=r"(g[1]), "=r"(g[2]), "=r"(g[3])
+                 : "l"(t), "r"(layer), "f"(x), "f"(y), "f"(0.0f));
+}
+
 __device__ __forceinline__ void fetch_corners(const SamplerParams& P, const double* fl, float* v) {
+    if (P.mlayered) {
+        const float x = (float)fl[0] + 1.0f, y = (float)fl[1] + 1.0f;
+        const int z0 = (int)fl[2];
+        const int l0 = z0 < 0 ? 0 : z0, l1 = z0 + 1 > P.msz[2] - 1 ? P.msz[2] - 1 : z0 + 1;
+        if (P.mbf16) {
+            uint32_t g0[4], g1[4];
+            gather_u32(P.mtex, l0, x, y, g0);
+            gather_u32(P.mtex, l1, x, y, g1);
+            v[0] = __uint_as_float(g0[3] << 16);
+            v[1] = __uint_as_float(g0[2] << 16);
+            v[2] = __uint_as_float(g0[0] << 16);
+            v[3] = __uint_as_float(g0[1] << 16);
+            v[4] = __uint_as_float(g1[3] << 16);
+            v[5] = __uint_as_float(g1[2] << 16);
+            v[6] = __uint_as_float(g1[0] << 16);
+            v[7] = __uint_as_float(g1[1] << 16);
+        } else {
+            float g0[4], g1[4];
+            gather_f32(P.mtex, l0, x, y, g0);
+            gather_f32(P.mtex, l1, x, y, g1);
+            v[0] = g0[3];
+            v[1] = g0[2];
+            v[2] = g0[0];
+            v[3] = g0[1];
+            v[4] = g1[3];
+            v[5] = g1[2];
+            v[6] = g1[0];
+            v[7] = g1[1];
+        }
+        return;
+    }
     float cx[2], cy[2], cz[2];
     cx[0] = (float)fl[0] + 0.5f;
     cy[0] = (float)fl[1] + 0.5f;
