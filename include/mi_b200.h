@@ -180,9 +180,18 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
 #define MI_METRIC_MEAN_SQUARES 1
 #define MI_METRIC_CORRELATION 2
 
+/* Layout of the moving volume's texture (the fast path's corner fetch). AUTO stores it
+ * as a 2-D layered texture (one layer per z slice; a cell's eight corners in two
+ * gathers) wherever the volume fits the device's layered limits, else as a 3-D
+ * texture (eight point fetches); 3D always uses the 3-D texture. Both give the same
+ * results bit for bit. No reference counterpart (a device storage choice). */
+#define MI_TEXTURE_AUTO 0
+#define MI_TEXTURE_3D 1
+
 typedef struct mi_metric_options {
     int moving_storage; /* MI_STORAGE_F32 (default) or MI_STORAGE_BF16 */
     int metric;         /* MI_METRIC_MATTES (default), MI_METRIC_MEAN_SQUARES, MI_METRIC_CORRELATION */
+    int texture;        /* MI_TEXTURE_AUTO (default) or MI_TEXTURE_3D */
 } mi_metric_options;
 
 /* mi_metric_create with options (NULL: the defaults). */

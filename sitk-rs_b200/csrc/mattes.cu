@@ -608,6 +608,9 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     const int metric = options ? options->metric : MI_METRIC_MATTES;
     if (metric != MI_METRIC_MATTES && metric != MI_METRIC_MEAN_SQUARES && metric != MI_METRIC_CORRELATION)
         return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "unknown metric kind");
+    const int texture = options ? options->texture : MI_TEXTURE_AUTO;
+    if (texture != MI_TEXTURE_AUTO && texture != MI_TEXTURE_3D)
+        return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "texture must be MI_TEXTURE_AUTO or MI_TEXTURE_3D");
     const bool mattes = metric == MI_METRIC_MATTES;
     if (!mattes) bins = 0;  // no histogram
     *out = nullptr;
@@ -738,7 +741,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         TRY_CUDA(cudaDeviceGetAttribute(&lh, cudaDevAttrMaxTexture2DLayeredHeight, ctx->device));
         TRY_CUDA(cudaDeviceGetAttribute(&ll, cudaDevAttrMaxTexture2DLayeredLayers, ctx->device));
         const bool layered = moving->geo.size[0] <= lw && moving->geo.size[1] <= lh && moving->geo.size[2] <= ll &&
-                             MOVING_LAYERED;
+                             MOVING_LAYERED && texture == MI_TEXTURE_AUTO;
         TRY_CUDA(cudaMalloc3DArray(&m->marray, &fmt, ext, layered ? cudaArrayLayered : 0));
         P.mlayered = layered ? 1 : 0;
         cudaMemcpy3DParms cp = {};

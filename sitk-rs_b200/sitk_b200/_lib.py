@@ -61,7 +61,7 @@ class MiMetricInfo(ctypes.Structure):
 
 
 class MiMetricOptions(ctypes.Structure):
-    _fields_ = [("moving_storage", ctypes.c_int), ("metric", ctypes.c_int)]
+    _fields_ = [("moving_storage", ctypes.c_int), ("metric", ctypes.c_int), ("texture", ctypes.c_int)]
 
 
 METRIC_MATTES, METRIC_MEAN_SQUARES, METRIC_CORRELATION = 0, 1, 2

@@ -209,14 +209,20 @@ class DeviceMattesMetric:
     def from_device_sampled(cls, fixed: DeviceImage, moving: DeviceImage, fixed_mask=None,
                             moving_mask=None, samples=None, bins: int = 50, *,
                             strategy: int | None = None, percentage: float = 1.0, seed: int = 0,
-                            moving_storage: str = "f32", _metric: int = _lib.METRIC_MATTES):
+                            moving_storage: str = "f32", texture: str = "auto",
+                            _metric: int = _lib.METRIC_MATTES):
         """`samples` is an explicit flat-index list (FixedSamples::selected_indices);
         alternatively `strategy`/`percentage`/`seed` draw on the device exactly as
         draw_samples does (registration/metric.rs:419-437). `moving_storage` "bf16"
-        keeps the moving volume rounded to BF16 (mi_metric_create_ex)."""
+        keeps the moving volume rounded to BF16 (mi_metric_create_ex). `texture` "3d"
+        keeps the moving volume in a 3-D texture instead of the layered one (same
+        results; MI_TEXTURE_3D)."""
         storage = {"f32": 0, "bf16": 1}.get(moving_storage)
         if storage is None:
             raise ValueError("moving_storage is 'f32' or 'bf16'")
+        tex = {"auto": 0, "3d": 1}.get(texture)
+        if tex is None:
+            raise ValueError("texture is 'auto' or '3d'")
         ctx = fixed.ctx
         smp = None
         keep = []
@@ -239,7 +245,7 @@ class DeviceMattesMetric:
                 keep.append(fmi)
                 fm_handle = fmi.handle
         h = ctypes.c_void_p()
-        opts = _lib.MiMetricOptions(storage, int(_metric))
+        opts = _lib.MiMetricOptions(storage, int(_metric), tex)
         _lib.check(_lib.load().mi_metric_create_ex(
             ctx.handle, fixed.handle, moving.handle, fm_handle,
             None if mm is None else mm.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
@@ -369,9 +375,10 @@ class DeviceMeanSquaresMetric(DeviceMattesMetric):
     @classmethod
     def from_device_sampled(cls, fixed: DeviceImage, moving: DeviceImage, fixed_mask=None, moving_mask=None,
                             samples=None, *, strategy: int | None = None, percentage: float = 1.0, seed: int = 0,
-                            moving_storage: str = "f32"):
+                            moving_storage: str = "f32", texture: str = "auto"):
         return super().from_device_sampled(fixed, moving, fixed_mask, moving_mask, samples, 0, strategy=strategy,
                                            percentage=percentage, seed=seed, moving_storage=moving_storage,
+                                           texture=texture,
                                            _metric=_lib.METRIC_MEAN_SQUARES)
 
 
@@ -387,9 +394,10 @@ class DeviceCorrelationMetric(DeviceMattesMetric):
     @classmethod
     def from_device_sampled(cls, fixed: DeviceImage, moving: DeviceImage, fixed_mask=None, moving_mask=None,
                             samples=None, *, strategy: int | None = None, percentage: float = 1.0, seed: int = 0,
-                            moving_storage: str = "f32"):
+                            moving_storage: str = "f32", texture: str = "auto"):
         return super().from_device_sampled(fixed, moving, fixed_mask, moving_mask, samples, 0, strategy=strategy,
                                            percentage=percentage, seed=seed, moving_storage=moving_storage,
+                                           texture=texture,
                                            _metric=_lib.METRIC_CORRELATION)
 
 

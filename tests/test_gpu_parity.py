@@ -309,3 +309,31 @@ def test_sample_order_is_the_gated_draw_in_brick_order(oracle_lib):
         nbx, nby = -(-nx // 8), -(-ny // 8)
         key = (((z >> 3) * nby + (y >> 3)) * nbx + (x >> 3)) * 512 + (z & 7) * 64 + (y & 7) * 8 + (x & 7)
         assert np.all(np.diff(key) >= 0)
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_layered_and_3d_textures_agree_bit_for_bit(storage):
+    # The corner fetch from the layered texture (two gathers per cell) and from the 3-D
+    # texture (eight point fetches) read the same stored voxels with the same edge clamp,
+    # so every metric gives the same bits; the pose reaches past the volume's edges.
+    sb = _sb()
+    p = small_pair(n=40, seed=21)
+    f, m = _upload_pair(p)
+    t = sb.VersorRigid3DTransform((0.05, -0.04, 0.03), (2.5, -1.75, 3.25), [19.5] * 3)
+    out = {}
+    for tex in ("auto", "3d"):
+        metric = sb.DeviceMattesMetric.from_device_sampled(f, m, bins=32, strategy=sb.SAMPLING_RANDOM,
+                                                           percentage=0.5, seed=3, moving_storage=storage,
+                                                           texture=tex)
+        mv = metric.evaluate(t)
+        dec = metric.sample_decisions(sb.transform_stage(t))
+        out[tex] = (mv.value, mv.derivative.copy(), mv.valid_points, dec["mi"].copy(), dec["status"].copy())
+    a, b = out["auto"], out["3d"]
+    assert a[0] == b[0] and a[2] == b[2] and a[2] > 0
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(a[3], b[3]) and np.array_equal(a[4], b[4])
+    ms = [sb.DeviceMeanSquaresMetric.from_device_sampled(f, m, strategy=sb.SAMPLING_RANDOM, percentage=0.5, seed=3,
+                                                         moving_storage=storage, texture=tex).evaluate(t)
+          for tex in ("auto", "3d")]
+    assert ms[0].value == ms[1].value and np.isfinite(ms[0].value)
+    assert np.array_equal(ms[0].derivative, ms[1].derivative)
