@@ -156,6 +156,23 @@ def load(path: str | None = None):
     return L
 
 
+_raw = None
+
+
+def load_raw():
+    """The same library through a second handle whose functions carry no argtypes, for
+    the per-evaluation call: ctypes then passes the caller's ready-made ctypes objects
+    without converting each argument (about 1.5 µs less per call). Callers pass exactly
+    the C types (c_void_p handle, int, ctypes arrays, byref)."""
+    global _raw
+    if _raw is None:
+        L = load()
+        R = ctypes.CDLL(L._name)
+        R.mi_metric_value_and_derivative.restype = ctypes.c_int
+        _raw = R
+    return _raw
+
+
 def check(status: int, ctx=None):
     if status != MI_OK:
         detail = ""

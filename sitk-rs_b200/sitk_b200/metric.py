@@ -199,7 +199,12 @@ class DeviceMattesMetric:
         self._n = ctypes.c_int64()
         self._vref = ctypes.byref(self._v)
         self._nref = ctypes.byref(self._n)
-        self._fn = _lib.load().mi_metric_value_and_derivative
+        # numpy views over the same buffers: parameters in and the derivative out without
+        # building Python lists
+        self._pnp = np.frombuffer(self._p, dtype=np.float64)
+        self._fpnp = np.frombuffer(self._fp, dtype=np.float64)
+        self._dnp = np.frombuffer(self._d, dtype=np.float64)
+        self._fn = _lib.load_raw().mi_metric_value_and_derivative
 
     @classmethod
     def from_device(cls, fixed: DeviceImage, moving: DeviceImage, bins: int = 50):
@@ -301,19 +306,18 @@ class DeviceMattesMetric:
     def evaluate(self, transform: ParametricTransform) -> MetricValue:
         if getattr(transform, "BSPLINE", None):
             return self._bspline(transform, True)
-        params = transform.params.tolist()
-        fixed = transform.fixed_params.tolist()
-        n, nf = len(params), len(fixed)
+        params, fixed = transform.params, transform.fixed_params
+        n, nf = params.shape[0], fixed.shape[0]
         if n > 12 or nf > 12:
             raise ValueError("at most 12 parameters and 12 fixed parameters")
-        self._p[:n] = params
+        self._pnp[:n] = params
         if nf:
-            self._fp[:nf] = fixed
-        st = self._fn(self.handle, transform.kind, self._p, n, self._fp if nf else None, nf, self._vref, self._d,
+            self._fpnp[:nf] = fixed
+        st = self._fn(self.handle, int(transform.kind), self._p, n, self._fp if nf else None, nf, self._vref, self._d,
                       self._nref)
         if st:
             _lib.check(st, self.ctx.handle)
-        return MetricValue(self._v.value, np.array(self._d[:n]), self._n.value)
+        return MetricValue(self._v.value, self._dnp[:n].copy(), self._n.value)
 
     def evaluate_stages(self, stages, jac0, jacc) -> MetricValue:
         st = np.ascontiguousarray(stages, dtype=np.float64).ravel()
