@@ -180,11 +180,13 @@ mi_status mi_metric_create(mi_context* ctx, const mi_image* fixed, const mi_imag
 #define MI_METRIC_MEAN_SQUARES 1
 #define MI_METRIC_CORRELATION 2
 
-/* Layout of the moving volume's texture (the fast path's corner fetch). AUTO stores it
- * as a 2-D layered texture (one layer per z slice; a cell's eight corners in two
- * gathers) wherever the volume fits the device's layered limits, else as a 3-D
- * texture (eight point fetches); 3D always uses the 3-D texture. Both give the same
- * results bit for bit. No reference counterpart (a device storage choice). */
+/* Layout of the moving volume's texture (the fast path's corner fetch). AUTO stores it,
+ * for the Mattes metric, as a 2-D layered texture (one layer per z slice; a cell's
+ * eight corners in two gathers) wherever the volume fits the device's layered limits,
+ * and otherwise (and for mean squares and correlation, whose FP64 kernels measured
+ * faster with it) as a 3-D texture read by eight point fetches; 3D always uses the
+ * 3-D texture. Both give the same results bit for bit. No reference counterpart (a
+ * device storage choice). */
 #define MI_TEXTURE_AUTO 0
 #define MI_TEXTURE_3D 1
 

@@ -741,7 +741,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         TRY_CUDA(cudaDeviceGetAttribute(&lh, cudaDevAttrMaxTexture2DLayeredHeight, ctx->device));
         TRY_CUDA(cudaDeviceGetAttribute(&ll, cudaDevAttrMaxTexture2DLayeredLayers, ctx->device));
         const bool layered = moving->geo.size[0] <= lw && moving->geo.size[1] <= lh && moving->geo.size[2] <= ll &&
-                             MOVING_LAYERED && texture == MI_TEXTURE_AUTO;
+                             MOVING_LAYERED && texture == MI_TEXTURE_AUTO && mattes;
         TRY_CUDA(cudaMalloc3DArray(&m->marray, &fmt, ext, layered ? cudaArrayLayered : 0));
         P.mlayered = layered ? 1 : 0;
         cudaMemcpy3DParms cp = {};
