@@ -183,11 +183,26 @@ struct EvalArgs {
     // once the stream completes (the kernel's completion makes the stores visible) with
     // no device-to-host copy
     double* result_host = nullptr;
+    // the evaluation's sequence number, written into result_host's last slot after a
+    // system-scope fence once everything else is there (the host may poll it)
+    unsigned long long seq = 0;
 };
 constexpr int RESULT_ERR = 2 + MI_MAX_PARAMS;  // result slot holding the error word
 constexpr int RESULT_DOUBLES = RESULT_ERR + 2;
 __device__ __forceinline__ unsigned int* error_word(const EvalArgs& a) {
     return reinterpret_cast<unsigned int*>(a.result + RESULT_ERR);
+}
+
+// Run by the whole last CTA after it has written the result: the sequence number goes
+// into the mirror's last slot behind a system-scope fence, so a host that sees it sees
+// the whole result.
+__device__ __forceinline__ void publish_seq(const EvalArgs& a) {
+    if (!a.result_host) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence_system();
+        *reinterpret_cast<volatile unsigned long long*>(a.result_host + RESULT_ERR + 1) = a.seq;
+    }
 }
 
 // Programmatic dependent launch: the histogram pass lets the launch that follows it

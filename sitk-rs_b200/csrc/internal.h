@@ -97,6 +97,7 @@ struct Workspace {
     unsigned int* done_counter = nullptr;
     double* host_result = nullptr;       // pinned mirror of result (mapped)
     double* host_result_dev = nullptr;   // the mirror's device address
+    unsigned long long seq = 0;          // evaluations published through the mirror
     // per-sample records pass 1 hands pass 2 (struct of arrays, sample order):
     // moving bin (0 = not a valid sample), Parzen fraction, moving gradient
     uint16_t* rec_bins = nullptr;

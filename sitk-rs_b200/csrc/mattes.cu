@@ -103,6 +103,7 @@ k_tail(int B, double moving_bin_size, EvalArgs a) {
     if (!t.degenerate) value_slices_share(B, a, t, ts, (int)blockIdx.x, (int)gridDim.x);
     __syncthreads();
     if (threadIdx.x < 32) fold_value(B, a, t);
+    publish_seq(a);
     for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) a.ghist[i] = 0ull;
     if (a.gcols)
         for (int i = threadIdx.x; i < B; i += blockDim.x) a.gcols[i] = 0ull;
@@ -117,6 +118,7 @@ k_deriv(SamplerParams P, JacobianForm J, EvalArgs a) {
     if (!last_to_arrive(a.sync)) return;
     deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
     if (threadIdx.x < 32) fold_value(P.bins, a, t);
+    publish_seq(a);
     if (threadIdx.x == 0) a.sync[0] = 0u;
     for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
     if (a.gcols)
@@ -494,6 +496,7 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     // the split form's last kernel copies the result into the mapped mirror; the
     // fused form, whose CTAs may leave early on a barrier timeout, is copied back
     a.result_host = ws.fused ? nullptr : ws.host_result_dev;
+    a.seq = ++ws.seq;
     JacobianForm J;
     J.nparams = want_derivative ? nparams : 0;
     for (int i = 0; i < 3 * J.nparams; ++i) {
@@ -554,7 +557,28 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         MI_CHECK_CUDA(ctx, cudaMemcpyAsync(ws.host_result, ws.result, RESULT_DOUBLES * sizeof(double),
                                            cudaMemcpyDeviceToHost, st));
     if (timing) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[4], st));
-    MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+    if (a.result_host && !timing) {
+        // wait for the published sequence number in the mapped mirror rather than for the
+        // stream (whose last kernel may still be clearing the histogram for the next
+        // evaluation); the stream is queried every 256 polls, so a failed launch still
+        // ends the wait with its error, and a finished stream without the number is
+        // reported as an error
+        const volatile unsigned long long* flag =
+            reinterpret_cast<const volatile unsigned long long*>(ws.host_result + RESULT_ERR + 1);
+        for (uint32_t spin = 1;; ++spin) {
+            if (*flag == a.seq) break;
+            if ((spin & 255u) == 0u) {
+                const cudaError_t q = cudaStreamQuery(st);
+                if (q == cudaSuccess) {
+                    if (*flag == a.seq) break;
+                    return set_error(ctx, MI_ERR_CUDA, "the evaluation finished without publishing its result");
+                }
+                if (q != cudaErrorNotReady) return cuda_status(ctx, q, "cudaStreamQuery");
+            }
+        }
+    } else {
+        MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+    }
     unsigned int err = 0;
     std::memcpy(&err, ws.host_result + RESULT_ERR, sizeof(err));
     if (err) {
@@ -881,6 +905,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));
     TRY_CUDA(cudaMemsetAsync(ws.result, 0, RESULT_DOUBLES * 8, st));
     TRY_CUDA(cudaHostAlloc(&ws.host_result, RESULT_DOUBLES * 8, cudaHostAllocMapped));
+    std::memset(ws.host_result, 0, RESULT_DOUBLES * 8);  // no stale sequence number
     TRY_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ws.host_result_dev), ws.host_result, 0));
     TRY_CUDA(cudaStreamSynchronize(st));
 #undef TRY_CUDA
