@@ -237,7 +237,11 @@ mi_status mi_metric_value(mi_metric* m, const double* stages, int nstage, double
 /* DeviceMattesMetric::evaluate (device.rs:767-800) for a transform family:
  * value = −MI and derivative = +∇(−MI) w.r.t. the family's parameters
  * (the optimizer subtracts it). Degenerate histograms give value = DBL_MAX and a
- * zero derivative (mattes.rs:590-609). */
+ * zero derivative (mattes.rs:590-609).
+ * These evaluation calls return once the result is in host memory. The metric's
+ * last kernel may still be clearing its histogram for the next evaluation on the
+ * context's stream. Later work on that stream (including the next evaluation, and
+ * mi_metric_destroy, which synchronises it) runs after it. */
 mi_status mi_metric_value_and_derivative(mi_metric* m, int kind, const double* params,
                                          int nparams, const double* fixed_params, int nfixed,
                                          double* value, double* derivative, int64_t* valid);
