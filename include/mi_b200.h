@@ -222,8 +222,8 @@ mi_status mi_metric_sample_order(mi_metric* m, uint32_t* out, int64_t n);
 mi_status mi_metric_value_and_derivative_bspline(mi_metric* m, const double* fixed18, const double* coef,
                                                  int64_t ncoef, double* value, double* derivative, int64_t* valid);
 /* Test hook (no reference counterpart): each sample's outcome on the B-spline path in
- * the metric's sample order (ascending voxel): moving bin | fixed bin << 8 when valid,
- * else 0. n ≥ the sample count. */
+ * the metric's sample order (mi_metric_sample_order): moving bin | fixed bin << 8 when
+ * valid, else 0. n ≥ the sample count. */
 mi_status mi_metric_bspline_records(mi_metric* m, const double* fixed18, const double* coef, int64_t ncoef,
                                     uint16_t* records, int64_t n);
 mi_status mi_metric_destroy(mi_metric* m);
