@@ -238,6 +238,16 @@ def test_refusals_are_named():
     with pytest.raises(sb.MiError) as e:
         sb.DeviceImage.upload(np.zeros((4, 4, 4), dtype=np.complex64))
     assert e.value.name == "MI_ERR_UNSUPPORTED_PIXEL_TYPE"
+    # an unknown texture layout is refused through the C ABI options
+    import ctypes
+    from sitk_b200 import _lib
+    opts = _lib.MiMetricOptions(0, 0, 7)
+    h = ctypes.c_void_p()
+    st = _lib.load().mi_metric_create_ex(f.ctx.handle, f.handle, m.handle, None, None, None, 32,
+                                         ctypes.byref(opts), ctypes.byref(h))
+    assert _lib.STATUS_NAMES[st] == "MI_ERR_INVALID_ARGUMENT" and not h.value
+    # the whole grid without a mask is walked in voxel order
+    assert np.array_equal(metric.sample_order(), np.arange(16 ** 3, dtype=np.uint32))
 
 
 @pytest.mark.parametrize("dtype", [np.uint8, np.int16, np.uint16, np.int32, np.float64, np.int64])
