@@ -130,6 +130,7 @@ struct MomentsWs {
     unsigned int* counter = nullptr; // [2] arrival counters
     double* host = nullptr;          // pinned, mapped mirror of the folded moments
     double* host_dev = nullptr;      // the mirror's device address
+    float* fval = nullptr;           // each sample's fixed value, in sample order (null: the whole grid)
 };
 }  // namespace mi
 

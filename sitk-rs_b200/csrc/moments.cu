@@ -47,7 +47,8 @@ __host__ __device__ constexpr int slots() {
 }
 
 struct MomArgs {
-    const float* fixed;        // the fixed volume (the sample's value is fixed[flat])
+    const float* fixed;        // each sample's fixed value, in sample order (the fixed volume
+                               // itself when every voxel is a sample)
     const uint8_t* mmask;
     const uint32_t* samples;   // flat indices in brick order, or null for the whole grid
     uint32_t n;
@@ -167,15 +168,16 @@ __global__ void __launch_bounds__(MOM_BLOCK) k_moments(const SamplerParams P, co
         }
     }
     const uint32_t stride = gridDim.x * blockDim.x;
-    // the next sample's index and this sample's fixed value are requested before the
-    // sampler runs, so those loads overlap its corner gathers
+    // the next sample's index and this sample's fixed value (a coalesced read: the values
+    // are gathered once, at set-up) are requested before the sampler runs, so those
+    // loads overlap its corner gathers
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t flat = s < a.n ? (a.samples ? __ldg(a.samples + s) : s) : 0u;
     for (; s < a.n; s += stride) {
         const uint32_t sn = s + stride;
         const uint32_t cur = flat;
         flat = sn < a.n ? (a.samples ? __ldg(a.samples + sn) : sn) : 0u;
-        const double fv = (double)__ldg(a.fixed + cur);
+        const double fv = (double)__ldg(a.fixed + s);
         double mv, g[3], x[3];
         if (!sample64<WANT_G>(P, cur, a.mmask, mv, g, x)) continue;
         if (MODE == MODE_MS) {
@@ -254,6 +256,15 @@ __global__ void __launch_bounds__(MOM_BLOCK) k_moments(const SamplerParams P, co
     }
 }
 
+// Each sample's fixed value, gathered once: the fixed image and the samples do not
+// change over the metric's life, so the evaluations read them contiguously instead of
+// gathering from the whole fixed volume.
+__global__ void k_gather_fixed(const float* __restrict__ fixed, const uint32_t* __restrict__ samples, int64_t n,
+                               float* __restrict__ out) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+        out[s] = fixed[samples[s]];
+}
+
 template <int MODE, bool GRAD>
 int occupancy() {
     int occ = 0;
@@ -276,6 +287,12 @@ mi_status moments_setup(mi_metric* m) {
     MI_CHECK_CUDA(ctx, cudaMalloc(&w.counter, 2 * sizeof(unsigned int)));
     MI_CHECK_CUDA(ctx, cudaMemsetAsync(w.counter, 0, 2 * sizeof(unsigned int), st));
     MI_CHECK_CUDA(ctx, cudaMemsetAsync(w.result, 0, 2 * NCC2_SLOTS * sizeof(double), st));
+    if (m->samples && m->n_samples > 0) {
+        MI_CHECK_CUDA(ctx, cudaMalloc(&w.fval, (size_t)m->n_samples * sizeof(float)));
+        const int g = (int)std::max<int64_t>(1, std::min<int64_t>((m->n_samples + 255) / 256, (int64_t)ctx->num_sms * 8));
+        k_gather_fixed<<<g, 256, 0, st>>>(m->fixed, m->samples, m->n_samples, w.fval);
+        MI_CHECK_CUDA(ctx, cudaGetLastError());
+    }
     MI_CHECK_CUDA(ctx, cudaHostAlloc(&w.host, NCC2_SLOTS * sizeof(double), cudaHostAllocMapped));
     MI_CHECK_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&w.host_dev), w.host, 0));
     return MI_OK;
@@ -286,6 +303,7 @@ void moments_free(mi_metric* m) {
     cudaFree(w.partials);
     cudaFree(w.result);
     cudaFree(w.counter);
+    cudaFree(w.fval);
     if (w.host) cudaFreeHost(w.host);
     w = MomentsWs{};
 }
@@ -298,7 +316,7 @@ mi_status evaluate_moments(mi_metric* m, const SamplerParams& P, const double* j
     cudaStream_t st = ctx->stream;
     const bool timing = ws.timing != 0;
     MomArgs a;
-    a.fixed = m->fixed;
+    a.fixed = w.fval ? w.fval : m->fixed;
     a.mmask = m->mmask;
     a.samples = m->samples;
     a.n = (uint32_t)m->n_samples;
