@@ -185,7 +185,9 @@ __device__ int bs_sample(const SamplerParams& P, const BSplineDev& S, const doub
 #pragma unroll
     for (int d = 0; d < 3; ++d)
         if (!(c[d] >= -0.5 && c[d] < P.mhi[d])) return BS_OUTSIDE;
-    const double mv = exact_value(P, c, moving);
+    // the value's eight corners serve the gradient too (the same clamped cell)
+    float v[8];
+    const double mv = exact_value_corners(P, c, moving, v);
     // the interpolant's exact gradient on the same cell, in FP64 (a continuous weight)
     double fl[3], fr[3];
 #pragma unroll
@@ -193,8 +195,6 @@ __device__ int bs_sample(const SamplerParams& P, const BSplineDev& S, const doub
         fl[d] = floor(c[d]);
         fr[d] = c[d] - fl[d];
     }
-    float v[8];
-    fetch_corners(P, fl, v);
     double gi[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int t = 0; t < 8; ++t) {

@@ -118,8 +118,10 @@ __device__ __forceinline__ void exact_index(const SamplerParams& P, uint32_t i, 
 // The reference's trilinear value at an exact continuous index that has passed the
 // inside test: weights w_d[0] = 1 − frac, w_d[1] = frac, the corner weight the host's
 // running product ((w0·w1)·w2) (its leading 1.0· is exact), summed in corner order.
-__device__ __forceinline__ double exact_value(const SamplerParams& P, const double* c,
-                                              const float* __restrict__ moving) {
+// The eight clamped corners it reads are left in v (corner t at bit offsets
+// (t & 1, (t >> 1) & 1, t >> 2)), for a caller that also needs the gradient.
+__device__ __forceinline__ double exact_value_corners(const SamplerParams& P, const double* c,
+                                                      const float* __restrict__ moving, float* v) {
     double fr[3], om[3];
     int64_t b0[3], b1[3];
 #pragma unroll
@@ -138,15 +140,29 @@ __device__ __forceinline__ double exact_value(const SamplerParams& P, const doub
     const double w10 = __dmul_rn(fr[0], om[1]);
     const double w01 = __dmul_rn(om[0], fr[1]);
     const double w11 = __dmul_rn(fr[0], fr[1]);
-    double mv = __dmul_rn(__dmul_rn(w00, om[2]), (double)__ldg(moving + (b0[0] + oy0 + oz0)));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, om[2]), (double)__ldg(moving + (b1[0] + oy0 + oz0))));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, om[2]), (double)__ldg(moving + (b0[0] + oy1 + oz0))));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, om[2]), (double)__ldg(moving + (b1[0] + oy1 + oz0))));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w00, fr[2]), (double)__ldg(moving + (b0[0] + oy0 + oz1))));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, fr[2]), (double)__ldg(moving + (b1[0] + oy0 + oz1))));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, fr[2]), (double)__ldg(moving + (b0[0] + oy1 + oz1))));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, fr[2]), (double)__ldg(moving + (b1[0] + oy1 + oz1))));
+    v[0] = __ldg(moving + (b0[0] + oy0 + oz0));
+    v[1] = __ldg(moving + (b1[0] + oy0 + oz0));
+    v[2] = __ldg(moving + (b0[0] + oy1 + oz0));
+    v[3] = __ldg(moving + (b1[0] + oy1 + oz0));
+    v[4] = __ldg(moving + (b0[0] + oy0 + oz1));
+    v[5] = __ldg(moving + (b1[0] + oy0 + oz1));
+    v[6] = __ldg(moving + (b0[0] + oy1 + oz1));
+    v[7] = __ldg(moving + (b1[0] + oy1 + oz1));
+    double mv = __dmul_rn(__dmul_rn(w00, om[2]), (double)v[0]);
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, om[2]), (double)v[1]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, om[2]), (double)v[2]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, om[2]), (double)v[3]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w00, fr[2]), (double)v[4]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, fr[2]), (double)v[5]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, fr[2]), (double)v[6]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, fr[2]), (double)v[7]));
     return mv;
+}
+
+__device__ __forceinline__ double exact_value(const SamplerParams& P, const double* c,
+                                              const float* __restrict__ moving) {
+    float v[8];
+    return exact_value_corners(P, c, moving, v);
 }
 
 // The sampler: fast path with exact fallback (see the file comment), in two stages
