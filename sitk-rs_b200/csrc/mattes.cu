@@ -2,21 +2,24 @@
 // kernels.
 //
 // One evaluation (DeviceMattesMetric::evaluate, registration/device.rs:767-800) is two
-// launches and one 8·(2+P)-byte copy back:
+// launches; the result reaches the host through mapped pinned memory, with no copy:
 //   k_hist   pass 1: sampler (value and gradient) → Parzen joint histogram, per CTA
 //            in shared memory as u32 fixed point (native shared atomics), flushed
-//            into a global u64 histogram. Integer adds are exact, so the histogram does
-//            not depend on the order. Each sample also leaves a 17-byte record
-//            (moving bin, Parzen fraction, moving gradient) for pass 2. The last CTA
-//            to finish runs the tail (registration/mattes.rs:273-328): normalisation,
-//            marginals, −MI and the pRatio·nFactor table, and re-zeroes the global
-//            histogram for the next evaluation.
-//   k_deriv  pass 2: streams the records → 12 moments A[d] = Σ w g_d,
-//            B[d][e] = Σ w g_d (x_e − x_ref,e), w = Σ_taps B₃′·pRatio (the form of the
-//            reference's mattes_deriv, cuda/ops/mattes.rs:319-381), FP32 per thread and
-//            FP64 from the warp reduction on, in a fixed shuffle/tree order into per-CTA
-//            partials; the last CTA folds the partials in CTA order and contracts them
-//            with the transform's Jacobian form (registration/cuda.rs:505-524).
+//            with the joint part's column sums into global u64 counters. Integer adds
+//            are exact, so the histogram does not depend on the order. Each sample also
+//            leaves an 18-byte record (both Parzen bins, Parzen fraction, moving
+//            gradient) for pass 2.
+//   k_deriv  launched as a programmatic dependent of k_hist. Every CTA forms the tail
+//            (registration/mattes.rs:273-328: normalisation, marginals, −MI slices and
+//            the pRatio·nFactor table) from the integer histogram, then streams the
+//            records → 12 moments A[d] = Σ w g_d, B[d][e] = Σ w g_d (x_e − x_ref,e),
+//            w = Σ_taps B₃′·pRatio (the form of the reference's mattes_deriv,
+//            cuda/ops/mattes.rs:319-381), FP32 per thread and FP64 from the warp
+//            reduction on, in a fixed shuffle/tree order into per-CTA partials. The last
+//            CTA folds the partials in a fixed order, contracts them with the
+//            transform's Jacobian form (registration/cuda.rs:505-524), writes value,
+//            valid and derivative into the host's mapped mirror with a sequence number,
+//            and re-zeroes the global histogram for the next evaluation.
 // Every reduction order is a function of the launch shape alone, so repeated
 // evaluations are bit-identical. No kernel waits on another CTA.
 
