@@ -41,13 +41,14 @@ typedef enum {
     MI_ERR_SAMPLE_INDEX_OUT_OF_GRID = 10, /* CudaError::SampleIndexOutOfGrid */
     MI_ERR_MASK_SIZE_MISMATCH = 11,   /* RegistrationError::MaskSizeMismatch */
     MI_ERR_NON_AFFINE_TRANSFORM = 12, /* DeviceMetricError::NonAffineTransform */
-    MI_ERR_POINT_MAP_STAGE_COUNT = 13,/* CudaError::PointMapStageCount (more than MI_MAX_STAGES) */
+    MI_ERR_POINT_MAP_STAGE_COUNT = 13,/* CudaError::PointMapStageCount: no stage, or more than MI_MAX_STAGES */
     MI_ERR_TOO_MANY_HISTOGRAM_BINS = 14, /* bins > MI_MAX_BINS (the shared-memory histogram's limit): no reference counterpart */
     MI_ERR_TIMEOUT = 15,              /* a bounded device wait gave up (fused form's grid barrier) */
     MI_ERR_NOT_CONVERGED = 16         /* reserved */
 } mi_status;
 
-#define MI_MAX_STAGES 4
+/* Point-map stages the device replays (cuda/ops/resident.rs:74 MAX_STAGES). */
+#define MI_MAX_STAGES 8
 #define MI_MAX_BINS 128
 #define MI_MAX_PARAMS 12
 
@@ -230,7 +231,8 @@ mi_status mi_metric_destroy(mi_metric* m);
 
 /* DeviceMattesMetric::value (device.rs:734-737): value = −MI at the point map given
  * as `nstage` stages of 12 doubles (matrix row-major, then offset), replayed in
- * order: p ← M·p + t (matrix_offset.rs:102-109). `valid` may be NULL. */
+ * order: p ← M·p + t (matrix_offset.rs:102-109). 1 ≤ nstage ≤ MI_MAX_STAGES, else
+ * MI_ERR_POINT_MAP_STAGE_COUNT (resident.rs:698-703). `valid` may be NULL. */
 mi_status mi_metric_value(mi_metric* m, const double* stages, int nstage, double* value,
                           int64_t* valid);
 
@@ -469,24 +471,34 @@ mi_status mi_initnet_prepare(mi_context* ctx, const mi_image* fixed, const mi_im
 /* Largest histogram the allocation-free entry point can hold. */
 #define MI_NOALLOC_MAX_BINS 64
 
-/* The metric value for callers that cannot allocate device memory: code running
- * while a CUDA graph is captured, hosts that give the library a fixed memory budget,
- * real-time loops that must not reach the allocator. It calls no cudaMalloc,
+/* The metric value for callers that cannot allocate device memory (no counterpart in
+ * the reference): an application that embeds the metric under a fixed device-memory
+ * budget it manages itself, or a real-time loop that must not reach the allocator
+ * (cudaMalloc and cudaFree may synchronise the device). It calls no cudaMalloc,
  * cudaFree or allocating routine; its only scratch is one fixed-size array in the
- * library's device memory (a joint histogram of at most MI_NOALLOC_MAX_BINS bins,
- * 33 KB), which every GPU that loads the library holds until the process exits.
+ * library's device memory (a joint histogram of at most MI_NOALLOC_MAX_BINS bins and
+ * one counter, 33 KB), which every GPU that loads the library holds until the process
+ * exits.
  *
  * Inputs and outputs belong to the caller and are device pointers: the fixed and
  * moving volumes (f32, x-fastest) with their geometries; an optional list of
  * n_samples flat fixed-grid voxels (NULL = every voxel); the histogram geometry
  * `info` (bins and intensity ranges, e.g. from mi_metric_info_get); the point map as
- * `nstage` stages of 12 doubles; and `result`, two doubles that receive −MI and the
- * valid-sample count. No masks. Work is queued on the context's stream and the
- * call returns without waiting: result is ready once that stream has reached it.
+ * `nstage` stages of 12 doubles (1 ≤ nstage ≤ MI_MAX_STAGES, else
+ * MI_ERR_POINT_MAP_STAGE_COUNT); and `result`, two doubles that receive −MI and the
+ * valid-sample count. No masks. Work is queued on the context's stream and the call
+ * returns without waiting: result is ready once that stream has reached it.
+ *
+ * The sample list is device memory the host cannot inspect. An index at or beyond the
+ * fixed grid's voxel count is skipped on the device (neither volume is read for it)
+ * and the call reports the failure through `result`: result[0] = NaN and result[1] =
+ * −(number of such indices).
  *
  * The first call on a device looks the scratch array up for that device; make that
- * first call before any stream capture begins. Every call on a device shares the
- * array (each call clears it first), so calls whose work overlaps on the GPU race:
+ * first call before any stream capture begins. The address found then belongs to the
+ * device's primary context: do not call this entry point on a device after
+ * cudaDeviceReset in the same process. Every call on a device shares the array (each
+ * call clears it first, on its stream), so calls whose work overlaps on the GPU race:
  * serialise them. bins > MI_NOALLOC_MAX_BINS is refused with
  * MI_ERR_TOO_MANY_HISTOGRAM_BINS. */
 mi_status mi_metric_value_noalloc(mi_context* ctx, const float* fixed, const mi_geometry* fixed_geometry,

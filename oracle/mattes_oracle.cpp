@@ -609,6 +609,81 @@ void finish(const Geometry& G, Accum& A, int np, bool want_deriv, double* value,
     *value = -sum;
 }
 
+// A point map given as stages (matrix row-major, offset; 12 doubles each), replayed
+// one by one as p ← mat_vec(M, p) + offset (transform/matrix_offset.rs:102-109), with
+// a parameter Jacobian that is affine in the fixed point, J(x) = J0 + Σ_e x_e·C_e
+// (the form registration/cuda.rs:294-363 affine_form recovers from a transform).
+struct StageMap {
+    int nstage = 0;
+    int nparams = 0;
+    double st[8][12];
+    double jac0[36];
+    double jacc[3][36];
+    void transform_point(const double* x, double* y) const {
+        double p[3] = {x[0], x[1], x[2]};
+        for (int k = 0; k < nstage; ++k) {
+            double q[3];
+            mat_vec(st[k], p, q);
+            for (int d = 0; d < 3; ++d) p[d] = q[d] + st[k][9 + d];
+        }
+        for (int d = 0; d < 3; ++d) y[d] = p[d];
+    }
+    void jacobian(const double* x, double* j) const {
+        for (int i = 0; i < 3 * nparams; ++i) j[i] = jac0[i] + x[0] * jacc[0][i] + x[1] * jacc[1][i] + x[2] * jacc[2][i];
+    }
+};
+
+// `draw` is the sampling strategy's draw BEFORE the fixed-mask filter (NULL = the
+// whole grid). Per-sample outputs, when non-null, are indexed in post-filter sample
+// order: status 0 = outside/masked, 1 = moving value out of range, 2 = valid; fi/mi
+// are the Parzen bins of a valid sample. `nthreads` > 1 splits the samples into
+// contiguous chunks with private accumulators folded in thread-index order (the
+// reference's deterministic rayon rule, core/parallel.rs:766); 1 is the serial walk.
+template <class TransformT>
+int evaluate_with(const Problem& P, int bins, const TransformT& T, int want_derivative, int nthreads,
+                  double* value, double* deriv, int64_t* valid, int8_t* status, int32_t* fi_out, int32_t* mi_out,
+                  double* joint_out, double* fixed_marginal_out) {
+    double fmin, fmax, mmin, mmax;
+    ranges(P, &fmin, &fmax, &mmin, &mmax);
+    Geometry G;
+    int st = make_geometry(fmin, fmax, mmin, mmax, bins, G);
+    if (st) return st;
+    const bool wd = want_derivative != 0;
+    const int np = T.nparams;
+    if (nthreads < 1) nthreads = 1;
+    std::vector<Accum> parts(nthreads);
+    for (auto& a : parts) {
+        a.joint.assign((size_t)bins * bins, 0.0);
+        a.fixed_marginal.assign(bins, 0.0);
+        if (wd) a.jpd.assign((size_t)bins * bins * np, 0.0);
+    }
+    const int64_t n = P.n;
+    if (nthreads == 1) {
+        for (int64_t s = 0; s < n; ++s) sample_body(P, G, T, s, wd, parts[0], status, fi_out, mi_out);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t) {
+            pool.emplace_back([&, t]() {
+                int64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
+                for (int64_t s = lo; s < hi; ++s)
+                    sample_body(P, G, T, s, wd, parts[t], status, fi_out, mi_out);
+            });
+        }
+        for (auto& th : pool) th.join();
+        for (int t = 1; t < nthreads; ++t) {
+            for (size_t i = 0; i < parts[0].joint.size(); ++i) parts[0].joint[i] += parts[t].joint[i];
+            for (int i = 0; i < bins; ++i) parts[0].fixed_marginal[i] += parts[t].fixed_marginal[i];
+            for (size_t i = 0; i < parts[0].jpd.size(); ++i) parts[0].jpd[i] += parts[t].jpd[i];
+            parts[0].valid += parts[t].valid;
+        }
+    }
+    Accum& A = parts[0];
+    if (joint_out) std::memcpy(joint_out, A.joint.data(), A.joint.size() * sizeof(double));
+    if (fixed_marginal_out) std::memcpy(fixed_marginal_out, A.fixed_marginal.data(), bins * sizeof(double));
+    finish(G, A, np, wd, value, deriv, valid);
+    return OR_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -672,12 +747,6 @@ int or_metric_geometry(const float* fixed, const or_geometry* fg, const float* m
 // The whole metric: value = −MI, derivative = +∇(−MI) (mattes.rs:522-676), or the
 // value-only walk (mattes.rs:442-500) when want_derivative is 0.
 //
-// `draw` is the sampling strategy's draw BEFORE the fixed-mask filter (NULL = the
-// whole grid). Per-sample outputs, when non-null, are indexed in post-filter sample
-// order: status 0 = outside/masked, 1 = moving value out of range, 2 = valid; fi/mi
-// are the Parzen bins of a valid sample. `nthreads` > 1 splits the samples into
-// contiguous chunks with private accumulators folded in thread-index order (the
-// reference's deterministic rayon rule, core/parallel.rs:766); 1 is the serial walk.
 int or_mattes_evaluate(const float* fixed, const or_geometry* fg, const float* moving,
                        const or_geometry* mg, const uint8_t* fmask, const uint8_t* mmask,
                        const int64_t* draw, int64_t ndraw, int bins, int kind,
@@ -688,47 +757,33 @@ int or_mattes_evaluate(const float* fixed, const or_geometry* fg, const float* m
     Problem P;
     int st = prepare(fixed, fg, moving, mg, fmask, mmask, draw, ndraw, P);
     if (st) return st;
-    double fmin, fmax, mmin, mmax;
-    ranges(P, &fmin, &fmax, &mmin, &mmax);
-    Geometry G;
-    st = make_geometry(fmin, fmax, mmin, mmax, bins, G);
-    if (st) return st;
     Transform T;
     if (!make_transform(kind, params, fixed_params, nfixed, T)) return OR_BAD_ARGUMENT;
-    const bool wd = want_derivative != 0;
-    const int np = T.nparams;
-    if (nthreads < 1) nthreads = 1;
-    std::vector<Accum> parts(nthreads);
-    for (auto& a : parts) {
-        a.joint.assign((size_t)bins * bins, 0.0);
-        a.fixed_marginal.assign(bins, 0.0);
-        if (wd) a.jpd.assign((size_t)bins * bins * np, 0.0);
+    return evaluate_with(P, bins, T, want_derivative, nthreads, value, deriv, valid, status, fi_out, mi_out,
+                         joint_out, fixed_marginal_out);
+}
+
+// The same metric at a point map of 1..8 stages with an affine-in-x Jacobian form
+// (jac0: 3×nparams row-major; jacc: three such blocks).
+int or_mattes_evaluate_stages(const float* fixed, const or_geometry* fg, const float* moving,
+                              const or_geometry* mg, const uint8_t* fmask, const uint8_t* mmask,
+                              const int64_t* draw, int64_t ndraw, int bins, const double* stages, int nstage,
+                              const double* jac0, const double* jacc, int nparams, int nthreads, double* value,
+                              double* deriv, int64_t* valid, int8_t* status, int32_t* fi_out, int32_t* mi_out) {
+    if (nstage < 1 || nstage > 8 || nparams < 1 || nparams > 12) return OR_BAD_ARGUMENT;
+    Problem P;
+    int st = prepare(fixed, fg, moving, mg, fmask, mmask, draw, ndraw, P);
+    if (st) return st;
+    StageMap T;
+    T.nstage = nstage;
+    T.nparams = nparams;
+    for (int k = 0; k < nstage; ++k)
+        for (int i = 0; i < 12; ++i) T.st[k][i] = stages[k * 12 + i];
+    for (int i = 0; i < 3 * nparams; ++i) {
+        T.jac0[i] = jac0[i];
+        for (int e = 0; e < 3; ++e) T.jacc[e][i] = jacc[e * 3 * nparams + i];
     }
-    const int64_t n = P.n;
-    if (nthreads == 1) {
-        for (int64_t s = 0; s < n; ++s) sample_body(P, G, T, s, wd, parts[0], status, fi_out, mi_out);
-    } else {
-        std::vector<std::thread> pool;
-        for (int t = 0; t < nthreads; ++t) {
-            pool.emplace_back([&, t]() {
-                int64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
-                for (int64_t s = lo; s < hi; ++s)
-                    sample_body(P, G, T, s, wd, parts[t], status, fi_out, mi_out);
-            });
-        }
-        for (auto& th : pool) th.join();
-        for (int t = 1; t < nthreads; ++t) {
-            for (size_t i = 0; i < parts[0].joint.size(); ++i) parts[0].joint[i] += parts[t].joint[i];
-            for (int i = 0; i < bins; ++i) parts[0].fixed_marginal[i] += parts[t].fixed_marginal[i];
-            for (size_t i = 0; i < parts[0].jpd.size(); ++i) parts[0].jpd[i] += parts[t].jpd[i];
-            parts[0].valid += parts[t].valid;
-        }
-    }
-    Accum& A = parts[0];
-    if (joint_out) std::memcpy(joint_out, A.joint.data(), A.joint.size() * sizeof(double));
-    if (fixed_marginal_out) std::memcpy(fixed_marginal_out, A.fixed_marginal.data(), bins * sizeof(double));
-    finish(G, A, np, wd, value, deriv, valid);
-    return OR_OK;
+    return evaluate_with(P, bins, T, 1, nthreads, value, deriv, valid, status, fi_out, mi_out, nullptr, nullptr);
 }
 
 // One level of registration with the reference's regular-step gradient descent

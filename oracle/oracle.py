@@ -73,6 +73,10 @@ def lib():
                                      ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      dp, dp, i64p, i8p, i32p, i32p, dp, dp]
     L.or_mattes_evaluate.restype = ctypes.c_int
+    L.or_mattes_evaluate_stages.argtypes = [fp, gp, fp, gp, u8p, u8p, i64p, ctypes.c_int64, ctypes.c_int, dp,
+                                            ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int, dp, dp, i64p, i8p,
+                                            i32p, i32p]
+    L.or_mattes_evaluate_stages.restype = ctypes.c_int
     L.or_transform.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp, dp, dp]
     L.or_transform.restype = ctypes.c_int
     L.or_cubic_bspline.argtypes = [dp, dp, dp, ctypes.c_int64]
@@ -183,6 +187,44 @@ def evaluate(fixed, fgeo, moving, mgeo, bins, kind, params, fixed_params=None, f
         out.update(status=status, fi=fi, mi=mi)
     if histogram:
         out.update(joint=joint, fixed_marginal=margin)
+    return out
+
+
+def evaluate_stages(fixed, fgeo, moving, mgeo, bins, stages, jac0, jacc, fmask=None, mmask=None, draw=None,
+                    nthreads=1, per_sample=False):
+    """value and derivative at a point map of 1..8 stages (12 doubles each, replayed in
+    order, matrix_offset.rs:102-109) with the Jacobian J(x) = jac0 + Σ_e x_e·jacc[e]
+    (jac0 3×P row-major, jacc three such blocks)."""
+    fixed = np.ascontiguousarray(fixed, dtype=np.float32)
+    moving = np.ascontiguousarray(moving, dtype=np.float32)
+    fm = None if fmask is None else np.ascontiguousarray(fmask, dtype=np.uint8)
+    mm = None if mmask is None else np.ascontiguousarray(mmask, dtype=np.uint8)
+    dr = None if draw is None else np.ascontiguousarray(draw, dtype=np.int64)
+    st = np.ascontiguousarray(stages, dtype=np.float64).ravel()
+    j0 = np.ascontiguousarray(jac0, dtype=np.float64).ravel()
+    jc = np.ascontiguousarray(jacc, dtype=np.float64).ravel()
+    nparams = j0.size // 3
+    deriv = np.zeros(nparams)
+    value = ctypes.c_double(0.0)
+    valid = ctypes.c_int64(0)
+    status = fi = mi = None
+    if per_sample:
+        nvox = int(np.prod([fgeo.size[i] for i in range(3)]))
+        n = nvox if dr is None else len(dr)
+        status = np.full(n, -1, dtype=np.int8)
+        fi = np.full(n, -1, dtype=np.int32)
+        mi = np.full(n, -1, dtype=np.int32)
+    r = lib().or_mattes_evaluate_stages(
+        _ptr(fixed, ctypes.c_float), ctypes.byref(fgeo), _ptr(moving, ctypes.c_float), ctypes.byref(mgeo),
+        _ptr(fm, ctypes.c_uint8), _ptr(mm, ctypes.c_uint8), _ptr(dr, ctypes.c_int64), 0 if dr is None else len(dr),
+        bins, _ptr(st, ctypes.c_double), st.size // 12, _ptr(j0, ctypes.c_double), _ptr(jc, ctypes.c_double),
+        nparams, nthreads, ctypes.byref(value), _ptr(deriv, ctypes.c_double), ctypes.byref(valid),
+        _ptr(status, ctypes.c_int8), _ptr(fi, ctypes.c_int32), _ptr(mi, ctypes.c_int32))
+    if r:
+        raise OracleError(r)
+    out = {"value": value.value, "derivative": deriv, "valid": valid.value}
+    if per_sample:
+        out.update(status=status, fi=fi, mi=mi)
     return out
 
 

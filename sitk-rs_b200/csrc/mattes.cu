@@ -456,10 +456,12 @@ mi_status fill_params(mi_metric* m, const double* stages, int nstage, SamplerPar
 mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double* jac0, const double* jacc,
                    int nparams, bool want_derivative, double* value, double* derivative, int64_t* valid) {
     mi_context* ctx = m->ctx;
-    if (nstage < 0 || nstage > MI_MAX_STAGES)
+    // an empty list, or one longer than MI_MAX_STAGES, is refused by name
+    // (cuda/ops/resident.rs:698-703 upload_point_map)
+    if (nstage < 1 || nstage > MI_MAX_STAGES)
         return set_error(ctx, MI_ERR_POINT_MAP_STAGE_COUNT,
-                         "the device replays at most " + std::to_string(MI_MAX_STAGES) + " point-map stages");
-    if (nstage > 0 && !stages) return MI_ERR_INVALID_ARGUMENT;
+                         "the device replays 1 to " + std::to_string(MI_MAX_STAGES) + " point-map stages");
+    if (!stages) return MI_ERR_INVALID_ARGUMENT;
     if (want_derivative && (nparams < 1 || nparams > MI_MAX_PARAMS || !jac0 || !jacc || !derivative))
         return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "bad Jacobian form");
     MI_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -1033,7 +1035,9 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
     if (m->metric_kind != MI_METRIC_MATTES)
         return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "per-sample Parzen decisions exist for the Mattes metric only");
     if (n < m->n_samples) return set_error(ctx, MI_ERR_INVALID_ARGUMENT, "output arrays shorter than the sample count");
-    if (nstage < 0 || nstage > MI_MAX_STAGES) return set_error(ctx, MI_ERR_POINT_MAP_STAGE_COUNT, "too many stages");
+    if (nstage < 1 || nstage > MI_MAX_STAGES)
+        return set_error(ctx, MI_ERR_POINT_MAP_STAGE_COUNT,
+                         "the device replays 1 to " + std::to_string(MI_MAX_STAGES) + " point-map stages");
     MI_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
     SamplerParams P;
     mi_status s = fill_params(m, stages, nstage, P);

@@ -1,18 +1,26 @@
 // Mattes value for callers that cannot allocate device memory.
 //
-// Some callers of this library may not call cudaMalloc at all: code that runs while
-// a CUDA graph is being captured (an allocation inside capture is an error), hosts
-// that hand the library a fixed memory budget up front, or real-time loops that
-// must not hit the allocator. mi_metric_value_noalloc serves them. It evaluates the
-// metric value over device buffers the caller owns, and its only scratch — the
-// joint histogram the passes accumulate into — lives in one file-scope
-// `static __device__` array of a fixed size (MI_NOALLOC_MAX_BINS bins), which every
-// GPU that loads the library holds until the process exits.
+// Some callers of this library may not call cudaMalloc at all: an application that
+// embeds the metric and hands it a fixed device-memory budget up front (it owns every
+// buffer, and a library that allocates on its own breaks that accounting), or a
+// real-time loop that must not reach the allocator (cudaMalloc and cudaFree may
+// synchronise the device and take milliseconds). mi_metric_value_noalloc serves them.
+// It evaluates the metric value over device buffers the caller owns, and its only
+// scratch — the joint histogram the passes accumulate into, plus one word that counts
+// rejected sample indices — lives in one file-scope `static __device__` array of a
+// fixed size (MI_NOALLOC_MAX_BINS bins), which every GPU that loads the library holds
+// until the process exits.
 //
 // The array is shared by every call on a device and keeps the last call's contents,
 // so each call clears it on its own stream before use; two calls whose work overlaps
 // on the GPU (different streams, or different host threads on one stream without
 // ordering) race on it and must be serialised by the caller.
+//
+// The caller's sample list lives in device memory, so the host cannot check it: the
+// histogram pass skips every index at or beyond the fixed grid's voxel count (it
+// reads neither the fixed volume nor the moving volume for it) and counts it, and the
+// tail then reports the call as failed through the result (value NaN, valid count
+// minus the number of rejected indices).
 //
 // The histogram pass here decides every sample with the exact FP64 chain of
 // sampler.cuh (exact_index / exact_value) and reads the fixed value directly, so it
@@ -38,14 +46,17 @@ bool invert3(const double* m, double* inv);
 namespace {
 
 constexpr int NA_BLOCK = 256;
-constexpr int NA_SCRATCH = MI_NOALLOC_MAX_BINS * MI_NOALLOC_MAX_BINS + MI_NOALLOC_MAX_BINS;
+constexpr int NA_SCRATCH = MI_NOALLOC_MAX_BINS * MI_NOALLOC_MAX_BINS + MI_NOALLOC_MAX_BINS + 1;
 
-// The scratch: joint histogram (B² taps in 2^-k fixed point) then the fixed
-// marginal (B counts), u64.
+// The scratch: joint histogram (B² taps in 2^-k fixed point), the fixed marginal
+// (B counts), then the count of rejected sample indices, u64.
 static __device__ __align__(256) unsigned long long g_noalloc_hist[NA_SCRATCH];
 
 // Device address of g_noalloc_hist per device, looked up once per device with that
-// device current (a host reference to the symbol is only a host-side stand-in).
+// device current (a host reference to the symbol is only a host-side stand-in). The
+// address belongs to the device's primary context: after cudaDeviceReset the module
+// is loaded again and this cached address is stale, so a process that resets a device
+// must not call mi_metric_value_noalloc on it afterwards.
 std::mutex g_setup_mutex;
 unsigned long long* g_hist_addr[256] = {};
 
@@ -64,16 +75,22 @@ mi_status scratch_address(mi_context* ctx, unsigned long long** out) {
 
 __global__ void __launch_bounds__(NA_BLOCK)
 k_noalloc_hist(mi::SamplerParams P, const float* __restrict__ fixed, const float* __restrict__ moving,
-               const uint32_t* __restrict__ samples, uint32_t n, float hist_scale,
+               const uint32_t* __restrict__ samples, uint32_t n, uint32_t nvox, float hist_scale,
                unsigned long long* __restrict__ hist) {
     extern __shared__ unsigned int nsh[];
     const int B = P.bins;
     const int nb = B * B + B;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) nsh[i] = 0u;
+    // the shared histogram, then the CTA's count of rejected indices
+    for (int i = threadIdx.x; i <= nb; i += blockDim.x) nsh[i] = 0u;
     __syncthreads();
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
         const uint32_t flat = samples ? samples[s] : s;
+        if (flat >= nvox) {
+            // not a voxel of the fixed grid: neither volume is read for it
+            atomicAdd(nsh + nb, 1u);
+            continue;
+        }
         uint32_t i, j, k;
         mi::grid_index(P, flat, i, j, k);
         double c[3];
@@ -97,7 +114,7 @@ k_noalloc_hist(mi::SamplerParams P, const float* __restrict__ fixed, const float
         atomicAdd(nsh + B * B + fi, 1u);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    for (int i = threadIdx.x; i <= nb; i += blockDim.x) {
         const unsigned int v = nsh[i];
         if (v) atomicAdd(hist + i, (unsigned long long)v);
     }
@@ -124,7 +141,8 @@ __device__ double na_block_sum(double v, double* red) {
 }
 
 // −MI from the finished histogram (registration/mattes.rs:273-328) into result[0],
-// the valid count into result[1].
+// the valid count into result[1]; NaN and minus the number of rejected sample indices
+// when the pass skipped any.
 __global__ void __launch_bounds__(NA_BLOCK)
 k_noalloc_tail(int B, double moving_bin_size, double hist_inv, const unsigned long long* __restrict__ hist,
                double* __restrict__ result) {
@@ -132,6 +150,14 @@ k_noalloc_tail(int B, double moving_bin_size, double hist_inv, const unsigned lo
     __shared__ double fm[MI_NOALLOC_MAX_BINS], mm[MI_NOALLOC_MAX_BINS], lfm[MI_NOALLOC_MAX_BINS];
     __shared__ double red[32];
     const int B2 = B * B;
+    const unsigned long long rejected = hist[B2 + B];
+    if (rejected) {
+        if (threadIdx.x == 0) {
+            result[0] = __longlong_as_double(0x7ff8000000000000ll);
+            result[1] = -(double)rejected;
+        }
+        return;
+    }
     double part = 0.0, cnt = 0.0;
     for (int i = threadIdx.x; i < B2; i += blockDim.x) {
         jp[i] = (double)hist[i] * hist_inv;
@@ -185,8 +211,10 @@ extern "C" mi_status mi_metric_value_noalloc(mi_context* ctx, const float* fixed
     using namespace mi;
     if (!ctx || !fixed || !fixed_geometry || !moving || !moving_geometry || !info || !result)
         return MI_ERR_INVALID_ARGUMENT;
-    if (nstage < 0 || nstage > MI_MAX_STAGES || (nstage > 0 && !stages))
-        return set_error(ctx, MI_ERR_POINT_MAP_STAGE_COUNT, "the device replays at most 4 point-map stages");
+    if (nstage < 1 || nstage > MI_MAX_STAGES)
+        return set_error(ctx, MI_ERR_POINT_MAP_STAGE_COUNT,
+                         "the device replays 1 to " + std::to_string(MI_MAX_STAGES) + " point-map stages");
+    if (!stages) return MI_ERR_INVALID_ARGUMENT;
     const int B = info->bins;
     if (B < 2 * PADDING + 1) return set_error(ctx, MI_ERR_TOO_FEW_HISTOGRAM_BINS, "need at least 5 histogram bins");
     if (B > MI_NOALLOC_MAX_BINS)
@@ -250,9 +278,10 @@ extern "C" mi_status mi_metric_value_noalloc(mi_context* ctx, const float* fixed
     int kbits = 22;
     while (kbits > 0 && std::ldexp(1.0, kbits) * (2.0 / 3.0) * cta_max + cta_max >= 4294967295.0 * 0.98) --kbits;
     cudaStream_t st = ctx->stream;
-    MI_CHECK_CUDA(ctx, cudaMemsetAsync(hist, 0, (size_t)(B * B + B) * sizeof(unsigned long long), st));
-    k_noalloc_hist<<<grid, NA_BLOCK, (size_t)(B * B + B) * sizeof(unsigned int), st>>>(
-        P, fixed, moving, samples, (uint32_t)n, (float)std::ldexp(1.0, kbits), hist);
+    // the histogram, the marginal and the rejected-index count start at zero
+    MI_CHECK_CUDA(ctx, cudaMemsetAsync(hist, 0, (size_t)(B * B + B + 1) * sizeof(unsigned long long), st));
+    k_noalloc_hist<<<grid, NA_BLOCK, (size_t)(B * B + B + 1) * sizeof(unsigned int), st>>>(
+        P, fixed, moving, samples, (uint32_t)n, (uint32_t)nvox, (float)std::ldexp(1.0, kbits), hist);
     k_noalloc_tail<<<1, NA_BLOCK, 0, st>>>(B, P.moving_bin_size, std::ldexp(1.0, -kbits), hist, result);
     MI_CHECK_CUDA(ctx, cudaGetLastError());
     return MI_OK;

@@ -40,9 +40,11 @@ def bf16_round(v):
 
 
 def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
-             strategy=None, pct=1.0, seed=0, mmask=None, fmask=None, explicit=None, moving_storage="f32"):
+             strategy=None, pct=1.0, seed=0, mmask=None, fmask=None, explicit=None, moving_storage="f32",
+             nthreads=1, other_form=True):
     """With moving_storage "bf16" the oracle runs on the moving volume rounded to BF16
-    (the values the device metric samples), so the same exact contract applies."""
+    (the values the device metric samples), so the same exact contract applies.
+    other_form=False skips the comparison with the other launch form."""
     sb = _sb()
     f, m = _upload_pair(p, spacing, origin)
     if moving_storage == "bf16":
@@ -60,7 +62,7 @@ def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0
     g = _oracle_geo(oracle, n, spacing, origin)
     ref = oracle.evaluate(p.fixed, g, p.moving, g, bins, transform.kind, transform.params,
                           transform.fixed_params, fmask=fmask, mmask=mmask, draw=draw,
-                          per_sample=True)
+                          per_sample=True, nthreads=nthreads)
     info = metric.info()
     ginfo = oracle.geometry_info(p.fixed, g, p.moving, g, bins, fmask=fmask, mmask=mmask, draw=draw)
     for k in ("fixed_min", "fixed_max", "moving_min", "moving_max", "fixed_bin_size", "moving_bin_size",
@@ -98,6 +100,8 @@ def _compare(oracle, p, n, transform, bins, spacing=(1.0, 1.0, 1.0), origin=(0.0
     # value-only path agrees with evaluate
     v = metric.value(transform)
     assert v == mv.value
+    if not other_form:
+        return metric, mv, ref, dec
     # the split launch form (two kernels) computes the same histogram and tail, so
     # the same value bits; its derivative sums the moments over another partition of
     # the samples (FP32 within a thread, FP64 from the warp on), so the two forms agree
@@ -232,9 +236,10 @@ def test_refusals_are_named():
         sb.DeviceMattesMetric.from_device(f, sing, 32)
     assert e.value.name == "MI_ERR_SINGULAR_DIRECTION"
     metric = sb.DeviceMattesMetric.from_device(f, m, 32)
-    with pytest.raises(sb.MiError) as e:
-        metric.value_stages(np.zeros(12 * 5))
-    assert e.value.name == "MI_ERR_POINT_MAP_STAGE_COUNT"
+    for bad in (np.zeros(0), np.zeros(12 * 9)):
+        with pytest.raises(sb.MiError) as e:
+            metric.value_stages(bad)
+        assert e.value.name == "MI_ERR_POINT_MAP_STAGE_COUNT"
     with pytest.raises(sb.MiError) as e:
         sb.DeviceImage.upload(np.zeros((4, 4, 4), dtype=np.complex64))
     assert e.value.name == "MI_ERR_UNSUPPORTED_PIXEL_TYPE"
