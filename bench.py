@@ -45,6 +45,26 @@ PCT = 0.10
 SEED = 20261203
 # a pose near the generating transform's inverse (versor right part, translation)
 POSE = [0.021, -0.034, 0.047, 3.1, -4.2, 2.6]
+# what the evaluation computes in: each sample's value, gradient and Parzen taps in
+# FP32 (an exact FP64 chain wherever a decision could differ from the reference's),
+# the joint histogram in u32/u64 fixed point (exact integer sums), the tail, the
+# moments' cross-warp sums and the contraction in FP64
+DTYPE = "f32 samples, u32/u64 fixed-point histogram, f64 reductions"
+
+
+def workload_config(samples: int, world: int = 1) -> dict:
+    """The `config` object of the benchmark line, the same in both arms."""
+    return {"workload": WORKLOAD, "fixed": [N, N, N], "moving": [N, N, N], "bins": BINS,
+            "sampling": "random 10%", "samples": samples, "seed": SEED, "transform": "VersorRigid3D",
+            "pose": POSE,
+            "l2": "flushed before every evaluation (256 MiB write, then a 256 MiB read of another buffer so the "
+                  "write-backs fall outside the timed region)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+# the learned initialiser's weights, trained by the library's own kernels with
+#   python bench.py --initnet --initnet-save sitk-rs_b200/sitk_b200/data/initnet_128cubed.npz
+WEIGHTS = os.path.join(ROOT, "sitk-rs_b200", "sitk_b200", "data", "initnet_128cubed.npz")
 
 
 def _env_int(name, default):
@@ -167,6 +187,14 @@ def time_oracle(pair, draw, nthreads: int, budget_s: float, min_evals: int = 1):
     return times
 
 
+def cpu_protocol(pair, draw, nthreads: int, runs: int = 6, warm_s: float = 2.0):
+    """The CPU baseline protocol: at least warm_s seconds of untimed evaluations, then
+    the median of `runs` timed ones (seconds per evaluation, and the runs)."""
+    time_oracle(pair, draw, nthreads, warm_s, min_evals=1)
+    times = time_oracle(pair, draw, nthreads, 0.0, min_evals=runs)
+    return statistics.median(times), times
+
+
 def run_reference(args, rank: int, world: int):
     if rank != 0:
         return 0
@@ -175,21 +203,20 @@ def run_reference(args, rank: int, world: int):
     pair = make_workload(SEED)
     draw = oracle.draw_samples(N ** 3, 2, PCT, SEED)
     cores = os.cpu_count() or 1
-    times = time_oracle(pair, draw, cores, 0.0, min_evals=args.warmup)  # warm-up
-    times = []
-    for _ in range(args.steps):
-        times += time_oracle(pair, draw, cores, 0.0, min_evals=1)
+    # at least 2 s and `warmup` evaluations untimed, then `steps` timed evaluations
+    time_oracle(pair, draw, cores, 2.0, min_evals=max(args.warmup, 1))
+    times = time_oracle(pair, draw, cores, 0.0, min_evals=args.steps)
     total = sum(times)
     value = args.steps / total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "samples": int(draw.size), "bins": BINS},
+        "data": "synthetic", "config": workload_config(int(draw.size), world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} full evaluations of the workload (C++ FP64 restatement of "
-                                   f"the reference CPU metric, {cores} threads, per-thread histograms "
-                                   "folded in thread order)"},
+                         "sample": f"{args.steps} full evaluations of the workload after a >= 2 s warm-up "
+                                   f"(C++ FP64 restatement of the reference CPU metric, {cores} threads, "
+                                   "per-thread histograms folded in thread order)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -240,6 +267,70 @@ def time_registration(pair, ctx, dev):
             "tre_corners_mm": {"mean": float(np.mean(err)), "max": float(np.max(err))}}
 
 
+def time_full_grid(metric, t, l2_flush, steps: int):
+    """The same pair and pose with every voxel of the 256³ fixed grid a sample
+    (16,777,216 samples): value+derivative evaluations, L2 flushed before each, device
+    time per evaluation and per kernel (CUDA events), and the histogram pass's
+    roofline: per pass S·4 B (fixed) + min(V_m, 8S)·4 B (moving)."""
+    from sitk_b200.metric import enable_timing, read_timing
+    S = int(metric.info()["n_samples"])
+    for _ in range(3):
+        l2_flush()
+        metric.evaluate(t)
+    out = {}
+    for per_kernel in (False, True):
+        enable_timing(metric, True, per_kernel=per_kernel)
+        read_timing(metric)
+        for _ in range(steps):
+            l2_flush()
+            r = metric.evaluate(t)
+        ms, nev = read_timing(metric)
+        enable_timing(metric, False)
+        if per_kernel:
+            out["kernel_ms"] = {"k_hist": ms[1] / nev, "k_deriv": ms[2] / nev}
+        else:
+            out["ms_per_eval"] = ms[0] / nev
+    peak, peak_kind = _peaks()
+    pass_bytes = S * 4 + min(N ** 3, 8 * S) * 4
+    kh = out["kernel_ms"]["k_hist"]
+    return {"samples": S, "evals_per_s": 1e3 / out["ms_per_eval"], "ms_per_eval": out["ms_per_eval"],
+            "kernel_ms": out["kernel_ms"], "steps": steps, "value": r.value, "valid": r.valid_points,
+            "roofline": {"bound": "hbm", "kernel": "k_hist", "bytes_alg_per_launch": pass_bytes,
+                         "achieved": pass_bytes / (kh / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": pass_bytes / (kh / 1e3) / 1e9 / peak, "peak_source": peak_kind},
+            "evaluation_roofline": {"bytes_alg_per_eval": 2 * pass_bytes,
+                                    "frac": 2 * pass_bytes / (out["ms_per_eval"] / 1e3) / 1e9 / peak}}
+
+
+def time_learned(args):
+    """The batched + learned form against the plain single-pair GPU driver on held-out
+    128³ pairs (rotation ±20°, translation ±20 mm, scale 0.9–1.1; affine, 50 bins, 10 %
+    random sampling, ≤ 200 iterations): the network (the committed weights) proposes
+    each pair's start, the batched optimizer refines all pairs together, and a proposal
+    counts only when its refined metric value is within 1e-3 of the plain run's final
+    value from the centred start, or lower. Host wall clock around synchronous calls."""
+    from sitk_b200 import initnet as I
+    net = I.InitNet(seed=SEED, max_batch=64)
+    meta = net.load(WEIGHTS)
+    spec = I.PairSpec(n=128, nblobs=40, rot_deg=20.0, trans_mm=20.0, scale=(0.9, 1.1))
+    run = I.PlainRun(bins=50, percentage=0.1, iterations=200)
+    first = 10_000_001
+    ev = I.evaluate(net, range(first, first + args.learned_pairs), spec, run, single_pairs=args.learned_single)
+    net.close()
+    rps = ev["registrations_per_s"]
+    accepted_rate = ev["accepted"] * rps["batched_learned"]
+    return {"pairs": ev["pairs"], "held_out_seeds": [first, first + args.learned_pairs - 1],
+            "accepted": ev["accepted"], "registrations_per_s": accepted_rate,
+            "batched_learned_registrations_per_s": rps["batched_learned"],
+            "plain_single_pair_registrations_per_s": rps["single_pair_plain"],
+            "speedup_vs_plain_single_pair": accepted_rate / rps["single_pair_plain"],
+            "batched_plain_registrations_per_s": rps["batched_plain"],
+            "iterations": ev["iterations"], "tre_mm_p50": {k: v["p50"] for k, v in ev["tre_mm"].items()},
+            "single_pair_iterations_to_plain_final": ev["single_pair_iterations_to_plain_final"],
+            "weights": os.path.relpath(WEIGHTS, ROOT), "training": meta,
+            "timing": "host wall clock around synchronous library calls; metric creation excluded"}
+
+
 def time_batch(ctx, dev, seed: int):
     """The batched workload: 64 affine pairs, edge n ~ U{48..192} per pair (seeded),
     50 bins, 20 % random sampling, regular-step gradient descent (≤ 100 iterations)
@@ -272,7 +363,8 @@ def time_batch(ctx, dev, seed: int):
     wall = time.perf_counter() - t0
     chunk, copies, nchunks = batch.shape()
     ev = np.array([r.evaluations for r in res], dtype=np.float64)
-    per_pair = ev * (wall / ev.max())
+    # device-timed: from the run's first pass to the optimizer step at which each pair stopped
+    per_pair = batch.pair_seconds()
     batch.close()
     # the single-pair driver, pair after pair
     plain = []
@@ -290,7 +382,8 @@ def time_batch(ctx, dev, seed: int):
     return {"pairs": 64, "edge": [min(sizes), max(sizes)], "bins": 50, "sampling": "random 20%",
             "samples_total": int(sum(int(0.2 * n ** 3) for n in sizes)),
             "generate_s": gen_s, "first_call_s": tune_s, "wall_s": wall, "registrations_per_s": 64 / wall,
-            "per_pair_s": {"p50": float(np.percentile(per_pair, 50)), "p99": float(np.percentile(per_pair, 99))},
+            "per_pair_s": {"p50": float(np.percentile(per_pair, 50)), "p99": float(np.percentile(per_pair, 99)),
+                           "timing": "device global timer, run start to the step at which the pair stopped"},
             "evaluations": {"mean": float(ev.mean()), "max": int(ev.max())},
             "shape": {"chunk": chunk, "copies": copies, "chunks": nchunks},
             "single_pair_driver": {"wall_s": float(sum(plain)), "registrations_per_s": 64 / sum(plain),
@@ -317,6 +410,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     m = sb.DeviceImage.upload(pair.moving, ctx=ctx)
     metric = sb.DeviceMattesMetric.from_device_sampled(f, m, bins=BINS, strategy=sb.SAMPLING_RANDOM,
                                                        percentage=PCT, seed=SEED)
+    # the whole 256³ grid as the sample set (16.8 M samples): the survey's full-grid point
+    full_metric = None if args.no_full_grid or rank != 0 else sb.DeviceMattesMetric.from_device(f, m, BINS)
     siblings = None
     if not args.no_siblings and rank == 0:
         siblings = {name: cls.from_device_sampled(f, m, strategy=sb.SAMPLING_RANDOM, percentage=PCT, seed=SEED)
@@ -436,10 +531,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
         draw = oracle.draw_samples(vm, 2, PCT, SEED)
-        times = time_oracle(pair, draw, 1, args.cpu_budget)
-        cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{len(times)} full evaluations of the same workload, serial C++ FP64 "
-                         f"restatement of the reference CPU metric (~{sum(times):.1f} s)"}
+        med, times = cpu_protocol(pair, draw, 1)
+        cpu = {"value": 1.0 / med, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"median of {len(times)} full evaluations of the same workload after a >= 2 s "
+                         "warm-up, serial C++ FP64 restatement of the reference CPU metric "
+                         f"(runs {min(times):.3f}-{max(times):.3f} s)"}
 
     clocks = sampler.summary() if sampler else None
     sib = None
@@ -480,18 +576,21 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         bms = sum(a.elapsed_time(b) for a, b in bs_ev) / len(bs_ev)
         sib["mattes_bspline_8x8x8"] = {"evals_per_s": 1e3 / bms, "ms_per_eval": bms, "parameters": bst.nparams,
                                        "timing": "end to end per call (events around the synchronous call)"}
+    full = None
+    if full_metric is not None:
+        full = time_full_grid(full_metric, t, l2_flush, min(args.steps, 50))
+        full_metric.close()
     reg = None if args.no_registration else time_registration(pair, ctx, dev)
+    learned = None
+    if not args.no_learned and rank == 0 and os.path.exists(WEIGHTS):
+        learned = time_learned(args)
     batch = None if args.no_batch else time_batch(ctx, dev, SEED)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "fixed": [N, N, N], "moving": [N, N, N], "bins": BINS,
-                   "sampling": "random 10%", "samples": S, "transform": "VersorRigid3D",
-                   "l2": "flushed before every evaluation (256 MiB write, then a 256 MiB read of "
-                         "another buffer so the write-backs fall outside the timed region)",
-                   "form": "fused (one cooperative kernel)" if fused else "split (two kernels)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "vs_baseline": None, "dtype": DTYPE, "data": "synthetic",
+        "config": workload_config(S, world),
+        "form": "fused (one cooperative kernel)" if fused else "split (two kernels)",
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * (6 + 3),
                 "d2h_bytes_per_step": 8 * (2 + 6)},
         "gpu_launches": launches_per_eval * args.steps,  # in the timed loop of `value`
@@ -504,8 +603,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "result": {"value": last.value, "valid": last.valid_points},
+        "full_grid": full,
         "registration": reg,
         "batch": batch,
+        "learned": learned,
         "other_metrics": sib,
     }
     print(json.dumps(line), flush=True)
@@ -536,6 +637,12 @@ def run_initnet(args, rank: int, world: int, local_rank: int):
     net = I.InitNet(seed=SEED, max_batch=64)
     losses, train_s = I.train(net, data["x"], data["labels"], epochs=args.initnet_epochs)
     del data
+    if args.initnet_save:
+        os.makedirs(os.path.dirname(os.path.abspath(args.initnet_save)), exist_ok=True)
+        net.save(args.initnet_save, training_pairs=args.initnet_train, epochs=args.initnet_epochs, seed=SEED,
+                 first_seed=1, loss_first_epoch=losses[0], loss_last_epoch=losses[-1],
+                 command=f"python bench.py --initnet --initnet-train {args.initnet_train} "
+                         f"--initnet-epochs {args.initnet_epochs} --initnet-save <path>")
     ev = I.evaluate(net, range(10_000_001, 10_000_001 + args.initnet_test), spec, run,
                     single_pairs=args.initnet_single)
     net.close()
@@ -670,7 +777,6 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-registration", action="store_true",
                     help="skip the full three-level registration run reported beside the metric")
@@ -688,6 +794,14 @@ def main():
     ap.add_argument("--initnet-test", type=int, default=512)
     ap.add_argument("--initnet-epochs", type=int, default=20)
     ap.add_argument("--initnet-single", type=int, default=32)
+    ap.add_argument("--initnet-save", default=None,
+                    help="write the trained network's weights to this .npz file")
+    ap.add_argument("--no-full-grid", action="store_true",
+                    help="skip the full-grid (every voxel a sample) point reported beside the metric")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the batched + learned-initialiser comparison reported beside the metric")
+    ap.add_argument("--learned-pairs", type=int, default=128)
+    ap.add_argument("--learned-single", type=int, default=16)
     ap.add_argument("--storage-study", action="store_true",
                     help="run the f32/bf16 moving-storage study (512^3) instead of the metric benchmark")
     ap.add_argument("--storage-n", type=int, default=512)

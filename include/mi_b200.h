@@ -145,6 +145,20 @@ mi_status mi_image_read_meta(mi_context* ctx, const char* path, mi_image** out);
  * device. */
 mi_status mi_image_read_meta_host(const char* path, mi_geometry* geometry, float* dst, size_t n_elements);
 
+/* NIfTI-1 reader for 3-D scalar volumes (io/nifti.rs read): a single .nii, a .hdr +
+ * .img pair or an Analyze-7.5 pair, each optionally gzip-compressed (a name ending in
+ * .gz is read through zlib); the header in either byte order; the ten scalar
+ * datatypes; scl_slope / scl_inter applied (NIfTI only; integers cast to f32 first,
+ * the result f32); geometry as the reference's reader forms it (the sform or qform
+ * chosen as NiftiImageIO does, RAS+ turned into LPS, spacing in millimetres), and the
+ * voxels uploaded with mi_image_upload's f32 cast. Refused by name: dimensions other
+ * than 3 after trailing unit dimensions are dropped, vector and matrix intents,
+ * unknown datatypes, truncated voxel data (MI_ERR_INVALID_ARGUMENT); complex and RGB
+ * datatypes (MI_ERR_UNSUPPORTED_PIXEL_TYPE). */
+mi_status mi_image_read_nifti(mi_context* ctx, const char* path, mi_image** out);
+/* The same on the host only (geometry, and the f32 voxels when dst is not NULL). */
+mi_status mi_image_read_nifti_host(const char* path, mi_geometry* geometry, float* dst, size_t n_elements);
+
 /* ---- metric (registration/device.rs:632-800 DeviceMattesMetric) ----------- */
 
 /* from_device / from_device_sampled (device.rs:644-696). The metric copies both
@@ -412,6 +426,11 @@ mi_status mi_batch_create(mi_context* ctx, int npairs, const mi_image* const* fi
 mi_status mi_batch_register(mi_batch* b, const mi_rsgd_config* cfg, int autotune, double* params_inout,
                             mi_rsgd_result* results);
 mi_status mi_batch_shape(const mi_batch* b, int* chunk, int* copies, int* nchunks);
+/* Per-pair completion times of the last mi_batch_register (no reference counterpart):
+ * seconds[p] is the device global timer's interval from the start of that run's first
+ * pass to the optimizer step at which pair p stopped (to the end of the run for a pair
+ * that ran out of iterations). n ≥ npairs; MI_ERR_INVALID_ARGUMENT before any run. */
+mi_status mi_batch_pair_seconds(const mi_batch* b, double* seconds, int n);
 mi_status mi_batch_destroy(mi_batch* b);
 
 /* ---- synthetic pairs (no reference counterpart) ------------------------------ */

@@ -20,7 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmi_b200.so")
 
 CU_SOURCES = ["context.cu", "mattes.cu", "noalloc.cu", "pyramid.cu", "batch.cu", "synth.cu", "initnet.cu", "moments.cu", "bspline.cu"]
-CPP_SOURCES = ["transforms.cpp", "geometry.cpp", "register.cpp", "io.cpp"]
+CPP_SOURCES = ["transforms.cpp", "geometry.cpp", "register.cpp", "io.cpp", "nifti.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

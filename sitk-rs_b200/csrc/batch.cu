@@ -61,7 +61,17 @@ struct PairDev {
     int active;
     int evaluations;
     unsigned int done;  // derivative chunks of this pair finished in the current pass
+    unsigned long long stop_ns;  // device global timer when the pair stopped (0: running)
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// The device global timer into *t (one thread): the start and end marks of a run.
+__global__ void k_stamp(unsigned long long* t) { *t = global_ns(); }
 
 // The next point map of an affine or translation family (transforms.cpp: the
 // AffineTransform offset center + t − A·center, mat_vec from 0.0; a translation is
@@ -92,15 +102,18 @@ __device__ __forceinline__ void load_params(const SamplerParams& src, SamplerPar
 }
 
 __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
-k_batch_hist(PairDev* __restrict__ pairs, const Chunk* __restrict__ chunks, int nchunks) {
+k_batch_hist(PairDev* __restrict__ pairs, const Chunk* __restrict__ chunks, int nchunks, uint32_t* __restrict__ exq,
+             uint32_t exq_cap) {
     extern __shared__ unsigned int sh[];
     __shared__ SamplerParams sP;
+    // this CTA's queue for the exact chain: a chunk at a time, so at most a chunk's samples
+    const ExactQueue q{MI_EXACT_DEFERRED ? exq + (size_t)blockIdx.x * exq_cap : nullptr, exq_cap};
     for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
         const Chunk ch = chunks[c];
         PairDev& pd = pairs[ch.pair];
         if (!pd.active) continue;
         load_params(pd.P, sP);
-        hist_phase<true>(sP, pd.a, sh, SampleRange{ch.begin, ch.end, threadIdx.x & ~31u, blockDim.x});
+        hist_phase<true>(sP, pd.a, sh, SampleRange{ch.begin, ch.end, threadIdx.x & ~31u, blockDim.x}, q);
         __syncthreads();
     }
 }
@@ -151,6 +164,7 @@ __global__ void k_batch_update(PairDev* __restrict__ pairs, int npairs, mi_rsgd_
     for (int k = 0; k < pd.nparams; ++k) grad[k] = pd.a.result[2 + k];
     if (rsgd::after_evaluation(pd.state, cfg, pd.corners, pd.scales, grad, pd.params)) {
         pd.active = 0;
+        pd.stop_ns = global_ns();
         atomicSub(active_count, 1u);
         return;
     }
@@ -179,6 +193,10 @@ struct mi_batch {
     size_t partials_cap = 0;      // doubles
     unsigned int* d_active = nullptr;
     unsigned int* h_active = nullptr;  // pinned
+    unsigned long long* d_marks = nullptr;  // device global timer at the start and end of the last run
+    uint32_t* d_exq = nullptr;              // per-CTA queues of samples for the exact chain
+    size_t exq_len = 0;
+    std::vector<double> pair_seconds;       // per pair: start of the last run to its stop
     int grid_hist = 0, grid_deriv = 0;
     int chunk = 0, copies = 0, fine_copies = 0;
     cudaGraph_t graph = nullptr;
@@ -259,6 +277,13 @@ mi_status shape_batch(mi_batch* b, int chunk, int copies) {
     MI_CHECK_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_batch_deriv, DERIV_BLOCK, ds));
     b->grid_hist = std::max(1, std::min(b->nchunks, ctx->num_sms * std::max(occ_h, 1)));
     b->grid_deriv = std::max(1, std::min(b->nchunks, ctx->num_sms * std::max(occ_d, 1)));
+    if ((size_t)b->grid_hist * chunk > b->exq_len) {
+        cudaFree(b->d_exq);
+        b->d_exq = nullptr;
+        b->exq_len = 0;
+        MI_CHECK_CUDA(ctx, cudaMalloc(&b->d_exq, (size_t)b->grid_hist * chunk * sizeof(uint32_t)));
+        b->exq_len = (size_t)b->grid_hist * chunk;
+    }
     release_graph(b);
     return MI_OK;
 }
@@ -273,7 +298,7 @@ mi_status launch_pass(mi_batch* b, const mi_rsgd_config& cfg, bool update) {
     cudaStream_t st = b->ctx->stream;
     const int B = b->bins;
     k_batch_hist<<<b->grid_hist, HIST_BLOCK, batch_hist_smem(B, b->copies, b->fine_copies), st>>>(
-        b->d_pairs, b->d_chunks, b->nchunks);
+        b->d_pairs, b->d_chunks, b->nchunks, b->d_exq, (uint32_t)b->chunk);
     k_batch_deriv<<<b->grid_deriv, DERIV_BLOCK, deriv_smem(B), st>>>(b->d_pairs, b->d_chunks, b->nchunks);
     if (update) k_batch_update<<<(b->npairs + 63) / 64, 64, 0, st>>>(b->d_pairs, b->npairs, cfg, b->d_active);
     MI_CHECK_CUDA(b->ctx, cudaGetLastError());
@@ -301,6 +326,7 @@ mi_status seed_pairs(mi_batch* b, const mi_rsgd_config& cfg, const double* param
         if (!point_map_fill(pd.P, f.stage, 1)) return set_error(b->ctx, MI_ERR_INVALID_ARGUMENT, "non-finite point map");
         pd.active = 1;
         pd.evaluations = 0;
+        pd.stop_ns = 0ull;
         pd.done = 0u;
         pd.value = 0.0;
         pd.valid = 0.0;
@@ -407,6 +433,8 @@ void free_batch(mi_batch* b) {
     cudaFree(b->d_chunks);
     cudaFree(b->d_partials);
     cudaFree(b->d_active);
+    cudaFree(b->d_marks);
+    cudaFree(b->d_exq);
     if (b->h_active) cudaFreeHost(b->h_active);
     for (mi_metric* m : b->metrics)
         if (m) mi_metric_destroy(m);
@@ -490,6 +518,7 @@ mi_status mi_batch_create(mi_context* ctx, int npairs, const mi_image* const* fi
         if (e == cudaSuccess) e = cudaMalloc(&b->d_partials, max_chunks * NMOM * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&b->d_active, sizeof(unsigned int));
         if (e == cudaSuccess) e = cudaMallocHost(&b->h_active, sizeof(unsigned int));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_marks, 2 * sizeof(unsigned long long));
         if (e != cudaSuccess) s = cuda_status(ctx, e, "mi_batch_create");
         b->partials_cap = max_chunks * NMOM;
     }
@@ -523,12 +552,22 @@ mi_status mi_batch_register(mi_batch* b, const mi_rsgd_config* cfg, int autotune
         if ((s = build_graph(b, *cfg)) != MI_OK) return s;
     // every pair makes at most iterations + 1 evaluations
     const int max_replays = (cfg->iterations + 1 + b->graph_passes - 1) / b->graph_passes + 1;
+    k_stamp<<<1, 1, 0, ctx->stream>>>(b->d_marks);
     for (int r = 0; r < max_replays; ++r) {
         MI_CHECK_CUDA(ctx, cudaGraphLaunch(b->exec, ctx->stream));
         MI_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         if (*b->h_active == 0u) break;
     }
+    k_stamp<<<1, 1, 0, ctx->stream>>>(b->d_marks + 1);
+    MI_CHECK_CUDA(ctx, cudaGetLastError());
+    unsigned long long marks[2] = {0ull, 0ull};
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(marks, b->d_marks, sizeof(marks), cudaMemcpyDeviceToHost, ctx->stream));
     MI_CHECK_CUDA(ctx, cudaMemcpy(b->host.data(), b->d_pairs, b->host.size() * sizeof(PairDev), cudaMemcpyDeviceToHost));
+    b->pair_seconds.assign(b->npairs, 0.0);
+    for (int p = 0; p < b->npairs; ++p) {
+        const unsigned long long stop = b->host[p].stop_ns ? b->host[p].stop_ns : marks[1];
+        b->pair_seconds[p] = stop > marks[0] ? (double)(stop - marks[0]) * 1e-9 : 0.0;
+    }
     for (int p = 0; p < b->npairs; ++p) {
         const PairDev& pd = b->host[p];
         for (int k = 0; k < b->nparams; ++k) params_inout[(size_t)p * b->nparams + k] = pd.params[k];
@@ -538,6 +577,13 @@ mi_status mi_batch_register(mi_batch* b, const mi_rsgd_config* cfg, int autotune
         results[p].stop_reason = pd.active ? MI_STOP_MAX_ITERATIONS : pd.state.stop;
         results[p].evaluations = pd.evaluations;
     }
+    return MI_OK;
+}
+
+mi_status mi_batch_pair_seconds(const mi_batch* b, double* seconds, int n) {
+    if (!b || !seconds || n < b->npairs) return MI_ERR_INVALID_ARGUMENT;
+    if ((int)b->pair_seconds.size() != b->npairs) return MI_ERR_INVALID_ARGUMENT;
+    for (int p = 0; p < b->npairs; ++p) seconds[p] = b->pair_seconds[p];
     return MI_OK;
 }
 

@@ -19,21 +19,19 @@
 namespace mi {
 namespace {
 
-// Launch shape of the histogram pass: HIST_ILP samples per thread in flight (their
-// corner gathers issued together), and a register cap that keeps HIST_MIN_BLOCKS
-// CTAs of HIST_BLOCK threads resident per SM.
-#ifndef MI_HIST_ILP
-#define MI_HIST_ILP 1
-#endif
-// Resident CTAs per SM the derivative kernel's register budget is sized for. Every
-// CTA of k_deriv forms the tail itself, so fewer, larger CTAs repeat it less: two per
-// SM measured fastest on the 256³ workload (22.6 µs against 23.5 with three and 26.9
-// with four).
+// Launch shapes: resident CTAs per SM the histogram and derivative kernels' register
+// budgets are sized for.
 #ifndef MI_DERIV_MIN_BLOCKS
 #define MI_DERIV_MIN_BLOCKS 2
 #endif
 #ifndef MI_HIST_MIN_BLOCKS
 #define MI_HIST_MIN_BLOCKS 2
+#endif
+// Samples the fast path cannot decide: 1 queues them and runs the exact chain after the
+// histogram phase's main loop (the loop then carries none of the exact chain's state),
+// 0 runs it inside the loop.
+#ifndef MI_EXACT_DEFERRED
+#define MI_EXACT_DEFERRED 1
 #endif
 // Histogram copies per CTA (coarse and fine parts) and the fine part's threshold
 // 2^-MI_HIST_FINE_T (see k_hist).
@@ -69,12 +67,6 @@ constexpr bool MOVING_LAYERED = MI_MOVING_LAYERED != 0;
 #endif
 constexpr int HIST_BLOCK = MI_HIST_BLOCK;
 constexpr int HIST_MIN_BLOCKS = MI_HIST_MIN_BLOCKS;
-constexpr int HIST_ILP = MI_HIST_ILP;
-// With one sample per thread, prefetch the next sample's index (see hist_phase).
-#ifndef MI_HIST_PREFETCH
-#define MI_HIST_PREFETCH 1
-#endif
-constexpr bool HIST_PREFETCH = MI_HIST_PREFETCH != 0;
 // Threads per derivative CTA (at least TAIL_BLOCK: the tail's column sums use
 // TAIL_BLOCK threads).
 #ifndef MI_DERIV_BLOCK
@@ -120,7 +112,8 @@ size_t hist_smem(int B) {
 constexpr int TAIL_BLOCK = 256;
 __host__ __device__ inline int tail_groups(int B) { return TAIL_BLOCK / B; }
 __host__ __device__ inline size_t tail_smem(int B) {
-    return ((size_t)B * B + B + (size_t)tail_groups(B) * B + B) * 8 + ((2 * (size_t)B + 7) & ~(size_t)7) + 8;
+    return ((size_t)B * B + B + (size_t)tail_groups(B) * B + B) * 8 + ((2 * (size_t)B + 7) & ~(size_t)7) + 8 +
+           (size_t)2 * B * 8;
 }
 size_t deriv_smem(int B) { return 32 * (size_t)NMOM * sizeof(double) + tail_smem(B) + (size_t)B * B * sizeof(float); }
 // The fused kernel reuses one dynamic allocation for its phases. The derivative
@@ -157,8 +150,8 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 }
 
 // Device buffers and per-launch constants shared by the evaluation kernels.
-//   sync[0] done counter of the final phase, sync[2] grid-barrier counter of the
-//   fused kernel.
+//   sync[0] done counter of the final phase, sync[1] arrival counter of the split
+//   form's histogram pass, sync[2] grid-barrier counter of the fused kernel.
 //   result: value, valid, derivative[MI_MAX_PARAMS], then the error word.
 struct EvalArgs {
     const float* moving;
@@ -176,6 +169,9 @@ struct EvalArgs {
     float* rec_g;
     double* partials;
     double* vsum;  // value slice sums (value_slices(B))
+    float* gpr = nullptr;  // the pRatio·nFactor table (B² floats) the split form's tail leaves for k_deriv
+    uint32_t* exq = nullptr;  // per-CTA queues of samples handed to the exact chain (exq_cap each)
+    uint32_t exq_cap = 0;
     unsigned int* sync;
     double* result;
     // mapped pinned mirror of result (or null): the split form's last kernel writes value,
@@ -239,9 +235,18 @@ __device__ __forceinline__ SampleRange grid_samples(uint32_t n) {
     return SampleRange{0u, n, blockIdx.x * blockDim.x + (threadIdx.x & ~31u), gridDim.x * blockDim.x};
 }
 
+// The samples a histogram phase hands to the exact chain: this CTA's queue in global
+// memory (sample indices, room for every sample the phase can see), drained after the
+// phase's main loop. Null: the exact chain runs in the loop.
+struct ExactQueue {
+    uint32_t* base;
+    uint32_t cap;
+};
+
 template <bool RECORD>
 __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArgs& a, unsigned int* sh,
-                                           const SampleRange r) {
+                                           const SampleRange r, const ExactQueue exq = ExactQueue{nullptr, 0u}) {
+    __shared__ unsigned int exq_count;
     const int B = P.bins;
     const int nb = B * B + B;
     const int copies = a.copies, fine_copies = a.fine_copies;
@@ -254,6 +259,7 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
     unsigned long long* colacc = reinterpret_cast<unsigned long long*>(sh + copies * cstride + fine_copies * fstride);
     if (a.gcols)
         for (int i = threadIdx.x; i < B; i += blockDim.x) colacc[i] = 0ull;
+    if (threadIdx.x == 0) exq_count = 0u;
     __syncthreads();
     unsigned int* sh_joint = sh;
     unsigned int* sh_fixed = sh + B * B;
@@ -264,11 +270,6 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
     const uint32_t* __restrict__ samples = a.samples;
     const uint8_t* __restrict__ fbin = a.fbin;
     const float hist_scale = a.hist_scale, fine_scale = a.fine_scale;
-    // With MI_HIST_ILP 2, two samples per iteration: both samples' corner gathers are
-    // issued (prep) before either is finished, so each thread keeps two gathers in
-    // flight. One sample per iteration (the default) measured 5 % faster on the 256³
-    // workload: the two-sample form needs more than the 64 registers that four
-    // resident CTAs allow and spills.
     // The CTA keeps `copies` interleaved copies of the histogram and lane l adds into
     // copy l mod copies: neighbouring lanes, whose sorted samples usually share a bin
     // pair, then add to different addresses instead of replaying on one. The copies
@@ -277,11 +278,7 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
     unsigned int* my_joint = sh_joint + (lane & (copies - 1)) * cstride;
     unsigned int* my_fixed = sh_fixed + (lane & (copies - 1)) * cstride;
     unsigned int* my_fine = sh_fine + (lane & (fine_copies - 1)) * fstride;
-    auto account = [&](const Prep& p, uint32_t s, bool real, int fi) {
-        if (!real) return;
-        Sample o;
-        o.exact = false;
-        const int st = finish<RECORD>(P, p, moving, o);
+    auto account = [&](int st, const Sample& o, uint32_t s, int fi) {
         if (st != SAMPLE_VALID) {
             if (RECORD) a.rec_bins[s] = 0;
             return;
@@ -310,54 +307,48 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
             a.rec_g[2 * (size_t)npad + s] = o.g[2];
         }
     };
-    // whole warps iterate together: the loop bound is the warp's first sample
+    // Whole warps iterate together (the loop bound is the warp's first sample). The
+    // next sample's index and this sample's fixed bin are requested at the top of the
+    // iteration, so their loads overlap this sample's corner gathers instead of adding
+    // two memory round trips per sample. A sample the fast path cannot decide goes to
+    // the exact chain, out of line.
     const uint32_t wbase = r.begin + r.warp_first;
-    if (HIST_ILP == 2) {
-        // two samples per iteration, the next pair's indices requested a pair ahead
-        uint32_t s = wbase + lane;
-        uint32_t fa = s < n ? (samples ? __ldg(samples + s) : s) : 0u;
-        uint32_t fb = s + stride < n ? (samples ? __ldg(samples + s + stride) : s + stride) : fa;
-        for (uint32_t b = wbase; b < n; b += 2 * stride) {
-            const uint32_t s2 = s + stride;
-            const bool one = s < n, two = s2 < n;
-            const int fia = one ? (int)__ldg(fbin + s) : 0, fib = two ? (int)__ldg(fbin + s2) : 0;
-            const uint32_t sn = s + 2 * stride, sn2 = sn + stride;
-            const uint32_t fna = sn < n ? (samples ? __ldg(samples + sn) : sn) : 0u;
-            const uint32_t fnb = sn2 < n ? (samples ? __ldg(samples + sn2) : sn2) : fna;
-            Prep pa, pb;
-            prep<RECORD>(P, fa, moving, mmask, pa);
-            prep<RECORD>(P, fb, moving, mmask, pb);
-            account(pa, s, one, fia);
-            account(pb, s2, two, fib);
-            s = sn;
-            fa = fna;
-            fb = fnb;
+    uint32_t s = wbase + lane;
+    uint32_t flat = s < n ? (samples ? __ldg(samples + s) : s) : 0u;
+    for (uint32_t b = wbase; b < n; b += stride) {
+        const bool one = s < n;
+        const int fi = one ? (int)__ldg(fbin + s) : 0;
+        const uint32_t sn = s + stride;
+        const uint32_t flat_next = sn < n ? (samples ? __ldg(samples + sn) : sn) : 0u;
+        if (one) {
+            Prep p;
+            Sample o;
+            int st = prep_fast<RECORD>(P, flat, mmask, p);
+            if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
+            if (st == SAMPLE_EXACT) {
+                if (exq.base) {
+                    exq.base[atomicAdd(&exq_count, 1u)] = s;
+                } else {
+                    Sample e;
+                    st = sample_exact<RECORD>(P, flat, moving, mmask, e);
+                    account(st, e, s, fi);
+                }
+            } else {
+                account(st, o, s, fi);
+            }
         }
-    } else if (HIST_PREFETCH) {
-        // the next sample's index and this sample's fixed bin are requested at the top
-        // of the iteration, so their loads overlap this sample's corner gathers instead
-        // of adding two memory round trips per sample
-        uint32_t s = wbase + lane;
-        uint32_t flat = s < n ? (samples ? __ldg(samples + s) : s) : 0u;
-        for (uint32_t b = wbase; b < n; b += stride) {
-            const bool one = s < n;
-            const int fi = one ? (int)__ldg(fbin + s) : 0;
-            const uint32_t sn = s + stride;
-            const uint32_t flat_next = sn < n ? (samples ? __ldg(samples + sn) : sn) : 0u;
-            Prep pa;
-            prep<RECORD>(P, flat, moving, mmask, pa);
-            account(pa, s, one, fi);
-            s = sn;
-            flat = flat_next;
-        }
-    } else {
-        for (uint32_t b = wbase; b < n; b += stride) {
-            const uint32_t s = b + lane;
-            const bool one = s < n;
-            const int fi = one ? (int)__ldg(fbin + s) : 0;
-            Prep pa;
-            prep<RECORD>(P, one ? (samples ? __ldg(samples + s) : s) : 0u, moving, mmask, pa);
-            account(pa, s, one, fi);
+        s = sn;
+        flat = flat_next;
+    }
+    if (exq.base) {
+        // the queued samples through the exact chain, spread over the CTA
+        __syncthreads();
+        const unsigned int nq = exq_count;
+        for (unsigned int q = threadIdx.x; q < nq; q += blockDim.x) {
+            const uint32_t sq = __ldcg(exq.base + q);
+            Sample e;
+            const int st = sample_exact<RECORD>(P, samples ? __ldg(samples + sq) : sq, moving, mmask, e);
+            account(st, e, sq, (int)__ldg(fbin + sq));
         }
     }
     __syncthreads();
@@ -402,6 +393,8 @@ struct TailSmem {
     uint8_t* okm;              // B
     uint8_t* okf;              // B
     unsigned long long* jmin;  // 1: the least joint count whose joint probability exceeds ε
+    double* lcol;              // B: ln(column sum)
+    double* lfm;               // B: ln(fixed marginal)
 };
 __device__ __forceinline__ TailSmem tail_layout(int B, unsigned char* base) {
     TailSmem t;
@@ -411,6 +404,8 @@ __device__ __forceinline__ TailSmem tail_layout(int B, unsigned char* base) {
     t.okm = reinterpret_cast<uint8_t*>(t.col + B);
     t.okf = t.okm + B;
     t.jmin = reinterpret_cast<unsigned long long*>(t.okm + ((2 * B + 7) & ~7));
+    t.lcol = reinterpret_cast<double*>(t.jmin + 1);
+    t.lfm = t.lcol + B;
     return t;
 }
 
@@ -453,6 +448,49 @@ __device__ void tail_fetch(int B, const EvalArgs& a, const TailSmem& ts) {
     __syncthreads();
 }
 
+// The integer marginals' totals and the normalisers, computed by every warp from the
+// column sums and fixed counts (integer sums: any order, same bits).
+__device__ __forceinline__ TailCtx tail_scalars(int B, const unsigned long long* col, const unsigned long long* cnt,
+                                                double hist_inv, double moving_bin_size) {
+    const int lane = threadIdx.x & 31;
+    TailCtx t;
+    t.total = 0ull;
+    t.valid = 0ull;
+    for (int m = lane; m < B; m += 32) {
+        t.total += col[m];
+        t.valid += cnt[m];
+    }
+    t.total = warp_sum_u64(t.total);
+    t.valid = warp_sum_u64(t.valid);
+    t.dt = (double)t.total;
+    t.joint_sum = t.dt * hist_inv;
+    t.degenerate = t.valid == 0ull || t.joint_sum < DBL_EPSILON;
+    t.n_factor = t.degenerate ? 0.0 : 1.0 / (moving_bin_size * (double)t.valid);
+    return t;
+}
+
+// Column m and row m's per-margin quantities: the ε flags of the moving and fixed
+// marginals (mm = col/total, fm = count/joint_sum; mattes.rs:305-320) and their
+// logarithms ln(col) and ln(fm) in FP64, so that a bin's term needs one logarithm.
+__device__ __forceinline__ void margin_terms(int m, const unsigned long long* col, const unsigned long long* cnt,
+                                             const TailCtx& t, uint8_t* okm, uint8_t* okf, double* lcol,
+                                             double* lfm) {
+    const double fm = (double)cnt[m] / t.joint_sum;
+    okm[m] = (double)col[m] / t.dt > DBL_EPSILON;
+    okf[m] = fm > DBL_EPSILON;
+    lcol[m] = log((double)col[m]);
+    lfm[m] = log(fm);
+}
+
+// jp = jv/total > ε is monotone in the integer jv: its least jv, found once starting
+// next to ε·total, so the table tests an integer instead of dividing.
+__device__ __forceinline__ unsigned long long least_joint(double dt) {
+    unsigned long long c = (unsigned long long)(DBL_EPSILON * dt);
+    for (int it = 0; it < 64 && c > 0ull && (double)(c - 1ull) / dt > DBL_EPSILON; ++it) --c;
+    for (int it = 0; it < 64 && !((double)c / dt > DBL_EPSILON); ++it) ++c;
+    return c > 0ull ? c : 1ull;
+}
+
 // The rest of the tail on the fetched histogram.
 __device__ TailCtx tail_finish(int B, double moving_bin_size, const EvalArgs& a, const TailSmem& ts) {
     const int B2 = B * B;
@@ -473,32 +511,9 @@ __device__ TailCtx tail_finish(int B, double moving_bin_size, const EvalArgs& a,
         __syncthreads();
     }
     const unsigned long long* cnt = ts.hist + B2;
-    const int lane = threadIdx.x & 31;
-    TailCtx t;
-    t.total = 0ull;
-    t.valid = 0ull;
-    for (int m = lane; m < B; m += 32) {
-        t.total += ts.col[m];
-        t.valid += cnt[m];
-    }
-    t.total = warp_sum_u64(t.total);
-    t.valid = warp_sum_u64(t.valid);
-    t.dt = (double)t.total;
-    t.joint_sum = t.dt * a.hist_inv;
-    t.degenerate = t.valid == 0ull || t.joint_sum < DBL_EPSILON;
-    t.n_factor = t.degenerate ? 0.0 : 1.0 / (moving_bin_size * (double)t.valid);
-    if ((int)threadIdx.x < B) {
-        ts.okm[threadIdx.x] = (double)ts.col[threadIdx.x] / t.dt > DBL_EPSILON;
-        ts.okf[threadIdx.x] = (double)cnt[threadIdx.x] / t.joint_sum > DBL_EPSILON;
-    }
-    if (threadIdx.x == blockDim.x - 1) {
-        // jp = jv/total > ε is monotone in the integer jv: find its least jv once,
-        // starting next to ε·total, so the table tests an integer instead of dividing
-        unsigned long long c = (unsigned long long)(DBL_EPSILON * t.dt);
-        for (int it = 0; it < 64 && c > 0ull && (double)(c - 1ull) / t.dt > DBL_EPSILON; ++it) --c;
-        for (int it = 0; it < 64 && !((double)c / t.dt > DBL_EPSILON); ++it) ++c;
-        *ts.jmin = c > 0ull ? c : 1ull;
-    }
+    const TailCtx t = tail_scalars(B, ts.col, cnt, a.hist_inv, moving_bin_size);
+    if ((int)threadIdx.x < B) margin_terms(threadIdx.x, ts.col, cnt, t, ts.okm, ts.okf, ts.lcol, ts.lfm);
+    if (threadIdx.x == blockDim.x - 1) *ts.jmin = least_joint(t.dt);
     __syncthreads();
     return t;
 }
@@ -517,6 +532,11 @@ __device__ __forceinline__ float log_ratio(float a, float b) { return logf(__fdi
 // table is FP32; the ratio of the two exact integers carries a few units of 2^-24,
 // far below what the derivative's tolerance sees). The entry's (row, column) advance
 // with the thread's stride, so no per-entry division.
+__device__ __forceinline__ float pr_entry(unsigned long long jv, unsigned long long col, bool ok, unsigned long long jmin,
+                                         float nf) {
+    return ok && jv >= jmin ? log_ratio((float)jv, (float)col) * nf : 0.0f;
+}
+
 __device__ void pr_table(int B, const TailCtx& t, const TailSmem& ts, float* pr) {
     const int B2 = B * B;
     const float nf = (float)t.n_factor;
@@ -524,10 +544,7 @@ __device__ void pr_table(int B, const TailCtx& t, const TailSmem& ts, float* pr)
     int f = (int)threadIdx.x / B, m = (int)threadIdx.x - f * B;
     const int df = (int)blockDim.x / B, dm = (int)blockDim.x - df * B;
     for (int i = threadIdx.x; i < B2; i += blockDim.x) {
-        const unsigned long long jv = ts.hist[i];
-        float r = 0.0f;
-        if (ts.okf[f] && ts.okm[m] && jv >= jmin) r = log_ratio((float)jv, (float)ts.col[m]) * nf;
-        pr[i] = r;
+        pr[i] = pr_entry(ts.hist[i], ts.col[m], ts.okf[f] && ts.okm[m], jmin, nf);
         f += df;
         m += dm;
         if (m >= B) {
@@ -543,22 +560,31 @@ __device__ void pr_table(int B, const TailCtx& t, const TailSmem& ts, float* pr)
 // same bits, so every launch form reports the same value.
 __host__ __device__ inline int value_slices(int B) { return (B * B + 31) / 32; }
 
+// One bin's term of −MI's sum, jp·(ln(jp/mm) − ln fm) with jp/mm = jv/col, formed in
+// FP64 as (jv/total)·(ln jv − ln col − ln fm) from the margins' logarithms; 0 where the
+// reference skips the bin (jp, mm or fm not above ε: `ok` holds the two marginal
+// flags, jv ≥ jmin is jp > ε).
+__device__ __forceinline__ double value_term(unsigned long long jv, bool ok, unsigned long long jmin, double lcol,
+                                             double lfm, const TailCtx& t) {
+    if (!ok || jv < jmin) return 0.0;
+    return ((double)jv / t.dt) * ((log((double)jv) - lcol) - lfm);
+}
+
+__device__ __forceinline__ double slice_sum(double term) {
+#pragma unroll
+    for (int off = 16; off; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);
+    return term;
+}
+
 __device__ double value_slice(int B, const TailCtx& t, const TailSmem& ts, int slice) {
     const int lane = threadIdx.x & 31;
     const int i = slice * 32 + lane;
     double term = 0.0;
     if (i < B * B) {
-        const unsigned long long jv = ts.hist[i];
         const int f = i / B, m = i - f * B;
-        const double jp = (double)jv / t.dt;
-        const double mm = (double)ts.col[m] / t.dt;
-        const double fm = (double)ts.hist[B * B + f] / t.joint_sum;
-        if (fm > DBL_EPSILON && mm > DBL_EPSILON && jp > DBL_EPSILON)
-            term = jp * (log((double)jv / (double)ts.col[m]) - log(fm));
+        term = value_term(ts.hist[i], ts.okf[f] && ts.okm[m], *ts.jmin, ts.lcol[m], ts.lfm[f], t);
     }
-#pragma unroll
-    for (int off = 16; off; off >>= 1) term += __shfl_xor_sync(0xffffffffu, term, off);
-    return term;
+    return slice_sum(term);
 }
 
 // This CTA's share of the value slices: with the CTAs numbered 0..units−1 (this one
@@ -576,14 +602,21 @@ __device__ void value_slices_share(int B, const EvalArgs& a, const TailCtx& t, c
     }
 }
 
+// One warp: −MI from the slice sums in slice order (lane-strided, then a fixed xor
+// tree).
+__device__ __forceinline__ double fold_slices(const double* vs, int ns, bool global) {
+    const int lane = threadIdx.x & 31;
+    double v = 0.0;
+    for (int s = lane; s < ns; s += 32) v += global ? __ldcg(vs + s) : vs[s];
+#pragma unroll
+    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
 // One warp: value and valid into result (lane 0), from the slice sums.
 __device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
     const int lane = threadIdx.x & 31;
-    const int ns = value_slices(B);
-    double v = 0.0;
-    for (int s = lane; s < ns; s += 32) v += __ldcg(a.vsum + s);
-#pragma unroll
-    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    const double v = fold_slices(a.vsum, value_slices(B), true);
     if (lane == 0) {
         const double r0 = t.degenerate ? DBL_MAX : -v, r1 = (double)t.valid;
         a.result[0] = r0;
@@ -594,6 +627,102 @@ __device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
             a.result_host[RESULT_ERR] = 0.0;  // the split form has no barrier to time out
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// The split form's tail, once per evaluation: run by the whole CTA of the histogram
+// pass that flushes last (no other CTA waits for it). It reads the finished global
+// histogram from L2 once, leaves the pRatio·nFactor table in global memory (a.gpr)
+// for the derivative pass, writes value and valid into a.result (and, for the
+// value-only evaluation, into the mapped mirror with the sequence number), and clears
+// the global histogram, its column sums and the arrival counter for the next
+// evaluation. Every quantity is formed by the same functions as the per-CTA tail
+// (tail_scalars, least_joint, pr_entry, value_term, slice_sum, fold_slices), so the
+// table and the value have the same bits in every launch form.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline size_t tail_once_smem(int B) {
+    return (size_t)4 * B * 8 + (size_t)value_slices(B) * 8 + (((size_t)2 * B + 7) & ~(size_t)7) + 8;
+}
+
+__device__ __forceinline__ void tail_once(int B, double moving_bin_size, const EvalArgs& a, unsigned char* base, bool mirror) {
+    const int B2 = B * B;
+    const int ns = value_slices(B);
+    unsigned long long* col = reinterpret_cast<unsigned long long*>(base);
+    unsigned long long* cnt = col + B;
+    double* lcol = reinterpret_cast<double*>(cnt + B);
+    double* lfm = lcol + B;
+    double* vs = lfm + B;
+    uint8_t* okm = reinterpret_cast<uint8_t*>(vs + ns);
+    uint8_t* okf = okm + B;
+    unsigned long long* jmin_s = reinterpret_cast<unsigned long long*>(okm + ((2 * B + 7) & ~7));
+    const int lane = threadIdx.x & 31;
+    const int wfirst = (int)threadIdx.x - lane;
+    const int bd = (int)blockDim.x;
+    // The bins go in whole warps, eight per thread per round: bin i = i0 + u·bd + lane,
+    // so the warp's 32 lanes hold value slice (i0 + u·bd)/32. The first round's bins
+    // are requested together with the column sums and fixed counts.
+    constexpr int R = 2;
+    unsigned long long jv[R];
+    auto load_round = [&](int i0) {
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int i = i0 + u * bd + lane;
+            jv[u] = i < B2 ? __ldcg(a.ghist + i) : 0ull;
+        }
+    };
+    load_round(wfirst);
+    for (int i = threadIdx.x; i < B; i += bd) {
+        col[i] = __ldcg(a.gcols + i);
+        cnt[i] = __ldcg(a.ghist + B2 + i);
+    }
+    __syncthreads();
+    const TailCtx t = tail_scalars(B, col, cnt, a.hist_inv, moving_bin_size);
+    if ((int)threadIdx.x < B) margin_terms(threadIdx.x, col, cnt, t, okm, okf, lcol, lfm);
+    if (threadIdx.x == blockDim.x - 1) *jmin_s = least_joint(t.dt);
+    __syncthreads();
+    const unsigned long long jmin = *jmin_s;
+    const float nf = (float)t.n_factor;
+    for (int i0 = wfirst; i0 < ns * 32; i0 += R * bd) {
+        if (i0 != wfirst) load_round(i0);
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int iw = i0 + u * bd;  // warp-uniform: the slice's first bin
+            if (iw < ns * 32) {
+                const int i = iw + lane;
+                double term = 0.0;
+                if (i < B2) {
+                    float r = 0.0f;
+                    if (!t.degenerate) {
+                        const int f = i / B, m = i - f * B;
+                        const bool ok = okf[f] && okm[m];
+                        r = pr_entry(jv[u], col[m], ok, jmin, nf);
+                        term = value_term(jv[u], ok, jmin, lcol[m], lfm[f], t);
+                    }
+                    a.gpr[i] = r;
+                }
+                term = slice_sum(term);
+                if (lane == 0) vs[iw >> 5] = term;
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const double v = fold_slices(vs, ns, false);
+        if (lane == 0) {
+            const double r0 = t.degenerate ? DBL_MAX : -v, r1 = (double)t.valid;
+            a.result[0] = r0;
+            a.result[1] = r1;
+            if (mirror && a.result_host) {
+                a.result_host[0] = r0;
+                a.result_host[1] = r1;
+                a.result_host[RESULT_ERR] = 0.0;
+            }
+        }
+    }
+    for (int i = threadIdx.x; i < B2 + B; i += bd) a.ghist[i] = 0ull;
+    for (int i = threadIdx.x; i < B; i += bd) a.gcols[i] = 0ull;
+    if (threadIdx.x == 0) a.sync[1] = 0u;
+    if (mirror) publish_seq(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -669,6 +798,44 @@ __device__ __forceinline__ void store_moments(const float* acc, double* red, dou
     }
 }
 
+// The record stream of a derivative phase: this thread's four-sample groups, the
+// next group's loads issued before the current group is accumulated; `cur` holds the
+// first group, already requested by the caller.
+struct RecordGroup {
+    uint2 b;
+    float4 f, gx, gy, gz;
+    uint4 fl;
+};
+__device__ __forceinline__ void load_group(const EvalArgs& a, uint32_t q, RecordGroup& g) {
+    const uint32_t npad = a.npad;
+    g.b = __ldcg(reinterpret_cast<const uint2*>(a.rec_bins) + q);
+    g.f = __ldcg(reinterpret_cast<const float4*>(a.rec_f) + q);
+    g.gx = __ldcg(reinterpret_cast<const float4*>(a.rec_g) + q);
+    g.gy = __ldcg(reinterpret_cast<const float4*>(a.rec_g + npad) + q);
+    g.gz = __ldcg(reinterpret_cast<const float4*>(a.rec_g + 2 * (size_t)npad) + q);
+    g.fl = a.samples ? __ldg(reinterpret_cast<const uint4*>(a.samples) + q)
+                     : make_uint4(4 * q, 4 * q + 1, 4 * q + 2, 4 * q + 3);
+}
+
+__device__ __forceinline__ void stream_records(const SamplerParams& P, const EvalArgs& a, const float* pr, uint32_t q,
+                                               uint32_t ngroups, uint32_t stride, RecordGroup cur, float* acc) {
+    const int B = P.bins;
+    auto one = [&](uint32_t bins, float f, float gx, float gy, float gz, uint32_t flat) {
+        if (bins & 0xffu) accumulate_moments(P, pr, B, bins & 0xffu, bins >> 8, f, gx, gy, gz, flat, acc);
+    };
+    while (q < ngroups) {
+        const uint32_t qn = q + stride;
+        RecordGroup nxt;
+        if (qn < ngroups) load_group(a, qn, nxt);
+        one(cur.b.x & 0xffffu, cur.f.x, cur.gx.x, cur.gy.x, cur.gz.x, cur.fl.x);
+        one(cur.b.x >> 16, cur.f.y, cur.gx.y, cur.gy.y, cur.gz.y, cur.fl.y);
+        one(cur.b.y & 0xffffu, cur.f.z, cur.gx.z, cur.gy.z, cur.gz.z, cur.fl.z);
+        one(cur.b.y >> 16, cur.f.w, cur.gx.w, cur.gy.w, cur.gz.w, cur.fl.w);
+        cur = nxt;
+        q = qn;
+    }
+}
+
 __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double* dsh, const GroupWork w) {
     const int B = P.bins;
     double* red = dsh;  // 32 * NMOM
@@ -678,58 +845,42 @@ __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double
     float acc[NMOM];
 #pragma unroll
     for (int i = 0; i < NMOM; ++i) acc[i] = 0.0f;
-    const uint32_t stride = w.stride;
-    const uint32_t npad = a.npad;
-    const uint32_t ngroups = w.end;
-    const uint2* b4p = reinterpret_cast<const uint2*>(a.rec_bins);
-    const float4* f4p = reinterpret_cast<const float4*>(a.rec_f);
-    const float4* gx4p = reinterpret_cast<const float4*>(a.rec_g);
-    const float4* gy4p = reinterpret_cast<const float4*>(a.rec_g + npad);
-    const float4* gz4p = reinterpret_cast<const float4*>(a.rec_g + 2 * (size_t)npad);
-    const uint4* s4p = reinterpret_cast<const uint4*>(a.samples);
-    // the next group's records are loaded before the current group is accumulated
-    struct Group {
-        uint2 b;
-        float4 f, gx, gy, gz;
-        uint4 fl;
-    };
-    auto load = [&](uint32_t q, Group& g) {
-        g.b = __ldcg(b4p + q);
-        g.f = __ldcg(f4p + q);
-        g.gx = __ldcg(gx4p + q);
-        g.gy = __ldcg(gy4p + q);
-        g.gz = __ldcg(gz4p + q);
-        g.fl = a.samples ? __ldg(s4p + q) : make_uint4(4 * q, 4 * q + 1, 4 * q + 2, 4 * q + 3);
-    };
-    auto one = [&](uint32_t bins, float f, float gx, float gy, float gz, uint32_t flat) {
-        if (bins & 0xffu) accumulate_moments(P, pr, B, bins & 0xffu, bins >> 8, f, gx, gy, gz, flat, acc);
-    };
-    uint32_t q = w.begin + w.first;
-    Group cur;
+    const uint32_t q = w.begin + w.first;
+    RecordGroup cur;
     // the histogram's loads go out first (every CTA waits on them); the first record
     // group's loads then overlap the rest of the tail
     tail_fetch(B, a, ts);
-    if (q < ngroups) load(q, cur);
+    if (q < w.end) load_group(a, q, cur);
     const TailCtx t = tail_finish(B, P.moving_bin_size, a, ts);
     if (!t.degenerate) pr_table(B, t, ts, pr);
     __syncthreads();
     // a warp with a value slice sums it before its share of the records
     if (!t.degenerate) value_slices_share(B, a, t, ts, w.unit, w.units);
-    if (!t.degenerate) {
-        while (q < ngroups) {
-            const uint32_t qn = q + stride;
-            Group nxt;
-            if (qn < ngroups) load(qn, nxt);
-            one(cur.b.x & 0xffffu, cur.f.x, cur.gx.x, cur.gy.x, cur.gz.x, cur.fl.x);
-            one(cur.b.x >> 16, cur.f.y, cur.gx.y, cur.gy.y, cur.gz.y, cur.fl.y);
-            one(cur.b.y & 0xffffu, cur.f.z, cur.gx.z, cur.gy.z, cur.gz.z, cur.fl.z);
-            one(cur.b.y >> 16, cur.f.w, cur.gx.w, cur.gy.w, cur.gz.w, cur.fl.w);
-            cur = nxt;
-            q = qn;
-        }
-    }
+    if (!t.degenerate) stream_records(P, a, pr, q, w.end, w.stride, cur, acc);
     store_moments(acc, red, w.part, w.part_stride);
     return t;
+}
+
+// The split form's derivative pass: the table the histogram pass's tail left in
+// a.gpr is copied into shared memory (its loads issued together with the first record
+// group's), then this CTA's records are streamed into the moments. A degenerate
+// evaluation's table is all zeros, so its moments are zero.
+__host__ __device__ inline size_t stream_smem(int B) { return 32 * (size_t)NMOM * sizeof(double) + (size_t)B * B * sizeof(float); }
+
+__device__ void stream_phase(const SamplerParams& P, const EvalArgs& a, double* dsh, const GroupWork w) {
+    const int B2 = P.bins * P.bins;
+    double* red = dsh;
+    float* pr = reinterpret_cast<float*>(dsh + 32 * NMOM);
+    float acc[NMOM];
+#pragma unroll
+    for (int i = 0; i < NMOM; ++i) acc[i] = 0.0f;
+    const uint32_t q = w.begin + w.first;
+    RecordGroup cur;
+    if (q < w.end) load_group(a, q, cur);
+    for (int i = threadIdx.x; i < B2; i += blockDim.x) pr[i] = __ldcg(a.gpr + i);
+    __syncthreads();
+    stream_records(P, a, pr, q, w.end, w.stride, cur, acc);
+    store_moments(acc, red, w.part, w.part_stride);
 }
 
 // Run by the last CTA to finish the derivative phase: fold the `count` partials of
@@ -760,7 +911,21 @@ __device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const 
     if (threadIdx.x < NMOM) {
         double v = 0.0;
         for (int l = 0; l < FOLD; ++l) v += fold[threadIdx.x * FOLD + l];
-        mom[threadIdx.x] = v;
+        fold[threadIdx.x] = v;
+    }
+    __syncthreads();
+    // The records carry the interpolant's gradient in index space; the physical
+    // gradient is g_phys[d] = Σ_j g_idx[j]·M[j][d] (M the moving physical→index matrix,
+    // registration/metric.rs:848-861), a linear map applied here once to the sums:
+    // A_d = Σ_j M[j][d]·A_j, B[d][e] = Σ_j M[j][d]·B[j][e].
+    if (threadIdx.x < NMOM) {
+        const int t = threadIdx.x;
+        const int d = t < 3 ? t : (t - 3) / 3;
+        const int src = t < 3 ? 0 : 3 + (t - 3) % 3;
+        const int step = t < 3 ? 1 : 3;
+        double v = 0.0;
+        for (int j = 0; j < 3; ++j) v += P.mp2i[j * 3 + d] * fold[src + j * step];
+        mom[t] = v;
     }
     __syncthreads();
     const int np = J.nparams;

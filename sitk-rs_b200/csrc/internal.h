@@ -59,7 +59,6 @@ struct SamplerParams {
     double bin_hi;  // (double)(bins − 3), the top Parzen bin
     // fast path: fixed physical point relative to xref in FP32, x − xref ≈ xA·(i,j,k) + xb
     float xA[9], xb[3];
-    float mp2if[9];  // physical→index matrix in FP32 (gradient only)
     int msz[3];      // moving size, 32-bit (the volume is below 2^32 voxels)
     uint32_t ms1, ms2;  // moving strides, 32-bit
     cudaTextureObject_t mtex;  // the moving volume as a texture (point, clamp, unnormalised)
@@ -81,9 +80,16 @@ struct SamplerParams {
     double fixed_bin_size, moving_bin_size;
     double fixed_nmin, moving_nmin;
     double moving_min, moving_max;
-    // FP32 copies for the fast Parzen decision (the range ends are f32 voxel values,
-    // so exact); cerr_f ≥ cerr
-    float mmin_f, mmax_f, inv_bin_f, nmin_f, rmag_f, bin_hi_f, cerr_f;
+    // The fast path's range and Parzen decisions (sampler.cuh finish_fast): FP32 copies
+    // of the reciprocal bin size and normalised minimum, the top bin, and the metric's
+    // global bounds, formed per point map by point_map_fill from vmax (the largest
+    // |voxel| of the moving volume): the fast value is within dv = vmax·(8·cerr +
+    // 32·2^-24) of the reference's for every sample, the range thresholds are the
+    // range ends ∓ (dv plus rounding slack) rounded outward to f32, and dterm bounds
+    // the Parzen term's distance from the reference's.
+    double vmax;
+    float inv_bin_f, nmin_f, bin_hi_f;
+    float rlo_out, rlo_in, rhi_in, rhi_out, dterm;
     // derivative moments are taken about this point to limit cancellation
     double xref[3];
 };
@@ -93,6 +99,9 @@ struct Workspace {
     unsigned long long* hist = nullptr;  // [bins*bins] joint (2^-32 fixed point), [bins] fixed marginal, [1] valid
     double* partials = nullptr;          // [grid_deriv][12]
     double* vsum = nullptr;              // value slice sums
+    float* gpr = nullptr;                // pRatio·nFactor table the split form's tail leaves for k_deriv
+    uint32_t* exq = nullptr;             // per-CTA queues of samples for the exact chain
+    uint32_t exq_cap_hist = 0, exq_cap_eval = 0;  // queue length per CTA of k_hist / of the fused kernel
     double* result = nullptr;            // [2 + MI_MAX_PARAMS]: value, valid, derivative
     unsigned int* done_counter = nullptr;
     double* host_result = nullptr;       // pinned mirror of result (mapped)

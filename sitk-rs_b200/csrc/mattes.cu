@@ -8,18 +8,21 @@
 //            with the joint part's column sums into global u64 counters. Integer adds
 //            are exact, so the histogram does not depend on the order. Each sample also
 //            leaves an 18-byte record (both Parzen bins, Parzen fraction, moving
-//            gradient) for pass 2.
-//   k_deriv  launched as a programmatic dependent of k_hist. Every CTA forms the tail
-//            (registration/mattes.rs:273-328: normalisation, marginals, −MI slices and
-//            the pRatio·nFactor table) from the integer histogram, then streams the
-//            records → 12 moments A[d] = Σ w g_d, B[d][e] = Σ w g_d (x_e − x_ref,e),
-//            w = Σ_taps B₃′·pRatio (the form of the reference's mattes_deriv,
-//            cuda/ops/mattes.rs:319-381), FP32 per thread and FP64 from the warp
-//            reduction on, in a fixed shuffle/tree order into per-CTA partials. The last
-//            CTA folds the partials in a fixed order, contracts them with the
-//            transform's Jacobian form (registration/cuda.rs:505-524), writes value,
-//            valid and derivative into the host's mapped mirror with a sequence number,
-//            and re-zeroes the global histogram for the next evaluation.
+//            gradient) for pass 2. The CTA that flushes last forms the tail once
+//            (registration/mattes.rs:273-328: normalisation, marginals, −MI and the
+//            pRatio·nFactor table) from the integer histogram, leaves the table in
+//            global memory, writes value and valid, and clears the histogram for the
+//            next evaluation.
+//   k_deriv  launched as a programmatic dependent of k_hist. Every CTA copies the table
+//            into shared memory, then streams its records → 12 moments
+//            A[d] = Σ w g_d, B[d][e] = Σ w g_d (x_e − x_ref,e), w = Σ_taps B₃′·pRatio
+//            (the form of the reference's mattes_deriv, cuda/ops/mattes.rs:319-381),
+//            FP32 per thread and FP64 from the warp reduction on, in a fixed
+//            shuffle/tree order into per-CTA partials. The last CTA folds the partials
+//            in a fixed order, contracts them with the transform's Jacobian form
+//            (registration/cuda.rs:505-524) and writes value, valid and derivative into
+//            the host's mapped mirror with a sequence number.
+// A value-only evaluation is k_hist alone: its tail publishes the result.
 // Every reduction order is a function of the launch shape alone, so repeated
 // evaluations are bit-identical. No kernel waits on another CTA.
 
@@ -55,17 +58,27 @@ namespace {
 //   valid) and its share of the derivative moments → the last CTA to finish folds
 //   the moments, writes the derivative, re-zeroes the global histogram and resets
 //   the counters. The value-only form runs the tail in CTA 0 alone.
-// The split form (k_hist, then k_deriv or k_tail) does the same work with a kernel
-// boundary in place of the barrier.
+// The split form (k_hist, then k_deriv) does the same work with a kernel boundary in
+// place of the barrier, and forms the tail once, in k_hist's last CTA.
 // ---------------------------------------------------------------------------
+// This CTA's queue of samples for the exact chain (k_hist, k_eval: a grid-stride walk,
+// so at most exq_cap = ceil(n / (grid·block))·block samples per CTA).
+__device__ __forceinline__ ExactQueue exact_queue(const EvalArgs& a) {
+#if MI_EXACT_DEFERRED
+    return ExactQueue{a.exq + (size_t)blockIdx.x * a.exq_cap, a.exq_cap};
+#else
+    return ExactQueue{nullptr, 0u};
+#endif
+}
+
 template <bool DERIV>
 __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
-k_eval(SamplerParams P, JacobianForm J, EvalArgs a) {
+k_eval(const __grid_constant__ SamplerParams P, const __grid_constant__ JacobianForm J, EvalArgs a) {
     extern __shared__ __align__(16) unsigned char esh[];
     unsigned int* sh = reinterpret_cast<unsigned int*>(esh);
     double* dsh = reinterpret_cast<double*>(esh);
     const int B = P.bins;
-    hist_phase<DERIV>(P, a, sh, grid_samples(a.n));
+    hist_phase<DERIV>(P, a, sh, grid_samples(a.n), exact_queue(a));
     if (!grid_barrier(a, 1)) return;
     TailCtx t;
     if (DERIV) {
@@ -88,48 +101,45 @@ k_eval(SamplerParams P, JacobianForm J, EvalArgs a) {
         for (int i = threadIdx.x; i < B; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
+// Histogram pass of the split form. The CTA that flushes last forms the tail once
+// (tail_once): the pRatio·nFactor table for k_deriv and the value; for the value-only
+// evaluation (RECORD false) it also publishes the result, so that evaluation is this
+// one launch.
+size_t hist_kernel_smem(int B) { return std::max(hist_smem(B), tail_once_smem(B)); }
+
 template <bool RECORD>
 __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
-k_hist(SamplerParams P, EvalArgs a) {
-    extern __shared__ unsigned int sh[];
+k_hist(const __grid_constant__ SamplerParams P, EvalArgs a) {
+    extern __shared__ __align__(16) unsigned int sh[];
     pdl_launch_dependents();
-    hist_phase<RECORD>(P, a, sh, grid_samples(a.n));
+    hist_phase<RECORD>(P, a, sh, grid_samples(a.n), exact_queue(a));
+    if (!last_to_arrive(a.sync + 1)) return;
+    tail_once(P.bins, P.moving_bin_size, a, reinterpret_cast<unsigned char*>(sh), !RECORD);
 }
 
-// Value-only tail of the split form: one CTA.
-__global__ void __launch_bounds__(TAIL_BLOCK)
-k_tail(int B, double moving_bin_size, EvalArgs a) {
-    extern __shared__ __align__(16) unsigned char tsh[];
-    pdl_wait();
-    const TailSmem ts = tail_layout(B, tsh);
-    const TailCtx t = tail_prepare(B, moving_bin_size, a, ts);
-    if (!t.degenerate) value_slices_share(B, a, t, ts, (int)blockIdx.x, (int)gridDim.x);
-    __syncthreads();
-    if (threadIdx.x < 32) fold_value(B, a, t);
-    publish_seq(a);
-    for (int i = threadIdx.x; i < B * B + B; i += blockDim.x) a.ghist[i] = 0ull;
-    if (a.gcols)
-        for (int i = threadIdx.x; i < B; i += blockDim.x) a.gcols[i] = 0ull;
-}
-
-// Tail and derivative pass of the split form.
+// Derivative pass of the split form, a programmatic dependent of k_hist: the moments
+// of this CTA's records with the table k_hist's tail left; the last CTA folds them,
+// contracts them with the Jacobian form and publishes value, valid and derivative.
 __global__ void __launch_bounds__(DERIV_BLOCK, DERIV_MIN_BLOCKS)
-k_deriv(SamplerParams P, JacobianForm J, EvalArgs a) {
+k_deriv(const __grid_constant__ SamplerParams P, const __grid_constant__ JacobianForm J, EvalArgs a) {
     extern __shared__ double dsh[];
     pdl_wait();
-    const TailCtx t = deriv_phase(P, a, dsh, grid_groups(a));
+    stream_phase(P, a, dsh, grid_groups(a));
     if (!last_to_arrive(a.sync)) return;
-    deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
-    if (threadIdx.x < 32) fold_value(P.bins, a, t);
+    // k_hist's tail wrote value and valid (value DBL_MAX when degenerate)
+    const double r0 = __ldcg(a.result), r1 = __ldcg(a.result + 1);
+    deriv_fold(P, J, a, r0 == DBL_MAX, a.partials, gridDim.x);
+    if (threadIdx.x == 0 && a.result_host) {
+        a.result_host[0] = r0;
+        a.result_host[1] = r1;
+        a.result_host[RESULT_ERR] = 0.0;
+    }
     publish_seq(a);
     if (threadIdx.x == 0) a.sync[0] = 0u;
-    for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
-    if (a.gcols)
-        for (int i = threadIdx.x; i < P.bins; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
 // Per-sample decisions of the same sampler the kernels use, for the exactness tests.
-__global__ void k_decisions(SamplerParams P, const float* __restrict__ moving,
+__global__ void k_decisions(const __grid_constant__ SamplerParams P, const float* __restrict__ moving,
                             const uint8_t* __restrict__ mmask, const uint32_t* __restrict__ samples,
                             const uint8_t* __restrict__ fbin, int64_t n, int8_t* __restrict__ status,
                             int32_t* __restrict__ fb, int32_t* __restrict__ mb, int64_t* __restrict__ flat_out,
@@ -294,6 +304,8 @@ void free_metric(mi_metric* m) {
     cudaFree(m->ws.hist);
     cudaFree(m->ws.partials);
     cudaFree(m->ws.vsum);
+    cudaFree(m->ws.gpr);
+    cudaFree(m->ws.exq);
     cudaFree(m->ws.result);
     cudaFree(m->ws.done_counter);
     cudaFree(m->ws.rec_bins);
@@ -496,6 +508,9 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.rec_g = want_derivative ? ws.rec_g : nullptr;
     a.partials = ws.partials;
     a.vsum = ws.vsum;
+    a.gpr = ws.gpr;
+    a.exq = ws.exq;
+    a.exq_cap = ws.fused ? ws.exq_cap_eval : ws.exq_cap_hist;
     a.sync = ws.done_counter;
     a.result = ws.result;
     // the split form's last kernel copies the result into the mapped mirror; the
@@ -528,29 +543,24 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
     } else {
         if (want_derivative)
-            k_hist<true><<<ws.grid_hist, HIST_BLOCK, hist_smem(B), st>>>(P, a);
+            k_hist<true><<<ws.grid_hist, HIST_BLOCK, hist_kernel_smem(B), st>>>(P, a);
         else
-            k_hist<false><<<ws.grid_hist, HIST_BLOCK, hist_smem(B), st>>>(P, a);
+            k_hist<false><<<ws.grid_hist, HIST_BLOCK, hist_kernel_smem(B), st>>>(P, a);
         if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
-        // the second kernel is launched as a programmatic dependent of k_hist (no
-        // event between them), so its launch overlaps k_hist's last CTAs
-        cudaLaunchConfig_t cfg = {};
-        cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = per_kernel ? 0 : 1;
         if (want_derivative) {
+            // launched as a programmatic dependent of k_hist (no event between them), so
+            // its launch overlaps k_hist's last CTAs
+            cudaLaunchConfig_t cfg = {};
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = per_kernel ? 0 : 1;
             cfg.gridDim = dim3((unsigned)ws.grid_deriv);
             cfg.blockDim = dim3(DERIV_BLOCK);
-            cfg.dynamicSmemBytes = deriv_smem(B);
+            cfg.dynamicSmemBytes = stream_smem(B);
             MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_deriv, P, J, a));
-        } else {
-            cfg.gridDim = dim3(1);
-            cfg.blockDim = dim3(TAIL_BLOCK);
-            cfg.dynamicSmemBytes = tail_smem(B);
-            MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_tail, B, P.moving_bin_size, a));
         }
         if (per_kernel) {
             MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[2], st));
@@ -709,6 +719,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     // (metric.rs:633-640, :913-924; MattesGeometry::new, mattes.rs:152-186).
     // Mean squares and correlation have no histogram and refuse no constant image.
     double fmin = 0.0, fmax = 0.0, mmin = 0.0, mmax = 0.0;
+    double vmax = 0.0;  // the largest |voxel| of the whole moving volume (the fast path's bounds)
     mi_metric_info& info = m->info;
     info.bins = bins;
     info.n_samples = m->n_samples;
@@ -718,6 +729,14 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         if (s != MI_OK) return fail(s);
         s = minmax(ctx, m->moving, nullptr, m->mmask, mvox, &mmin, &mmax, &anym);
         if (s != MI_OK) return fail(s);
+        double gmin = mmin, gmax = mmax;
+        if (m->mmask) {
+            // a corner may be any voxel, masked or not
+            bool anyg;
+            s = minmax(ctx, m->moving, nullptr, nullptr, mvox, &gmin, &gmax, &anyg);
+            if (s != MI_OK) return fail(s);
+        }
+        vmax = std::max(std::fabs(gmin), std::fabs(gmax));
         if (fmax - fmin <= DBL_EPSILON) return fail(set_error(ctx, MI_ERR_CONSTANT_FIXED, "constant intensity: fixed"));
         if (mmax - mmin <= DBL_EPSILON) return fail(set_error(ctx, MI_ERR_CONSTANT_MOVING, "constant intensity: moving"));
         const double denom = (double)(bins - 2 * PADDING);
@@ -747,10 +766,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     }
     P.mstride1 = moving->geo.size[0];
     P.mstride2 = moving->geo.size[0] * moving->geo.size[1];
-    for (int i = 0; i < 9; ++i) {
-        P.mp2i[i] = m_p2i[i];
-        P.mp2if[i] = (float)m_p2i[i];
-    }
+    for (int i = 0; i < 9; ++i) P.mp2i[i] = m_p2i[i];
     P.has_mmask = moving_mask ? 1 : 0;
     for (int d = 0; d < 3; ++d) P.msz[d] = (int)moving->geo.size[d];
     P.ms1 = (uint32_t)P.mstride1;
@@ -806,12 +822,10 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     P.moving_nmin = info.moving_normalized_min;
     P.moving_min = mmin;
     P.moving_max = mmax;
-    P.mmin_f = (float)mmin;
-    P.mmax_f = (float)mmax;
     P.inv_bin_f = (float)P.inv_moving_bin_size;
     P.nmin_f = (float)P.moving_nmin;
-    P.rmag_f = std::max(std::fabs(P.mmin_f), std::fabs(P.mmax_f));
     P.bin_hi_f = (float)(bins - PADDING - 1);
+    P.vmax = vmax;
     // x_ref: the fixed grid's physical centre; x − x_ref = M_f·idx + (o_f − x_ref)
     const double mid[3] = {0.5 * (double)(P.fsize0 - 1), 0.5 * (double)(P.fsize1 - 1), 0.5 * (double)(P.fsize2 - 1)};
     for (int r = 0; r < 3; ++r) {
@@ -837,15 +851,14 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     // Workspace and launch shapes.
     Workspace& ws = m->ws;
     const int B = bins;
-    TRY_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)deriv_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tail_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_kernel_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_kernel_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem(B)));
     TRY_CUDA(cudaFuncSetAttribute(k_eval<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
     TRY_CUDA(cudaFuncSetAttribute(k_eval<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
     int occ_h = 0, occ_d = 0, occ_e1 = 0, occ_e0 = 0, coop = 0;
-    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK, hist_smem(B)));
-    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_deriv, DERIV_BLOCK, deriv_smem(B)));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK, hist_kernel_smem(B)));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_deriv, DERIV_BLOCK, stream_smem(B)));
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e1, k_eval<true>, HIST_BLOCK, eval_smem(B)));
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e0, k_eval<false>, HIST_BLOCK, eval_smem(B)));
     TRY_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
@@ -905,6 +918,19 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         TRY_CUDA(cudaMalloc(&ws.partials, (size_t)pgrid * NMOM * 8));
     }
     TRY_CUDA(cudaMalloc(&ws.vsum, (size_t)value_slices(B) * 8));
+    TRY_CUDA(cudaMalloc(&ws.gpr, (size_t)B * B * sizeof(float)));
+    {
+        // a grid-stride walk gives a CTA at most ceil(n / (grid·block))·block samples
+        auto cap = [&](int grid) -> uint32_t {
+            if (grid < 1) return 0u;
+            const int64_t per = ((int64_t)m->n_samples + (int64_t)grid * HIST_BLOCK - 1) / ((int64_t)grid * HIST_BLOCK);
+            return (uint32_t)(per * HIST_BLOCK);
+        };
+        ws.exq_cap_hist = cap(ws.grid_hist);
+        ws.exq_cap_eval = cap(ws.grid_eval);
+        const size_t len = std::max((size_t)ws.grid_hist * ws.exq_cap_hist, (size_t)ws.grid_eval * ws.exq_cap_eval);
+        TRY_CUDA(cudaMalloc(&ws.exq, std::max<size_t>(len, 1) * sizeof(uint32_t)));
+    }
     TRY_CUDA(cudaMalloc(&ws.result, RESULT_DOUBLES * 8));
     TRY_CUDA(cudaMalloc(&ws.done_counter, 4 * sizeof(unsigned int)));
     TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));

@@ -33,6 +33,18 @@ MI_HD inline void pm_mat3_vec(const double* a, const double* v, double* out) {
     for (int i = 0; i < 3; ++i) out[i] = t[i];
 }
 
+// f32 roundings of x toward −∞ and +∞ (NaN stays NaN).
+MI_HD inline float f32_down(double x) {
+    float f = (float)x;
+    if ((double)f > x) f = nextafterf(f, -INFINITY);
+    return f;
+}
+MI_HD inline float f32_up(double x) {
+    float f = (float)x;
+    if ((double)f < x) f = nextafterf(f, INFINITY);
+    return f;
+}
+
 // P holds the metric's fixed part (grids, moving image, histogram geometry); this
 // fills the stage-dependent part. Returns false when the map is not finite.
 MI_HD inline bool point_map_fill(SamplerParams& P, const double* stages, int nstage) {
@@ -91,7 +103,25 @@ MI_HD inline bool point_map_fill(SamplerParams& P, const double* stages, int nst
     }
     if (!(cmax <= DBL_MAX)) return false;
     P.cerr = mul(mul(0x1p-40, add(1.0, cmax)), (double)(1 + nstage));
-    P.cerr_f = (float)mul(P.cerr, 1.000001);  // rounded to f32 and still ≥ cerr
+    {
+        // the fast path's global decision bounds (sampler.cuh finish_fast): the FP32
+        // trilinear value is within 32·2^-24·vmax of the value at the fast c (three
+        // levels of lerps add at most 12 such units), and the fast c's error moves it
+        // by at most 6·vmax per voxel (8 allowed)
+        const double dv = mul(P.vmax, add(mul(8.0, P.cerr), 32.0 * 0x1p-24));
+        const double rmag = fmax(fabs(P.moving_min), fabs(P.moving_max));
+        const double e = add(mul(dv, 1.001), mul(add(mul(2.0, P.vmax), rmag), 0x1p-20));
+        P.rlo_out = f32_down(sub(P.moving_min, e));
+        P.rlo_in = f32_up(add(P.moving_min, e));
+        P.rhi_in = f32_down(sub(P.moving_max, e));
+        P.rhi_out = f32_up(add(P.moving_max, e));
+        // |termf − term_ref| ≤ dv/binSize (the value) plus 2^-24 of each magnitude the
+        // FP32 term carries (the reciprocal bin size, the normalised minimum, the FMA and
+        // the rounding of termf ± dterm), each bounded by 4× here
+        const double inv = P.inv_moving_bin_size;
+        const double mag = add(add(add(mul(P.vmax, inv), fabs(P.moving_nmin)), (double)P.bins), 1.0);
+        P.dterm = f32_up(mul(add(mul(dv, inv), mul(mag, 0x1p-22)), 1.001));
+    }
     P.ilo = add(-0.5, mul(2.0, P.cerr));
     P.olo = sub(-0.5, mul(2.0, P.cerr));
     for (int d = 0; d < 3; ++d) {

@@ -44,7 +44,7 @@ constexpr int PADDING = 2;  // registration/mattes.rs:92
 enum : int { SAMPLE_OUTSIDE = 0, SAMPLE_OUT_OF_RANGE = 1, SAMPLE_VALID = 2 };
 
 struct Sample {
-    float g[3];     // moving physical gradient (GRAD)
+    float g[3];     // moving gradient in index space (GRAD); the physical gradient is Mᵀ·g
     float f;        // Parzen fraction: moving term − moving bin
     int mi;         // moving Parzen bin
     bool exact;     // a decision or the gradient's cell came from the exact chain
@@ -254,18 +254,23 @@ struct Prep {
     uint32_t flat;
     float fr[3];
     float v[8];
-    uint8_t mval;  // moving-mask byte at round(c) (1 without a mask)
-    bool ok;       // not decided outside
-    bool exact_c;  // c was recomputed exactly
 };
 
+// Outcome of a fast-path stage: a decision, or the sample handed to the exact chain.
+enum : int { SAMPLE_EXACT = 3 };
+
+// prep_fast(): the fast path's first stage. c from the composite map (within cerr of
+// the exact c). A sample whose inside test or mask rounding could flip within ±cerr,
+// or whose c lies within cerr of an integer (the interpolant's gradient jumps across
+// cell faces, so the cell must be the reference's), is handed to the exact chain
+// (SAMPLE_EXACT); a sample surely outside the moving buffer, or on a masked voxel, is
+// SAMPLE_OUTSIDE; otherwise the cell's fractions are kept and its eight corners
+// requested (SAMPLE_VALID). The value-only and the value+derivative passes hand the
+// same samples to the exact chain, so both form the same histogram bits.
 template <bool GRAD>
-__device__ __forceinline__ void prep(const SamplerParams& P, uint32_t flat, const float* __restrict__ moving,
-                                     const uint8_t* __restrict__ mmask, Prep& p) {
+__device__ __forceinline__ int prep_fast(const SamplerParams& P, uint32_t flat, const uint8_t* __restrict__ mmask,
+                                         Prep& p) {
     p.flat = flat;
-    p.ok = false;
-    p.exact_c = false;
-    p.mval = 1;
     uint32_t i, j, k;
     grid_index(P, flat, i, j, k);
     double c[3];
@@ -276,71 +281,56 @@ __device__ __forceinline__ void prep(const SamplerParams& P, uint32_t flat, cons
             c[r] = fma(P.cA[r * 3 + 2], dk, fma(P.cA[r * 3 + 1], dj, fma(P.cA[r * 3 + 0], di, P.cb[r])));
     }
     const double ce = P.cerr;
-    bool need_index = false;
+    bool uncertain = false;
     // inside test [−0.5, size − 0.5): the bounds ilo/ihi (surely inside) and olo/ohi
     // (surely outside) carry a margin of 2·ce
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (!(c[d] >= P.ilo && c[d] < P.ihi[d])) {
-            if (c[d] < P.olo || c[d] >= P.ohi[d]) return;
-            need_index = true;
+            if (c[d] < P.olo || c[d] >= P.ohi[d]) return SAMPLE_OUTSIDE;
+            uncertain = true;
         }
     }
     if (P.has_mmask) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const double h = c[d] + 0.5;
-            if (floor(h - ce) != floor(h + ce)) need_index = true;
+            if (floor(h - ce) != floor(h + ce)) uncertain = true;
         }
     }
-    double fl[3], frd[3];
+    double fl[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         fl[d] = floor(c[d]);
-        frd[d] = c[d] - fl[d];
-        if (GRAD && (frd[d] <= ce || frd[d] >= 1.0 - ce)) need_index = true;
+        const double frd = c[d] - fl[d];
+        if (frd <= ce || frd >= 1.0 - ce) uncertain = true;
+        p.fr[d] = (float)frd;
     }
-    if (need_index) {
-        exact_index(P, i, j, k, c);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            if (!(c[d] >= -0.5 && c[d] < P.mhi[d])) return;
-            fl[d] = floor(c[d]);
-            frd[d] = c[d] - fl[d];
-        }
-        p.exact_c = true;
-    }
+    if (uncertain) return SAMPLE_EXACT;
     if (P.has_mmask) {
-        // decided on c (certain, or exact)
+        // decided on c (certain)
         uint32_t mflat = 0;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const double r = floor(c[d] + 0.5);
-            if (!(r >= 0.0 && r < (double)P.msz[d])) return;
+            if (!(r >= 0.0 && r < (double)P.msz[d])) return SAMPLE_OUTSIDE;
             const uint32_t ri = (uint32_t)r;
             mflat += d == 0 ? ri : (d == 1 ? ri * P.ms1 : ri * P.ms2);
         }
-        p.mval = __ldg(mmask + mflat);
+        if (!__ldg(mmask + mflat)) return SAMPLE_OUTSIDE;
     }
     // The eight corners of the cell of c. c passed the inside test, so floor(c) ∈
-    // [−1, size − 1]. They are fetched from the moving volume's 3-D texture: point
-    // sampling at voxel centres returns the stored f32 voxel unchanged, clamp
-    // addressing is exactly the reference's clamp-to-edge of each corner index, and
-    // the block-linear layout keeps a cell's corners on a few cache lines.
-#pragma unroll
-    for (int d = 0; d < 3; ++d) p.fr[d] = (float)frd[d];
+    // [−1, size − 1]; the texture's point sampling at voxel centres returns the stored
+    // voxel unchanged and its clamp addressing is the reference's clamp-to-edge of each
+    // corner index.
     fetch_corners(P, fl, p.v);
-    p.ok = true;
+    return SAMPLE_VALID;
 }
 
+// The trilinear value at fractions fr of the cell with corners v (x-lerps, then y,
+// then z) and, for GRAD, the exact gradient of the interpolant in index space.
 template <bool GRAD>
-__device__ __forceinline__ int finish(const SamplerParams& P, const Prep& p, const float* __restrict__ moving,
-                                      Sample& o) {
-    if (!p.ok || !p.mval) return SAMPLE_OUTSIDE;
-    o.exact = p.exact_c;
-    const float* v = p.v;
-    const float* fr = p.fr;
-    // x-lerps, then y, then z
+__device__ __forceinline__ float trilinear(const float* v, const float* fr, float* gidx) {
     const float x00 = fmaf(fr[0], v[1] - v[0], v[0]);
     const float x10 = fmaf(fr[0], v[3] - v[2], v[2]);
     const float x01 = fmaf(fr[0], v[5] - v[4], v[4]);
@@ -348,79 +338,106 @@ __device__ __forceinline__ int finish(const SamplerParams& P, const Prep& p, con
     const float y0 = fmaf(fr[1], x10 - x00, x00);
     const float y1 = fmaf(fr[1], x11 - x01, x01);
     if (GRAD) {
-        // exact gradient of the trilinear interpolant in index space, then
-        // g_phys[d] = Σ_j g_idx[j]·M[j][d] (registration/metric.rs:848-861)
-        const float gz = y1 - y0;
-        const float gy = fmaf(fr[2], (x11 - x01) - (x10 - x00), x10 - x00);
         const float a0 = fmaf(fr[1], (v[3] - v[2]) - (v[1] - v[0]), v[1] - v[0]);
         const float a1 = fmaf(fr[1], (v[7] - v[6]) - (v[5] - v[4]), v[5] - v[4]);
-        const float gx = fmaf(fr[2], a1 - a0, a0);
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-            o.g[d] = gx * P.mp2if[0 * 3 + d] + gy * P.mp2if[1 * 3 + d] + gz * P.mp2if[2 * 3 + d];
+        gidx[0] = fmaf(fr[2], a1 - a0, a0);
+        gidx[1] = fmaf(fr[2], (x11 - x01) - (x10 - x00), x10 - x00);
+        gidx[2] = y1 - y0;
     }
-    const float mv = fmaf(fr[2], y1 - y0, y0);
-    // |mv − reference value| ≤ dv: three levels of FP32 lerps add at most 12 units of
-    // 2^-24 of the largest corner magnitude (32 allowed), plus the Lipschitz effect
-    // (≤ 6·vmax per voxel) of the continuous-index error ce.
-    float vmax = fabsf(v[0]);
-#pragma unroll
-    for (int t = 1; t < 8; ++t) vmax = fmaxf(vmax, fabsf(v[t]));
-    // The range and Parzen decisions in FP32 with a bound that covers the value's error
-    // dv and every FP32 rounding on the way: e bounds |mv − v_ref| plus the rounding of
-    // mv ± e (the 2^-20 terms are ≥ 16 ulps of every magnitude involved, the range ends
-    // are f32 voxel values and so exact); dt bounds |term − term_ref| with
-    // term_ref = v_ref/binSize − normMin (inv_bin_f and nmin_f carry 2^-24 relative
-    // error, the FMA one rounding, the reference's FP64 chain ≪ 2^-40) plus the
-    // rounding of term ± dt. Every operation is an explicitly rounded intrinsic, so no
-    // kernel that inlines this contracts it differently: a sample takes the same path
-    // in every kernel.
-    const float cef = p.exact_c ? 0.0f : P.cerr_f;
-    const float dvf = __fmul_rn(vmax, __fmaf_rn(8.0f, cef, 32.0f * 5.9604644775390625e-08f));
-    bool certain = dvf < 1e30f && isfinite(mv);
-    float termf = 0.0f;
-    int mi = 0;
-    if (certain) {
-        const float mag = __fadd_rn(__fadd_rn(fabsf(mv), P.rmag_f), vmax);
-        const float e = __fmaf_rn(dvf, 1.001f, __fmul_rn(mag, 9.5367431640625e-07f));
-        if (__fadd_rn(mv, e) < P.mmin_f || __fsub_rn(mv, e) > P.mmax_f) return SAMPLE_OUT_OF_RANGE;
-        certain = __fsub_rn(mv, e) >= P.mmin_f && __fadd_rn(mv, e) <= P.mmax_f;
-        termf = __fmaf_rn(mv, P.inv_bin_f, -P.nmin_f);
-        const float tmag = __fadd_rn(__fadd_rn(__fadd_rn(fabsf(__fmul_rn(mv, P.inv_bin_f)), fabsf(P.nmin_f)),
-                                               fabsf(termf)), 1.0f);
-        const float dt = __fmaf_rn(__fmul_rn(dvf, P.inv_bin_f), 1.001f, __fmul_rn(tmag, 2.384185791015625e-07f));
-        // truncation then clamp to [2, bins − 3] equals floor then clamp for every
-        // term (anything below 2 clamps to 2)
-        const float lo = fminf(fmaxf(floorf(__fsub_rn(termf, dt)), (float)PADDING), P.bin_hi_f);
-        const float hi = fminf(fmaxf(floorf(__fadd_rn(termf, dt)), (float)PADDING), P.bin_hi_f);
-        certain = certain && lo == hi;
-        mi = (int)lo;
-    }
-    if (!certain) {
-        uint32_t i, j, k;
-        grid_index(P, p.flat, i, j, k);
-        double c[3];
-        exact_index(P, i, j, k, c);
-        o.exact = true;
-        const double mvx = exact_value(P, c, moving);
-        if (mvx < P.moving_min || mvx > P.moving_max) return SAMPLE_OUT_OF_RANGE;
-        const double term = __dsub_rn(__ddiv_rn(mvx, P.moving_bin_size), P.moving_nmin);
-        mi = parzen_bin(term, P.bins);
-        o.f = (float)(term - (double)mi);
-    } else {
-        o.f = __fsub_rn(termf, (float)mi);
-    }
-    o.mi = mi;
+    return fmaf(fr[2], y1 - y0, y0);
+}
+
+// finish_fast(): the fast path's second stage. The FP32 trilinear value (and index-
+// space gradient), then the range and Parzen decisions against the metric's global
+// bounds (point_map_fill): |mv − v_ref| ≤ dv for every sample of the evaluation, so
+//   mv < rlo_out or mv > rhi_out            surely out of range,
+//   rlo_in ≤ mv ≤ rhi_in                    surely in range,
+// the thresholds being the range ends ∓ the bound rounded outward to f32; and the
+// Parzen term's floor is certain when floor(termf − dterm) = floor(termf + dterm)
+// after the clamp to [2, bins − 3]. Anything else is SAMPLE_EXACT. Every operation is
+// an explicitly rounded intrinsic, so every kernel that inlines this takes the same
+// path for a sample.
+template <bool GRAD>
+__device__ __forceinline__ int finish_fast(const SamplerParams& P, const Prep& p, Sample& o) {
+    const float mv = trilinear<GRAD>(p.v, p.fr, o.g);
+    if (mv < P.rlo_out || mv > P.rhi_out) return SAMPLE_OUT_OF_RANGE;
+    if (!(mv >= P.rlo_in && mv <= P.rhi_in)) return SAMPLE_EXACT;
+    const float termf = __fmaf_rn(mv, P.inv_bin_f, -P.nmin_f);
+    // truncation then clamp to [2, bins − 3] equals floor then clamp for every term
+    // (anything below 2 clamps to 2)
+    const float lo = fminf(fmaxf(floorf(__fsub_rn(termf, P.dterm)), (float)PADDING), P.bin_hi_f);
+    const float hi = fminf(fmaxf(floorf(__fadd_rn(termf, P.dterm)), (float)PADDING), P.bin_hi_f);
+    if (lo != hi) return SAMPLE_EXACT;
+    o.mi = (int)lo;
+    o.f = __fsub_rn(termf, lo);
     return SAMPLE_VALID;
 }
 
+// The exact chain for one sample, out of line (it is rare, and keeping it out of the
+// callers' loops keeps their register footprint to the fast path's): the reference's
+// continuous index, inside test, mask rounding, FP64 trilinear value and Parzen bin
+// (every decision the host's), and, for GRAD, the FP32 index-space gradient of the
+// interpolant on the eight corners the value read.
+#ifndef MI_EXACT_NOINLINE
+#define MI_EXACT_NOINLINE 0
+#endif
+#if MI_EXACT_NOINLINE
+#define MI_EXACT_INLINE __noinline__
+#else
+#define MI_EXACT_INLINE __forceinline__
+#endif
+template <bool GRAD>
+__device__ MI_EXACT_INLINE int sample_exact(const SamplerParams& P, uint32_t flat, const float* __restrict__ moving,
+                                         const uint8_t* __restrict__ mmask, Sample& o) {
+    uint32_t i, j, k;
+    grid_index(P, flat, i, j, k);
+    double c[3];
+    exact_index(P, i, j, k, c);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        if (!(c[d] >= -0.5 && c[d] < P.mhi[d])) return SAMPLE_OUTSIDE;
+    if (P.has_mmask) {
+        uint32_t mflat = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double r = floor(c[d] + 0.5);
+            if (!(r >= 0.0 && r < (double)P.msz[d])) return SAMPLE_OUTSIDE;
+            const uint32_t ri = (uint32_t)r;
+            mflat += d == 0 ? ri : (d == 1 ? ri * P.ms1 : ri * P.ms2);
+        }
+        if (!__ldg(mmask + mflat)) return SAMPLE_OUTSIDE;
+    }
+    float v[8];
+    const double mvx = exact_value_corners(P, c, moving, v);
+    if (mvx < P.moving_min || mvx > P.moving_max) return SAMPLE_OUT_OF_RANGE;
+    if (GRAD) {
+        float fr[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fr[d] = (float)__dsub_rn(c[d], floor(c[d]));
+        trilinear<true>(v, fr, o.g);
+    }
+    const double term = __dsub_rn(__ddiv_rn(mvx, P.moving_bin_size), P.moving_nmin);
+    o.mi = parzen_bin(term, P.bins);
+    o.f = (float)(term - (double)o.mi);
+    return SAMPLE_VALID;
+}
+
+// The whole sampler for one sample: the fast path, handing to the exact chain where it
+// cannot decide. o.exact reports which path decided.
 template <bool GRAD>
 __device__ __forceinline__ int sample(const SamplerParams& P, uint32_t flat, const float* __restrict__ moving,
                                       const uint8_t* __restrict__ mmask, Sample& o) {
     Prep p;
-    prep<GRAD>(P, flat, moving, mmask, p);
     o.exact = false;
-    return finish<GRAD>(P, p, moving, o);
+    int st = prep_fast<GRAD>(P, flat, mmask, p);
+    if (st == SAMPLE_VALID) st = finish_fast<GRAD>(P, p, o);
+    if (st == SAMPLE_EXACT) {
+        Sample e;
+        st = sample_exact<GRAD>(P, flat, moving, mmask, e);
+        o = e;
+        o.exact = true;
+    }
+    return st;
 }
 
 // The four Parzen taps of a sample. With f = term − mi ∈ [0, 1] the taps sit at

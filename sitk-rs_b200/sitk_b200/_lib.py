@@ -32,11 +32,11 @@ EXPORTED = [
     "mi_metric_timing_read", "mi_metric_value_noalloc", "mi_register_rsgd",
     "mi_centered_initialize", "mi_metric_set_fused", "mi_metric_get_fused", "mi_image_smooth",
     "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level", "mi_batch_create", "mi_batch_register",
-    "mi_batch_shape", "mi_batch_destroy", "mi_synth_pair", "mi_gemm_bf16_tn", "mi_initnet_create",
+    "mi_batch_shape", "mi_batch_pair_seconds", "mi_batch_destroy", "mi_synth_pair", "mi_gemm_bf16_tn", "mi_initnet_create",
     "mi_initnet_destroy", "mi_initnet_get", "mi_initnet_set", "mi_initnet_forward", "mi_initnet_train_step",
     "mi_initnet_prepare", "mi_metric_create_ex", "mi_image_resample_nearest",
     "mi_metric_value_and_derivative_bspline", "mi_metric_bspline_records", "mi_image_read_meta",
-    "mi_image_read_meta_host",
+    "mi_image_read_meta_host", "mi_image_read_nifti", "mi_image_read_nifti_host",
 ]
 
 

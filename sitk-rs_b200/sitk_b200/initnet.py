@@ -149,6 +149,23 @@ class InitNet:
         for l, (w, b) in enumerate(state):
             self.set(l, w, b)
 
+    def save(self, path: str, **meta) -> None:
+        """Weights and biases of every layer (float32) into an .npz file, with `meta`
+        (strings or numbers describing how they were trained)."""
+        arrays = {}
+        for l, (w, b) in enumerate(self.state()):
+            arrays[f"w{l}"] = w
+            arrays[f"b{l}"] = b
+        for k, v in meta.items():
+            arrays[f"meta_{k}"] = np.asarray(v)
+        np.savez_compressed(path, **arrays)
+
+    def load(self, path: str) -> dict:
+        """Weights written by save(); returns the stored meta entries."""
+        with np.load(path) as z:
+            self.load_state([(z[f"w{l}"], z[f"b{l}"]) for l in range(N_LAYERS)])
+            return {k[5:]: z[k].item() if z[k].ndim == 0 else z[k].tolist() for k in z.files if k.startswith("meta_")}
+
     def propose(self, x) -> np.ndarray:
         """Affine parameters (B × 12) for network inputs x."""
         return decode(self.forward(x).double().cpu().numpy())

@@ -106,10 +106,14 @@ class DeviceImage:
 
     @classmethod
     def read(cls, path: str, ctx: "Context | None" = None) -> "DeviceImage":
-        """A MetaImage file (.mha / .mhd) read and uploaded (mi_image_read_meta)."""
+        """A MetaImage (.mha / .mhd, mi_image_read_meta) or NIfTI-1 (.nii, .hdr / .img,
+        optionally .gz, mi_image_read_nifti) file read and uploaded, by its extension."""
         ctx = ctx or default_context()
         h = ctypes.c_void_p()
-        _lib.check(_lib.load().mi_image_read_meta(ctx.handle, os.fsencode(path), ctypes.byref(h)), ctx.handle)
+        if _is_nifti_name(path):
+            _lib.check(_nifti_lib().mi_image_read_nifti(ctx.handle, os.fsencode(path), ctypes.byref(h)), ctx.handle)
+        else:
+            _lib.check(_lib.load().mi_image_read_meta(ctx.handle, os.fsencode(path), ctypes.byref(h)), ctx.handle)
         geo = _lib.MiGeometry()
         _lib.check(_lib.load().mi_image_geometry(h, ctypes.byref(geo)))
         return cls(h, ctx, geo)
@@ -485,6 +489,37 @@ def pyramid_level(fixed: DeviceImage, moving: DeviceImage, sigma: float, factors
     _lib.check(L.mi_image_geometry(hf, ctypes.byref(gf)))
     _lib.check(L.mi_image_geometry(hm, ctypes.byref(gm)))
     return DeviceImage(hf, fixed.ctx, gf), DeviceImage(hm, moving.ctx, gm)
+
+
+def _is_nifti_name(path: str) -> bool:
+    p = os.fspath(path).lower()
+    return p.endswith((".nii", ".nii.gz", ".hdr", ".hdr.gz", ".img", ".img.gz"))
+
+
+def _nifti_lib():
+    L = _lib.load()
+    if not getattr(L, "_nifti_bound", False):
+        L.mi_image_read_nifti.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.mi_image_read_nifti.restype = ctypes.c_int
+        L.mi_image_read_nifti_host.argtypes = [ctypes.c_char_p, ctypes.POINTER(_lib.MiGeometry),
+                                               ctypes.POINTER(ctypes.c_float), ctypes.c_size_t]
+        L.mi_image_read_nifti_host.restype = ctypes.c_int
+        L._nifti_bound = True
+    return L
+
+
+def read_nifti_host(path: str):
+    """A NIfTI-1 file read on the host alone (mi_image_read_nifti_host): (voxels as a
+    float32 [z, y, x] array, rescaled and cast as the reader does, geometry)."""
+    L = _nifti_lib()
+    geo = _lib.MiGeometry()
+    p = os.fsencode(path)
+    _lib.check(L.mi_image_read_nifti_host(p, ctypes.byref(geo), None, 0))
+    nx, ny, nz = (int(geo.size[i]) for i in range(3))
+    out = np.empty((nz, ny, nx), dtype=np.float32)
+    _lib.check(L.mi_image_read_nifti_host(p, ctypes.byref(geo), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                          out.size))
+    return out, geo
 
 
 def read_meta_host(path: str):

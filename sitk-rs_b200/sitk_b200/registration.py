@@ -203,6 +203,17 @@ class BatchRegistration:
                            r.evaluations) for r in res]
         return p, out
 
+    def pair_seconds(self) -> np.ndarray:
+        """Per pair, the device-timed interval from the start of the last register() run
+        to the optimizer step at which the pair stopped (mi_batch_pair_seconds)."""
+        out = np.zeros(self.n)
+        L = _lib.load()
+        L.mi_batch_pair_seconds.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+        L.mi_batch_pair_seconds.restype = ctypes.c_int
+        _lib.check(L.mi_batch_pair_seconds(self.handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.n),
+                   self.ctx.handle)
+        return out
+
     def shape(self):
         """(chunk size, histogram copies, chunk count) in use."""
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

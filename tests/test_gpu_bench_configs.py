@@ -59,12 +59,7 @@ def test_config3_512cubed_euler_64_bins(oracle_lib, storage):
     n = 512
     ctx = sb.Context(0)
     f, m, _ = synth.make_pair_device(n, 120, 20261203 + 3, 10.0, 5.0, None, ctx=ctx)
-
-    class Pair:
-        pass
-
-    p = Pair()
-    p.fixed, p.moving = f.to_host(), m.to_host()
+    p = synth.Pair(f.to_host(), m.to_host(), np.eye(3), np.zeros(3), np.zeros(3))
     f.free()
     m.free()
     c = [(n - 1) / 2.0] * 3
