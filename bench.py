@@ -668,6 +668,77 @@ def run_initnet(args, rank: int, world: int, local_rank: int):
     return 0
 
 
+def run_gemm_study(args, rank: int, world: int, local_rank: int):
+    """The learned initialiser's tensor-core GEMM (mi_gemm_bf16_tn: C = A·Bᵀ, BF16
+    operands, FP32 accumulation in tensor memory) on the shapes its layers run for a
+    64-pair batch (forward im2col products and the weight gradients, whose K is the
+    batch's voxel count), plus square shapes where the tensor cores, not memory, bound
+    it. Each call is synchronous; per-call device time from CUDA events around
+    `--steps` calls on the library's stream (the per-call launch and result check are
+    in it, which dominates the small shapes: the ncu launch list gives their kernel
+    time). Results are checked against torch's FP32 product of the same operands."""
+    import ctypes
+    import torch
+    import sitk_b200 as sb
+    from sitk_b200 import _lib
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    ctx = sb.Context(local_rank)
+    L = _lib.load()
+    L.mi_gemm_bf16_tn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+    L.mi_gemm_bf16_tn.restype = ctypes.c_int
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local_rank)
+    shapes = [("conv0 forward", 262144, 16, 56), ("conv1 forward", 32768, 32, 432), ("conv2 forward", 4096, 64, 864),
+              ("conv3 forward", 512, 128, 1728), ("fc1 forward", 64, 256, 1024),
+              ("conv0 weight gradient", 16, 56, 262144), ("conv1 weight gradient", 32, 432, 32768),
+              ("conv2 weight gradient", 64, 864, 4096), ("square 4096", 4096, 4096, 4096),
+              ("square 8192", 8192, 8192, 8192)]
+    peak_t = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak_t = float(json.load(fh)["bf16_tflops"])
+    except Exception:
+        peak_t = 1590.0
+    hbm, _ = _peaks()
+    out = []
+    g = torch.Generator(device="cpu").manual_seed(SEED)
+    for name, M, N, K in shapes:
+        A = torch.randn((M, K), generator=g).to(torch.bfloat16).cuda()
+        B = torch.randn((N, K), generator=g).to(torch.bfloat16).cuda()
+        C = torch.empty((M, N), dtype=torch.float32, device="cuda")
+
+        def call():
+            _lib.check(L.mi_gemm_bf16_tn(ctx.handle, M, N, K, A.data_ptr(), K, B.data_ptr(), K, C.data_ptr(), N),
+                       ctx.handle)
+
+        for _ in range(2):
+            call()
+        ref = (A.float() @ B.float().T)
+        err = float((C - ref).abs().max() / ref.abs().max())
+        reps = max(3, min(args.steps, 50))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        flops = 2.0 * M * N * K
+        bytes_ = 2.0 * (M * K + N * K) + 4.0 * M * N
+        out.append({"shape": name, "M": M, "N": N, "K": K, "ms_per_call": ms, "tflops": flops / (ms / 1e3) / 1e12,
+                    "tflops_frac_of_measured_bf16": flops / (ms / 1e3) / 1e12 / peak_t,
+                    "gbs": bytes_ / (ms / 1e3) / 1e9, "gbs_frac_of_measured_hbm": bytes_ / (ms / 1e3) / 1e9 / hbm,
+                    "max_rel_err_vs_fp32": err})
+        del A, B, C, ref
+    print(json.dumps({"metric": "tensor-core GEMM (mi_gemm_bf16_tn) per call", "unit": "TFLOP/s", "n_gpus": 1,
+                      "dtype": "bf16 operands, f32 accumulation", "peak_bf16_tflops": peak_t,
+                      "peak_hbm_gbs": hbm, "shapes": out}), flush=True)
+    return 0
+
+
 def bf16_round(v):
     """f32 → nearest BF16 (ties to even), widened back to f32 (finite inputs)."""
     b = np.ascontiguousarray(v, dtype=np.float32).view(np.uint32).astype(np.uint64)
@@ -805,6 +876,8 @@ def main():
     ap.add_argument("--storage-study", action="store_true",
                     help="run the f32/bf16 moving-storage study (512^3) instead of the metric benchmark")
     ap.add_argument("--storage-n", type=int, default=512)
+    ap.add_argument("--gemm-study", action="store_true",
+                    help="time the learned initialiser's tensor-core GEMM on its layer shapes instead")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
@@ -815,6 +888,8 @@ def main():
         return run_initnet(args, rank, world, local_rank)
     if args.storage_study:
         return run_storage_study(args, rank, world, local_rank)
+    if args.gemm_study:
+        return run_gemm_study(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

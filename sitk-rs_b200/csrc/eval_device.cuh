@@ -27,6 +27,12 @@ namespace {
 #ifndef MI_HIST_MIN_BLOCKS
 #define MI_HIST_MIN_BLOCKS 2
 #endif
+// 1: the histogram pass's main loop issues the next sample's corner gathers before it
+// finishes the current one; 0: one sample at a time.
+#ifndef MI_HIST_PIPELINE
+#define MI_HIST_PIPELINE 0
+#endif
+constexpr bool HIST_PIPELINE = MI_HIST_PIPELINE != 0;
 // Samples the fast path cannot decide: 1 queues them and runs the exact chain after the
 // histogram phase's main loop (the loop then carries none of the exact chain's state),
 // 0 runs it inside the loop.
@@ -307,38 +313,74 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
             a.rec_g[2 * (size_t)npad + s] = o.g[2];
         }
     };
-    // Whole warps iterate together (the loop bound is the warp's first sample). The
-    // next sample's index and this sample's fixed bin are requested at the top of the
-    // iteration, so their loads overlap this sample's corner gathers instead of adding
-    // two memory round trips per sample. A sample the fast path cannot decide goes to
-    // the exact chain, out of line.
+    // Whole warps iterate together (the loop bound is the warp's first sample).
     const uint32_t wbase = r.begin + r.warp_first;
-    uint32_t s = wbase + lane;
-    uint32_t flat = s < n ? (samples ? __ldg(samples + s) : s) : 0u;
-    for (uint32_t b = wbase; b < n; b += stride) {
-        const bool one = s < n;
-        const int fi = one ? (int)__ldg(fbin + s) : 0;
-        const uint32_t sn = s + stride;
-        const uint32_t flat_next = sn < n ? (samples ? __ldg(samples + sn) : sn) : 0u;
-        if (one) {
-            Prep p;
-            Sample o;
-            int st = prep_fast<RECORD>(P, flat, mmask, p);
-            if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
-            if (st == SAMPLE_EXACT) {
-                if (exq.base) {
-                    exq.base[atomicAdd(&exq_count, 1u)] = s;
-                } else {
-                    Sample e;
-                    st = sample_exact<RECORD>(P, flat, moving, mmask, e);
-                    account(st, e, s, fi);
-                }
+    // A sample the fast path cannot decide goes to the exact chain: queued (or, without
+    // a queue, run here, out of line).
+    auto settle = [&](int st, const Prep& p, uint32_t s, int fi) {
+        Sample o;
+        if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
+        if (st == SAMPLE_EXACT) {
+            if (exq.base) {
+                exq.base[atomicAdd(&exq_count, 1u)] = s;
             } else {
-                account(st, o, s, fi);
+                Sample e;
+                st = sample_exact<RECORD>(P, p.flat, moving, mmask, e);
+                account(st, e, s, fi);
             }
+        } else {
+            account(st, o, s, fi);
         }
-        s = sn;
-        flat = flat_next;
+    };
+    if (HIST_PIPELINE) {
+        // Software-pipelined: the next sample's corner gathers are issued before this
+        // sample is finished, so each thread keeps two samples' gathers in flight while
+        // only one sample's finish is live. The index two samples ahead and the next
+        // fixed bin are requested a step earlier still.
+        constexpr int NONE = -1;
+        uint32_t s = wbase + lane;
+        const uint32_t s1 = s + stride;
+        uint32_t flat_next = s1 < n ? (samples ? __ldg(samples + s1) : s1) : 0u;
+        Prep pc;
+        int stc = NONE, fic = 0;
+        if (s < n) {
+            stc = prep_fast<RECORD>(P, samples ? __ldg(samples + s) : s, mmask, pc);
+            fic = (int)__ldg(fbin + s);
+        }
+        for (uint32_t b = wbase; b < n; b += stride) {
+            const uint32_t sn = s + stride, sn2 = sn + stride;
+            const uint32_t flat_next2 = sn2 < n ? (samples ? __ldg(samples + sn2) : sn2) : 0u;
+            Prep pn;
+            int stn = NONE, fin = 0;
+            if (sn < n) {
+                fin = (int)__ldg(fbin + sn);
+                stn = prep_fast<RECORD>(P, flat_next, mmask, pn);
+            }
+            if (stc != NONE) settle(stc, pc, s, fic);
+            pc = pn;
+            stc = stn;
+            fic = fin;
+            s = sn;
+            flat_next = flat_next2;
+        }
+    } else {
+        // The next sample's index and this sample's fixed bin are requested at the top of
+        // the iteration, so their loads overlap this sample's corner gathers instead of
+        // adding two memory round trips per sample.
+        uint32_t s = wbase + lane;
+        uint32_t flat = s < n ? (samples ? __ldg(samples + s) : s) : 0u;
+        for (uint32_t b = wbase; b < n; b += stride) {
+            const bool one = s < n;
+            const int fi = one ? (int)__ldg(fbin + s) : 0;
+            const uint32_t sn = s + stride;
+            const uint32_t flat_next = sn < n ? (samples ? __ldg(samples + sn) : sn) : 0u;
+            if (one) {
+                Prep p;
+                settle(prep_fast<RECORD>(P, flat, mmask, p), p, s, fi);
+            }
+            s = sn;
+            flat = flat_next;
+        }
     }
     if (exq.base) {
         // the queued samples through the exact chain, spread over the CTA
@@ -523,28 +565,24 @@ __device__ TailCtx tail_prepare(int B, double moving_bin_size, const EvalArgs& a
     return tail_finish(B, moving_bin_size, a, ts);
 }
 
-// ln(a/b) for positive a, b in FP32: the quotient by the fast reciprocal (a few ulps)
-// and the accurate logf.
-__device__ __forceinline__ float log_ratio(float a, float b) { return logf(__fdividef(a, b)); }
-
-// pRatio·nFactor of every bin into pr (shared memory, FP32): 0 where the reference
-// skips the bin (jp, mm or fm not above ε), else ln(joint/col)·nFactor in FP32 (the
-// table is FP32; the ratio of the two exact integers carries a few units of 2^-24,
-// far below what the derivative's tolerance sees). The entry's (row, column) advance
-// with the thread's stride, so no per-entry division.
-__device__ __forceinline__ float pr_entry(unsigned long long jv, unsigned long long col, bool ok, unsigned long long jmin,
-                                         float nf) {
-    return ok && jv >= jmin ? log_ratio((float)jv, (float)col) * nf : 0.0f;
+// A bin's pRatio·nFactor (mattes.rs:305-320): ln(jp/mm)·nFactor = (ln jv − ln col)·
+// nFactor, formed in FP64 from the bin's ln jv and its column's ln col and rounded once
+// to the FP32 table the derivative pass reads; 0 where the reference skips the bin.
+__device__ __forceinline__ float pr_entry(bool take, double ljv, double lcol, double n_factor) {
+    return take ? (float)((ljv - lcol) * n_factor) : 0.0f;
 }
 
+// pRatio·nFactor of every bin into pr (shared memory). The entry's (row, column)
+// advance with the thread's stride, so no per-entry division.
 __device__ void pr_table(int B, const TailCtx& t, const TailSmem& ts, float* pr) {
     const int B2 = B * B;
-    const float nf = (float)t.n_factor;
     const unsigned long long jmin = *ts.jmin;
     int f = (int)threadIdx.x / B, m = (int)threadIdx.x - f * B;
     const int df = (int)blockDim.x / B, dm = (int)blockDim.x - df * B;
     for (int i = threadIdx.x; i < B2; i += blockDim.x) {
-        pr[i] = pr_entry(ts.hist[i], ts.col[m], ts.okf[f] && ts.okm[m], jmin, nf);
+        const unsigned long long jv = ts.hist[i];
+        const bool take = ts.okf[f] && ts.okm[m] && jv >= jmin;
+        pr[i] = pr_entry(take, take ? log((double)jv) : 0.0, ts.lcol[m], t.n_factor);
         f += df;
         m += dm;
         if (m >= B) {
@@ -564,10 +602,9 @@ __host__ __device__ inline int value_slices(int B) { return (B * B + 31) / 32; }
 // FP64 as (jv/total)·(ln jv − ln col − ln fm) from the margins' logarithms; 0 where the
 // reference skips the bin (jp, mm or fm not above ε: `ok` holds the two marginal
 // flags, jv ≥ jmin is jp > ε).
-__device__ __forceinline__ double value_term(unsigned long long jv, bool ok, unsigned long long jmin, double lcol,
-                                             double lfm, const TailCtx& t) {
-    if (!ok || jv < jmin) return 0.0;
-    return ((double)jv / t.dt) * ((log((double)jv) - lcol) - lfm);
+__device__ __forceinline__ double value_term(unsigned long long jv, bool take, double ljv, double lcol, double lfm,
+                                             const TailCtx& t) {
+    return take ? ((double)jv / t.dt) * ((ljv - lcol) - lfm) : 0.0;
 }
 
 __device__ __forceinline__ double slice_sum(double term) {
@@ -582,7 +619,9 @@ __device__ double value_slice(int B, const TailCtx& t, const TailSmem& ts, int s
     double term = 0.0;
     if (i < B * B) {
         const int f = i / B, m = i - f * B;
-        term = value_term(ts.hist[i], ts.okf[f] && ts.okm[m], *ts.jmin, ts.lcol[m], ts.lfm[f], t);
+        const unsigned long long jv = ts.hist[i];
+        const bool take = ts.okf[f] && ts.okm[m] && jv >= *ts.jmin;
+        term = value_term(jv, take, take ? log((double)jv) : 0.0, ts.lcol[m], ts.lfm[f], t);
     }
     return slice_sum(term);
 }
@@ -681,7 +720,6 @@ __device__ __forceinline__ void tail_once(int B, double moving_bin_size, const E
     if (threadIdx.x == blockDim.x - 1) *jmin_s = least_joint(t.dt);
     __syncthreads();
     const unsigned long long jmin = *jmin_s;
-    const float nf = (float)t.n_factor;
     for (int i0 = wfirst; i0 < ns * 32; i0 += R * bd) {
         if (i0 != wfirst) load_round(i0);
 #pragma unroll
@@ -694,9 +732,10 @@ __device__ __forceinline__ void tail_once(int B, double moving_bin_size, const E
                     float r = 0.0f;
                     if (!t.degenerate) {
                         const int f = i / B, m = i - f * B;
-                        const bool ok = okf[f] && okm[m];
-                        r = pr_entry(jv[u], col[m], ok, jmin, nf);
-                        term = value_term(jv[u], ok, jmin, lcol[m], lfm[f], t);
+                        const bool take = okf[f] && okm[m] && jv[u] >= jmin;
+                        const double ljv = take ? log((double)jv[u]) : 0.0;
+                        r = pr_entry(take, ljv, lcol[m], t.n_factor);
+                        term = value_term(jv[u], take, ljv, lcol[m], lfm[f], t);
                     }
                     a.gpr[i] = r;
                 }
