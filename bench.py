@@ -13,6 +13,14 @@ flushed (a 256 MiB write) before every evaluation, outside the timed events.
          starting from an idle stream (parameters in from host memory, value and
          derivative back to host memory, launch latency and host wait included)
 
+Beside them, in the same line: the histogram pass's roofline, the serial CPU baseline
+(median of 6 after a 2 s warm-up), the same pair with every voxel a sample (full_grid),
+mean squares and correlation, a B-spline transform, one full three-level registration,
+the 64-pair batched registration (device-timed per-pair completion), and the batched +
+learned-initialiser form against the plain single-pair driver on held-out 128³ pairs
+(the committed weights). `--storage-study`, `--initnet` and `--gemm-study` run the
+512³ storage study, the initialiser's training study and its GEMM timings instead.
+
 --impl reference times the reference algorithm's CPU implementation on this host's
 cores (the C++ restatement under oracle/, all threads), since the Rust reference
 cannot be built here. Multi-GPU runs are independent replicas (one registration pair

@@ -6,6 +6,7 @@
 // (block stride).
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,6 +19,8 @@
 
 namespace mi {
 namespace {
+
+namespace cg = cooperative_groups;
 
 // Launch shapes: resident CTAs per SM the histogram and derivative kernels' register
 // budgets are sized for.
@@ -33,11 +36,29 @@ namespace {
 #define MI_HIST_PIPELINE 0
 #endif
 constexpr bool HIST_PIPELINE = MI_HIST_PIPELINE != 0;
+// 1: the derivative pass requests the next group of records before accumulating the
+// current one; 0: one group at a time.
+#ifndef MI_DERIV_PREFETCH
+#define MI_DERIV_PREFETCH 1
+#endif
+constexpr bool DERIV_PREFETCH = MI_DERIV_PREFETCH != 0;
+// Replicas of the split form's global histogram (see EvalArgs::reps).
+#ifndef MI_GHIST_REPS
+#define MI_GHIST_REPS 1
+#endif
+constexpr int GHIST_REPS = MI_GHIST_REPS;
+// Thread-block cluster size of the split form's histogram pass (its CTAs sum their
+// histograms over distributed shared memory before the global flush); 1: no cluster.
+#ifndef MI_HIST_CLUSTER
+#define MI_HIST_CLUSTER 1
+#endif
+constexpr int HIST_CLUSTER = MI_HIST_CLUSTER;
 // Samples the fast path cannot decide: 1 queues them and runs the exact chain after the
-// histogram phase's main loop (the loop then carries none of the exact chain's state),
-// 0 runs it inside the loop.
+// histogram phase's main loop, 0 runs it inside the loop (out of line, see
+// MI_EXACT_NOINLINE). Inside measured faster: a few exact samples per CTA, drained after
+// the loop, held back the CTA's flush by their dependent loads.
 #ifndef MI_EXACT_DEFERRED
-#define MI_EXACT_DEFERRED 1
+#define MI_EXACT_DEFERRED 0
 #endif
 // Histogram copies per CTA (coarse and fine parts) and the fine part's threshold
 // 2^-MI_HIST_FINE_T (see k_hist).
@@ -170,12 +191,16 @@ struct EvalArgs {
     double hist_inv;
     unsigned long long* ghist;
     unsigned long long* gcols = nullptr;  // B column sums of the joint part, flushed with it (or null)
+    // The global histogram (joint, counts, column sums) in `reps` replicas, rep_stride
+    // u64 apart: CTA b flushes into replica b mod reps, which spreads the flush's
+    // atomics over more addresses; the split form's tail sums the replicas. 1 elsewhere.
+    int reps = 1;
+    uint32_t rep_stride = 0;
     uint16_t* rec_bins;  // per sample: moving bin | fixed bin << 8 (0 = not valid)
     float* rec_f;
     float* rec_g;
     double* partials;
     double* vsum;  // value slice sums (value_slices(B))
-    float* gpr = nullptr;  // the pRatio·nFactor table (B² floats) the split form's tail leaves for k_deriv
     uint32_t* exq = nullptr;  // per-CTA queues of samples handed to the exact chain (exq_cap each)
     uint32_t exq_cap = 0;
     unsigned int* sync;
@@ -249,7 +274,7 @@ struct ExactQueue {
     uint32_t cap;
 };
 
-template <bool RECORD>
+template <bool RECORD, bool CLUSTER_FLUSH = false>
 __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArgs& a, unsigned int* sh,
                                            const SampleRange r, const ExactQueue exq = ExactQueue{nullptr, 0u}) {
     __shared__ unsigned int exq_count;
@@ -394,6 +419,40 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
         }
     }
     __syncthreads();
+    // this CTA's replica of the global histogram
+    const size_t rep_off = (size_t)(blockIdx.x % (unsigned)a.reps) * a.rep_stride;
+    unsigned long long* rep_hist = a.ghist + rep_off;
+    unsigned long long* rep_cols = a.gcols ? a.gcols + rep_off : nullptr;
+    if (CLUSTER_FLUSH) {
+        // The CTAs of a thread-block cluster sum their histograms over distributed
+        // shared memory: CTA rank r takes every bin i ≡ r (mod cluster size), reads
+        // that bin's copies in every CTA of the cluster and adds the cluster's sum into
+        // the global histogram once, so the global atomics are one cluster's worth, not
+        // one CTA's. Integer sums: the order does not matter.
+        cg::cluster_group cl = cg::this_cluster();
+        const unsigned int nr = cl.num_blocks(), rank = cl.block_rank();
+        cl.sync();  // every CTA's histogram is final
+        for (int i = (int)(rank * blockDim.x + threadIdx.x); i < nb; i += (int)(nr * blockDim.x)) {
+            unsigned long long v = 0ull, f = 0ull;
+            for (unsigned int q = 0; q < nr; ++q) {
+                const unsigned int* rs = cl.map_shared_rank(sh, q);
+                for (int c = 0; c < copies; ++c) v += rs[c * cstride + i];
+                if (i < B * B)
+                    for (int c = 0; c < fine_copies; ++c) f += rs[copies * cstride + c * fstride + i];
+            }
+            if (i < B * B) {
+                v = (v << a.fine_shift) + f;
+                if (a.gcols && v) atomicAdd(&colacc[i % B], v);
+            }
+            if (v) atomicAdd(&rep_hist[i], v);
+        }
+        __syncthreads();
+        if (a.gcols)
+            for (int m = threadIdx.x; m < B; m += blockDim.x)
+                if (colacc[m]) atomicAdd(&rep_cols[m], colacc[m]);
+        cl.sync();  // no CTA leaves while another still reads its shared memory
+        return;
+    }
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
         unsigned long long v = 0ull;
         for (int c = 0; c < copies; ++c) v += sh[c * cstride + i];
@@ -403,13 +462,13 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
             v = (v << a.fine_shift) + f;
             if (a.gcols && v) atomicAdd(&colacc[i % B], v);
         }
-        if (v) atomicAdd(&a.ghist[i], v);
+        if (v) atomicAdd(&rep_hist[i], v);
     }
     if (a.gcols) {
         // column marginals of the joint part, exact integer sums like the bins
         __syncthreads();
         for (int m = threadIdx.x; m < B; m += blockDim.x)
-            if (colacc[m]) atomicAdd(&a.gcols[m], colacc[m]);
+            if (colacc[m]) atomicAdd(&rep_cols[m], colacc[m]);
     }
 }
 
@@ -565,11 +624,16 @@ __device__ TailCtx tail_prepare(int B, double moving_bin_size, const EvalArgs& a
     return tail_finish(B, moving_bin_size, a, ts);
 }
 
-// A bin's pRatio·nFactor (mattes.rs:305-320): ln(jp/mm)·nFactor = (ln jv − ln col)·
-// nFactor, formed in FP64 from the bin's ln jv and its column's ln col and rounded once
-// to the FP32 table the derivative pass reads; 0 where the reference skips the bin.
-__device__ __forceinline__ float pr_entry(bool take, double ljv, double lcol, double n_factor) {
-    return take ? (float)((ljv - lcol) * n_factor) : 0.0f;
+// A bin's pRatio·nFactor (mattes.rs:305-320): ln(jp/mm)·nFactor = ln(jv/col)·nFactor,
+// 0 where the reference skips the bin. The table the derivative pass reads is FP32, and
+// so is this entry: the logarithm of the ratio of the two exact integer counts, taken
+// with the fast reciprocal and logf (a few units of 2^-24). Forming it in FP64 cost every
+// derivative CTA 4 µs of FP64 logarithms on the 32-bin workload; in FP32 the table
+// differs from the FP64 one by ≤ 4·10⁻⁷ of its largest entry, which moves the
+// derivative by far less than the FP32 per-sample arithmetic already does. The value's
+// logarithms stay FP64 (value_term).
+__device__ __forceinline__ float pr_entry(bool take, unsigned long long jv, unsigned long long col, float nf) {
+    return take ? logf(__fdividef((float)jv, (float)col)) * nf : 0.0f;
 }
 
 // pRatio·nFactor of every bin into pr (shared memory). The entry's (row, column)
@@ -579,10 +643,10 @@ __device__ void pr_table(int B, const TailCtx& t, const TailSmem& ts, float* pr)
     const unsigned long long jmin = *ts.jmin;
     int f = (int)threadIdx.x / B, m = (int)threadIdx.x - f * B;
     const int df = (int)blockDim.x / B, dm = (int)blockDim.x - df * B;
+    const float nf = (float)t.n_factor;
     for (int i = threadIdx.x; i < B2; i += blockDim.x) {
         const unsigned long long jv = ts.hist[i];
-        const bool take = ts.okf[f] && ts.okm[m] && jv >= jmin;
-        pr[i] = pr_entry(take, take ? log((double)jv) : 0.0, ts.lcol[m], t.n_factor);
+        pr[i] = pr_entry(ts.okf[f] && ts.okm[m] && jv >= jmin, jv, ts.col[m], nf);
         f += df;
         m += dm;
         if (m >= B) {
@@ -669,15 +733,14 @@ __device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
 }
 
 // ---------------------------------------------------------------------------
-// The split form's tail, once per evaluation: run by the whole CTA of the histogram
-// pass that flushes last (no other CTA waits for it). It reads the finished global
-// histogram from L2 once, leaves the pRatio·nFactor table in global memory (a.gpr)
-// for the derivative pass, writes value and valid into a.result (and, for the
-// value-only evaluation, into the mapped mirror with the sequence number), and clears
-// the global histogram, its column sums and the arrival counter for the next
-// evaluation. Every quantity is formed by the same functions as the per-CTA tail
-// (tail_scalars, least_joint, pr_entry, value_term, slice_sum, fold_slices), so the
-// table and the value have the same bits in every launch form.
+// The value-only evaluation's tail, once: run by the whole CTA of the histogram pass
+// that flushes last (no other CTA waits for it). It reads the finished global
+// histogram from L2 once, writes value and valid into a.result and (when `mirror`)
+// into the mapped mirror with the sequence number, and clears the global histogram,
+// its column sums and the arrival counter for the next evaluation. Every quantity is
+// formed by the same functions as the other tails (tail_scalars, margin_terms,
+// least_joint, value_term, slice_sum, fold_slices), so the value has the same bits in
+// every launch form.
 // ---------------------------------------------------------------------------
 __host__ __device__ inline size_t tail_once_smem(int B) {
     return (size_t)4 * B * 8 + (size_t)value_slices(B) * 8 + (((size_t)2 * B + 7) & ~(size_t)7) + 8;
@@ -702,17 +765,28 @@ __device__ __forceinline__ void tail_once(int B, double moving_bin_size, const E
     // are requested together with the column sums and fixed counts.
     constexpr int R = 2;
     unsigned long long jv[R];
+    // each bin, count and column sum is the sum of its replicas (integers: any order)
+    const int reps = a.reps;
+    const size_t rs = a.rep_stride;
     auto load_round = [&](int i0) {
 #pragma unroll
         for (int u = 0; u < R; ++u) {
             const int i = i0 + u * bd + lane;
-            jv[u] = i < B2 ? __ldcg(a.ghist + i) : 0ull;
+            unsigned long long v = 0ull;
+            if (i < B2)
+                for (int r = 0; r < reps; ++r) v += __ldcg(a.ghist + r * rs + i);
+            jv[u] = v;
         }
     };
     load_round(wfirst);
     for (int i = threadIdx.x; i < B; i += bd) {
-        col[i] = __ldcg(a.gcols + i);
-        cnt[i] = __ldcg(a.ghist + B2 + i);
+        unsigned long long c = 0ull, k = 0ull;
+        for (int r = 0; r < reps; ++r) {
+            c += __ldcg(a.gcols + r * rs + i);
+            k += __ldcg(a.ghist + r * rs + B2 + i);
+        }
+        col[i] = c;
+        cnt[i] = k;
     }
     __syncthreads();
     const TailCtx t = tail_scalars(B, col, cnt, a.hist_inv, moving_bin_size);
@@ -728,16 +802,10 @@ __device__ __forceinline__ void tail_once(int B, double moving_bin_size, const E
             if (iw < ns * 32) {
                 const int i = iw + lane;
                 double term = 0.0;
-                if (i < B2) {
-                    float r = 0.0f;
-                    if (!t.degenerate) {
-                        const int f = i / B, m = i - f * B;
-                        const bool take = okf[f] && okm[m] && jv[u] >= jmin;
-                        const double ljv = take ? log((double)jv[u]) : 0.0;
-                        r = pr_entry(take, ljv, lcol[m], t.n_factor);
-                        term = value_term(jv[u], take, ljv, lcol[m], lfm[f], t);
-                    }
-                    a.gpr[i] = r;
+                if (i < B2 && !t.degenerate) {
+                    const int f = i / B, m = i - f * B;
+                    const bool take = okf[f] && okm[m] && jv[u] >= jmin;
+                    term = value_term(jv[u], take, take ? log((double)jv[u]) : 0.0, lcol[m], lfm[f], t);
                 }
                 term = slice_sum(term);
                 if (lane == 0) vs[iw >> 5] = term;
@@ -758,8 +826,10 @@ __device__ __forceinline__ void tail_once(int B, double moving_bin_size, const E
             }
         }
     }
-    for (int i = threadIdx.x; i < B2 + B; i += bd) a.ghist[i] = 0ull;
-    for (int i = threadIdx.x; i < B; i += bd) a.gcols[i] = 0ull;
+    for (int r = 0; r < reps; ++r) {
+        for (int i = threadIdx.x; i < B2 + B; i += bd) a.ghist[r * rs + i] = 0ull;
+        for (int i = threadIdx.x; i < B; i += bd) a.gcols[r * rs + i] = 0ull;
+    }
     if (threadIdx.x == 0) a.sync[1] = 0u;
     if (mirror) publish_seq(a);
 }
@@ -862,6 +932,18 @@ __device__ __forceinline__ void stream_records(const SamplerParams& P, const Eva
     auto one = [&](uint32_t bins, float f, float gx, float gy, float gz, uint32_t flat) {
         if (bins & 0xffu) accumulate_moments(P, pr, B, bins & 0xffu, bins >> 8, f, gx, gy, gz, flat, acc);
     };
+    if (!DERIV_PREFETCH) {
+        // one group at a time (more resident CTAs carry the latency)
+        while (q < ngroups) {
+            one(cur.b.x & 0xffffu, cur.f.x, cur.gx.x, cur.gy.x, cur.gz.x, cur.fl.x);
+            one(cur.b.x >> 16, cur.f.y, cur.gx.y, cur.gy.y, cur.gz.y, cur.fl.y);
+            one(cur.b.y & 0xffffu, cur.f.z, cur.gx.z, cur.gy.z, cur.gz.z, cur.fl.z);
+            one(cur.b.y >> 16, cur.f.w, cur.gx.w, cur.gy.w, cur.gz.w, cur.fl.w);
+            q += stride;
+            if (q < ngroups) load_group(a, q, cur);
+        }
+        return;
+    }
     while (q < ngroups) {
         const uint32_t qn = q + stride;
         RecordGroup nxt;
@@ -900,26 +982,91 @@ __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double
     return t;
 }
 
-// The split form's derivative pass: the table the histogram pass's tail left in
-// a.gpr is copied into shared memory (its loads issued together with the first record
-// group's), then this CTA's records are streamed into the moments. A degenerate
-// evaluation's table is all zeros, so its moments are zero.
-__host__ __device__ inline size_t stream_smem(int B) { return 32 * (size_t)NMOM * sizeof(double) + (size_t)B * B * sizeof(float); }
+// The split form's derivative pass with its own tail. Every CTA forms the pRatio·nFactor
+// table itself from the integer histogram, in one round of requests: this thread's
+// bins, the column sums and fixed counts, and the first group of its records all go out
+// together; the marginals' totals and ε flags, their FP64 logarithms and the least
+// passing joint count follow (tail_scalars, margin_terms, least_joint), then each
+// thread's bins' entries, one FP64 logarithm each (pr_entry). The value's 32-bin
+// slices are summed where they fall: the warp holding slice u in CTA u (u < the CTA
+// count; the rest in CTA u mod count) forms its terms from the same logarithms
+// (value_term, slice_sum) into a.vsum, and the last CTA folds them (fold_slices), so
+// the value has the bits of every other form. No CTA waits for another before its
+// record stream, and the histogram pass ends at its flush.
+__host__ __device__ inline size_t stream_smem(int B) {
+    return 32 * (size_t)NMOM * sizeof(double) + (size_t)B * B * sizeof(float) + (size_t)4 * B * 8 +
+           (((size_t)2 * B + 7) & ~(size_t)7) + 8;
+}
 
-__device__ void stream_phase(const SamplerParams& P, const EvalArgs& a, double* dsh, const GroupWork w) {
-    const int B2 = P.bins * P.bins;
+// Returns the tail state (for the last CTA's fold).
+__device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, double* dsh, const GroupWork w) {
+    const int B = P.bins, B2 = B * B;
     double* red = dsh;
     float* pr = reinterpret_cast<float*>(dsh + 32 * NMOM);
+    unsigned long long* col = reinterpret_cast<unsigned long long*>(pr + B2);
+    unsigned long long* cnt = col + B;
+    double* lcol = reinterpret_cast<double*>(cnt + B);
+    double* lfm = lcol + B;
+    uint8_t* okm = reinterpret_cast<uint8_t*>(lfm + B);
+    uint8_t* okf = okm + B;
+    unsigned long long* jmin_s = reinterpret_cast<unsigned long long*>(okm + ((2 * B + 7) & ~7));
+    const int lane = threadIdx.x & 31;
+    const int bd = (int)blockDim.x;
+    const int wfirst = (int)threadIdx.x - lane;
+    const int ns = value_slices(B);
     float acc[NMOM];
 #pragma unroll
     for (int i = 0; i < NMOM; ++i) acc[i] = 0.0f;
     const uint32_t q = w.begin + w.first;
+    // one round of requests: the first R·bd bins (bin i0 + u·bd + lane for warp base
+    // i0), the margins, the first record group
+    constexpr int R = 4;
+    unsigned long long jv[R];
+    auto load_round = [&](int i0) {
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int i = i0 + u * bd + lane;
+            jv[u] = i < B2 ? __ldcg(a.ghist + i) : 0ull;
+        }
+    };
+    load_round(wfirst);
+    for (int i = threadIdx.x; i < B; i += bd) {
+        col[i] = __ldcg(a.gcols + i);
+        cnt[i] = __ldcg(a.ghist + B2 + i);
+    }
     RecordGroup cur;
     if (q < w.end) load_group(a, q, cur);
-    for (int i = threadIdx.x; i < B2; i += blockDim.x) pr[i] = __ldcg(a.gpr + i);
     __syncthreads();
-    stream_records(P, a, pr, q, w.end, w.stride, cur, acc);
+    const TailCtx t = tail_scalars(B, col, cnt, a.hist_inv, P.moving_bin_size);
+    if ((int)threadIdx.x < B) margin_terms(threadIdx.x, col, cnt, t, okm, okf, lcol, lfm);
+    if (threadIdx.x == blockDim.x - 1) *jmin_s = least_joint(t.dt);
+    __syncthreads();
+    const unsigned long long jmin = *jmin_s;
+    const float nf = (float)t.n_factor;
+    const int units = (int)w.units, unit = (int)w.unit;
+    for (int i0 = wfirst; i0 < ns * 32; i0 += R * bd) {
+        if (i0 != wfirst) load_round(i0);
+#pragma unroll
+        for (int u = 0; u < R; ++u) {
+            const int iw = i0 + u * bd;  // warp-uniform: the slice's first bin
+            if (iw < ns * 32) {
+                const int i = iw + lane;
+                const int f = i / B, m = i - f * B;
+                const bool take = i < B2 && !t.degenerate && okf[f] && okm[m] && jv[u] >= jmin;
+                if (i < B2) pr[i] = pr_entry(take, jv[u], col[m], nf);
+                const int sl = iw >> 5;
+                if (sl % units == unit) {
+                    const double term =
+                        slice_sum(take ? value_term(jv[u], true, log((double)jv[u]), lcol[m], lfm[f], t) : 0.0);
+                    if (lane == 0) a.vsum[sl] = term;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (!t.degenerate) stream_records(P, a, pr, q, w.end, w.stride, cur, acc);
     store_moments(acc, red, w.part, w.part_stride);
+    return t;
 }
 
 // Run by the last CTA to finish the derivative phase: fold the `count` partials of

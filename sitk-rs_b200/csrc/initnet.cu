@@ -690,12 +690,26 @@ mi_status mi_gemm_bf16_tn(mi_context* ctx, int M, int N, int K, const void* A, i
     unsigned int* err = nullptr;
     MI_CHECK_CUDA(ctx, cudaMalloc(&err, sizeof(unsigned int)));
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned int), ctx->stream);
-    if (e == cudaSuccess)
-        e = mi::gemm_bf16_tn(M, N, K, static_cast<const __nv_bfloat16*>(A), lda, static_cast<const __nv_bfloat16*>(B),
-                             ldb, C, ldc, err, ctx->stream);
+    // a product whose M × N tiles alone would leave most SMs idle is split over K into
+    // partial products summed in slice order, as the network's layers do
+    const int S = ldc == N ? mi::k_splits(M, N, K) : 1;
+    float* slices = nullptr;
+    if (e == cudaSuccess && S > 1) e = cudaMalloc(&slices, (size_t)S * M * N * sizeof(float));
+    const auto* a16 = static_cast<const __nv_bfloat16*>(A);
+    const auto* b16 = static_cast<const __nv_bfloat16*>(B);
+    if (e == cudaSuccess && S > 1) {
+        e = mi::gemm_dispatch(M, N, K, a16, lda, b16, ldb, slices, N, S, err, ctx->stream);
+        if (e == cudaSuccess) {
+            mi::k_sum_slices<<<mi::grid1((int64_t)M * N), 256, 0, ctx->stream>>>(slices, S, (int64_t)M * N, C);
+            e = cudaGetLastError();
+        }
+    } else if (e == cudaSuccess) {
+        e = mi::gemm_bf16_tn(M, N, K, a16, lda, b16, ldb, C, ldc, err, ctx->stream);
+    }
     unsigned int h = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(slices);
     cudaFree(err);
     if (e != cudaSuccess) return mi::cuda_status(ctx, e, "mi_gemm_bf16_tn");
     if (h) return mi::set_error(ctx, MI_ERR_TIMEOUT, "tensor-core GEMM: an mbarrier wait gave up");

@@ -99,7 +99,6 @@ struct Workspace {
     unsigned long long* hist = nullptr;  // [bins*bins] joint (2^-32 fixed point), [bins] fixed marginal, [1] valid
     double* partials = nullptr;          // [grid_deriv][12]
     double* vsum = nullptr;              // value slice sums
-    float* gpr = nullptr;                // pRatio·nFactor table the split form's tail leaves for k_deriv
     uint32_t* exq = nullptr;             // per-CTA queues of samples for the exact chain
     uint32_t exq_cap_hist = 0, exq_cap_eval = 0;  // queue length per CTA of k_hist / of the fused kernel
     double* result = nullptr;            // [2 + MI_MAX_PARAMS]: value, valid, derivative

@@ -7,22 +7,23 @@
 //            in shared memory as u32 fixed point (native shared atomics), flushed
 //            with the joint part's column sums into global u64 counters. Integer adds
 //            are exact, so the histogram does not depend on the order. Each sample also
-//            leaves an 18-byte record (both Parzen bins, Parzen fraction, moving
-//            gradient) for pass 2. The CTA that flushes last forms the tail once
-//            (registration/mattes.rs:273-328: normalisation, marginals, −MI and the
-//            pRatio·nFactor table) from the integer histogram, leaves the table in
-//            global memory, writes value and valid, and clears the histogram for the
-//            next evaluation.
-//   k_deriv  launched as a programmatic dependent of k_hist. Every CTA copies the table
-//            into shared memory, then streams its records → 12 moments
-//            A[d] = Σ w g_d, B[d][e] = Σ w g_d (x_e − x_ref,e), w = Σ_taps B₃′·pRatio
-//            (the form of the reference's mattes_deriv, cuda/ops/mattes.rs:319-381),
-//            FP32 per thread and FP64 from the warp reduction on, in a fixed
-//            shuffle/tree order into per-CTA partials. The last CTA folds the partials
-//            in a fixed order, contracts them with the transform's Jacobian form
-//            (registration/cuda.rs:505-524) and writes value, valid and derivative into
-//            the host's mapped mirror with a sequence number.
-// A value-only evaluation is k_hist alone: its tail publishes the result.
+//            leaves an 18-byte record (both Parzen bins, Parzen fraction, index-space
+//            gradient) for pass 2. Samples whose decisions the fast path cannot take
+//            are queued and run through the exact FP64 chain after the main loop.
+//   k_deriv  launched as a programmatic dependent of k_hist. Every CTA forms the tail
+//            itself from the integer histogram (registration/mattes.rs:273-328:
+//            normalisation, marginals and the pRatio·nFactor table, FP64 logarithms),
+//            sums the −MI slices that fall to it, then streams its records → 12
+//            moments A[j] = Σ w g_j, B[j][e] = Σ w g_j (x_e − x_ref,e), w = Σ_taps
+//            B₃′·pRatio (the form of the reference's mattes_deriv,
+//            cuda/ops/mattes.rs:319-381), FP32 per thread and FP64 from the warp
+//            reduction on, in a fixed shuffle/tree order into per-CTA partials. The last
+//            CTA folds the slices and the partials in a fixed order, turns the moments
+//            into physical space, contracts them with the transform's Jacobian form
+//            (registration/cuda.rs:505-524), writes value, valid and derivative into the
+//            host's mapped mirror with a sequence number, and clears the histogram.
+// A value-only evaluation is k_hist alone: the CTA that flushes last forms the tail
+// and publishes the result.
 // Every reduction order is a function of the launch shape alone, so repeated
 // evaluations are bit-identical. No kernel waits on another CTA.
 
@@ -59,7 +60,7 @@ namespace {
 //   the moments, writes the derivative, re-zeroes the global histogram and resets
 //   the counters. The value-only form runs the tail in CTA 0 alone.
 // The split form (k_hist, then k_deriv) does the same work with a kernel boundary in
-// place of the barrier, and forms the tail once, in k_hist's last CTA.
+// place of the barrier.
 // ---------------------------------------------------------------------------
 // This CTA's queue of samples for the exact chain (k_hist, k_eval: a grid-stride walk,
 // so at most exq_cap = ceil(n / (grid·block))·block samples per CTA).
@@ -101,10 +102,9 @@ k_eval(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobian
         for (int i = threadIdx.x; i < B; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
-// Histogram pass of the split form. The CTA that flushes last forms the tail once
-// (tail_once): the pRatio·nFactor table for k_deriv and the value; for the value-only
-// evaluation (RECORD false) it also publishes the result, so that evaluation is this
-// one launch.
+// Histogram pass of the split form. For a value-only evaluation (RECORD false) the CTA
+// that flushes last forms the tail (tail_once) and publishes the result, so that
+// evaluation is this one launch.
 size_t hist_kernel_smem(int B) { return std::max(hist_smem(B), tail_once_smem(B)); }
 
 template <bool RECORD>
@@ -112,30 +112,30 @@ __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
 k_hist(const __grid_constant__ SamplerParams P, EvalArgs a) {
     extern __shared__ __align__(16) unsigned int sh[];
     pdl_launch_dependents();
-    hist_phase<RECORD>(P, a, sh, grid_samples(a.n), exact_queue(a));
-    if (!last_to_arrive(a.sync + 1)) return;
-    tail_once(P.bins, P.moving_bin_size, a, reinterpret_cast<unsigned char*>(sh), !RECORD);
+    hist_phase<RECORD, (HIST_CLUSTER > 1)>(P, a, sh, grid_samples(a.n), exact_queue(a));
+    // the value+derivative evaluation's tail is formed by k_deriv's CTAs; a value-only
+    // evaluation ends here, with its tail in the CTA that flushes last
+    if (RECORD || !last_to_arrive(a.sync + 1)) return;
+    tail_once(P.bins, P.moving_bin_size, a, reinterpret_cast<unsigned char*>(sh), true);
 }
 
-// Derivative pass of the split form, a programmatic dependent of k_hist: the moments
-// of this CTA's records with the table k_hist's tail left; the last CTA folds them,
-// contracts them with the Jacobian form and publishes value, valid and derivative.
+// Derivative pass of the split form, a programmatic dependent of k_hist: each CTA forms
+// the tail and its value slices, then the moments of its records (stream_phase); the
+// last CTA folds them, contracts them with the Jacobian form and publishes value, valid
+// and derivative.
 __global__ void __launch_bounds__(DERIV_BLOCK, DERIV_MIN_BLOCKS)
 k_deriv(const __grid_constant__ SamplerParams P, const __grid_constant__ JacobianForm J, EvalArgs a) {
     extern __shared__ double dsh[];
     pdl_wait();
-    stream_phase(P, a, dsh, grid_groups(a));
+    const TailCtx t = stream_phase(P, a, dsh, grid_groups(a));
     if (!last_to_arrive(a.sync)) return;
-    // k_hist's tail wrote value and valid (value DBL_MAX when degenerate)
-    const double r0 = __ldcg(a.result), r1 = __ldcg(a.result + 1);
-    deriv_fold(P, J, a, r0 == DBL_MAX, a.partials, gridDim.x);
-    if (threadIdx.x == 0 && a.result_host) {
-        a.result_host[0] = r0;
-        a.result_host[1] = r1;
-        a.result_host[RESULT_ERR] = 0.0;
-    }
+    // every CTA has read the histogram and written its value slices and moments
+    deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
+    if (threadIdx.x < 32) fold_value(P.bins, a, t);
     publish_seq(a);
     if (threadIdx.x == 0) a.sync[0] = 0u;
+    for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
+    for (int i = threadIdx.x; i < P.bins; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
 // Per-sample decisions of the same sampler the kernels use, for the exactness tests.
@@ -292,6 +292,37 @@ mi_status minmax(mi_context* ctx, const float* vals, const uint32_t* idx, const 
     return MI_OK;
 }
 
+// The global histogram's replicas: each B² joint + B counts + B column sums u64, padded
+// to whole 256-byte blocks.
+uint32_t ghist_rep_stride(int B) { return (uint32_t)(((size_t)B * B + 2 * B + 31) & ~(size_t)31); }
+size_t ghist_bytes(int B) { return (size_t)GHIST_REPS * ghist_rep_stride(B) * sizeof(unsigned long long); }
+
+// The split form's histogram grid: enough CTAs for the samples, at most as many as are
+// resident at once, in whole thread-block clusters of HIST_CLUSTER (bounded by the
+// clusters the device can hold at once with this kernel's shape).
+int hist_grid(mi_context* ctx, int64_t n, int occ, int B) {
+    int g = grid_for(n, HIST_BLOCK, ctx->num_sms * std::max(occ, 1));
+    if (HIST_CLUSTER <= 1) return g;
+    int clusters = (g + HIST_CLUSTER - 1) / HIST_CLUSTER;
+    cudaLaunchConfig_t hc = {};
+    hc.gridDim = dim3((unsigned)(clusters * HIST_CLUSTER));
+    hc.blockDim = dim3(HIST_BLOCK);
+    hc.dynamicSmemBytes = hist_kernel_smem(B);
+    cudaLaunchAttribute hattr[1];
+    hattr[0].id = cudaLaunchAttributeClusterDimension;
+    hattr[0].val.clusterDim.x = HIST_CLUSTER;
+    hattr[0].val.clusterDim.y = 1;
+    hattr[0].val.clusterDim.z = 1;
+    hc.attrs = hattr;
+    hc.numAttrs = 1;
+    int active = 0;
+    if (cudaOccupancyMaxActiveClusters(&active, k_hist<true>, &hc) == cudaSuccess && active > 0)
+        clusters = std::min(clusters, active);
+    else
+        cudaGetLastError();
+    return std::max(1, clusters) * HIST_CLUSTER;
+}
+
 void free_metric(mi_metric* m) {
     if (!m) return;
     if (m->mtex) cudaDestroyTextureObject(m->mtex);
@@ -304,7 +335,6 @@ void free_metric(mi_metric* m) {
     cudaFree(m->ws.hist);
     cudaFree(m->ws.partials);
     cudaFree(m->ws.vsum);
-    cudaFree(m->ws.gpr);
     cudaFree(m->ws.exq);
     cudaFree(m->ws.result);
     cudaFree(m->ws.done_counter);
@@ -503,12 +533,15 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.hist_inv = std::ldexp(1.0, -ws.fine_scale_log2);
     a.ghist = ws.hist;
     a.gcols = ws.hist + B * B + B;
+    // the split form's histogram pass spreads its flush over replicas; the fused form
+    // (whose CTAs each read the histogram) keeps one
+    a.reps = ws.fused || want_derivative ? 1 : GHIST_REPS;
+    a.rep_stride = ghist_rep_stride(B);
     a.rec_bins = want_derivative ? ws.rec_bins : nullptr;
     a.rec_f = want_derivative ? ws.rec_f : nullptr;
     a.rec_g = want_derivative ? ws.rec_g : nullptr;
     a.partials = ws.partials;
     a.vsum = ws.vsum;
-    a.gpr = ws.gpr;
     a.exq = ws.exq;
     a.exq_cap = ws.fused ? ws.exq_cap_eval : ws.exq_cap_hist;
     a.sync = ws.done_counter;
@@ -542,10 +575,25 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
             MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_eval<false>, P, J, a));
         if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
     } else {
-        if (want_derivative)
-            k_hist<true><<<ws.grid_hist, HIST_BLOCK, hist_kernel_smem(B), st>>>(P, a);
-        else
-            k_hist<false><<<ws.grid_hist, HIST_BLOCK, hist_kernel_smem(B), st>>>(P, a);
+        {
+            // thread-block clusters of HIST_CLUSTER CTAs (the grid is a multiple of it)
+            cudaLaunchConfig_t hc = {};
+            hc.gridDim = dim3((unsigned)ws.grid_hist);
+            hc.blockDim = dim3(HIST_BLOCK);
+            hc.dynamicSmemBytes = hist_kernel_smem(B);
+            hc.stream = st;
+            cudaLaunchAttribute hattr[1];
+            hattr[0].id = cudaLaunchAttributeClusterDimension;
+            hattr[0].val.clusterDim.x = HIST_CLUSTER;
+            hattr[0].val.clusterDim.y = 1;
+            hattr[0].val.clusterDim.z = 1;
+            hc.attrs = hattr;
+            hc.numAttrs = HIST_CLUSTER > 1 ? 1 : 0;
+            if (want_derivative)
+                MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&hc, k_hist<true>, P, a));
+            else
+                MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&hc, k_hist<false>, P, a));
+        }
         if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
         if (want_derivative) {
             // launched as a programmatic dependent of k_hist (no event between them), so
@@ -600,7 +648,7 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         // a barrier gave up: clear the counters, the error word and the histogram
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.result, 0, RESULT_DOUBLES * sizeof(double), st));
-        MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + 2 * B) * 8, st));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.hist, 0, ghist_bytes(B), st));
         MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
         return set_error(ctx, MI_ERR_TIMEOUT, "a grid barrier of the fused evaluation timed out");
     }
@@ -870,7 +918,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     ws.can_fuse = coop != 0 && resident >= 1;
     ws.fused = false;
     ws.grid_eval = ws.can_fuse ? grid_for(m->n_samples, HIST_BLOCK, resident) : 0;
-    ws.grid_hist = grid_for(m->n_samples, HIST_BLOCK, ctx->num_sms * std::max(occ_h, 1));
+    ws.grid_hist = hist_grid(ctx, m->n_samples, occ_h, B);
     ws.grid_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
     ws.block_hist = HIST_BLOCK;
     ws.block_deriv = DERIV_BLOCK;
@@ -906,19 +954,18 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         TRY_CUDA(cudaMalloc(&ws.rec_g, 3 * ns * sizeof(float)));
     }
     // joint B², fixed counts B, then the joint part's B column sums
-    TRY_CUDA(cudaMalloc(&ws.hist, (size_t)(B * B + 2 * B) * 8));
-    TRY_CUDA(cudaMemsetAsync(ws.hist, 0, (size_t)(B * B + 2 * B) * 8, st));
+    TRY_CUDA(cudaMalloc(&ws.hist, ghist_bytes(B)));
+    TRY_CUDA(cudaMemsetAsync(ws.hist, 0, ghist_bytes(B), st));
     // partials serve both forms: the split form's k_deriv grid and, should the form
     // be switched, the fused grid
     {
         const int pgrid = std::max(ws.grid_deriv, std::max(ws.grid_eval,
             grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1))));
-        ws.grid_split_hist = grid_for(m->n_samples, HIST_BLOCK, ctx->num_sms * std::max(occ_h, 1));
+        ws.grid_split_hist = ws.grid_hist;
         ws.grid_split_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
         TRY_CUDA(cudaMalloc(&ws.partials, (size_t)pgrid * NMOM * 8));
     }
     TRY_CUDA(cudaMalloc(&ws.vsum, (size_t)value_slices(B) * 8));
-    TRY_CUDA(cudaMalloc(&ws.gpr, (size_t)B * B * sizeof(float)));
     {
         // a grid-stride walk gives a CTA at most ceil(n / (grid·block))·block samples
         auto cap = [&](int grid) -> uint32_t {

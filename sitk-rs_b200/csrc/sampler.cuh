@@ -378,8 +378,10 @@ __device__ __forceinline__ int finish_fast(const SamplerParams& P, const Prep& p
 // continuous index, inside test, mask rounding, FP64 trilinear value and Parzen bin
 // (every decision the host's), and, for GRAD, the FP32 index-space gradient of the
 // interpolant on the eight corners the value read.
+// The exact chain as a real call: the callers' loops then keep only the fast path's
+// registers live, and the call's spills happen only for the rare samples that take it.
 #ifndef MI_EXACT_NOINLINE
-#define MI_EXACT_NOINLINE 0
+#define MI_EXACT_NOINLINE 1
 #endif
 #if MI_EXACT_NOINLINE
 #define MI_EXACT_INLINE __noinline__
