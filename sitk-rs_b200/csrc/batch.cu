@@ -323,6 +323,7 @@ mi_status seed_pairs(mi_batch* b, const mi_rsgd_config& cfg, const double* param
         s = transform_form(b->kind, pp, b->nparams, fp.empty() ? nullptr : fp.data(), (int)fp.size(), &f);
         if (s != MI_OK) return s;
         pd.P = m->base;
+        pd.P.brick_bl = 0;  // the batch walks the sample list by grid index
         if (!point_map_fill(pd.P, f.stage, 1)) return set_error(b->ctx, MI_ERR_INVALID_ARGUMENT, "non-finite point map");
         pd.active = 1;
         pd.evaluations = 0;

@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 
 #include "internal.h"
@@ -25,6 +27,22 @@ mi_status cuda_status(mi_context* ctx, cudaError_t e, const char* where) {
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) s = MI_ERR_NO_DEVICE;
     std::string msg = std::string(where) + ": " + cudaGetErrorString(e);
     return set_error(ctx, s, msg);
+}
+
+// A kernel's dynamic shared-memory limit is a property of the function on the
+// current device, shared by every metric in the process: it is only ever raised,
+// so a metric created later with a smaller need does not shrink it under an
+// earlier one.
+mi_status raise_smem_limit(mi_context* ctx, const void* fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> lim;
+    std::lock_guard<std::mutex> g(mu);
+    size_t& cur = lim[{ctx->device, fn}];
+    if (bytes <= cur) return MI_OK;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "cudaFuncSetAttribute");
+    cur = bytes;
+    return MI_OK;
 }
 
 }  // namespace mi

@@ -130,11 +130,11 @@ int hist_fine_copies(int B) {
 }
 // The copies, then B u64 column sums of the CTA's histogram (used when the launch
 // flushes column marginals, EvalArgs::gcols).
-size_t hist_smem(int B) {
-    return ((size_t)hist_copies(B) * hist_copy_stride(B) + (size_t)hist_fine_copies(B) * hist_fine_stride(B)) *
-               sizeof(unsigned int) +
+__host__ __device__ inline size_t hist_region_bytes(int B, int copies, int fine_copies) {
+    return ((size_t)copies * hist_copy_stride(B) + (size_t)fine_copies * hist_fine_stride(B)) * sizeof(unsigned int) +
            (size_t)B * sizeof(unsigned long long);
 }
+size_t hist_smem(int B) { return hist_region_bytes(B, hist_copies(B), hist_fine_copies(B)); }
 // Shared memory of the tail (see TailSmem).
 constexpr int TAIL_BLOCK = 256;
 __host__ __device__ inline int tail_groups(int B) { return TAIL_BLOCK / B; }
@@ -213,6 +213,15 @@ struct EvalArgs {
     // the evaluation's sequence number, written into result_host's last slot after a
     // system-scope fence once everything else is there (the host may poll it)
     unsigned long long seq = 0;
+    // the single-metric evaluation's brick layout (brick.cuh): a code per padded
+    // sample, the run (brick) of every chunk of 32, each run's packed brick coordinates
+    // and x(brick origin) − x_ref
+    const uint32_t* codes = nullptr;
+    const uint32_t* chunk_run = nullptr;
+    const uint32_t* run_brick = nullptr;
+    const float4* run_xbase = nullptr;
+    uint32_t nchunks = 0;
+    float4* rec4 = nullptr;  // brick layout's records: gx, gy, gz, Parzen fraction per padded sample
 };
 constexpr int RESULT_ERR = 2 + MI_MAX_PARAMS;  // result slot holding the error word
 constexpr int RESULT_DOUBLES = RESULT_ERR + 2;
@@ -957,6 +966,20 @@ __device__ __forceinline__ void stream_records(const SamplerParams& P, const Eva
     }
 }
 
+// The record source of a derivative phase: how a four-sample group is requested and
+// streamed. GridRecords reads the grid-index layout (sample list of flat indices);
+// the brick layout's source is BrickRecords (brick.cuh).
+struct GridRecords {
+    using Group = RecordGroup;
+    static __device__ __forceinline__ void load(const EvalArgs& a, uint32_t q, Group& g) { load_group(a, q, g); }
+    static __device__ __forceinline__ void stream(const SamplerParams& P, const EvalArgs& a, const float* pr,
+                                                  uint32_t q, uint32_t ngroups, uint32_t stride, Group cur,
+                                                  float* acc) {
+        stream_records(P, a, pr, q, ngroups, stride, cur, acc);
+    }
+};
+
+template <class Src = GridRecords>
 __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double* dsh, const GroupWork w) {
     const int B = P.bins;
     double* red = dsh;  // 32 * NMOM
@@ -967,17 +990,17 @@ __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double
 #pragma unroll
     for (int i = 0; i < NMOM; ++i) acc[i] = 0.0f;
     const uint32_t q = w.begin + w.first;
-    RecordGroup cur;
+    typename Src::Group cur;
     // the histogram's loads go out first (every CTA waits on them); the first record
     // group's loads then overlap the rest of the tail
     tail_fetch(B, a, ts);
-    if (q < w.end) load_group(a, q, cur);
+    if (q < w.end) Src::load(a, q, cur);
     const TailCtx t = tail_finish(B, P.moving_bin_size, a, ts);
     if (!t.degenerate) pr_table(B, t, ts, pr);
     __syncthreads();
     // a warp with a value slice sums it before its share of the records
     if (!t.degenerate) value_slices_share(B, a, t, ts, w.unit, w.units);
-    if (!t.degenerate) stream_records(P, a, pr, q, w.end, w.stride, cur, acc);
+    if (!t.degenerate) Src::stream(P, a, pr, q, w.end, w.stride, cur, acc);
     store_moments(acc, red, w.part, w.part_stride);
     return t;
 }
@@ -999,6 +1022,7 @@ __host__ __device__ inline size_t stream_smem(int B) {
 }
 
 // Returns the tail state (for the last CTA's fold).
+template <class Src = GridRecords>
 __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, double* dsh, const GroupWork w) {
     const int B = P.bins, B2 = B * B;
     double* red = dsh;
@@ -1034,8 +1058,8 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
         col[i] = __ldcg(a.gcols + i);
         cnt[i] = __ldcg(a.ghist + B2 + i);
     }
-    RecordGroup cur;
-    if (q < w.end) load_group(a, q, cur);
+    typename Src::Group cur;
+    if (q < w.end) Src::load(a, q, cur);
     __syncthreads();
     const TailCtx t = tail_scalars(B, col, cnt, a.hist_inv, P.moving_bin_size);
     if ((int)threadIdx.x < B) margin_terms(threadIdx.x, col, cnt, t, okm, okf, lcol, lfm);
@@ -1064,7 +1088,7 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
         }
     }
     __syncthreads();
-    if (!t.degenerate) stream_records(P, a, pr, q, w.end, w.stride, cur, acc);
+    if (!t.degenerate) Src::stream(P, a, pr, q, w.end, w.stride, cur, acc);
     store_moments(acc, red, w.part, w.part_stride);
     return t;
 }

@@ -92,6 +92,17 @@ struct SamplerParams {
     float rlo_out, rlo_in, rhi_in, rhi_out, dterm;
     // derivative moments are taken about this point to limit cancellation
     double xref[3];
+    // The brick path (brick.cuh): samples grouped in bricks of 2^brick_bl voxels per
+    // axis (0: no brick layout); per brick the composite map at the brick's origin,
+    // per sample c = c(origin) + cA·δ (FP64 FMAs, δ the offset inside the brick), within
+    // 2·cerr of the exact chain. Formed per point map by point_map_fill:
+    //   face_lo, face_hi  an FP32 fraction outside (face_lo, face_hi) may lie within
+    //                     2·cerr of a cell face
+    //   lo_ext, hi_ext    per axis, the least and greatest of c − c(origin) over a
+    //                     brick, widened by 4·cerr (the per-brick inside test)
+    int brick_bl;
+    float face_lo, face_hi;
+    double lo_ext[3], hi_ext[3];
 };
 
 // Per-metric device scratch and the host-side view of it.
@@ -111,6 +122,7 @@ struct Workspace {
     uint16_t* rec_bins = nullptr;
     float* rec_f = nullptr;
     float* rec_g = nullptr;              // [3][n_samples]
+    float4* rec4 = nullptr;              // brick layout: gx, gy, gz, fraction per padded sample
     float hist_scale = 0.f;              // fixed-point scale of a joint-histogram tap
     int hist_scale_log2 = 0;
     int fine_scale_log2 = 0;              // scale of the fine part; the global bins' unit is 2^-this
@@ -151,9 +163,18 @@ struct mi_metric {
     uint8_t* mmask = nullptr;     // device moving mask or null
     cudaArray_t marray = nullptr; // the moving volume in a block-linear 3-D array
     cudaTextureObject_t mtex = 0; // point-sampling, clamp-to-edge texture over marray
-    uint32_t* samples = nullptr;  // device flat indices (8³-brick order); null = the whole grid
+    uint32_t* samples = nullptr;  // device flat indices in walk order; null = the whole grid (not Mattes)
     uint8_t* fbin = nullptr;      // device fixed Parzen bin of every sample (exact, set-up time)
     int64_t n_samples = 0;
+    // the Mattes metric's brick layout (brick.cuh): bricks of 2^brick_bl voxels per
+    // axis, each brick's samples padded to chunks of 32
+    int brick_bl = 0;
+    uint32_t* codes = nullptr;      // [nchunks·32] offset in the brick | fixed bin; padding BRICK_PAD
+    uint32_t* chunk_run = nullptr;  // [nchunks] run (non-empty brick) of each chunk
+    uint32_t* run_brick = nullptr;  // [nruns] packed brick coordinates
+    float4* run_xbase = nullptr;    // [nruns] x(brick origin) − x_ref
+    int64_t nchunks = 0, nruns = 0;
+    int table_cap = 1;              // brick-table entries a histogram CTA needs
     int bins = 0;
     mi_metric_info info{};
     mi::SamplerParams base{};     // everything except the stages
@@ -175,6 +196,8 @@ namespace mi {
 
 mi_status set_error(mi_context* ctx, mi_status s, const std::string& msg);
 mi_status cuda_status(mi_context* ctx, cudaError_t e, const char* where);
+// Raises (never lowers) a kernel's dynamic shared-memory limit on the context's device.
+mi_status raise_smem_limit(mi_context* ctx, const void* fn, size_t bytes);
 
 // Host-side transform families (transforms.cpp).
 struct AffineForm {

@@ -30,9 +30,12 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_run_length_encode.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
 
 #include <algorithm>
+#include <utility>
 
 #include <cfloat>
 #include <cmath>
@@ -43,6 +46,7 @@
 #include "internal.h"
 #include "sampler.cuh"
 #include "eval_device.cuh"
+#include "brick.cuh"
 #include "point_map.h"
 
 namespace mi {
@@ -62,14 +66,17 @@ namespace {
 // The split form (k_hist, then k_deriv) does the same work with a kernel boundary in
 // place of the barrier.
 // ---------------------------------------------------------------------------
-// This CTA's queue of samples for the exact chain (k_hist, k_eval: a grid-stride walk,
-// so at most exq_cap = ceil(n / (grid·block))·block samples per CTA).
-__device__ __forceinline__ ExactQueue exact_queue(const EvalArgs& a) {
-#if MI_EXACT_DEFERRED
-    return ExactQueue{a.exq + (size_t)blockIdx.x * a.exq_cap, a.exq_cap};
-#else
-    return ExactQueue{nullptr, 0u};
-#endif
+// The brick table follows the histogram in the histogram kernels' shared memory (at
+// a 16-byte boundary); table_cap entries, sized at set-up for the launch's grid.
+__host__ __device__ inline size_t brick_table_offset(int B, int copies, int fine_copies) {
+    return (hist_region_bytes(B, copies, fine_copies) + 15) & ~(size_t)15;
+}
+size_t hist_kernel_smem(int B, int table_cap) {
+    return std::max(brick_table_offset(B, hist_copies(B), hist_fine_copies(B)) + (size_t)table_cap * sizeof(BrickBase),
+                    tail_once_smem(B));
+}
+__device__ __forceinline__ BrickBase* brick_table_ptr(unsigned char* base, int B, const EvalArgs& a) {
+    return reinterpret_cast<BrickBase*>(base + brick_table_offset(B, a.copies, a.fine_copies));
 }
 
 template <bool DERIV>
@@ -79,11 +86,11 @@ k_eval(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobian
     unsigned int* sh = reinterpret_cast<unsigned int*>(esh);
     double* dsh = reinterpret_cast<double*>(esh);
     const int B = P.bins;
-    hist_phase<DERIV>(P, a, sh, grid_samples(a.n), exact_queue(a));
+    brick_hist_phase<DERIV>(P, a, sh, brick_table_ptr(esh, B, a));
     if (!grid_barrier(a, 1)) return;
     TailCtx t;
     if (DERIV) {
-        t = deriv_phase(P, a, dsh, grid_groups(a));
+        t = deriv_phase<BrickRecords>(P, a, dsh, grid_groups(a));
     } else {
         const TailSmem ts = tail_layout(B, esh);
         t = tail_prepare(B, P.moving_bin_size, a, ts);
@@ -105,18 +112,16 @@ k_eval(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobian
 // Histogram pass of the split form. For a value-only evaluation (RECORD false) the CTA
 // that flushes last forms the tail (tail_once) and publishes the result, so that
 // evaluation is this one launch.
-size_t hist_kernel_smem(int B) { return std::max(hist_smem(B), tail_once_smem(B)); }
-
 template <bool RECORD>
 __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
 k_hist(const __grid_constant__ SamplerParams P, EvalArgs a) {
-    extern __shared__ __align__(16) unsigned int sh[];
+    extern __shared__ __align__(16) unsigned char hsh[];
     pdl_launch_dependents();
-    hist_phase<RECORD, (HIST_CLUSTER > 1)>(P, a, sh, grid_samples(a.n), exact_queue(a));
+    brick_hist_phase<RECORD>(P, a, reinterpret_cast<unsigned int*>(hsh), brick_table_ptr(hsh, P.bins, a));
     // the value+derivative evaluation's tail is formed by k_deriv's CTAs; a value-only
     // evaluation ends here, with its tail in the CTA that flushes last
     if (RECORD || !last_to_arrive(a.sync + 1)) return;
-    tail_once(P.bins, P.moving_bin_size, a, reinterpret_cast<unsigned char*>(sh), true);
+    tail_once(P.bins, P.moving_bin_size, a, hsh, true);
 }
 
 // Derivative pass of the split form, a programmatic dependent of k_hist: each CTA forms
@@ -127,7 +132,7 @@ __global__ void __launch_bounds__(DERIV_BLOCK, DERIV_MIN_BLOCKS)
 k_deriv(const __grid_constant__ SamplerParams P, const __grid_constant__ JacobianForm J, EvalArgs a) {
     extern __shared__ double dsh[];
     pdl_wait();
-    const TailCtx t = stream_phase(P, a, dsh, grid_groups(a));
+    const TailCtx t = stream_phase<BrickRecords>(P, a, dsh, grid_groups(a));
     if (!last_to_arrive(a.sync)) return;
     // every CTA has read the histogram and written its value slices and moments
     deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
@@ -138,23 +143,31 @@ k_deriv(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobia
     for (int i = threadIdx.x; i < P.bins; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
-// Per-sample decisions of the same sampler the kernels use, for the exactness tests.
+// Per-sample decisions of the brick sampler the kernels use, for the exactness tests,
+// per padded position (a padding lane reports status −1).
 __global__ void k_decisions(const __grid_constant__ SamplerParams P, const float* __restrict__ moving,
-                            const uint8_t* __restrict__ mmask, const uint32_t* __restrict__ samples,
-                            const uint8_t* __restrict__ fbin, int64_t n, int8_t* __restrict__ status,
-                            int32_t* __restrict__ fb, int32_t* __restrict__ mb, int64_t* __restrict__ flat_out,
-                            int8_t* __restrict__ exact_out) {
+                            const uint8_t* __restrict__ mmask, const uint32_t* __restrict__ codes,
+                            const uint32_t* __restrict__ chunk_run, const uint32_t* __restrict__ run_brick,
+                            int64_t npad, int8_t* __restrict__ status, int32_t* __restrict__ fb,
+                            int32_t* __restrict__ mb, int64_t* __restrict__ flat_out, int8_t* __restrict__ exact_out) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
-        const uint32_t flat = samples ? samples[s] : (uint32_t)s;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npad; p += stride) {
+        const uint32_t code = codes[p];
+        if (code == BRICK_PAD) {
+            status[p] = -1;
+            continue;
+        }
+        const uint32_t packed = run_brick[chunk_run[p / BRICK_CHUNK]];
+        const BrickBase b = brick_base(P, packed);
         Sample o;
-        o.exact = false;
-        const int st = sample<false>(P, flat, moving, mmask, o);
-        status[s] = (int8_t)st;
-        fb[s] = st == SAMPLE_VALID ? (int)fbin[s] : -1;
-        mb[s] = st == SAMPLE_VALID ? o.mi : -1;
-        flat_out[s] = flat;
-        exact_out[s] = o.exact ? 1 : 0;
+        const int st = brick_sample<false>(P, b, code, moving, mmask, o);
+        uint32_t i, j, k;
+        brick_ijk(P, packed, code, i, j, k);
+        status[p] = (int8_t)st;
+        fb[p] = st == SAMPLE_VALID ? (int)(code >> (3 * P.brick_bl)) : -1;
+        mb[p] = st == SAMPLE_VALID ? o.mi : -1;
+        flat_out[p] = (int64_t)i + P.fsize0 * ((int64_t)j + P.fsize1 * (int64_t)k);
+        exact_out[p] = o.exact ? 1 : 0;
     }
 }
 
@@ -186,6 +199,90 @@ __global__ void k_brick_key(const uint32_t* __restrict__ idx, int64_t count, int
         const int64_t brick = ((z >> lb) * nby + (y >> lb)) * nbx + (x >> lb);
         key[t] = ((unsigned long long)brick << (3 * lb)) |
                  (unsigned long long)((((z & m) << lb | (y & m)) << lb) | (x & m));
+    }
+}
+
+// Sort key of a voxel in the brick layout's order: bricks of 2^bl voxels per axis
+// (x-fastest), inside a brick its 8³ sub-bricks (x-fastest), inside those the voxels
+// (x-fastest). 3 ≤ bl ≤ 6.
+__global__ void k_brick_key_bl(const uint32_t* __restrict__ idx, int64_t count, int64_t nx, int64_t ny, int bl,
+                               int64_t nbx, int64_t nby, unsigned long long* __restrict__ key) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = idx[t];
+        const int64_t x = v % nx, row = v / nx;
+        const int64_t y = row % ny, z = row / ny;
+        const int64_t brick = ((z >> bl) * nby + (y >> bl)) * nbx + (x >> bl);
+        const int sb = bl - 3;
+        const int64_t sm = ((int64_t)1 << sb) - 1;
+        const int64_t sub = ((((z >> 3) & sm) << sb | ((y >> 3) & sm)) << sb) | ((x >> 3) & sm);
+        const int64_t local = ((z & 7) << 6) | ((y & 7) << 3) | (x & 7);
+        key[t] = ((unsigned long long)brick << (3 * bl)) | (unsigned long long)((sub << 9) | local);
+    }
+}
+
+// The brick of each sample (its index in the bricks' x-fastest order).
+__global__ void k_brick_of(const uint32_t* __restrict__ idx, int64_t count, int64_t nx, int64_t ny, int bl,
+                           int64_t nbx, int64_t nby, uint32_t* __restrict__ bid) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = idx[t];
+        const int64_t x = v % nx, row = v / nx;
+        const int64_t y = row % ny, z = row / ny;
+        bid[t] = (uint32_t)(((z >> bl) * nby + (y >> bl)) * nbx + (x >> bl));
+    }
+}
+
+__global__ void k_run_chunks(const int* __restrict__ counts, int64_t nruns, uint32_t* __restrict__ nch) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nruns; r += (int64_t)gridDim.x * blockDim.x)
+        nch[r] = (uint32_t)((counts[r] + BRICK_CHUNK - 1) / BRICK_CHUNK);
+}
+
+// Per run (a non-empty brick): its packed coordinates, x(origin) − x_ref in FP32, and
+// the run index of each of its chunks.
+__global__ void k_run_fill(const uint32_t* __restrict__ bid, int64_t nruns, const uint32_t* __restrict__ chunk_off,
+                           const uint32_t* __restrict__ nch, int64_t nbx, int64_t nby, int bl, SamplerParams P,
+                           uint32_t* __restrict__ run_brick, float4* __restrict__ run_xbase,
+                           uint32_t* __restrict__ chunk_run) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nruns; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = bid[r];
+        const int64_t bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+        run_brick[r] = (uint32_t)(bx | (by << 10) | (bz << 20));
+        const double o[3] = {(double)(bx << bl), (double)(by << bl), (double)(bz << bl)};
+        float xb[3];
+        for (int d = 0; d < 3; ++d) {
+            const double x = P.forigin[d] + P.fi2p[d * 3] * o[0] + P.fi2p[d * 3 + 1] * o[1] + P.fi2p[d * 3 + 2] * o[2];
+            xb[d] = (float)(x - P.xref[d]);
+        }
+        run_xbase[r] = make_float4(xb[0], xb[1], xb[2], 0.0f);
+        for (uint32_t c = 0; c < nch[r]; ++c) chunk_run[chunk_off[r] + c] = (uint32_t)r;
+    }
+}
+
+// The codes: one CTA per run, sample t of the run at padded position chunk_off·32 + t:
+// its offset in the brick (bl bits per axis) and its fixed bin above them.
+__global__ void k_scatter_codes(const uint32_t* __restrict__ samples, const uint8_t* __restrict__ fbin,
+                                const int* __restrict__ counts, const uint32_t* __restrict__ run_start,
+                                const uint32_t* __restrict__ chunk_off, int64_t nx, int64_t ny, int bl,
+                                uint32_t* __restrict__ codes) {
+    const int64_t r = blockIdx.x;
+    const int64_t n = counts[r];
+    const int64_t s0 = run_start[r], p0 = (int64_t)chunk_off[r] * BRICK_CHUNK;
+    const int64_t msk = ((int64_t)1 << bl) - 1;
+    for (int64_t t = threadIdx.x; t < n; t += blockDim.x) {
+        const int64_t v = samples[s0 + t];
+        const int64_t x = v % nx, row = v / nx;
+        const int64_t y = row % ny, z = row / ny;
+        codes[p0 + t] = (uint32_t)((x & msk) | ((y & msk) << bl) | ((z & msk) << (2 * bl)) |
+                                   ((int64_t)fbin[s0 + t] << (3 * bl)));
+    }
+}
+
+// The most runs (table entries) any CTA of a `grid`-CTA histogram launch meets.
+__global__ void k_table_need(const uint32_t* __restrict__ chunk_run, uint32_t nchunks, uint32_t grid,
+                             unsigned int* __restrict__ need) {
+    const uint32_t per = (nchunks + grid - 1) / grid;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < grid; c += gridDim.x * blockDim.x) {
+        const uint32_t c0 = min(c * per, nchunks), c1 = min(c0 + per, nchunks);
+        if (c0 < c1) atomicMax(need, chunk_run[c1 - 1] - chunk_run[c0] + 1);
     }
 }
 
@@ -297,32 +394,6 @@ mi_status minmax(mi_context* ctx, const float* vals, const uint32_t* idx, const 
 uint32_t ghist_rep_stride(int B) { return (uint32_t)(((size_t)B * B + 2 * B + 31) & ~(size_t)31); }
 size_t ghist_bytes(int B) { return (size_t)GHIST_REPS * ghist_rep_stride(B) * sizeof(unsigned long long); }
 
-// The split form's histogram grid: enough CTAs for the samples, at most as many as are
-// resident at once, in whole thread-block clusters of HIST_CLUSTER (bounded by the
-// clusters the device can hold at once with this kernel's shape).
-int hist_grid(mi_context* ctx, int64_t n, int occ, int B) {
-    int g = grid_for(n, HIST_BLOCK, ctx->num_sms * std::max(occ, 1));
-    if (HIST_CLUSTER <= 1) return g;
-    int clusters = (g + HIST_CLUSTER - 1) / HIST_CLUSTER;
-    cudaLaunchConfig_t hc = {};
-    hc.gridDim = dim3((unsigned)(clusters * HIST_CLUSTER));
-    hc.blockDim = dim3(HIST_BLOCK);
-    hc.dynamicSmemBytes = hist_kernel_smem(B);
-    cudaLaunchAttribute hattr[1];
-    hattr[0].id = cudaLaunchAttributeClusterDimension;
-    hattr[0].val.clusterDim.x = HIST_CLUSTER;
-    hattr[0].val.clusterDim.y = 1;
-    hattr[0].val.clusterDim.z = 1;
-    hc.attrs = hattr;
-    hc.numAttrs = 1;
-    int active = 0;
-    if (cudaOccupancyMaxActiveClusters(&active, k_hist<true>, &hc) == cudaSuccess && active > 0)
-        clusters = std::min(clusters, active);
-    else
-        cudaGetLastError();
-    return std::max(1, clusters) * HIST_CLUSTER;
-}
-
 void free_metric(mi_metric* m) {
     if (!m) return;
     if (m->mtex) cudaDestroyTextureObject(m->mtex);
@@ -332,6 +403,10 @@ void free_metric(mi_metric* m) {
     cudaFree(m->mmask);
     cudaFree(m->samples);
     cudaFree(m->fbin);
+    cudaFree(m->codes);
+    cudaFree(m->chunk_run);
+    cudaFree(m->run_brick);
+    cudaFree(m->run_xbase);
     cudaFree(m->ws.hist);
     cudaFree(m->ws.partials);
     cudaFree(m->ws.vsum);
@@ -341,6 +416,7 @@ void free_metric(mi_metric* m) {
     cudaFree(m->ws.rec_bins);
     cudaFree(m->ws.rec_f);
     cudaFree(m->ws.rec_g);
+    cudaFree(m->ws.rec4);
     if (m->ws.host_result) cudaFreeHost(m->ws.host_result);
     for (int i = 0; i < 5; ++i)
         if (m->ws.ev[i]) cudaEventDestroy(m->ws.ev[i]);
@@ -353,13 +429,29 @@ void free_metric(mi_metric* m) {
     delete m;
 }
 
+// The brick edge of the layout: the smallest of 16, 32, 64 voxels that leaves on average
+// at least 200 samples per brick (few padding lanes, few bricks per CTA), and at least
+// large enough that no axis has more than 1024 bricks (the packed coordinates).
+int choose_brick_bl(const int64_t* size, int64_t n) {
+    const int64_t nvox = size[0] * size[1] * size[2];
+    int bl = 4;
+    while (bl < 6 && (double)n * (double)((int64_t)1 << (3 * bl)) < 200.0 * (double)nvox) ++bl;
+    for (int d = 0; d < 3; ++d)
+        while (bl < 6 && ((size[d] + ((int64_t)1 << bl) - 1) >> bl) > 1024) ++bl;
+    return bl;
+}
+
 // Build the sample list: the strategy's draw, gated by the fixed mask, sorted into
 // brick order (SAMPLE_BRICK_LOG2). The histogram is a sum of exact integers and so
 // does not depend on the order; sorting only buys locality.
+// With `bricks` (the Mattes metric) the whole grid is materialised too, and the sort
+// key is the brick layout's (brick_key_bl): bricks of 2^bl voxels per axis, bl chosen
+// from the sample density (choose_brick_bl), then 8³ sub-bricks, then voxels, each
+// x-fastest; m->brick_bl records bl.
 mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mask, const mi_sampling* smp,
-                        int64_t nvox) {
+                        int64_t nvox, bool bricks) {
     const int strategy = smp ? smp->strategy : MI_SAMPLING_NONE;
-    if (strategy == MI_SAMPLING_NONE && !fixed_mask) {
+    if (strategy == MI_SAMPLING_NONE && !fixed_mask && !bricks) {
         m->samples = nullptr;
         m->n_samples = nvox;
         return MI_OK;
@@ -439,7 +531,37 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
         kept = out;
         nkept = h;
     }
-    if (nkept > 1 && SAMPLE_BRICK_LOG2 > 0) {
+    const int64_t fsz[3] = {m->fgeo.size[0], m->fgeo.size[1], m->fgeo.size[2]};
+    if (bricks) m->brick_bl = choose_brick_bl(fsz, nkept);
+    if (nkept > 1 && bricks) {
+        const int bl = m->brick_bl;
+        const int64_t nx = fsz[0], ny = fsz[1];
+        const int64_t nbx = (nx + (1 << bl) - 1) >> bl, nby = (ny + (1 << bl) - 1) >> bl;
+        const int64_t nbz = (fsz[2] + (1 << bl) - 1) >> bl;
+        const uint64_t kmax = (uint64_t)(nbx * nby * nbz) << (3 * bl);
+        int bits = 1;
+        while (bits < 64 && ((uint64_t)1 << bits) < kmax) ++bits;
+        unsigned long long *keys = nullptr, *keys_out = nullptr;
+        uint32_t* sorted = nullptr;
+        MI_CHECK_CUDA(ctx, cudaMalloc(&keys, (size_t)nkept * 8));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&keys_out, (size_t)nkept * 8));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&sorted, pad4(nkept) * 4));
+        k_brick_key_bl<<<grid_for(nkept, block, ctx->num_sms * 8), block, 0, st>>>(kept, nkept, nx, ny, bl, nbx, nby,
+                                                                                  keys);
+        MI_CHECK_CUDA(ctx, cudaGetLastError());
+        tmp_bytes = 0;
+        MI_CHECK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys_out, kept, sorted,
+                                                           (int)nkept, 0, bits, st));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&tmp, tmp_bytes));
+        MI_CHECK_CUDA(ctx, cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_out, kept, sorted, (int)nkept,
+                                                           0, bits, st));
+        MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+        cudaFree(tmp);
+        cudaFree(keys);
+        cudaFree(keys_out);
+        cudaFree(kept);
+        kept = sorted;
+    } else if (nkept > 1 && SAMPLE_BRICK_LOG2 > 0) {
         const int lb = SAMPLE_BRICK_LOG2;
         const int64_t nx = m->fgeo.size[0], ny = m->fgeo.size[1], nz = m->fgeo.size[2];
         const int64_t nbx = (nx + (1 << lb) - 1) >> lb, nby = (ny + (1 << lb) - 1) >> lb;
@@ -485,6 +607,121 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
     return MI_OK;
 }
 
+// The brick layout of a sorted sample list (build_samples with bricks) and its fixed
+// bins: runs of samples per brick (CUB run-length encoding), each padded to whole
+// chunks of 32, the codes scattered to their padded positions.
+mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams& P) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = m->n_samples;
+    const int bl = m->brick_bl;
+    const int64_t nx = m->fgeo.size[0], ny = m->fgeo.size[1];
+    const int64_t nbx = (nx + (1 << bl) - 1) >> bl, nby = (ny + (1 << bl) - 1) >> bl;
+    const int block = 256;
+    if (n == 0) {
+        // one chunk of padding keeps every launch shape non-empty
+        m->nchunks = 1;
+        m->nruns = 1;
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->codes, BRICK_CHUNK * 4));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->codes, 0xFF, BRICK_CHUNK * 4, st));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->chunk_run, 4));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->chunk_run, 0, 4, st));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->run_brick, 4));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->run_brick, 0, 4, st));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->run_xbase, sizeof(float4)));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->run_xbase, 0, sizeof(float4), st));
+        MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+        return MI_OK;
+    }
+    uint32_t *bid = nullptr, *uniq = nullptr, *nch = nullptr, *chunk_off = nullptr, *run_start = nullptr;
+    int *counts = nullptr, *nruns_d = nullptr;
+    void* tmp = nullptr;
+    size_t tb = 0;
+    auto done = [&](mi_status s) {
+        cudaStreamSynchronize(st);
+        cudaFree(bid);
+        cudaFree(uniq);
+        cudaFree(nch);
+        cudaFree(chunk_off);
+        cudaFree(run_start);
+        cudaFree(counts);
+        cudaFree(nruns_d);
+        cudaFree(tmp);
+        return s;
+    };
+#define TRY_L(expr)                                                      \
+    do {                                                                 \
+        cudaError_t _e = (expr);                                         \
+        if (_e != cudaSuccess) return done(cuda_status(ctx, _e, #expr)); \
+    } while (0)
+    TRY_L(cudaMalloc(&bid, (size_t)n * 4));
+    TRY_L(cudaMalloc(&uniq, (size_t)n * 4));
+    TRY_L(cudaMalloc(&counts, (size_t)n * 4));
+    TRY_L(cudaMalloc(&nruns_d, sizeof(int)));
+    k_brick_of<<<grid_for(n, block, ctx->num_sms * 8), block, 0, st>>>(m->samples, n, nx, ny, bl, nbx, nby, bid);
+    TRY_L(cudaGetLastError());
+    TRY_L(cub::DeviceRunLengthEncode::Encode(nullptr, tb, bid, uniq, counts, nruns_d, (int)n, st));
+    TRY_L(cudaMalloc(&tmp, tb));
+    TRY_L(cub::DeviceRunLengthEncode::Encode(tmp, tb, bid, uniq, counts, nruns_d, (int)n, st));
+    int nruns = 0;
+    TRY_L(cudaMemcpyAsync(&nruns, nruns_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRY_L(cudaStreamSynchronize(st));
+    cudaFree(tmp);
+    tmp = nullptr;
+    TRY_L(cudaMalloc(&nch, (size_t)nruns * 4));
+    TRY_L(cudaMalloc(&chunk_off, (size_t)nruns * 4));
+    TRY_L(cudaMalloc(&run_start, (size_t)nruns * 4));
+    k_run_chunks<<<grid_for(nruns, block, ctx->num_sms * 8), block, 0, st>>>(counts, nruns, nch);
+    TRY_L(cudaGetLastError());
+    tb = 0;
+    size_t tb2 = 0;
+    TRY_L(cub::DeviceScan::ExclusiveSum(nullptr, tb, nch, chunk_off, nruns, st));
+    TRY_L(cub::DeviceScan::ExclusiveSum(nullptr, tb2, reinterpret_cast<const uint32_t*>(counts), run_start, nruns, st));
+    TRY_L(cudaMalloc(&tmp, std::max(tb, tb2)));
+    TRY_L(cub::DeviceScan::ExclusiveSum(tmp, tb, nch, chunk_off, nruns, st));
+    TRY_L(cub::DeviceScan::ExclusiveSum(tmp, tb2, reinterpret_cast<const uint32_t*>(counts), run_start, nruns, st));
+    uint32_t last[2] = {0, 0};
+    TRY_L(cudaMemcpyAsync(&last[0], chunk_off + nruns - 1, 4, cudaMemcpyDeviceToHost, st));
+    TRY_L(cudaMemcpyAsync(&last[1], nch + nruns - 1, 4, cudaMemcpyDeviceToHost, st));
+    TRY_L(cudaStreamSynchronize(st));
+    const int64_t nchunks = (int64_t)last[0] + last[1];
+    if (nchunks * BRICK_CHUNK >= ((int64_t)1 << 32))
+        return done(set_error(ctx, MI_ERR_INVALID_ARGUMENT, "too many samples for the brick layout"));
+    m->nchunks = nchunks;
+    m->nruns = nruns;
+    TRY_L(cudaMalloc(&m->codes, (size_t)nchunks * BRICK_CHUNK * 4));
+    TRY_L(cudaMemsetAsync(m->codes, 0xFF, (size_t)nchunks * BRICK_CHUNK * 4, st));
+    TRY_L(cudaMalloc(&m->chunk_run, (size_t)nchunks * 4));
+    TRY_L(cudaMalloc(&m->run_brick, (size_t)nruns * 4));
+    TRY_L(cudaMalloc(&m->run_xbase, (size_t)nruns * sizeof(float4)));
+    k_run_fill<<<grid_for(nruns, block, ctx->num_sms * 8), block, 0, st>>>(uniq, nruns, chunk_off, nch, nbx, nby, bl,
+                                                                           P, m->run_brick, m->run_xbase, m->chunk_run);
+    TRY_L(cudaGetLastError());
+    k_scatter_codes<<<(unsigned)nruns, block, 0, st>>>(m->samples, m->fbin, counts, run_start, chunk_off, nx, ny, bl,
+                                                       m->codes);
+    TRY_L(cudaGetLastError());
+#undef TRY_L
+    return done(MI_OK);
+}
+
+// Brick-table entries a `grid`-CTA histogram launch needs.
+mi_status brick_table_need(mi_context* ctx, const mi_metric* m, int grid, int* need) {
+    unsigned int* d = nullptr;
+    MI_CHECK_CUDA(ctx, cudaMalloc(&d, sizeof(unsigned int)));
+    unsigned int h = 1;
+    cudaError_t e = cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        k_table_need<<<grid_for(grid, 256, 64), 256, 0, ctx->stream>>>(m->chunk_run, (uint32_t)m->nchunks,
+                                                                       (uint32_t)grid, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "brick_table_need");
+    *need = (int)std::max(h, 1u);
+    return MI_OK;
+}
+
 // Per-evaluation sampler constants: the stages and the composite map (point_map.h).
 mi_status fill_params(mi_metric* m, const double* stages, int nstage, SamplerParams& P) {
     P = m->base;
@@ -524,7 +761,12 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.samples = m->samples;
     a.fbin = m->fbin;
     a.n = n;
-    a.npad = (n + 3u) & ~3u;
+    a.npad = (uint32_t)(m->nchunks * BRICK_CHUNK);
+    a.codes = m->codes;
+    a.chunk_run = m->chunk_run;
+    a.run_brick = m->run_brick;
+    a.run_xbase = m->run_xbase;
+    a.nchunks = (uint32_t)m->nchunks;
     a.hist_scale = ws.hist_scale;
     a.fine_scale = (float)std::ldexp(1.0, ws.fine_scale_log2);
     a.fine_shift = ws.fine_scale_log2 - ws.hist_scale_log2;
@@ -540,10 +782,9 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.rec_bins = want_derivative ? ws.rec_bins : nullptr;
     a.rec_f = want_derivative ? ws.rec_f : nullptr;
     a.rec_g = want_derivative ? ws.rec_g : nullptr;
+    a.rec4 = want_derivative ? ws.rec4 : nullptr;
     a.partials = ws.partials;
     a.vsum = ws.vsum;
-    a.exq = ws.exq;
-    a.exq_cap = ws.fused ? ws.exq_cap_eval : ws.exq_cap_hist;
     a.sync = ws.done_counter;
     a.result = ws.result;
     // the split form's last kernel copies the result into the mapped mirror; the
@@ -562,7 +803,7 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)ws.grid_eval);
         cfg.blockDim = dim3(HIST_BLOCK);
-        cfg.dynamicSmemBytes = eval_smem(B);
+        cfg.dynamicSmemBytes = std::max(hist_kernel_smem(B, m->table_cap), eval_smem(B));
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
@@ -576,19 +817,11 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
     } else {
         {
-            // thread-block clusters of HIST_CLUSTER CTAs (the grid is a multiple of it)
             cudaLaunchConfig_t hc = {};
             hc.gridDim = dim3((unsigned)ws.grid_hist);
             hc.blockDim = dim3(HIST_BLOCK);
-            hc.dynamicSmemBytes = hist_kernel_smem(B);
+            hc.dynamicSmemBytes = hist_kernel_smem(B, m->table_cap);
             hc.stream = st;
-            cudaLaunchAttribute hattr[1];
-            hattr[0].id = cudaLaunchAttributeClusterDimension;
-            hattr[0].val.clusterDim.x = HIST_CLUSTER;
-            hattr[0].val.clusterDim.y = 1;
-            hattr[0].val.clusterDim.z = 1;
-            hc.attrs = hattr;
-            hc.numAttrs = HIST_CLUSTER > 1 ? 1 : 0;
             if (want_derivative)
                 MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&hc, k_hist<true>, P, a));
             else
@@ -760,7 +993,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         TRY_CUDA(cudaMalloc(&m->mmask, (size_t)mvox));
         TRY_CUDA(cudaMemcpyAsync(m->mmask, moving_mask, (size_t)mvox, cudaMemcpyHostToDevice, st));
     }
-    mi_status s = build_samples(ctx, m, fixed_mask, sampling, nvox);
+    mi_status s = build_samples(ctx, m, fixed_mask, sampling, nvox, mattes);
     if (s != MI_OK) return fail(s);
 
     // Histogram geometry from the sampled fixed values and the masked moving volume
@@ -874,6 +1107,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     P.nmin_f = (float)P.moving_nmin;
     P.bin_hi_f = (float)(bins - PADDING - 1);
     P.vmax = vmax;
+    P.brick_bl = mattes ? m->brick_bl : 0;
     // x_ref: the fixed grid's physical centre; x − x_ref = M_f·idx + (o_f − x_ref)
     const double mid[3] = {0.5 * (double)(P.fsize0 - 1), 0.5 * (double)(P.fsize1 - 1), 0.5 * (double)(P.fsize2 - 1)};
     for (int r = 0; r < 3; ++r) {
@@ -896,42 +1130,88 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
                                                                               m->n_samples, m->fbin);
     TRY_CUDA(cudaGetLastError());
 
-    // Workspace and launch shapes.
+    // The brick layout of the samples (brick.cuh).
+    s = build_brick_layout(ctx, m, P);
+    if (s != MI_OK) return fail(s);
+
+    // Workspace and launch shapes. The histogram kernels' shared memory holds the CTA
+    // histogram and the brick table, whose size depends on the grid; the grid depends
+    // on the occupancy that the shared memory allows: sized for the provisional grid
+    // (HIST_MIN_BLOCKS CTAs per SM), re-sized if fewer fit.
     Workspace& ws = m->ws;
     const int B = bins;
-    TRY_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_kernel_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_kernel_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_eval<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_eval<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
+    const int64_t npad = m->nchunks * BRICK_CHUNK;
+    const int nwarps_hist = HIST_BLOCK / 32;
+    const int64_t warp_units = std::max<int64_t>(m->nchunks, 1);
+    auto hist_grid_for = [&](int occ) {
+        return grid_for((warp_units + nwarps_hist - 1) / nwarps_hist * HIST_BLOCK, HIST_BLOCK,
+                        ctx->num_sms * std::max(occ, 1));
+    };
     int occ_h = 0, occ_d = 0, occ_e1 = 0, occ_e0 = 0, coop = 0;
-    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK, hist_kernel_smem(B)));
+    {
+        int grid0 = hist_grid_for(HIST_MIN_BLOCKS), cap = 1;
+        s = brick_table_need(ctx, m, grid0, &cap);
+        if (s != MI_OK) return fail(s);
+        s = raise_smem_limit(ctx, (const void*)k_hist<true>, hist_kernel_smem(B, cap));
+        if (s != MI_OK) return fail(s);
+        TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK,
+                                                               hist_kernel_smem(B, cap)));
+        ws.grid_hist = hist_grid_for(occ_h);
+        if (ws.grid_hist != grid0) {
+            s = brick_table_need(ctx, m, ws.grid_hist, &cap);
+            if (s != MI_OK) return fail(s);
+        }
+        m->table_cap = cap;
+    }
+    const size_t hsm = hist_kernel_smem(B, m->table_cap);
+    const size_t esm = std::max(hsm, eval_smem(B));
+    {
+        const std::pair<const void*, size_t> lims[] = {{(const void*)k_hist<true>, hsm},
+                                                       {(const void*)k_hist<false>, hsm},
+                                                       {(const void*)k_deriv, stream_smem(B)},
+                                                       {(const void*)k_eval<true>, esm},
+                                                       {(const void*)k_eval<false>, esm}};
+        for (const auto& l : lims) {
+            s = raise_smem_limit(ctx, l.first, l.second);
+            if (s != MI_OK) return fail(s);
+        }
+    }
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_deriv, DERIV_BLOCK, stream_smem(B)));
-    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e1, k_eval<true>, HIST_BLOCK, eval_smem(B)));
-    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e0, k_eval<false>, HIST_BLOCK, eval_smem(B)));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e1, k_eval<true>, HIST_BLOCK, esm));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e0, k_eval<false>, HIST_BLOCK, esm));
     TRY_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
-    // The fused form needs every CTA resident (a cooperative launch).
+    // The fused form needs every CTA resident (a cooperative launch); it runs on the
+    // split form's histogram grid when that is resident (same brick tables), else on
+    // fewer CTAs with tables sized for them.
     const int resident = ctx->num_sms * std::min(occ_e1, occ_e0);
     // The split form is the default: the fused kernel's device time is the same, and
     // a cooperative launch waits for the stream to drain, which adds its latency to
     // every synchronous evaluation.
     ws.can_fuse = coop != 0 && resident >= 1;
     ws.fused = false;
-    ws.grid_eval = ws.can_fuse ? grid_for(m->n_samples, HIST_BLOCK, resident) : 0;
-    ws.grid_hist = hist_grid(ctx, m->n_samples, occ_h, B);
-    ws.grid_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
+    ws.grid_eval = ws.can_fuse ? std::min(ws.grid_hist, resident) : 0;
+    if (ws.can_fuse && ws.grid_eval != ws.grid_hist) {
+        int cap = 1;
+        s = brick_table_need(ctx, m, ws.grid_eval, &cap);
+        if (s != MI_OK) return fail(s);
+        if (cap > m->table_cap) ws.can_fuse = false;  // the fused form would need more shared memory
+    }
+    ws.grid_deriv = grid_for(npad / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
     ws.block_hist = HIST_BLOCK;
     ws.block_deriv = DERIV_BLOCK;
-    // Fixed-point scales of the histogram taps. A thread takes at most per_thread
-    // samples, and a copy of the CTA histogram is fed by HIST_BLOCK/copies threads, so
-    // it sees at most copy_max samples; each adds at most one tap to a bin (coarse
-    // taps ≤ 2/3, fine taps < 2^-FINE_T). Every counter must stay below 2^32 and every
-    // rounded tap below 2^22 (the magic-add rounding): k ≤ 22, kf ≤ FINE_T + 22. The global
-    // u64 bin, in units of 2^-kf, takes at most n_samples·(2/3)·2^kf.
+    // Fixed-point scales of the histogram taps. A CTA walks ceil(nchunks / grid) chunks,
+    // its warps taking every (HIST_BLOCK/32)-th, one sample per lane: a thread takes at
+    // most per_thread samples, and a copy of the CTA histogram is fed by
+    // HIST_BLOCK/copies threads, so it sees at most copy_max samples; each adds at most
+    // one tap to a bin (coarse taps ≤ 2/3, fine taps < 2^-FINE_T). Every counter must
+    // stay below 2^32 and every rounded tap below 2^22 (the magic-add rounding): k ≤ 22,
+    // kf ≤ FINE_T + 22. The global u64 bin, in units of 2^-kf, takes at most
+    // n_samples·(2/3)·2^kf.
     {
         // both forms' histogram grids (the form can be switched after creation)
         const int64_t hgrid = ws.can_fuse ? std::min(ws.grid_hist, ws.grid_eval) : ws.grid_hist;
-        const int64_t per_thread = (m->n_samples + hgrid * HIST_BLOCK - 1) / (hgrid * HIST_BLOCK);
+        const int64_t per_cta = (warp_units + hgrid - 1) / hgrid;
+        const int64_t per_thread = (per_cta + nwarps_hist - 1) / nwarps_hist;
         const double lim = 4294967295.0 * 0.98;
         const double coarse_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_copies(B)), 1);
         const double fine_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_fine_copies(B)), 1);
@@ -946,12 +1226,13 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         ws.fine_scale_log2 = kf;
     }
     {
-        // padded to whole groups of four samples; padding records keep moving bin 0
-        const size_t ns = pad4(m->n_samples);
+        // one record per padded sample; padding records keep moving bin 0
+        const size_t ns = (size_t)npad;
         TRY_CUDA(cudaMalloc(&ws.rec_bins, ns * sizeof(uint16_t)));
         TRY_CUDA(cudaMemsetAsync(ws.rec_bins, 0, ns * sizeof(uint16_t), st));
         TRY_CUDA(cudaMalloc(&ws.rec_f, ns * sizeof(float)));
         TRY_CUDA(cudaMalloc(&ws.rec_g, 3 * ns * sizeof(float)));
+        TRY_CUDA(cudaMalloc(&ws.rec4, ns * sizeof(float4)));
     }
     // joint B², fixed counts B, then the joint part's B column sums
     TRY_CUDA(cudaMalloc(&ws.hist, ghist_bytes(B)));
@@ -959,25 +1240,12 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     // partials serve both forms: the split form's k_deriv grid and, should the form
     // be switched, the fused grid
     {
-        const int pgrid = std::max(ws.grid_deriv, std::max(ws.grid_eval,
-            grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1))));
+        const int pgrid = std::max(ws.grid_deriv, ws.grid_eval);
         ws.grid_split_hist = ws.grid_hist;
-        ws.grid_split_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
+        ws.grid_split_deriv = ws.grid_deriv;
         TRY_CUDA(cudaMalloc(&ws.partials, (size_t)pgrid * NMOM * 8));
     }
     TRY_CUDA(cudaMalloc(&ws.vsum, (size_t)value_slices(B) * 8));
-    {
-        // a grid-stride walk gives a CTA at most ceil(n / (grid·block))·block samples
-        auto cap = [&](int grid) -> uint32_t {
-            if (grid < 1) return 0u;
-            const int64_t per = ((int64_t)m->n_samples + (int64_t)grid * HIST_BLOCK - 1) / ((int64_t)grid * HIST_BLOCK);
-            return (uint32_t)(per * HIST_BLOCK);
-        };
-        ws.exq_cap_hist = cap(ws.grid_hist);
-        ws.exq_cap_eval = cap(ws.grid_eval);
-        const size_t len = std::max((size_t)ws.grid_hist * ws.exq_cap_hist, (size_t)ws.grid_eval * ws.exq_cap_eval);
-        TRY_CUDA(cudaMalloc(&ws.exq, std::max<size_t>(len, 1) * sizeof(uint32_t)));
-    }
     TRY_CUDA(cudaMalloc(&ws.result, RESULT_DOUBLES * 8));
     TRY_CUDA(cudaMalloc(&ws.done_counter, 4 * sizeof(unsigned int)));
     TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));
@@ -1115,12 +1383,15 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
     SamplerParams P;
     mi_status s = fill_params(m, stages, nstage, P);
     if (s != MI_OK) return s;
-    const int64_t ns = m->n_samples;
-    const size_t cap = (size_t)std::max<int64_t>(ns, 1);
+    const int64_t np = m->nchunks * BRICK_CHUNK;
+    const size_t cap = (size_t)std::max<int64_t>(np, 1);
     int8_t *d_st = nullptr, *d_ex = nullptr;
     int32_t *d_fb = nullptr, *d_mb = nullptr;
     int64_t* d_fl = nullptr;
     cudaStream_t st = ctx->stream;
+    std::vector<int8_t> h_st(cap), h_ex(cap);
+    std::vector<int32_t> h_fb(cap), h_mb(cap);
+    std::vector<int64_t> h_fl(cap);
     cudaError_t e = cudaMalloc(&d_st, cap);
     if (e == cudaSuccess) e = cudaMalloc(&d_ex, cap);
     if (e == cudaSuccess) e = cudaMalloc(&d_fb, cap * 4);
@@ -1128,15 +1399,15 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
     if (e == cudaSuccess) e = cudaMalloc(&d_fl, cap * 8);
     if (e == cudaSuccess) {
         const int block = 256;
-        k_decisions<<<grid_for(ns, block, ctx->num_sms * 8), block, 0, st>>>(P, m->moving, m->mmask, m->samples, m->fbin,
-                                                                             ns, d_st, d_fb, d_mb, d_fl, d_ex);
+        k_decisions<<<grid_for(np, block, ctx->num_sms * 8), block, 0, st>>>(
+            P, m->moving, m->mmask, m->codes, m->chunk_run, m->run_brick, np, d_st, d_fb, d_mb, d_fl, d_ex);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess && status) e = cudaMemcpyAsync(status, d_st, (size_t)ns, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && exact) e = cudaMemcpyAsync(exact, d_ex, (size_t)ns, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && fixed_bin) e = cudaMemcpyAsync(fixed_bin, d_fb, (size_t)ns * 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && moving_bin) e = cudaMemcpyAsync(moving_bin, d_mb, (size_t)ns * 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && flat) e = cudaMemcpyAsync(flat, d_fl, (size_t)ns * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_st.data(), d_st, (size_t)np, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_ex.data(), d_ex, (size_t)np, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_fb.data(), d_fb, (size_t)np * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_mb.data(), d_mb, (size_t)np * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_fl.data(), d_fl, (size_t)np * 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(d_st);
     cudaFree(d_ex);
@@ -1144,6 +1415,19 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
     cudaFree(d_mb);
     cudaFree(d_fl);
     if (e != cudaSuccess) return cuda_status(ctx, e, "mi_metric_sample_decisions");
+    // the padded walk without its padding lanes is the sample order
+    int64_t o = 0;
+    for (int64_t p = 0; p < np; ++p) {
+        if (h_st[p] < 0) continue;
+        if (o >= m->n_samples) return set_error(ctx, MI_ERR_CUDA, "brick layout holds more samples than the metric");
+        if (status) status[o] = h_st[p];
+        if (fixed_bin) fixed_bin[o] = h_fb[p];
+        if (moving_bin) moving_bin[o] = h_mb[p];
+        if (flat) flat[o] = h_fl[p];
+        if (exact) exact[o] = h_ex[p];
+        ++o;
+    }
+    if (o != m->n_samples) return set_error(ctx, MI_ERR_CUDA, "brick layout holds fewer samples than the metric");
     return MI_OK;
 }
 

@@ -106,9 +106,10 @@ MI_HD inline bool point_map_fill(SamplerParams& P, const double* stages, int nst
     {
         // the fast path's global decision bounds (sampler.cuh finish_fast): the FP32
         // trilinear value is within 32·2^-24·vmax of the value at the fast c (three
-        // levels of lerps add at most 12 such units), and the fast c's error moves it
-        // by at most 6·vmax per voxel (8 allowed)
-        const double dv = mul(P.vmax, add(mul(8.0, P.cerr), 32.0 * 0x1p-24));
+        // levels of lerps add at most 12 such units), and the fast c's error (cerr, or
+        // 2·cerr on the brick path) moves it by at most 6·vmax per voxel of it (16·cerr
+        // allowed)
+        const double dv = mul(P.vmax, add(mul(16.0, P.cerr), 32.0 * 0x1p-24));
         const double rmag = fmax(fabs(P.moving_min), fabs(P.moving_max));
         const double e = add(mul(dv, 1.001), mul(add(mul(2.0, P.vmax), rmag), 0x1p-20));
         P.rlo_out = f32_down(sub(P.moving_min, e));
@@ -121,6 +122,25 @@ MI_HD inline bool point_map_fill(SamplerParams& P, const double* stages, int nst
         const double inv = P.inv_moving_bin_size;
         const double mag = add(add(add(mul(P.vmax, inv), fabs(P.moving_nmin)), (double)P.bins), 1.0);
         P.dterm = f32_up(mul(add(mul(dv, inv), mul(mag, 0x1p-22)), 1.001));
+    }
+    if (P.brick_bl > 0) {
+        // The brick path: c = c(origin) + cA·δ by FP64 FMAs, δ ∈ [0, 2^bl)³; against the
+        // grid-index FMA form it differs by a few FP64 units of the magnitudes, far
+        // inside cerr's margin, so it is within 2·cerr of the exact chain.
+        const double span = (double)((1 << P.brick_bl) - 1);
+        const double ce = mul(2.0, P.cerr);
+        for (int d = 0; d < 3; ++d) {
+            double lo = 0.0, hi = 0.0;
+            for (int e = 0; e < 3; ++e) {
+                const double a = mul(P.cA[d * 3 + e], span);
+                lo = add(lo, fmin(0.0, a));
+                hi = add(hi, fmax(0.0, a));
+            }
+            P.lo_ext[d] = sub(lo, mul(2.0, ce));
+            P.hi_ext[d] = add(hi, mul(2.0, ce));
+        }
+        P.face_lo = f32_up(ce);
+        P.face_hi = f32_down(sub(1.0, ce));
     }
     P.ilo = add(-0.5, mul(2.0, P.cerr));
     P.olo = sub(-0.5, mul(2.0, P.cerr));

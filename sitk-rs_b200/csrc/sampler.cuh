@@ -389,10 +389,9 @@ __device__ __forceinline__ int finish_fast(const SamplerParams& P, const Prep& p
 #define MI_EXACT_INLINE __forceinline__
 #endif
 template <bool GRAD>
-__device__ MI_EXACT_INLINE int sample_exact(const SamplerParams& P, uint32_t flat, const float* __restrict__ moving,
-                                         const uint8_t* __restrict__ mmask, Sample& o) {
-    uint32_t i, j, k;
-    grid_index(P, flat, i, j, k);
+__device__ MI_EXACT_INLINE int sample_exact_ijk(const SamplerParams& P, uint32_t i, uint32_t j, uint32_t k,
+                                             const float* __restrict__ moving, const uint8_t* __restrict__ mmask,
+                                             Sample& o) {
     double c[3];
     exact_index(P, i, j, k, c);
 #pragma unroll
@@ -422,6 +421,14 @@ __device__ MI_EXACT_INLINE int sample_exact(const SamplerParams& P, uint32_t fla
     o.mi = parzen_bin(term, P.bins);
     o.f = (float)(term - (double)o.mi);
     return SAMPLE_VALID;
+}
+
+template <bool GRAD>
+__device__ __forceinline__ int sample_exact(const SamplerParams& P, uint32_t flat, const float* __restrict__ moving,
+                                            const uint8_t* __restrict__ mmask, Sample& o) {
+    uint32_t i, j, k;
+    grid_index(P, flat, i, j, k);
+    return sample_exact_ijk<GRAD>(P, i, j, k, moving, mmask, o);
 }
 
 // The whole sampler for one sample: the fast path, handing to the exact chain where it

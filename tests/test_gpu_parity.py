@@ -251,8 +251,10 @@ def test_refusals_are_named():
     st = _lib.load().mi_metric_create_ex(f.ctx.handle, f.handle, m.handle, None, None, None, 32,
                                          ctypes.byref(opts), ctypes.byref(h))
     assert _lib.STATUS_NAMES[st] == "MI_ERR_INVALID_ARGUMENT" and not h.value
-    # the whole grid without a mask is walked in voxel order
-    assert np.array_equal(metric.sample_order(), np.arange(16 ** 3, dtype=np.uint32))
+    # the whole grid without a mask is every voxel once, walked in the brick order
+    order = metric.sample_order().astype(np.int64)
+    np.testing.assert_array_equal(np.sort(order), np.arange(16 ** 3))
+    assert np.all(np.diff(brick_order_key(order, 16, 16, 16 ** 3, 16 ** 3)) > 0)
 
 
 @pytest.mark.parametrize("dtype", [np.uint8, np.int16, np.uint16, np.int32, np.float64, np.int64])
@@ -304,9 +306,37 @@ def test_bf16_moving_storage_euler_64_bins(oracle_lib):
     assert np.max(np.abs(mv.derivative - ref_f["derivative"])) <= 0.1 * scale
 
 
+def brick_bl(nvox, n, sizes):
+    """The brick edge (log2) of the Mattes metric's sample layout: the smallest of 16,
+    32, 64 voxels with at least 200 samples per brick on average, and no more than
+    1024 bricks along any axis."""
+    bl = 4
+    while bl < 6 and n * (1 << (3 * bl)) < 200 * nvox:
+        bl += 1
+    for s in sizes:
+        while bl < 6 and -(-s // (1 << bl)) > 1024:
+            bl += 1
+    return bl
+
+
+def brick_order_key(order, nx, ny, nvox, n, nz=None):
+    """Sort key of the layout's walk: bricks (x-fastest), their 8³ sub-bricks
+    (x-fastest), the voxels (x-fastest)."""
+    bl = brick_bl(nvox, n, (nx, ny) if nz is None else (nx, ny, nz))
+    x, y, z = order % nx, (order // nx) % ny, order // (nx * ny)
+    nbx, nby = -(-nx // (1 << bl)), -(-ny // (1 << bl))
+    brick = ((z >> bl) * nby + (y >> bl)) * nbx + (x >> bl)
+    sm = (1 << (bl - 3)) - 1
+    sb_ = bl - 3
+    sub = ((((z >> 3) & sm) << sb_ | ((y >> 3) & sm)) << sb_) | ((x >> 3) & sm)
+    local = ((z & 7) << 6) | ((y & 7) << 3) | (x & 7)
+    return (brick << (3 * bl)) | (sub << 9) | local
+
+
 def test_sample_order_is_the_gated_draw_in_brick_order(oracle_lib):
     # The device walks the strategy's draw gated by the fixed mask, as the same multiset,
-    # in 8³-brick order (grid sizes that are not multiples of 8 leave partial bricks)
+    # in the brick layout's order (grid sizes that are not multiples of the brick leave
+    # partial bricks)
     sb = _sb()
     rng = np.random.default_rng(3)
     nz, ny, nx = 21, 29, 37
@@ -320,9 +350,7 @@ def test_sample_order_is_the_gated_draw_in_brick_order(oracle_lib):
         draw = np.asarray(oracle_lib.draw_samples(vol.size, strategy, pct, 11))
         draw = draw[fmask.ravel()[draw] != 0]
         np.testing.assert_array_equal(np.sort(order), np.sort(draw))
-        x, y, z = order % nx, (order // nx) % ny, order // (nx * ny)
-        nbx, nby = -(-nx // 8), -(-ny // 8)
-        key = (((z >> 3) * nby + (y >> 3)) * nbx + (x >> 3)) * 512 + (z & 7) * 64 + (y & 7) * 8 + (x & 7)
+        key = brick_order_key(order, nx, ny, vol.size, len(order), nz)
         assert np.all(np.diff(key) >= 0)
 
 
