@@ -294,6 +294,21 @@ mi_status mi_metric_timing_read(mi_metric* m, double* ms4, int64_t* n_evals);
 mi_status mi_metric_set_fused(mi_metric* m, int fused);
 mi_status mi_metric_get_fused(const mi_metric* m, int* fused);
 
+/* Corner source of the split form's histogram pass (no reference counterpart; the
+ * reference's sampler reads its FP64 copy of the moving volume per sample,
+ * cuda/ops/resident.rs:153-333). Off (the default): the eight corners of a sample's
+ * cell come through the moving volume's texture. On: per brick of the sample layout,
+ * one TMA box load stages the part of the moving volume the brick can touch in shared
+ * memory, and the corners are read from there (bricks whose cells reach the volume's
+ * edge keep the texture). Same decisions, same corners, same bits. Refused with
+ * MI_ERR_INVALID_ARGUMENT when the moving volume's x size is not a multiple of 4 or the
+ * driver has no tensor-map encoder; an evaluation whose box does not fit two buffers
+ * in shared memory runs the texture pass. A staged-tile wait that does not complete
+ * within its limit returns MI_ERR_TIMEOUT. mi_metric_get_tile_staging reports the
+ * setting and how many evaluations ran with staged tiles. */
+mi_status mi_metric_set_tile_staging(mi_metric* m, int on);
+mi_status mi_metric_get_tile_staging(const mi_metric* m, int* on, int64_t* tiled_evals);
+
 /* The point-map stage (matrix row-major, offset: 12 doubles) a transform family
  * stores and multiplies (transform/parametric.rs:549-553, :1103-1107, :1331-1335),
  * and its Jacobian's affine form J(x) = jac0 + Σ_e x_e·jac_c[e] (jac0: 3×nparams

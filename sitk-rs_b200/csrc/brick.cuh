@@ -152,172 +152,86 @@ __device__ __forceinline__ int brick_sample(const SamplerParams& P, const BrickB
     return st;
 }
 
-// The CTA's share of the chunks: a contiguous range of ceil(nchunks / grid), so its
-// bricks are a contiguous range of runs (the table).
-__device__ __forceinline__ void brick_cta_range(uint32_t nchunks, uint32_t& c0, uint32_t& c1) {
-    const uint32_t per = (nchunks + gridDim.x - 1) / gridDim.x;
-    c0 = min(blockIdx.x * per, nchunks);
-    c1 = min(c0 + per, nchunks);
+// The chunk groups of a histogram launch: group g holds chunks g·W … g·W + W − 1 (W =
+// warps per CTA, one chunk per warp), and CTA c walks the contiguous groups
+// [⌊c·n/grid⌋, ⌊(c + 1)·n/grid⌋) of the n groups, so neighbouring bricks, whose moving
+// footprints overlap, run on the same SM (dealing the groups out round-robin balanced
+// the CTAs but measured slower: 194 against 176 µs for the 256³ whole grid, as every
+// CTA then sweeps the whole volume through its caches). The CTA's brick table holds,
+// group after group, the runs each group touches (tab_runs[tab_off[cta] …]), and
+// chunk_entry[c] is the table entry of chunk c's brick; both are built at set-up for
+// the launch's grid.
+__device__ __forceinline__ void brick_groups(uint32_t ngroups, uint32_t& g0, uint32_t& g1) {
+    // CTA c: groups [⌊c·n/grid⌋, ⌊(c+1)·n/grid⌋), the counts differing by at most one
+    g0 = (uint32_t)(((uint64_t)blockIdx.x * ngroups) / gridDim.x);
+    g1 = (uint32_t)(((uint64_t)(blockIdx.x + 1) * ngroups) / gridDim.x);
+}
+__device__ __forceinline__ void brick_table(const SamplerParams& P, const EvalArgs& a, BrickBase* tab) {
+    const uint32_t e0 = __ldg(a.tab_off + blockIdx.x), e1 = __ldg(a.tab_off + blockIdx.x + 1);
+    for (uint32_t t = threadIdx.x; t < e1 - e0; t += blockDim.x)
+        tab[t] = brick_base(P, __ldg(a.run_brick + __ldg(a.tab_runs + e0 + t)));
 }
 
-// The CTA's brick table: the constants of every brick its chunks touch. Returns the
-// first run.
-__device__ __forceinline__ uint32_t brick_table(const SamplerParams& P, const EvalArgs& a, uint32_t c0, uint32_t c1,
-                                                BrickBase* tab) {
-    uint32_t run0 = 0;
-    if (c0 < c1) {
-        run0 = __ldg(a.chunk_run + c0);
-        const uint32_t nr = __ldg(a.chunk_run + c1 - 1) - run0 + 1;
-        for (uint32_t t = threadIdx.x; t < nr; t += blockDim.x) tab[t] = brick_base(P, __ldg(a.run_brick + run0 + t));
-    }
-    return run0;
-}
-
-// Pass 1 over the brick layout: the CTA's chunks, warp w taking chunks c0 + w, c0 + w +
-// warps, …, one sample per lane; the next chunk's codes and run are requested a chunk
-// ahead. The histogram and its flush are hist_phase's (same fixed-point parts, copies
-// and flush), the records are indexed by the padded sample position.
-template <bool RECORD>
-__device__ __forceinline__ void brick_hist_phase(const SamplerParams& P, const EvalArgs& a, unsigned int* sh,
-                                                 BrickBase* tab) {
-    const int B = P.bins;
-    const int nb = B * B + B;
-    const int copies = a.copies, fine_copies = a.fine_copies;
-    const int cstride = hist_copy_stride(B);
-    const int fstride = hist_fine_stride(B);
-    unsigned int* sh_fine = sh + copies * cstride;
-    for (int i = threadIdx.x; i < copies * cstride + fine_copies * fstride; i += blockDim.x) sh[i] = 0u;
-    unsigned long long* colacc = reinterpret_cast<unsigned long long*>(sh + copies * cstride + fine_copies * fstride);
+// The CTA histogram of a brick-layout histogram pass (hist_phase's parts: coarse and
+// fine u32 fixed-point copies, lane-interleaved, and the joint part's column sums),
+// zeroed by brick_hist_zero and added into the global u64 histogram by
+// brick_hist_flush; brick_account adds one sample's taps and writes its record.
+struct BrickHist {
+    unsigned int* joint;  // this lane's coarse copy
+    unsigned int* fixed;  // this lane's fixed-count copy
+    unsigned int* fine;   // this lane's fine copy
+};
+__device__ __forceinline__ void brick_hist_zero(const EvalArgs& a, unsigned int* sh, int B) {
+    const int cstride = hist_copy_stride(B), fstride = hist_fine_stride(B);
+    for (int i = threadIdx.x; i < a.copies * cstride + a.fine_copies * fstride; i += blockDim.x) sh[i] = 0u;
+    unsigned long long* colacc =
+        reinterpret_cast<unsigned long long*>(sh + a.copies * cstride + a.fine_copies * fstride);
     if (a.gcols)
         for (int i = threadIdx.x; i < B; i += blockDim.x) colacc[i] = 0ull;
-    uint32_t c0, c1;
-    brick_cta_range(a.nchunks, c0, c1);
-    const uint32_t run0 = brick_table(P, a, c0, c1, tab);
-    __syncthreads();
-    unsigned int* sh_joint = sh;
-    unsigned int* sh_fixed = sh + B * B;
-    const float* __restrict__ moving = a.moving;
-    const uint8_t* __restrict__ mmask = a.mmask;
-    const uint32_t* __restrict__ codes = a.codes;
-    const uint32_t* __restrict__ chunk_run = a.chunk_run;
-    const float hist_scale = a.hist_scale, fine_scale = a.fine_scale;
-    const int fshift = 3 * P.brick_bl;
+}
+__device__ __forceinline__ BrickHist brick_hist_lane(const EvalArgs& a, unsigned int* sh, int B) {
+    const int cstride = hist_copy_stride(B), fstride = hist_fine_stride(B);
     const int lane = threadIdx.x & 31;
-    unsigned int* my_joint = sh_joint + (lane & (copies - 1)) * cstride;
-    unsigned int* my_fixed = sh_fixed + (lane & (copies - 1)) * cstride;
-    unsigned int* my_fine = sh_fine + (lane & (fine_copies - 1)) * fstride;
-    auto account = [&](int st, const Sample& o, uint32_t s, int fi) {
-        if (st != SAMPLE_VALID) {
-            if (RECORD) a.rec_bins[s] = 0;
-            return;
-        }
-        float w[4];
-        bspline3_taps(o.f, w);
-        const int off = fi * B + (o.mi - 1);
-        unsigned int* row = my_joint + off;
-        unsigned int* frow = my_fine + off;
-        atomicAdd(row + 1, __float_as_uint(fmaf(w[1], hist_scale, 12582912.0f)) - 0x4B400000u);
-        atomicAdd(row + 2, __float_as_uint(fmaf(w[2], hist_scale, 12582912.0f)) - 0x4B400000u);
-#pragma unroll
-        for (int t = 0; t < 4; t += 3) {
-            const bool fine = w[t] < FINE_LIMIT;
-            atomicAdd((fine ? frow : row) + t,
-                      __float_as_uint(fmaf(w[t], fine ? fine_scale : hist_scale, 12582912.0f)) - 0x4B400000u);
-        }
-        atomicAdd(my_fixed + fi, 1u);
-        if (RECORD) {
-            a.rec_bins[s] = (uint16_t)(o.mi | (fi << 8));
-            a.rec4[s] = make_float4(o.g[0], o.g[1], o.g[2], o.f);
-        }
-    };
-    // a sample the fast path could not decide, through the exact chain (out of line)
-    auto settle = [&](int st, const Prep& p, uint32_t code, uint32_t packed, uint32_t s) {
-        const int fi = (int)(code >> fshift);
-        Sample o;
-        if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
-        if (st == SAMPLE_EXACT) {
-            // the exact chain's result in its own object, so that the fast path's stays in
-            // registers
-            uint32_t i, j, k;
-            brick_ijk(P, packed, code, i, j, k);
-            Sample e;
-            st = sample_exact_ijk<RECORD>(P, i, j, k, moving, mmask, e);
-            account(st, e, s, fi);
-        } else {
-            account(st, o, s, fi);
-        }
-    };
-    const uint32_t nw = blockDim.x >> 5;
-    uint32_t c = c0 + (threadIdx.x >> 5);
-    uint32_t code = c < c1 ? __ldg(codes + (size_t)c * BRICK_CHUNK + lane) : BRICK_PAD;
-    uint32_t run = c < c1 ? __ldg(chunk_run + c) : run0;
-    if (BRICK_PIPELINE) {
-        // Software-pipelined: the next chunk's corner gathers are requested before this
-        // chunk's sample is finished, so a thread keeps two samples' gathers in flight;
-        // codes are requested two chunks ahead.
-        constexpr int NONE = -1;
-        Prep pc;
-        int stc = NONE;
-        uint32_t pkc = 0u, codec = code;
-        if (c < c1 && code != BRICK_PAD) {
-            const BrickBase b = tab[run - run0];
-            pkc = b.packed;
-            stc = P.has_mmask ? brick_prep<true>(P, b, code, mmask, pc) : brick_prep<false>(P, b, code, mmask, pc);
-        }
-        uint32_t cn = c + nw;
-        uint32_t code_n = cn < c1 ? __ldg(codes + (size_t)cn * BRICK_CHUNK + lane) : BRICK_PAD;
-        uint32_t run_n = cn < c1 ? __ldg(chunk_run + cn) : run0;
-        for (; c < c1; c += nw) {
-            const uint32_t cn2 = cn + nw;
-            const uint32_t code_n2 = cn2 < c1 ? __ldg(codes + (size_t)cn2 * BRICK_CHUNK + lane) : BRICK_PAD;
-            const uint32_t run_n2 = cn2 < c1 ? __ldg(chunk_run + cn2) : run0;
-            Prep pn;
-            int stn = NONE;
-            uint32_t pkn = 0u;
-            if (cn < c1 && code_n != BRICK_PAD) {
-                const BrickBase b = tab[run_n - run0];
-                pkn = b.packed;
-                stn = P.has_mmask ? brick_prep<true>(P, b, code_n, mmask, pn)
-                                  : brick_prep<false>(P, b, code_n, mmask, pn);
-            }
-            if (stc != NONE) settle(stc, pc, codec, pkc, c * BRICK_CHUNK + lane);
-            pc = pn;
-            stc = stn;
-            pkc = pkn;
-            codec = code_n;
-            cn = cn2;
-            code_n = code_n2;
-            run_n = run_n2;
-        }
-    } else
-    for (; c < c1; c += nw) {
-        const uint32_t cn = c + nw;
-        const uint32_t code_n = cn < c1 ? __ldg(codes + (size_t)cn * BRICK_CHUNK + lane) : BRICK_PAD;
-        const uint32_t run_n = cn < c1 ? __ldg(chunk_run + cn) : run0;
-        if (code != BRICK_PAD) {
-            const BrickBase b = tab[run - run0];
-            const uint32_t s = c * BRICK_CHUNK + lane;
-            const int fi = (int)(code >> fshift);
-            Prep p;
-            Sample o;
-            int st = P.has_mmask ? brick_prep<true>(P, b, code, mmask, p) : brick_prep<false>(P, b, code, mmask, p);
-            if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
-            if (st == SAMPLE_EXACT) {
-                uint32_t i, j, k;
-                brick_ijk(P, b.packed, code, i, j, k);
-                Sample e;
-                st = sample_exact_ijk<RECORD>(P, i, j, k, moving, mmask, e);
-                account(st, e, s, fi);
-            } else {
-                account(st, o, s, fi);
-            }
-        }
-        code = code_n;
-        run = run_n;
+    BrickHist h;
+    h.joint = sh + (lane & (a.copies - 1)) * cstride;
+    h.fixed = sh + B * B + (lane & (a.copies - 1)) * cstride;
+    h.fine = sh + a.copies * cstride + (lane & (a.fine_copies - 1)) * fstride;
+    return h;
+}
+template <bool RECORD>
+__device__ __forceinline__ void brick_account(const EvalArgs& a, const BrickHist& h, int B, int st, const Sample& o,
+                                              uint32_t s, int fi) {
+    if (st != SAMPLE_VALID) {
+        if (RECORD) a.rec_bins[s] = 0;
+        return;
     }
-    __syncthreads();
-    unsigned long long* rep_hist = a.ghist;
-    unsigned long long* rep_cols = a.gcols;
+    float w[4];
+    bspline3_taps(o.f, w);
+    const int off = fi * B + (o.mi - 1);
+    unsigned int* row = h.joint + off;
+    unsigned int* frow = h.fine + off;
+    // round(w·scale) by the 1.5·2^23 magic add (w·scale < 2^22 for both parts)
+    atomicAdd(row + 1, __float_as_uint(fmaf(w[1], a.hist_scale, 12582912.0f)) - 0x4B400000u);
+    atomicAdd(row + 2, __float_as_uint(fmaf(w[2], a.hist_scale, 12582912.0f)) - 0x4B400000u);
+#pragma unroll
+    for (int t = 0; t < 4; t += 3) {
+        const bool fine = w[t] < FINE_LIMIT;
+        atomicAdd((fine ? frow : row) + t,
+                  __float_as_uint(fmaf(w[t], fine ? a.fine_scale : a.hist_scale, 12582912.0f)) - 0x4B400000u);
+    }
+    atomicAdd(h.fixed + fi, 1u);
+    if (RECORD) {
+        a.rec_bins[s] = (uint16_t)(o.mi | (fi << 8));
+        a.rec4[s] = make_float4(o.g[0], o.g[1], o.g[2], o.f);
+    }
+}
+// After the CTA's last sample (the caller synchronises the CTA first).
+__device__ __forceinline__ void brick_hist_flush(const EvalArgs& a, unsigned int* sh, int B) {
+    const int nb = B * B + B;
+    const int copies = a.copies, fine_copies = a.fine_copies;
+    const int cstride = hist_copy_stride(B), fstride = hist_fine_stride(B);
+    const unsigned int* sh_fine = sh + copies * cstride;
+    unsigned long long* colacc = reinterpret_cast<unsigned long long*>(sh + copies * cstride + fine_copies * fstride);
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
         unsigned long long v = 0ull;
         for (int cc = 0; cc < copies; ++cc) v += sh[cc * cstride + i];
@@ -327,17 +241,123 @@ __device__ __forceinline__ void brick_hist_phase(const SamplerParams& P, const E
             v = (v << a.fine_shift) + f;
             if (a.gcols && v) atomicAdd(&colacc[i % B], v);
         }
-        if (v) atomicAdd(&rep_hist[i], v);
+        if (v) atomicAdd(&a.ghist[i], v);
     }
     if (a.gcols) {
         __syncthreads();
         for (int m = threadIdx.x; m < B; m += blockDim.x)
-            if (colacc[m]) atomicAdd(&rep_cols[m], colacc[m]);
+            if (colacc[m]) atomicAdd(&a.gcols[m], colacc[m]);
     }
 }
 
+// A sample the fast path could not take to the end: finish_fast, then the exact chain
+// (out of line) where a decision is open; accounted either way. The exact chain's result
+// lives in its own object so that the fast path's stays in registers.
+template <bool RECORD>
+__device__ __forceinline__ void brick_settle(const SamplerParams& P, const EvalArgs& a, const BrickHist& h, int st,
+                                             const Prep& p, uint32_t code, uint32_t packed, uint32_t s) {
+    const int fi = (int)(code >> (3 * P.brick_bl));
+    Sample o;
+    if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
+    if (st == SAMPLE_EXACT) {
+        uint32_t i, j, k;
+        brick_ijk(P, packed, code, i, j, k);
+        Sample e;
+        st = sample_exact_ijk<RECORD>(P, i, j, k, a.moving, a.mmask, e);
+        brick_account<RECORD>(a, h, P.bins, st, e, s, fi);
+    } else {
+        brick_account<RECORD>(a, h, P.bins, st, o, s, fi);
+    }
+}
+
+// Pass 1 over the brick layout: the CTA's chunk groups (brick_table), one sample per
+// lane, the corners through the moving volume's texture.
+template <bool RECORD>
+__device__ __forceinline__ void brick_hist_phase(const SamplerParams& P, const EvalArgs& a, unsigned int* sh,
+                                                 BrickBase* tab) {
+    const int B = P.bins;
+    brick_hist_zero(a, sh, B);
+    brick_table(P, a, tab);
+    __syncthreads();
+    const uint8_t* __restrict__ mmask = a.mmask;
+    const uint32_t* __restrict__ codes = a.codes;
+    const int lane = threadIdx.x & 31;
+    const BrickHist h = brick_hist_lane(a, sh, B);
+    // this warp's chunk of each of the CTA's groups; the next group's code, run and table
+    // entry are requested a group ahead
+    const uint32_t nw = blockDim.x >> 5, warp = threadIdx.x >> 5;
+    const uint32_t nchunks = a.nchunks;
+    const uint32_t ngroups = (nchunks + nw - 1) / nw;
+    const uint32_t* __restrict__ centry = a.chunk_entry;
+    uint32_t g0, g1;
+    brick_groups(ngroups, g0, g1);
+    auto fetch = [&](uint32_t g, uint32_t& code, uint32_t& entry) {
+        const uint32_t c = g * nw + warp;
+        code = BRICK_PAD;
+        entry = 0u;
+        if (g < g1 && c < nchunks) {
+            code = __ldg(codes + (size_t)c * BRICK_CHUNK + lane);
+            entry = __ldg(centry + c);
+        }
+    };
+    uint32_t g = g0;
+    uint32_t code, entry;
+    fetch(g, code, entry);
+    if (BRICK_PIPELINE) {
+        // Software-pipelined: the next group's corner gathers are requested before this
+        // group's sample is finished, so a thread keeps two samples' gathers in flight.
+        constexpr int NONE = -1;
+        Prep pc;
+        int stc = NONE;
+        uint32_t pkc = 0u, codec = code;
+        if (code != BRICK_PAD) {
+            const BrickBase b = tab[entry];
+            pkc = b.packed;
+            stc = P.has_mmask ? brick_prep<true>(P, b, code, mmask, pc) : brick_prep<false>(P, b, code, mmask, pc);
+        }
+        uint32_t code_n, entry_n;
+        fetch(g + 1, code_n, entry_n);
+        for (; g < g1; ++g) {
+            uint32_t code_n2, entry_n2;
+            fetch(g + 2, code_n2, entry_n2);
+            Prep pn;
+            int stn = NONE;
+            uint32_t pkn = 0u;
+            if (code_n != BRICK_PAD) {
+                const BrickBase b = tab[entry_n];
+                pkn = b.packed;
+                stn = P.has_mmask ? brick_prep<true>(P, b, code_n, mmask, pn)
+                                  : brick_prep<false>(P, b, code_n, mmask, pn);
+            }
+            if (stc != NONE) brick_settle<RECORD>(P, a, h, stc, pc, codec, pkc, (g * nw + warp) * BRICK_CHUNK + lane);
+            pc = pn;
+            stc = stn;
+            pkc = pkn;
+            codec = code_n;
+            code_n = code_n2;
+            entry_n = entry_n2;
+        }
+    } else {
+        for (; g < g1; ++g) {
+            uint32_t code_n, entry_n;
+            fetch(g + 1, code_n, entry_n);
+            if (code != BRICK_PAD) {
+                const BrickBase b = tab[entry];
+                Prep p;
+                const int st =
+                    P.has_mmask ? brick_prep<true>(P, b, code, mmask, p) : brick_prep<false>(P, b, code, mmask, p);
+                brick_settle<RECORD>(P, a, h, st, p, code, b.packed, (g * nw + warp) * BRICK_CHUNK + lane);
+            }
+            code = code_n;
+            entry = entry_n;
+        }
+    }
+    __syncthreads();
+    brick_hist_flush(a, sh, B);
+}
+
 // Pass 2's record groups over the brick layout: four consecutive padded samples (one
-// chunk holds eight groups), their codes, and their brick's x(origin) − x_ref.
+// chunk holds eight groups), their codes, and their chunk's x(brick origin) − x_ref.
 struct BrickGroup {
     uint2 b;
     float4 r[4];  // per sample: gx, gy, gz, Parzen fraction
@@ -349,7 +369,7 @@ __device__ __forceinline__ void brick_load_group(const EvalArgs& a, uint32_t q, 
 #pragma unroll
     for (int u = 0; u < 4; ++u) g.r[u] = __ldcg(a.rec4 + 4 * (size_t)q + u);
     g.code = __ldg(reinterpret_cast<const uint4*>(a.codes) + q);
-    g.xb = __ldg(a.run_xbase + __ldg(a.chunk_run + (q >> 3)));
+    g.xb = __ldg(a.chunk_xbase + (q >> 3));
 }
 
 // One record's moments: w = Σ_taps B₃′·pRatio, A[d] += w g_d, B[d][e] += w g_d dx_e.

@@ -214,13 +214,18 @@ struct EvalArgs {
     // system-scope fence once everything else is there (the host may poll it)
     unsigned long long seq = 0;
     // the single-metric evaluation's brick layout (brick.cuh): a code per padded
-    // sample, the run (brick) of every chunk of 32, each run's packed brick coordinates
-    // and x(brick origin) − x_ref
+    // sample, the run (brick) of every chunk of 32 and its brick's x(origin) − x_ref,
+    // each run's packed brick coordinates
     const uint32_t* codes = nullptr;
     const uint32_t* chunk_run = nullptr;
     const uint32_t* run_brick = nullptr;
-    const float4* run_xbase = nullptr;
+    const float4* chunk_xbase = nullptr;
     uint32_t nchunks = 0;
+    // the histogram launch's brick tables (brick.cuh brick_table): per CTA its runs
+    // (tab_runs[tab_off[cta] … tab_off[cta + 1]]), per chunk its brick's entry
+    const uint32_t* tab_runs = nullptr;
+    const uint32_t* tab_off = nullptr;
+    const uint32_t* chunk_entry = nullptr;
     float4* rec4 = nullptr;  // brick layout's records: gx, gy, gz, Parzen fraction per padded sample
 };
 constexpr int RESULT_ERR = 2 + MI_MAX_PARAMS;  // result slot holding the error word
@@ -725,6 +730,15 @@ __device__ __forceinline__ double fold_slices(const double* vs, int ns, bool glo
     return v;
 }
 
+// The error word a histogram pass with staged tiles raises (sync[3], a wait that timed
+// out), as the result's error slot, and cleared for the next evaluation. Run by the one
+// thread that writes the result.
+__device__ __forceinline__ double carry_error(const EvalArgs& a) {
+    const unsigned int e = *reinterpret_cast<volatile unsigned int*>(a.sync + 3);
+    if (e) a.sync[3] = 0u;
+    return e ? __longlong_as_double((long long)e) : 0.0;
+}
+
 // One warp: value and valid into result (lane 0), from the slice sums.
 __device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
     const int lane = threadIdx.x & 31;
@@ -736,7 +750,7 @@ __device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
         if (a.result_host) {
             a.result_host[0] = r0;
             a.result_host[1] = r1;
-            a.result_host[RESULT_ERR] = 0.0;  // the split form has no barrier to time out
+            a.result_host[RESULT_ERR] = carry_error(a);  // a staged-tile wait that timed out
         }
     }
 }
@@ -831,7 +845,7 @@ __device__ __forceinline__ void tail_once(int B, double moving_bin_size, const E
             if (mirror && a.result_host) {
                 a.result_host[0] = r0;
                 a.result_host[1] = r1;
-                a.result_host[RESULT_ERR] = 0.0;
+                a.result_host[RESULT_ERR] = carry_error(a);
             }
         }
     }
@@ -1017,7 +1031,7 @@ __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double
 // the value has the bits of every other form. No CTA waits for another before its
 // record stream, and the histogram pass ends at its flush.
 __host__ __device__ inline size_t stream_smem(int B) {
-    return 32 * (size_t)NMOM * sizeof(double) + (size_t)B * B * sizeof(float) + (size_t)4 * B * 8 +
+    return 32 * (size_t)NMOM * sizeof(double) + (size_t)B * B * sizeof(float) + (size_t)2 * B * 8 +
            (((size_t)2 * B + 7) & ~(size_t)7) + 8;
 }
 
@@ -1029,9 +1043,7 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
     float* pr = reinterpret_cast<float*>(dsh + 32 * NMOM);
     unsigned long long* col = reinterpret_cast<unsigned long long*>(pr + B2);
     unsigned long long* cnt = col + B;
-    double* lcol = reinterpret_cast<double*>(cnt + B);
-    double* lfm = lcol + B;
-    uint8_t* okm = reinterpret_cast<uint8_t*>(lfm + B);
+    uint8_t* okm = reinterpret_cast<uint8_t*>(cnt + B);
     uint8_t* okf = okm + B;
     unsigned long long* jmin_s = reinterpret_cast<unsigned long long*>(okm + ((2 * B + 7) & ~7));
     const int lane = threadIdx.x & 31;
@@ -1061,34 +1073,67 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
     typename Src::Group cur;
     if (q < w.end) Src::load(a, q, cur);
     __syncthreads();
+    // The pRatio table needs the ε flags of the margins and the least passing joint
+    // count, not the margins' logarithms: those feed only the value, whose slices are
+    // summed after this CTA's records (off the path to its moments).
     const TailCtx t = tail_scalars(B, col, cnt, a.hist_inv, P.moving_bin_size);
-    if ((int)threadIdx.x < B) margin_terms(threadIdx.x, col, cnt, t, okm, okf, lcol, lfm);
-    if (threadIdx.x == blockDim.x - 1) *jmin_s = least_joint(t.dt);
+    if ((int)threadIdx.x < B) {
+        const int m = threadIdx.x;
+        okm[m] = (double)col[m] / t.dt > DBL_EPSILON;
+        okf[m] = (double)cnt[m] / t.joint_sum > DBL_EPSILON;
+    }
+    if (threadIdx.x < 32) {
+        // the least jv ≥ 1 with jv/total > ε (monotone in jv): eight candidates around
+        // ε·total tested at once; the serial search (least_joint) only when the boundary
+        // is not among them
+        const long long c0 = (long long)(DBL_EPSILON * t.dt);
+        const long long cand = c0 - 3 + lane;
+        const bool pass = lane < 8 && cand >= 1 && (double)cand / t.dt > DBL_EPSILON;
+        const unsigned int hit = __ballot_sync(0xffffffffu, pass) & 0xffu;
+        if (lane == 0) {
+            const int k = hit ? __ffs(hit) - 1 : 8;
+            *jmin_s = k >= 1 && k < 8 ? (unsigned long long)(c0 - 3 + k) : least_joint(t.dt);
+        }
+    }
     __syncthreads();
     const unsigned long long jmin = *jmin_s;
     const float nf = (float)t.n_factor;
-    const int units = (int)w.units, unit = (int)w.unit;
     for (int i0 = wfirst; i0 < ns * 32; i0 += R * bd) {
         if (i0 != wfirst) load_round(i0);
 #pragma unroll
         for (int u = 0; u < R; ++u) {
-            const int iw = i0 + u * bd;  // warp-uniform: the slice's first bin
-            if (iw < ns * 32) {
-                const int i = iw + lane;
+            const int i = i0 + u * bd + lane;
+            if (i < B2) {
                 const int f = i / B, m = i - f * B;
-                const bool take = i < B2 && !t.degenerate && okf[f] && okm[m] && jv[u] >= jmin;
-                if (i < B2) pr[i] = pr_entry(take, jv[u], col[m], nf);
-                const int sl = iw >> 5;
-                if (sl % units == unit) {
-                    const double term =
-                        slice_sum(take ? value_term(jv[u], true, log((double)jv[u]), lcol[m], lfm[f], t) : 0.0);
-                    if (lane == 0) a.vsum[sl] = term;
-                }
+                const bool take = !t.degenerate && okf[f] && okm[m] && jv[u] >= jmin;
+                pr[i] = pr_entry(take, jv[u], col[m], nf);
             }
         }
     }
     __syncthreads();
     if (!t.degenerate) Src::stream(P, a, pr, q, w.end, w.stride, cur, acc);
+    // the value slices that fall to this CTA (slices unit + units·(u + k·warps) to warp
+    // u), each bin's term from the logarithms the other forms take (margin_terms,
+    // value_term)
+    if (!t.degenerate) {
+        const int nwarp = bd >> 5;
+        for (int sl = (int)(threadIdx.x >> 5) * (int)w.units + (int)w.unit; sl < ns;
+             sl += nwarp * (int)w.units) {
+            const int i = sl * 32 + lane;
+            double term = 0.0;
+            if (i < B2) {
+                const int f = i / B, m = i - f * B;
+                const unsigned long long v = __ldcg(a.ghist + i);
+                if (okf[f] && okm[m] && v >= jmin) {
+                    const double lcol = log((double)col[m]);
+                    const double lfm = log((double)cnt[f] / t.joint_sum);
+                    term = value_term(v, true, log((double)v), lcol, lfm, t);
+                }
+            }
+            term = slice_sum(term);
+            if (lane == 0) a.vsum[sl] = term;
+        }
+    }
     store_moments(acc, red, w.part, w.part_stride);
     return t;
 }

@@ -107,6 +107,8 @@ struct SamplerParams {
 
 // Per-metric device scratch and the host-side view of it.
 struct Workspace {
+    int staging = 0;                     // corner source of the histogram pass: 0 texture, 1 TMA-staged tiles
+    int64_t tiled_evals = 0;             // evaluations whose histogram pass ran with staged tiles
     unsigned long long* hist = nullptr;  // [bins*bins] joint (2^-32 fixed point), [bins] fixed marginal, [1] valid
     double* partials = nullptr;          // [grid_deriv][12]
     double* vsum = nullptr;              // value slice sums
@@ -172,9 +174,22 @@ struct mi_metric {
     uint32_t* codes = nullptr;      // [nchunks·32] offset in the brick | fixed bin; padding BRICK_PAD
     uint32_t* chunk_run = nullptr;  // [nchunks] run (non-empty brick) of each chunk
     uint32_t* run_brick = nullptr;  // [nruns] packed brick coordinates
-    float4* run_xbase = nullptr;    // [nruns] x(brick origin) − x_ref
+    float4* chunk_xbase = nullptr;  // [nchunks] x(origin of the chunk's brick) − x_ref
     int64_t nchunks = 0, nruns = 0;
+    uint32_t* run_chunk0 = nullptr; // [nruns + 1] first chunk of every run
+    // TMA-staged moving tiles (tile.cuh): available when the linear moving volume meets the
+    // tensor-map rules; the map is re-encoded when an evaluation needs another box
+    bool tile_capable = false;
+    alignas(64) unsigned char tmap[128] = {};  // CUtensorMap of the moving volume
+    int tile_box[3] = {0, 0, 0};
+    int tile_grid = 0;              // one CTA per SM
+    int64_t tile_per_thread = 0;    // most samples a tile-pass thread takes
+    // the histogram launch's chunk-group tables (brick.cuh brick_table), for table_grid CTAs
+    uint32_t* tab_runs = nullptr;
+    uint32_t* tab_off = nullptr;
+    uint32_t* chunk_entry = nullptr;
     int table_cap = 1;              // brick-table entries a histogram CTA needs
+    int table_grid = 0;
     int bins = 0;
     mi_metric_info info{};
     mi::SamplerParams base{};     // everything except the stages

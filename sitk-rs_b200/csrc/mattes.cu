@@ -29,6 +29,7 @@
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_run_length_encode.cuh>
 #include <cub/device/device_scan.cuh>
@@ -47,6 +48,7 @@
 #include "sampler.cuh"
 #include "eval_device.cuh"
 #include "brick.cuh"
+#include "tile.cuh"
 #include "point_map.h"
 
 namespace mi {
@@ -143,6 +145,19 @@ k_deriv(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobia
     for (int i = threadIdx.x; i < P.bins; i += blockDim.x) a.gcols[i] = 0ull;
 }
 
+// The histogram pass with TMA-staged moving tiles (tile.cuh), one CTA per SM; a
+// value-only evaluation ends with the tail in the CTA that flushes last, as in k_hist.
+template <bool RECORD>
+__global__ void __launch_bounds__(TILE_BLOCK, 1)
+k_hist_tile(const __grid_constant__ SamplerParams P, EvalArgs a, const __grid_constant__ CUtensorMap tmap,
+            TileArgs T) {
+    extern __shared__ __align__(128) unsigned char tsh[];
+    pdl_launch_dependents();
+    tile_hist_phase<RECORD>(P, a, &tmap, T, tsh);
+    if (RECORD || !last_to_arrive(a.sync + 1)) return;
+    tail_once(P.bins, P.moving_bin_size, a, tsh, true);
+}
+
 // Per-sample decisions of the brick sampler the kernels use, for the exactness tests,
 // per padded position (a padding lane reports status −1).
 __global__ void k_decisions(const __grid_constant__ SamplerParams P, const float* __restrict__ moving,
@@ -236,11 +251,11 @@ __global__ void k_run_chunks(const int* __restrict__ counts, int64_t nruns, uint
         nch[r] = (uint32_t)((counts[r] + BRICK_CHUNK - 1) / BRICK_CHUNK);
 }
 
-// Per run (a non-empty brick): its packed coordinates, x(origin) − x_ref in FP32, and
-// the run index of each of its chunks.
+// Per run (a non-empty brick): its packed coordinates, and for each of its chunks the
+// run index and x(brick origin) − x_ref in FP32.
 __global__ void k_run_fill(const uint32_t* __restrict__ bid, int64_t nruns, const uint32_t* __restrict__ chunk_off,
                            const uint32_t* __restrict__ nch, int64_t nbx, int64_t nby, int bl, SamplerParams P,
-                           uint32_t* __restrict__ run_brick, float4* __restrict__ run_xbase,
+                           uint32_t* __restrict__ run_brick, float4* __restrict__ chunk_xbase,
                            uint32_t* __restrict__ chunk_run) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nruns; r += (int64_t)gridDim.x * blockDim.x) {
         const int64_t b = bid[r];
@@ -252,8 +267,10 @@ __global__ void k_run_fill(const uint32_t* __restrict__ bid, int64_t nruns, cons
             const double x = P.forigin[d] + P.fi2p[d * 3] * o[0] + P.fi2p[d * 3 + 1] * o[1] + P.fi2p[d * 3 + 2] * o[2];
             xb[d] = (float)(x - P.xref[d]);
         }
-        run_xbase[r] = make_float4(xb[0], xb[1], xb[2], 0.0f);
-        for (uint32_t c = 0; c < nch[r]; ++c) chunk_run[chunk_off[r] + c] = (uint32_t)r;
+        for (uint32_t c = 0; c < nch[r]; ++c) {
+            chunk_run[chunk_off[r] + c] = (uint32_t)r;
+            chunk_xbase[chunk_off[r] + c] = make_float4(xb[0], xb[1], xb[2], 0.0f);
+        }
     }
 }
 
@@ -273,16 +290,6 @@ __global__ void k_scatter_codes(const uint32_t* __restrict__ samples, const uint
         const int64_t y = row % ny, z = row / ny;
         codes[p0 + t] = (uint32_t)((x & msk) | ((y & msk) << bl) | ((z & msk) << (2 * bl)) |
                                    ((int64_t)fbin[s0 + t] << (3 * bl)));
-    }
-}
-
-// The most runs (table entries) any CTA of a `grid`-CTA histogram launch meets.
-__global__ void k_table_need(const uint32_t* __restrict__ chunk_run, uint32_t nchunks, uint32_t grid,
-                             unsigned int* __restrict__ need) {
-    const uint32_t per = (nchunks + grid - 1) / grid;
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < grid; c += gridDim.x * blockDim.x) {
-        const uint32_t c0 = min(c * per, nchunks), c1 = min(c0 + per, nchunks);
-        if (c0 < c1) atomicMax(need, chunk_run[c1 - 1] - chunk_run[c0] + 1);
     }
 }
 
@@ -406,7 +413,11 @@ void free_metric(mi_metric* m) {
     cudaFree(m->codes);
     cudaFree(m->chunk_run);
     cudaFree(m->run_brick);
-    cudaFree(m->run_xbase);
+    cudaFree(m->chunk_xbase);
+    cudaFree(m->run_chunk0);
+    cudaFree(m->tab_runs);
+    cudaFree(m->tab_off);
+    cudaFree(m->chunk_entry);
     cudaFree(m->ws.hist);
     cudaFree(m->ws.partials);
     cudaFree(m->ws.vsum);
@@ -627,8 +638,11 @@ mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams&
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->chunk_run, 0, 4, st));
         MI_CHECK_CUDA(ctx, cudaMalloc(&m->run_brick, 4));
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->run_brick, 0, 4, st));
-        MI_CHECK_CUDA(ctx, cudaMalloc(&m->run_xbase, sizeof(float4)));
-        MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->run_xbase, 0, sizeof(float4), st));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->chunk_xbase, sizeof(float4)));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->chunk_xbase, 0, sizeof(float4), st));
+        const uint32_t r0[2] = {0u, 1u};
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->run_chunk0, 2 * 4));
+        MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->run_chunk0, r0, 2 * 4, cudaMemcpyHostToDevice, st));
         MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
         return MI_OK;
     }
@@ -692,34 +706,171 @@ mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams&
     TRY_L(cudaMemsetAsync(m->codes, 0xFF, (size_t)nchunks * BRICK_CHUNK * 4, st));
     TRY_L(cudaMalloc(&m->chunk_run, (size_t)nchunks * 4));
     TRY_L(cudaMalloc(&m->run_brick, (size_t)nruns * 4));
-    TRY_L(cudaMalloc(&m->run_xbase, (size_t)nruns * sizeof(float4)));
+    TRY_L(cudaMalloc(&m->chunk_xbase, (size_t)nchunks * sizeof(float4)));
     k_run_fill<<<grid_for(nruns, block, ctx->num_sms * 8), block, 0, st>>>(uniq, nruns, chunk_off, nch, nbx, nby, bl,
-                                                                           P, m->run_brick, m->run_xbase, m->chunk_run);
+                                                                           P, m->run_brick, m->chunk_xbase, m->chunk_run);
     TRY_L(cudaGetLastError());
     k_scatter_codes<<<(unsigned)nruns, block, 0, st>>>(m->samples, m->fbin, counts, run_start, chunk_off, nx, ny, bl,
                                                        m->codes);
     TRY_L(cudaGetLastError());
+    // the first chunk of every run, and the chunk count after the last
+    TRY_L(cudaMalloc(&m->run_chunk0, ((size_t)nruns + 1) * 4));
+    TRY_L(cudaMemcpyAsync(m->run_chunk0, chunk_off, (size_t)nruns * 4, cudaMemcpyDeviceToDevice, st));
+    {
+        const uint32_t total = (uint32_t)nchunks;
+        TRY_L(cudaMemcpyAsync(m->run_chunk0 + nruns, &total, 4, cudaMemcpyHostToDevice, st));
+        TRY_L(cudaStreamSynchronize(st));
+    }
 #undef TRY_L
     return done(MI_OK);
 }
 
-// Brick-table entries a `grid`-CTA histogram launch needs.
-mi_status brick_table_need(mi_context* ctx, const mi_metric* m, int grid, int* need) {
-    unsigned int* d = nullptr;
-    MI_CHECK_CUDA(ctx, cudaMalloc(&d, sizeof(unsigned int)));
-    unsigned int h = 1;
-    cudaError_t e = cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) {
-        k_table_need<<<grid_for(grid, 256, 64), 256, 0, ctx->stream>>>(m->chunk_run, (uint32_t)m->nchunks,
-                                                                       (uint32_t)grid, d);
-        e = cudaGetLastError();
+// The brick tables of a `grid`-CTA histogram launch (brick.cuh brick_table): chunk
+// groups of W = HIST_BLOCK/32 consecutive chunks, CTA c taking groups
+// [⌊c·n/grid⌋, ⌊(c+1)·n/grid⌋) of the n groups;
+// per CTA, group after group, the runs the group touches; per chunk the table entry of
+// its brick.
+// Sets m->table_cap to the longest CTA table.
+mi_status build_brick_tables(mi_context* ctx, mi_metric* m, int grid) {
+    cudaStream_t st = ctx->stream;
+    const int64_t nch = m->nchunks;
+    const int64_t W = HIST_BLOCK / 32;
+    const int64_t ngroups = (nch + W - 1) / W;
+    std::vector<uint32_t> run((size_t)nch);
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(run.data(), m->chunk_run, (size_t)nch * 4, cudaMemcpyDeviceToHost, st));
+    MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+    std::vector<uint32_t> off((size_t)grid + 1, 0u), entry((size_t)nch, 0u), runs;
+    runs.reserve((size_t)(ngroups + m->nruns + grid));
+    int cap = 1;
+    for (int c = 0; c < grid; ++c) {
+        off[c] = (uint32_t)runs.size();
+        const int64_t g0 = (int64_t)c * ngroups / grid, g1 = (int64_t)(c + 1) * ngroups / grid;
+        for (int64_t g = g0; g < g1; ++g) {
+            const int64_t f = g * W, l = std::min(f + W, nch) - 1;
+            const uint32_t base = (uint32_t)(runs.size() - off[c]);
+            for (uint32_t r = run[(size_t)f]; r <= run[(size_t)l]; ++r) runs.push_back(r);
+            for (int64_t k = f; k <= l; ++k) entry[(size_t)k] = base + (run[(size_t)k] - run[(size_t)f]);
+        }
+        cap = std::max(cap, (int)(runs.size() - off[c]));
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    cudaFree(d);
-    if (e != cudaSuccess) return cuda_status(ctx, e, "brick_table_need");
-    *need = (int)std::max(h, 1u);
+    off[grid] = (uint32_t)runs.size();
+    if (runs.empty()) runs.push_back(0u);
+    cudaFree(m->tab_runs);
+    cudaFree(m->tab_off);
+    cudaFree(m->chunk_entry);
+    m->tab_runs = m->tab_off = m->chunk_entry = nullptr;
+    MI_CHECK_CUDA(ctx, cudaMalloc(&m->tab_runs, runs.size() * 4));
+    MI_CHECK_CUDA(ctx, cudaMalloc(&m->tab_off, off.size() * 4));
+    MI_CHECK_CUDA(ctx, cudaMalloc(&m->chunk_entry, entry.size() * 4));
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->tab_runs, runs.data(), runs.size() * 4, cudaMemcpyHostToDevice, st));
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->tab_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st));
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->chunk_entry, entry.data(), entry.size() * 4, cudaMemcpyHostToDevice, st));
+    MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
+    m->table_cap = cap;
+    m->table_grid = grid;
     return MI_OK;
+}
+
+// The tensor-map encoder of the driver (cuTensorMapEncodeTiled), found once.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The staged-tile pass's shape (tile.cuh): whether the linear moving volume meets the
+// tensor-map rules (row pitch a multiple of 16 bytes), its grid (one CTA per SM), and the
+// most samples one of its threads takes: over the CTAs' contiguous chunk ranges, the
+// sum over their runs of ceil(chunks / 16).
+mi_status tile_setup(mi_context* ctx, mi_metric* m) {
+    const int64_t nx = m->mgeo.size[0];
+    m->tile_capable = nx % 4 == 0 && tensor_map_encoder() != nullptr && m->nchunks > 0;
+    m->tile_grid = ctx->num_sms;
+    if (!m->tile_capable) return MI_OK;
+    const int64_t nch = m->nchunks;
+    std::vector<uint32_t> run((size_t)nch);
+    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(run.data(), m->chunk_run, (size_t)nch * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    MI_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int64_t most = 1;
+    const int64_t G = m->tile_grid;
+    for (int64_t c = 0; c < G; ++c) {
+        const int64_t c0 = c * nch / G, c1 = (c + 1) * nch / G;
+        int64_t sum = 0;
+        for (int64_t k = c0; k < c1;) {
+            int64_t e = k;
+            while (e < c1 && run[(size_t)e] == run[(size_t)k]) ++e;
+            sum += (e - k + TILE_CONSUMER_WARPS - 1) / TILE_CONSUMER_WARPS;
+            k = e;
+        }
+        most = std::max(most, sum);
+    }
+    m->tile_per_thread = most;
+    return MI_OK;
+}
+
+// The tile geometry of one evaluation (box from the brick's extent in moving index
+// space, the ring's depth from the shared memory left), the tensor map re-encoded when
+// the box changes. Returns false when the box does not fit two buffers.
+bool tile_args(mi_metric* m, const SamplerParams& P, TileArgs& T, size_t& smem) {
+    int cells[3];
+    for (int d = 0; d < 3; ++d) {
+        const double span = P.hi_ext[d] - P.lo_ext[d];
+        if (!(span >= 0.0 && span < 240.0)) return false;
+        cells[d] = (int)std::floor(span) + 3;
+    }
+    T.bx = (cells[0] + 3 + 3) & ~3;
+    T.by = cells[1];
+    T.bz = cells[2];
+    if (T.bx > 256 || T.by > 256 || T.bz > 256) return false;
+    T.tile_floats = (uint32_t)(T.bx * T.by * T.bz);
+    T.tile_stride = (T.tile_floats + 31u) & ~31u;
+    const int B = m->bins;
+    const size_t hist = (hist_region_bytes(B, hist_copies(B), hist_fine_copies(B)) + 127) & ~(size_t)127;
+    T.meta_off = (uint32_t)hist;
+    const size_t meta = ((size_t)TILE_MAX_STAGES * sizeof(TileMeta) + 127) & ~(size_t)127;
+    T.tile_off = (uint32_t)(hist + meta);
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, m->ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const size_t tile_bytes = (size_t)T.tile_stride * 4;
+    const size_t fixed = (size_t)T.tile_off + 2 * TILE_MAX_STAGES * 8;
+    if ((size_t)optin <= fixed) return false;
+    T.stages = (int)std::min<size_t>(TILE_MAX_STAGES, ((size_t)optin - fixed) / tile_bytes);
+    if (T.stages < 2) return false;
+    T.bar_off = (uint32_t)(T.tile_off + (size_t)T.stages * tile_bytes);
+    smem = std::max<size_t>((size_t)T.bar_off + 2 * (size_t)T.stages * 8, tail_once_smem(B));
+    if (T.bx != m->tile_box[0] || T.by != m->tile_box[1] || T.bz != m->tile_box[2]) {
+        const cuuint64_t dim[3] = {(cuuint64_t)m->mgeo.size[0], (cuuint64_t)m->mgeo.size[1],
+                                   (cuuint64_t)m->mgeo.size[2]};
+        const cuuint64_t stride[2] = {(cuuint64_t)m->mgeo.size[0] * 4,
+                                      (cuuint64_t)m->mgeo.size[0] * (cuuint64_t)m->mgeo.size[1] * 4};
+        const cuuint32_t box[3] = {(cuuint32_t)T.bx, (cuuint32_t)T.by, (cuuint32_t)T.bz};
+        const cuuint32_t es[3] = {1, 1, 1};
+        const CUresult r = tensor_map_encoder()(reinterpret_cast<CUtensorMap*>(m->tmap), CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                                3, m->moving, dim, stride, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            m->tile_box[0] = m->tile_box[1] = m->tile_box[2] = 0;
+            return false;
+        }
+        m->tile_box[0] = T.bx;
+        m->tile_box[1] = T.by;
+        m->tile_box[2] = T.bz;
+    }
+    T.run_chunk0 = m->run_chunk0;
+    T.err = m->ws.done_counter + 3;
+    return true;
 }
 
 // Per-evaluation sampler constants: the stages and the composite map (point_map.h).
@@ -765,8 +916,11 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.codes = m->codes;
     a.chunk_run = m->chunk_run;
     a.run_brick = m->run_brick;
-    a.run_xbase = m->run_xbase;
+    a.chunk_xbase = m->chunk_xbase;
     a.nchunks = (uint32_t)m->nchunks;
+    a.tab_runs = m->tab_runs;
+    a.tab_off = m->tab_off;
+    a.chunk_entry = m->chunk_entry;
     a.hist_scale = ws.hist_scale;
     a.fine_scale = (float)std::ldexp(1.0, ws.fine_scale_log2);
     a.fine_shift = ws.fine_scale_log2 - ws.hist_scale_log2;
@@ -816,7 +970,25 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
             MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_eval<false>, P, J, a));
         if (per_kernel) MI_CHECK_CUDA(ctx, cudaEventRecord(ws.ev[1], st));
     } else {
-        {
+        TileArgs T{};
+        size_t tsm = 0;
+        if (ws.staging == 1 && m->tile_capable && tile_args(m, P, T, tsm)) {
+            // the histogram pass with TMA-staged moving tiles, one CTA per SM
+            const void* fn = want_derivative ? (const void*)k_hist_tile<true> : (const void*)k_hist_tile<false>;
+            mi_status ls = raise_smem_limit(ctx, fn, tsm);
+            if (ls != MI_OK) return ls;
+            cudaLaunchConfig_t tc = {};
+            tc.gridDim = dim3((unsigned)m->tile_grid);
+            tc.blockDim = dim3(TILE_BLOCK);
+            tc.dynamicSmemBytes = tsm;
+            tc.stream = st;
+            const CUtensorMap& tmap = *reinterpret_cast<const CUtensorMap*>(m->tmap);
+            if (want_derivative)
+                MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&tc, k_hist_tile<true>, P, a, tmap, T));
+            else
+                MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&tc, k_hist_tile<false>, P, a, tmap, T));
+            ++ws.tiled_evals;
+        } else {
             cudaLaunchConfig_t hc = {};
             hc.gridDim = dim3((unsigned)ws.grid_hist);
             hc.blockDim = dim3(HIST_BLOCK);
@@ -883,7 +1055,8 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.result, 0, RESULT_DOUBLES * sizeof(double), st));
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(ws.hist, 0, ghist_bytes(B), st));
         MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
-        return set_error(ctx, MI_ERR_TIMEOUT, "a grid barrier of the fused evaluation timed out");
+        return set_error(ctx, MI_ERR_TIMEOUT, ws.fused ? "a grid barrier of the fused evaluation timed out"
+                                                         : "a staged-tile wait of the histogram pass timed out");
     }
     if (timing) {
         float t = 0.f;
@@ -1149,19 +1322,18 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     };
     int occ_h = 0, occ_d = 0, occ_e1 = 0, occ_e0 = 0, coop = 0;
     {
-        int grid0 = hist_grid_for(HIST_MIN_BLOCKS), cap = 1;
-        s = brick_table_need(ctx, m, grid0, &cap);
+        const int grid0 = hist_grid_for(HIST_MIN_BLOCKS);
+        s = build_brick_tables(ctx, m, grid0);
         if (s != MI_OK) return fail(s);
-        s = raise_smem_limit(ctx, (const void*)k_hist<true>, hist_kernel_smem(B, cap));
+        s = raise_smem_limit(ctx, (const void*)k_hist<true>, hist_kernel_smem(B, m->table_cap));
         if (s != MI_OK) return fail(s);
         TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK,
-                                                               hist_kernel_smem(B, cap)));
+                                                               hist_kernel_smem(B, m->table_cap)));
         ws.grid_hist = hist_grid_for(occ_h);
         if (ws.grid_hist != grid0) {
-            s = brick_table_need(ctx, m, ws.grid_hist, &cap);
+            s = build_brick_tables(ctx, m, ws.grid_hist);
             if (s != MI_OK) return fail(s);
         }
-        m->table_cap = cap;
     }
     const size_t hsm = hist_kernel_smem(B, m->table_cap);
     const size_t esm = std::max(hsm, eval_smem(B));
@@ -1189,18 +1361,17 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     // every synchronous evaluation.
     ws.can_fuse = coop != 0 && resident >= 1;
     ws.fused = false;
-    ws.grid_eval = ws.can_fuse ? std::min(ws.grid_hist, resident) : 0;
-    if (ws.can_fuse && ws.grid_eval != ws.grid_hist) {
-        int cap = 1;
-        s = brick_table_need(ctx, m, ws.grid_eval, &cap);
-        if (s != MI_OK) return fail(s);
-        if (cap > m->table_cap) ws.can_fuse = false;  // the fused form would need more shared memory
-    }
+    // the fused kernel walks the same chunk groups (same brick tables), so it needs the
+    // split form's histogram grid resident at once
+    ws.can_fuse = ws.can_fuse && resident >= ws.grid_hist;
+    ws.grid_eval = ws.can_fuse ? ws.grid_hist : 0;
+    s = tile_setup(ctx, m);
+    if (s != MI_OK) return fail(s);
     ws.grid_deriv = grid_for(npad / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
     ws.block_hist = HIST_BLOCK;
     ws.block_deriv = DERIV_BLOCK;
-    // Fixed-point scales of the histogram taps. A CTA walks ceil(nchunks / grid) chunks,
-    // its warps taking every (HIST_BLOCK/32)-th, one sample per lane: a thread takes at
+    // Fixed-point scales of the histogram taps. A CTA walks every grid-th group of
+    // HIST_BLOCK/32 chunks, one chunk per warp and one sample per lane: a thread takes at
     // most per_thread samples, and a copy of the CTA histogram is fed by
     // HIST_BLOCK/copies threads, so it sees at most copy_max samples; each adds at most
     // one tap to a bin (coarse taps ≤ 2/3, fine taps < 2^-FINE_T). Every counter must
@@ -1210,8 +1381,9 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     {
         // both forms' histogram grids (the form can be switched after creation)
         const int64_t hgrid = ws.can_fuse ? std::min(ws.grid_hist, ws.grid_eval) : ws.grid_hist;
-        const int64_t per_cta = (warp_units + hgrid - 1) / hgrid;
-        const int64_t per_thread = (per_cta + nwarps_hist - 1) / nwarps_hist;
+        const int64_t ngroups = (warp_units + nwarps_hist - 1) / nwarps_hist;
+        // one chunk per warp per group; the staged-tile pass's bound where it can run
+        const int64_t per_thread = std::max((ngroups + hgrid - 1) / hgrid, m->tile_capable ? m->tile_per_thread : 0);
         const double lim = 4294967295.0 * 0.98;
         const double coarse_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_copies(B)), 1);
         const double fine_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_fine_copies(B)), 1);
@@ -1342,6 +1514,25 @@ mi_status mi_metric_set_fused(mi_metric* m, int fused) {
 mi_status mi_metric_get_fused(const mi_metric* m, int* fused) {
     if (!m || !fused) return MI_ERR_INVALID_ARGUMENT;
     *fused = m->ws.fused ? 1 : 0;
+    return MI_OK;
+}
+
+mi_status mi_metric_set_tile_staging(mi_metric* m, int on) {
+    if (!m) return MI_ERR_INVALID_ARGUMENT;
+    if (m->metric_kind != MI_METRIC_MATTES)
+        return mi::set_error(m->ctx, MI_ERR_INVALID_ARGUMENT, "staged tiles are a Mattes-metric setting");
+    if (on && !m->tile_capable)
+        return mi::set_error(m->ctx, MI_ERR_INVALID_ARGUMENT,
+                             "staged tiles need the moving volume's x size to be a multiple of 4 and a driver "
+                             "with cuTensorMapEncodeTiled");
+    m->ws.staging = on ? 1 : 0;
+    return MI_OK;
+}
+
+mi_status mi_metric_get_tile_staging(const mi_metric* m, int* on, int64_t* tiled_evals) {
+    if (!m) return MI_ERR_INVALID_ARGUMENT;
+    if (on) *on = m->ws.staging;
+    if (tiled_evals) *tiled_evals = m->ws.tiled_evals;
     return MI_OK;
 }
 

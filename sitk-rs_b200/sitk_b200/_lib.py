@@ -37,6 +37,7 @@ EXPORTED = [
     "mi_initnet_prepare", "mi_metric_create_ex", "mi_image_resample_nearest",
     "mi_metric_value_and_derivative_bspline", "mi_metric_bspline_records", "mi_image_read_meta",
     "mi_image_read_meta_host", "mi_image_read_nifti", "mi_image_read_nifti_host",
+    "mi_metric_set_tile_staging", "mi_metric_get_tile_staging",
 ]
 
 
@@ -145,6 +146,10 @@ def load(path: str | None = None):
     L.mi_image_read_meta_host.restype = ctypes.c_int
     L.mi_pyramid_level.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_int, i64p, P(vp), P(vp)]
     L.mi_metric_get_fused.argtypes = [vp, P(ctypes.c_int)]
+    L.mi_metric_set_tile_staging.argtypes = [vp, ctypes.c_int]
+    L.mi_metric_set_tile_staging.restype = ctypes.c_int
+    L.mi_metric_get_tile_staging.argtypes = [vp, P(ctypes.c_int), i64p]
+    L.mi_metric_get_tile_staging.restype = ctypes.c_int
     for name in ["mi_image_smooth", "mi_shrink_geometry", "mi_image_resample", "mi_pyramid_level",
                  "mi_metric_set_fused", "mi_metric_get_fused", "mi_metric_timing_enable", "mi_metric_timing_read", "mi_transform_form", "mi_context_create", "mi_context_destroy", "mi_context_sync", "mi_image_upload",
                  "mi_image_from_device", "mi_image_to_host", "mi_image_geometry", "mi_image_free",

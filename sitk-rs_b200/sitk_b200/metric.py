@@ -461,6 +461,21 @@ def get_fused(metric: DeviceMattesMetric) -> bool:
     return bool(f.value)
 
 
+def set_tile_staging(metric: DeviceMattesMetric, on: bool) -> None:
+    """Choose the histogram pass's corner source: TMA-staged moving tiles in shared
+    memory (True) or the moving volume's texture (False, the default). Same bits."""
+    _lib.check(_lib.load().mi_metric_set_tile_staging(metric.handle, 1 if on else 0), metric.ctx.handle)
+
+
+def get_tile_staging(metric: DeviceMattesMetric) -> tuple[bool, int]:
+    """The staged-tile setting and how many evaluations ran with staged tiles."""
+    on = ctypes.c_int()
+    n = ctypes.c_int64()
+    _lib.check(_lib.load().mi_metric_get_tile_staging(metric.handle, ctypes.byref(on), ctypes.byref(n)),
+               metric.ctx.handle)
+    return bool(on.value), n.value
+
+
 def _copy_geo(g: _lib.MiGeometry) -> _lib.MiGeometry:
     out = _lib.MiGeometry()
     ctypes.pointer(out)[0] = g
