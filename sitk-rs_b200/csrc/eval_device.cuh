@@ -213,20 +213,14 @@ struct EvalArgs {
     // the evaluation's sequence number, written into result_host's last slot after a
     // system-scope fence once everything else is there (the host may poll it)
     unsigned long long seq = 0;
-    // the single-metric evaluation's brick layout (brick.cuh): a code per padded
-    // sample, the run (brick) of every chunk of 32 and its brick's x(origin) − x_ref,
-    // each run's packed brick coordinates
+    // the brick layout (brick.cuh) of the staged-tile histogram pass: a code per padded
+    // sample, the run (brick) of every chunk of 32, each run's packed brick coordinates
+    // and the walk-order position of its first sample
     const uint32_t* codes = nullptr;
     const uint32_t* chunk_run = nullptr;
     const uint32_t* run_brick = nullptr;
-    const float4* chunk_xbase = nullptr;
+    const uint32_t* run_start = nullptr;
     uint32_t nchunks = 0;
-    // the histogram launch's brick tables (brick.cuh brick_table): per CTA its runs
-    // (tab_runs[tab_off[cta] … tab_off[cta + 1]]), per chunk its brick's entry
-    const uint32_t* tab_runs = nullptr;
-    const uint32_t* tab_off = nullptr;
-    const uint32_t* chunk_entry = nullptr;
-    float4* rec4 = nullptr;  // brick layout's records: gx, gy, gz, Parzen fraction per padded sample
 };
 constexpr int RESULT_ERR = 2 + MI_MAX_PARAMS;  // result slot holding the error word
 constexpr int RESULT_DOUBLES = RESULT_ERR + 2;

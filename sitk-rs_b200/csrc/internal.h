@@ -124,7 +124,6 @@ struct Workspace {
     uint16_t* rec_bins = nullptr;
     float* rec_f = nullptr;
     float* rec_g = nullptr;              // [3][n_samples]
-    float4* rec4 = nullptr;              // brick layout: gx, gy, gz, fraction per padded sample
     float hist_scale = 0.f;              // fixed-point scale of a joint-histogram tap
     int hist_scale_log2 = 0;
     int fine_scale_log2 = 0;              // scale of the fine part; the global bins' unit is 2^-this
@@ -168,13 +167,14 @@ struct mi_metric {
     uint32_t* samples = nullptr;  // device flat indices in walk order; null = the whole grid (not Mattes)
     uint8_t* fbin = nullptr;      // device fixed Parzen bin of every sample (exact, set-up time)
     int64_t n_samples = 0;
-    // the Mattes metric's brick layout (brick.cuh): bricks of 2^brick_bl voxels per
-    // axis, each brick's samples padded to chunks of 32
+    // the Mattes metric's brick layout (brick.cuh), for the staged-tile histogram pass:
+    // the walk order's runs of samples per brick of 2^brick_bl voxels per axis, each run
+    // padded to chunks of 32
     int brick_bl = 0;
     uint32_t* codes = nullptr;      // [nchunks·32] offset in the brick | fixed bin; padding BRICK_PAD
     uint32_t* chunk_run = nullptr;  // [nchunks] run (non-empty brick) of each chunk
     uint32_t* run_brick = nullptr;  // [nruns] packed brick coordinates
-    float4* chunk_xbase = nullptr;  // [nchunks] x(origin of the chunk's brick) − x_ref
+    uint32_t* run_start = nullptr;  // [nruns] position of the run's first sample in the walk order
     int64_t nchunks = 0, nruns = 0;
     uint32_t* run_chunk0 = nullptr; // [nruns + 1] first chunk of every run
     // TMA-staged moving tiles (tile.cuh): available when the linear moving volume meets the
@@ -184,12 +184,6 @@ struct mi_metric {
     int tile_box[3] = {0, 0, 0};
     int tile_grid = 0;              // one CTA per SM
     int64_t tile_per_thread = 0;    // most samples a tile-pass thread takes
-    // the histogram launch's chunk-group tables (brick.cuh brick_table), for table_grid CTAs
-    uint32_t* tab_runs = nullptr;
-    uint32_t* tab_off = nullptr;
-    uint32_t* chunk_entry = nullptr;
-    int table_cap = 1;              // brick-table entries a histogram CTA needs
-    int table_grid = 0;
     int bins = 0;
     mi_metric_info info{};
     mi::SamplerParams base{};     // everything except the stages

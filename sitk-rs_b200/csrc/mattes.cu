@@ -68,17 +68,14 @@ namespace {
 // The split form (k_hist, then k_deriv) does the same work with a kernel boundary in
 // place of the barrier.
 // ---------------------------------------------------------------------------
-// The brick table follows the histogram in the histogram kernels' shared memory (at
-// a 16-byte boundary); table_cap entries, sized at set-up for the launch's grid.
-__host__ __device__ inline size_t brick_table_offset(int B, int copies, int fine_copies) {
-    return (hist_region_bytes(B, copies, fine_copies) + 15) & ~(size_t)15;
-}
-size_t hist_kernel_smem(int B, int table_cap) {
-    return std::max(brick_table_offset(B, hist_copies(B), hist_fine_copies(B)) + (size_t)table_cap * sizeof(BrickBase),
-                    tail_once_smem(B));
-}
-__device__ __forceinline__ BrickBase* brick_table_ptr(unsigned char* base, int B, const EvalArgs& a) {
-    return reinterpret_cast<BrickBase*>(base + brick_table_offset(B, a.copies, a.fine_copies));
+// This CTA's queue of samples for the exact chain (k_hist, k_eval: a grid-stride walk,
+// so at most exq_cap = ceil(n / (grid·block))·block samples per CTA).
+__device__ __forceinline__ ExactQueue exact_queue(const EvalArgs& a) {
+#if MI_EXACT_DEFERRED
+    return ExactQueue{a.exq + (size_t)blockIdx.x * a.exq_cap, a.exq_cap};
+#else
+    return ExactQueue{nullptr, 0u};
+#endif
 }
 
 template <bool DERIV>
@@ -88,11 +85,11 @@ k_eval(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobian
     unsigned int* sh = reinterpret_cast<unsigned int*>(esh);
     double* dsh = reinterpret_cast<double*>(esh);
     const int B = P.bins;
-    brick_hist_phase<DERIV>(P, a, sh, brick_table_ptr(esh, B, a));
+    hist_phase<DERIV>(P, a, sh, grid_samples(a.n), exact_queue(a));
     if (!grid_barrier(a, 1)) return;
     TailCtx t;
     if (DERIV) {
-        t = deriv_phase<BrickRecords>(P, a, dsh, grid_groups(a));
+        t = deriv_phase(P, a, dsh, grid_groups(a));
     } else {
         const TailSmem ts = tail_layout(B, esh);
         t = tail_prepare(B, P.moving_bin_size, a, ts);
@@ -114,16 +111,18 @@ k_eval(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobian
 // Histogram pass of the split form. For a value-only evaluation (RECORD false) the CTA
 // that flushes last forms the tail (tail_once) and publishes the result, so that
 // evaluation is this one launch.
+size_t hist_kernel_smem(int B) { return std::max(hist_smem(B), tail_once_smem(B)); }
+
 template <bool RECORD>
 __global__ void __launch_bounds__(HIST_BLOCK, HIST_MIN_BLOCKS)
 k_hist(const __grid_constant__ SamplerParams P, EvalArgs a) {
-    extern __shared__ __align__(16) unsigned char hsh[];
+    extern __shared__ __align__(16) unsigned int sh[];
     pdl_launch_dependents();
-    brick_hist_phase<RECORD>(P, a, reinterpret_cast<unsigned int*>(hsh), brick_table_ptr(hsh, P.bins, a));
+    hist_phase<RECORD, (HIST_CLUSTER > 1)>(P, a, sh, grid_samples(a.n), exact_queue(a));
     // the value+derivative evaluation's tail is formed by k_deriv's CTAs; a value-only
     // evaluation ends here, with its tail in the CTA that flushes last
     if (RECORD || !last_to_arrive(a.sync + 1)) return;
-    tail_once(P.bins, P.moving_bin_size, a, hsh, true);
+    tail_once(P.bins, P.moving_bin_size, a, reinterpret_cast<unsigned char*>(sh), true);
 }
 
 // Derivative pass of the split form, a programmatic dependent of k_hist: each CTA forms
@@ -134,7 +133,7 @@ __global__ void __launch_bounds__(DERIV_BLOCK, DERIV_MIN_BLOCKS)
 k_deriv(const __grid_constant__ SamplerParams P, const __grid_constant__ JacobianForm J, EvalArgs a) {
     extern __shared__ double dsh[];
     pdl_wait();
-    const TailCtx t = stream_phase<BrickRecords>(P, a, dsh, grid_groups(a));
+    const TailCtx t = stream_phase(P, a, dsh, grid_groups(a));
     if (!last_to_arrive(a.sync)) return;
     // every CTA has read the histogram and written its value slices and moments
     deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
@@ -158,31 +157,23 @@ k_hist_tile(const __grid_constant__ SamplerParams P, EvalArgs a, const __grid_co
     tail_once(P.bins, P.moving_bin_size, a, tsh, true);
 }
 
-// Per-sample decisions of the brick sampler the kernels use, for the exactness tests,
-// per padded position (a padding lane reports status −1).
+// Per-sample decisions of the same sampler the kernels use, for the exactness tests.
 __global__ void k_decisions(const __grid_constant__ SamplerParams P, const float* __restrict__ moving,
-                            const uint8_t* __restrict__ mmask, const uint32_t* __restrict__ codes,
-                            const uint32_t* __restrict__ chunk_run, const uint32_t* __restrict__ run_brick,
-                            int64_t npad, int8_t* __restrict__ status, int32_t* __restrict__ fb,
-                            int32_t* __restrict__ mb, int64_t* __restrict__ flat_out, int8_t* __restrict__ exact_out) {
+                            const uint8_t* __restrict__ mmask, const uint32_t* __restrict__ samples,
+                            const uint8_t* __restrict__ fbin, int64_t n, int8_t* __restrict__ status,
+                            int32_t* __restrict__ fb, int32_t* __restrict__ mb, int64_t* __restrict__ flat_out,
+                            int8_t* __restrict__ exact_out) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npad; p += stride) {
-        const uint32_t code = codes[p];
-        if (code == BRICK_PAD) {
-            status[p] = -1;
-            continue;
-        }
-        const uint32_t packed = run_brick[chunk_run[p / BRICK_CHUNK]];
-        const BrickBase b = brick_base(P, packed);
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += stride) {
+        const uint32_t flat = samples ? samples[s] : (uint32_t)s;
         Sample o;
-        const int st = brick_sample<false>(P, b, code, moving, mmask, o);
-        uint32_t i, j, k;
-        brick_ijk(P, packed, code, i, j, k);
-        status[p] = (int8_t)st;
-        fb[p] = st == SAMPLE_VALID ? (int)(code >> (3 * P.brick_bl)) : -1;
-        mb[p] = st == SAMPLE_VALID ? o.mi : -1;
-        flat_out[p] = (int64_t)i + P.fsize0 * ((int64_t)j + P.fsize1 * (int64_t)k);
-        exact_out[p] = o.exact ? 1 : 0;
+        o.exact = false;
+        const int st = sample<false>(P, flat, moving, mmask, o);
+        status[s] = (int8_t)st;
+        fb[s] = st == SAMPLE_VALID ? (int)fbin[s] : -1;
+        mb[s] = st == SAMPLE_VALID ? o.mi : -1;
+        flat_out[s] = flat;
+        exact_out[s] = o.exact ? 1 : 0;
     }
 }
 
@@ -251,35 +242,26 @@ __global__ void k_run_chunks(const int* __restrict__ counts, int64_t nruns, uint
         nch[r] = (uint32_t)((counts[r] + BRICK_CHUNK - 1) / BRICK_CHUNK);
 }
 
-// Per run (a non-empty brick): its packed coordinates, and for each of its chunks the
-// run index and x(brick origin) − x_ref in FP32.
+// Per run (a non-empty brick): its packed coordinates and the run index of each of its
+// chunks.
 __global__ void k_run_fill(const uint32_t* __restrict__ bid, int64_t nruns, const uint32_t* __restrict__ chunk_off,
-                           const uint32_t* __restrict__ nch, int64_t nbx, int64_t nby, int bl, SamplerParams P,
-                           uint32_t* __restrict__ run_brick, float4* __restrict__ chunk_xbase,
+                           const uint32_t* __restrict__ nch, int64_t nbx, int64_t nby, uint32_t* __restrict__ run_brick,
                            uint32_t* __restrict__ chunk_run) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nruns; r += (int64_t)gridDim.x * blockDim.x) {
         const int64_t b = bid[r];
         const int64_t bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
         run_brick[r] = (uint32_t)(bx | (by << 10) | (bz << 20));
-        const double o[3] = {(double)(bx << bl), (double)(by << bl), (double)(bz << bl)};
-        float xb[3];
-        for (int d = 0; d < 3; ++d) {
-            const double x = P.forigin[d] + P.fi2p[d * 3] * o[0] + P.fi2p[d * 3 + 1] * o[1] + P.fi2p[d * 3 + 2] * o[2];
-            xb[d] = (float)(x - P.xref[d]);
-        }
-        for (uint32_t c = 0; c < nch[r]; ++c) {
-            chunk_run[chunk_off[r] + c] = (uint32_t)r;
-            chunk_xbase[chunk_off[r] + c] = make_float4(xb[0], xb[1], xb[2], 0.0f);
-        }
+        for (uint32_t c = 0; c < nch[r]; ++c) chunk_run[chunk_off[r] + c] = (uint32_t)r;
     }
 }
 
 // The codes: one CTA per run, sample t of the run at padded position chunk_off·32 + t:
-// its offset in the brick (bl bits per axis) and its fixed bin above them.
+// its offset in the brick (bl bits per axis) and its fixed bin above them (fbin in walk
+// order, or by voxel for the whole grid).
 __global__ void k_scatter_codes(const uint32_t* __restrict__ samples, const uint8_t* __restrict__ fbin,
-                                const int* __restrict__ counts, const uint32_t* __restrict__ run_start,
-                                const uint32_t* __restrict__ chunk_off, int64_t nx, int64_t ny, int bl,
-                                uint32_t* __restrict__ codes) {
+                                bool fbin_by_flat, const int* __restrict__ counts,
+                                const uint32_t* __restrict__ run_start, const uint32_t* __restrict__ chunk_off,
+                                int64_t nx, int64_t ny, int bl, uint32_t* __restrict__ codes) {
     const int64_t r = blockIdx.x;
     const int64_t n = counts[r];
     const int64_t s0 = run_start[r], p0 = (int64_t)chunk_off[r] * BRICK_CHUNK;
@@ -289,7 +271,7 @@ __global__ void k_scatter_codes(const uint32_t* __restrict__ samples, const uint
         const int64_t x = v % nx, row = v / nx;
         const int64_t y = row % ny, z = row / ny;
         codes[p0 + t] = (uint32_t)((x & msk) | ((y & msk) << bl) | ((z & msk) << (2 * bl)) |
-                                   ((int64_t)fbin[s0 + t] << (3 * bl)));
+                                   ((int64_t)fbin[fbin_by_flat ? v : s0 + t] << (3 * bl)));
     }
 }
 
@@ -401,6 +383,32 @@ mi_status minmax(mi_context* ctx, const float* vals, const uint32_t* idx, const 
 uint32_t ghist_rep_stride(int B) { return (uint32_t)(((size_t)B * B + 2 * B + 31) & ~(size_t)31); }
 size_t ghist_bytes(int B) { return (size_t)GHIST_REPS * ghist_rep_stride(B) * sizeof(unsigned long long); }
 
+// The split form's histogram grid: enough CTAs for the samples, at most as many as are
+// resident at once, in whole thread-block clusters of HIST_CLUSTER (bounded by the
+// clusters the device can hold at once with this kernel's shape).
+int hist_grid(mi_context* ctx, int64_t n, int occ, int B) {
+    int g = grid_for(n, HIST_BLOCK, ctx->num_sms * std::max(occ, 1));
+    if (HIST_CLUSTER <= 1) return g;
+    int clusters = (g + HIST_CLUSTER - 1) / HIST_CLUSTER;
+    cudaLaunchConfig_t hc = {};
+    hc.gridDim = dim3((unsigned)(clusters * HIST_CLUSTER));
+    hc.blockDim = dim3(HIST_BLOCK);
+    hc.dynamicSmemBytes = hist_kernel_smem(B);
+    cudaLaunchAttribute hattr[1];
+    hattr[0].id = cudaLaunchAttributeClusterDimension;
+    hattr[0].val.clusterDim.x = HIST_CLUSTER;
+    hattr[0].val.clusterDim.y = 1;
+    hattr[0].val.clusterDim.z = 1;
+    hc.attrs = hattr;
+    hc.numAttrs = 1;
+    int active = 0;
+    if (cudaOccupancyMaxActiveClusters(&active, k_hist<true>, &hc) == cudaSuccess && active > 0)
+        clusters = std::min(clusters, active);
+    else
+        cudaGetLastError();
+    return std::max(1, clusters) * HIST_CLUSTER;
+}
+
 void free_metric(mi_metric* m) {
     if (!m) return;
     if (m->mtex) cudaDestroyTextureObject(m->mtex);
@@ -413,11 +421,8 @@ void free_metric(mi_metric* m) {
     cudaFree(m->codes);
     cudaFree(m->chunk_run);
     cudaFree(m->run_brick);
-    cudaFree(m->chunk_xbase);
     cudaFree(m->run_chunk0);
-    cudaFree(m->tab_runs);
-    cudaFree(m->tab_off);
-    cudaFree(m->chunk_entry);
+    cudaFree(m->run_start);
     cudaFree(m->ws.hist);
     cudaFree(m->ws.partials);
     cudaFree(m->ws.vsum);
@@ -427,7 +432,6 @@ void free_metric(mi_metric* m) {
     cudaFree(m->ws.rec_bins);
     cudaFree(m->ws.rec_f);
     cudaFree(m->ws.rec_g);
-    cudaFree(m->ws.rec4);
     if (m->ws.host_result) cudaFreeHost(m->ws.host_result);
     for (int i = 0; i < 5; ++i)
         if (m->ws.ev[i]) cudaEventDestroy(m->ws.ev[i]);
@@ -455,16 +459,18 @@ int choose_brick_bl(const int64_t* size, int64_t n) {
 // Build the sample list: the strategy's draw, gated by the fixed mask, sorted into
 // brick order (SAMPLE_BRICK_LOG2). The histogram is a sum of exact integers and so
 // does not depend on the order; sorting only buys locality.
-// With `bricks` (the Mattes metric) the whole grid is materialised too, and the sort
-// key is the brick layout's (brick_key_bl): bricks of 2^bl voxels per axis, bl chosen
-// from the sample density (choose_brick_bl), then 8³ sub-bricks, then voxels, each
-// x-fastest; m->brick_bl records bl.
+// With `bricks` (the Mattes metric) the sort key is the brick layout's (brick_key_bl):
+// bricks of 2^bl voxels per axis, bl chosen from the sample density (choose_brick_bl),
+// then 8³ sub-bricks, then voxels, each x-fastest; m->brick_bl records bl.
 mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mask, const mi_sampling* smp,
                         int64_t nvox, bool bricks) {
     const int strategy = smp ? smp->strategy : MI_SAMPLING_NONE;
-    if (strategy == MI_SAMPLING_NONE && !fixed_mask && !bricks) {
+    if (strategy == MI_SAMPLING_NONE && !fixed_mask) {
+        // the whole grid, walked in voxel order with no list (the brick layout is built
+        // from a sorted list of its own, build_brick_layout)
         m->samples = nullptr;
         m->n_samples = nvox;
+        if (bricks) m->brick_bl = choose_brick_bl(m->fgeo.size, nvox);
         return MI_OK;
     }
     int64_t count = 0;
@@ -618,10 +624,10 @@ mi_status build_samples(mi_context* ctx, mi_metric* m, const mi_image* fixed_mas
     return MI_OK;
 }
 
-// The brick layout of a sorted sample list (build_samples with bricks) and its fixed
-// bins: runs of samples per brick (CUB run-length encoding), each padded to whole
+// The brick layout of the walk (build_samples with bricks; the whole grid sorted here)
+// and its fixed bins: runs of samples per brick (CUB run-length encoding), each padded to whole
 // chunks of 32, the codes scattered to their padded positions.
-mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams& P) {
+mi_status build_brick_layout(mi_context* ctx, mi_metric* m) {
     cudaStream_t st = ctx->stream;
     const int64_t n = m->n_samples;
     const int bl = m->brick_bl;
@@ -638,8 +644,8 @@ mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams&
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->chunk_run, 0, 4, st));
         MI_CHECK_CUDA(ctx, cudaMalloc(&m->run_brick, 4));
         MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->run_brick, 0, 4, st));
-        MI_CHECK_CUDA(ctx, cudaMalloc(&m->chunk_xbase, sizeof(float4)));
-        MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->chunk_xbase, 0, sizeof(float4), st));
+        MI_CHECK_CUDA(ctx, cudaMalloc(&m->run_start, 4));
+        MI_CHECK_CUDA(ctx, cudaMemsetAsync(m->run_start, 0, 4, st));
         const uint32_t r0[2] = {0u, 1u};
         MI_CHECK_CUDA(ctx, cudaMalloc(&m->run_chunk0, 2 * 4));
         MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->run_chunk0, r0, 2 * 4, cudaMemcpyHostToDevice, st));
@@ -647,11 +653,13 @@ mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams&
         return MI_OK;
     }
     uint32_t *bid = nullptr, *uniq = nullptr, *nch = nullptr, *chunk_off = nullptr, *run_start = nullptr;
+    uint32_t* whole = nullptr;  // the whole grid's voxels in brick order (no walk list)
     int *counts = nullptr, *nruns_d = nullptr;
     void* tmp = nullptr;
     size_t tb = 0;
     auto done = [&](mi_status s) {
         cudaStreamSynchronize(st);
+        cudaFree(whole);
         cudaFree(bid);
         cudaFree(uniq);
         cudaFree(nch);
@@ -667,11 +675,44 @@ mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams&
         cudaError_t _e = (expr);                                         \
         if (_e != cudaSuccess) return done(cuda_status(ctx, _e, #expr)); \
     } while (0)
+    const uint32_t* list = m->samples;
+    if (!list) {
+        // the whole grid: its voxels sorted by the layout's key
+        unsigned long long *keys = nullptr, *keys_out = nullptr;
+        uint32_t* iota = nullptr;
+        const int64_t nbz = (m->fgeo.size[2] + (1 << bl) - 1) >> bl;
+        const uint64_t kmax = (uint64_t)(nbx * nby * nbz) << (3 * bl);
+        int bits = 1;
+        while (bits < 64 && ((uint64_t)1 << bits) < kmax) ++bits;
+        cudaError_t e = cudaMalloc(&keys, (size_t)n * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&keys_out, (size_t)n * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&iota, (size_t)n * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&whole, (size_t)n * 4);
+        if (e == cudaSuccess) {
+            k_iota_stride<<<grid_for(n, block, ctx->num_sms * 8), block, 0, st>>>(n, 1, iota);
+            k_brick_key_bl<<<grid_for(n, block, ctx->num_sms * 8), block, 0, st>>>(iota, n, nx, ny, bl, nbx, nby, keys);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess)
+            e = cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys_out, iota, whole, (int)n, 0, bits, st);
+        if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
+        if (e == cudaSuccess)
+            e = cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys_out, iota, whole, (int)n, 0, bits, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFree(keys);
+        cudaFree(keys_out);
+        cudaFree(iota);
+        cudaFree(tmp);
+        tmp = nullptr;
+        tb = 0;
+        if (e != cudaSuccess) return done(cuda_status(ctx, e, "brick layout of the whole grid"));
+        list = whole;
+    }
     TRY_L(cudaMalloc(&bid, (size_t)n * 4));
     TRY_L(cudaMalloc(&uniq, (size_t)n * 4));
     TRY_L(cudaMalloc(&counts, (size_t)n * 4));
     TRY_L(cudaMalloc(&nruns_d, sizeof(int)));
-    k_brick_of<<<grid_for(n, block, ctx->num_sms * 8), block, 0, st>>>(m->samples, n, nx, ny, bl, nbx, nby, bid);
+    k_brick_of<<<grid_for(n, block, ctx->num_sms * 8), block, 0, st>>>(list, n, nx, ny, bl, nbx, nby, bid);
     TRY_L(cudaGetLastError());
     TRY_L(cub::DeviceRunLengthEncode::Encode(nullptr, tb, bid, uniq, counts, nruns_d, (int)n, st));
     TRY_L(cudaMalloc(&tmp, tb));
@@ -706,14 +747,16 @@ mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams&
     TRY_L(cudaMemsetAsync(m->codes, 0xFF, (size_t)nchunks * BRICK_CHUNK * 4, st));
     TRY_L(cudaMalloc(&m->chunk_run, (size_t)nchunks * 4));
     TRY_L(cudaMalloc(&m->run_brick, (size_t)nruns * 4));
-    TRY_L(cudaMalloc(&m->chunk_xbase, (size_t)nchunks * sizeof(float4)));
-    k_run_fill<<<grid_for(nruns, block, ctx->num_sms * 8), block, 0, st>>>(uniq, nruns, chunk_off, nch, nbx, nby, bl,
-                                                                           P, m->run_brick, m->chunk_xbase, m->chunk_run);
+    k_run_fill<<<grid_for(nruns, block, ctx->num_sms * 8), block, 0, st>>>(uniq, nruns, chunk_off, nch, nbx, nby,
+                                                                           m->run_brick, m->chunk_run);
     TRY_L(cudaGetLastError());
-    k_scatter_codes<<<(unsigned)nruns, block, 0, st>>>(m->samples, m->fbin, counts, run_start, chunk_off, nx, ny, bl,
-                                                       m->codes);
+    k_scatter_codes<<<(unsigned)nruns, block, 0, st>>>(list, m->fbin, m->samples == nullptr, counts, run_start,
+                                                       chunk_off, nx, ny, bl, m->codes);
     TRY_L(cudaGetLastError());
-    // the first chunk of every run, and the chunk count after the last
+    // the first sample of every run in the walk order, the first chunk of every run and
+    // the chunk count after the last
+    TRY_L(cudaMalloc(&m->run_start, (size_t)nruns * 4));
+    TRY_L(cudaMemcpyAsync(m->run_start, run_start, (size_t)nruns * 4, cudaMemcpyDeviceToDevice, st));
     TRY_L(cudaMalloc(&m->run_chunk0, ((size_t)nruns + 1) * 4));
     TRY_L(cudaMemcpyAsync(m->run_chunk0, chunk_off, (size_t)nruns * 4, cudaMemcpyDeviceToDevice, st));
     {
@@ -723,52 +766,6 @@ mi_status build_brick_layout(mi_context* ctx, mi_metric* m, const SamplerParams&
     }
 #undef TRY_L
     return done(MI_OK);
-}
-
-// The brick tables of a `grid`-CTA histogram launch (brick.cuh brick_table): chunk
-// groups of W = HIST_BLOCK/32 consecutive chunks, CTA c taking groups
-// [⌊c·n/grid⌋, ⌊(c+1)·n/grid⌋) of the n groups;
-// per CTA, group after group, the runs the group touches; per chunk the table entry of
-// its brick.
-// Sets m->table_cap to the longest CTA table.
-mi_status build_brick_tables(mi_context* ctx, mi_metric* m, int grid) {
-    cudaStream_t st = ctx->stream;
-    const int64_t nch = m->nchunks;
-    const int64_t W = HIST_BLOCK / 32;
-    const int64_t ngroups = (nch + W - 1) / W;
-    std::vector<uint32_t> run((size_t)nch);
-    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(run.data(), m->chunk_run, (size_t)nch * 4, cudaMemcpyDeviceToHost, st));
-    MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
-    std::vector<uint32_t> off((size_t)grid + 1, 0u), entry((size_t)nch, 0u), runs;
-    runs.reserve((size_t)(ngroups + m->nruns + grid));
-    int cap = 1;
-    for (int c = 0; c < grid; ++c) {
-        off[c] = (uint32_t)runs.size();
-        const int64_t g0 = (int64_t)c * ngroups / grid, g1 = (int64_t)(c + 1) * ngroups / grid;
-        for (int64_t g = g0; g < g1; ++g) {
-            const int64_t f = g * W, l = std::min(f + W, nch) - 1;
-            const uint32_t base = (uint32_t)(runs.size() - off[c]);
-            for (uint32_t r = run[(size_t)f]; r <= run[(size_t)l]; ++r) runs.push_back(r);
-            for (int64_t k = f; k <= l; ++k) entry[(size_t)k] = base + (run[(size_t)k] - run[(size_t)f]);
-        }
-        cap = std::max(cap, (int)(runs.size() - off[c]));
-    }
-    off[grid] = (uint32_t)runs.size();
-    if (runs.empty()) runs.push_back(0u);
-    cudaFree(m->tab_runs);
-    cudaFree(m->tab_off);
-    cudaFree(m->chunk_entry);
-    m->tab_runs = m->tab_off = m->chunk_entry = nullptr;
-    MI_CHECK_CUDA(ctx, cudaMalloc(&m->tab_runs, runs.size() * 4));
-    MI_CHECK_CUDA(ctx, cudaMalloc(&m->tab_off, off.size() * 4));
-    MI_CHECK_CUDA(ctx, cudaMalloc(&m->chunk_entry, entry.size() * 4));
-    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->tab_runs, runs.data(), runs.size() * 4, cudaMemcpyHostToDevice, st));
-    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->tab_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st));
-    MI_CHECK_CUDA(ctx, cudaMemcpyAsync(m->chunk_entry, entry.data(), entry.size() * 4, cudaMemcpyHostToDevice, st));
-    MI_CHECK_CUDA(ctx, cudaStreamSynchronize(st));
-    m->table_cap = cap;
-    m->table_grid = grid;
-    return MI_OK;
 }
 
 // The tensor-map encoder of the driver (cuTensorMapEncodeTiled), found once.
@@ -912,15 +909,7 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.samples = m->samples;
     a.fbin = m->fbin;
     a.n = n;
-    a.npad = (uint32_t)(m->nchunks * BRICK_CHUNK);
-    a.codes = m->codes;
-    a.chunk_run = m->chunk_run;
-    a.run_brick = m->run_brick;
-    a.chunk_xbase = m->chunk_xbase;
-    a.nchunks = (uint32_t)m->nchunks;
-    a.tab_runs = m->tab_runs;
-    a.tab_off = m->tab_off;
-    a.chunk_entry = m->chunk_entry;
+    a.npad = (n + 3u) & ~3u;
     a.hist_scale = ws.hist_scale;
     a.fine_scale = (float)std::ldexp(1.0, ws.fine_scale_log2);
     a.fine_shift = ws.fine_scale_log2 - ws.hist_scale_log2;
@@ -936,11 +925,18 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
     a.rec_bins = want_derivative ? ws.rec_bins : nullptr;
     a.rec_f = want_derivative ? ws.rec_f : nullptr;
     a.rec_g = want_derivative ? ws.rec_g : nullptr;
-    a.rec4 = want_derivative ? ws.rec4 : nullptr;
     a.partials = ws.partials;
     a.vsum = ws.vsum;
+    a.exq = ws.exq;
+    a.exq_cap = ws.fused ? ws.exq_cap_eval : ws.exq_cap_hist;
     a.sync = ws.done_counter;
     a.result = ws.result;
+    // the brick layout, for the staged-tile histogram pass
+    a.codes = m->codes;
+    a.chunk_run = m->chunk_run;
+    a.run_brick = m->run_brick;
+    a.run_start = m->run_start;
+    a.nchunks = (uint32_t)m->nchunks;
     // the split form's last kernel copies the result into the mapped mirror; the
     // fused form, whose CTAs may leave early on a barrier timeout, is copied back
     a.result_host = ws.fused ? nullptr : ws.host_result_dev;
@@ -957,7 +953,7 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)ws.grid_eval);
         cfg.blockDim = dim3(HIST_BLOCK);
-        cfg.dynamicSmemBytes = std::max(hist_kernel_smem(B, m->table_cap), eval_smem(B));
+        cfg.dynamicSmemBytes = eval_smem(B);
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
@@ -989,11 +985,19 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
                 MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&tc, k_hist_tile<false>, P, a, tmap, T));
             ++ws.tiled_evals;
         } else {
+            // thread-block clusters of HIST_CLUSTER CTAs (the grid is a multiple of it)
             cudaLaunchConfig_t hc = {};
             hc.gridDim = dim3((unsigned)ws.grid_hist);
             hc.blockDim = dim3(HIST_BLOCK);
-            hc.dynamicSmemBytes = hist_kernel_smem(B, m->table_cap);
+            hc.dynamicSmemBytes = hist_kernel_smem(B);
             hc.stream = st;
+            cudaLaunchAttribute hattr[1];
+            hattr[0].id = cudaLaunchAttributeClusterDimension;
+            hattr[0].val.clusterDim.x = HIST_CLUSTER;
+            hattr[0].val.clusterDim.y = 1;
+            hattr[0].val.clusterDim.z = 1;
+            hc.attrs = hattr;
+            hc.numAttrs = HIST_CLUSTER > 1 ? 1 : 0;
             if (want_derivative)
                 MI_CHECK_CUDA(ctx, cudaLaunchKernelEx(&hc, k_hist<true>, P, a));
             else
@@ -1302,88 +1306,50 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     k_fixed_bins<<<grid_for(m->n_samples, 256, ctx->num_sms * 8), 256, 0, st>>>(P, m->fixed, m->samples,
                                                                               m->n_samples, m->fbin);
     TRY_CUDA(cudaGetLastError());
-
-    // The brick layout of the samples (brick.cuh).
-    s = build_brick_layout(ctx, m, P);
+    // The brick layout of the samples for the staged-tile histogram pass (tile.cuh).
+    s = build_brick_layout(ctx, m);
+    if (s != MI_OK) return fail(s);
+    s = tile_setup(ctx, m);
     if (s != MI_OK) return fail(s);
 
-    // Workspace and launch shapes. The histogram kernels' shared memory holds the CTA
-    // histogram and the brick table, whose size depends on the grid; the grid depends
-    // on the occupancy that the shared memory allows: sized for the provisional grid
-    // (HIST_MIN_BLOCKS CTAs per SM), re-sized if fewer fit.
+    // Workspace and launch shapes.
     Workspace& ws = m->ws;
     const int B = bins;
-    const int64_t npad = m->nchunks * BRICK_CHUNK;
-    const int nwarps_hist = HIST_BLOCK / 32;
-    const int64_t warp_units = std::max<int64_t>(m->nchunks, 1);
-    auto hist_grid_for = [&](int occ) {
-        return grid_for((warp_units + nwarps_hist - 1) / nwarps_hist * HIST_BLOCK, HIST_BLOCK,
-                        ctx->num_sms * std::max(occ, 1));
-    };
+    TRY_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_kernel_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_kernel_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_eval<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
+    TRY_CUDA(cudaFuncSetAttribute(k_eval<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
     int occ_h = 0, occ_d = 0, occ_e1 = 0, occ_e0 = 0, coop = 0;
-    {
-        const int grid0 = hist_grid_for(HIST_MIN_BLOCKS);
-        s = build_brick_tables(ctx, m, grid0);
-        if (s != MI_OK) return fail(s);
-        s = raise_smem_limit(ctx, (const void*)k_hist<true>, hist_kernel_smem(B, m->table_cap));
-        if (s != MI_OK) return fail(s);
-        TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK,
-                                                               hist_kernel_smem(B, m->table_cap)));
-        ws.grid_hist = hist_grid_for(occ_h);
-        if (ws.grid_hist != grid0) {
-            s = build_brick_tables(ctx, m, ws.grid_hist);
-            if (s != MI_OK) return fail(s);
-        }
-    }
-    const size_t hsm = hist_kernel_smem(B, m->table_cap);
-    const size_t esm = std::max(hsm, eval_smem(B));
-    {
-        const std::pair<const void*, size_t> lims[] = {{(const void*)k_hist<true>, hsm},
-                                                       {(const void*)k_hist<false>, hsm},
-                                                       {(const void*)k_deriv, stream_smem(B)},
-                                                       {(const void*)k_eval<true>, esm},
-                                                       {(const void*)k_eval<false>, esm}};
-        for (const auto& l : lims) {
-            s = raise_smem_limit(ctx, l.first, l.second);
-            if (s != MI_OK) return fail(s);
-        }
-    }
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK, hist_kernel_smem(B)));
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_deriv, DERIV_BLOCK, stream_smem(B)));
-    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e1, k_eval<true>, HIST_BLOCK, esm));
-    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e0, k_eval<false>, HIST_BLOCK, esm));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e1, k_eval<true>, HIST_BLOCK, eval_smem(B)));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e0, k_eval<false>, HIST_BLOCK, eval_smem(B)));
     TRY_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
-    // The fused form needs every CTA resident (a cooperative launch); it runs on the
-    // split form's histogram grid when that is resident (same brick tables), else on
-    // fewer CTAs with tables sized for them.
+    // The fused form needs every CTA resident (a cooperative launch).
     const int resident = ctx->num_sms * std::min(occ_e1, occ_e0);
     // The split form is the default: the fused kernel's device time is the same, and
     // a cooperative launch waits for the stream to drain, which adds its latency to
     // every synchronous evaluation.
     ws.can_fuse = coop != 0 && resident >= 1;
     ws.fused = false;
-    // the fused kernel walks the same chunk groups (same brick tables), so it needs the
-    // split form's histogram grid resident at once
-    ws.can_fuse = ws.can_fuse && resident >= ws.grid_hist;
-    ws.grid_eval = ws.can_fuse ? ws.grid_hist : 0;
-    s = tile_setup(ctx, m);
-    if (s != MI_OK) return fail(s);
-    ws.grid_deriv = grid_for(npad / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
+    ws.grid_eval = ws.can_fuse ? grid_for(m->n_samples, HIST_BLOCK, resident) : 0;
+    ws.grid_hist = hist_grid(ctx, m->n_samples, occ_h, B);
+    ws.grid_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
     ws.block_hist = HIST_BLOCK;
     ws.block_deriv = DERIV_BLOCK;
-    // Fixed-point scales of the histogram taps. A CTA walks every grid-th group of
-    // HIST_BLOCK/32 chunks, one chunk per warp and one sample per lane: a thread takes at
-    // most per_thread samples, and a copy of the CTA histogram is fed by
-    // HIST_BLOCK/copies threads, so it sees at most copy_max samples; each adds at most
-    // one tap to a bin (coarse taps ≤ 2/3, fine taps < 2^-FINE_T). Every counter must
-    // stay below 2^32 and every rounded tap below 2^22 (the magic-add rounding): k ≤ 22,
-    // kf ≤ FINE_T + 22. The global u64 bin, in units of 2^-kf, takes at most
-    // n_samples·(2/3)·2^kf.
+    // Fixed-point scales of the histogram taps. A thread takes at most per_thread
+    // samples, and a copy of the CTA histogram is fed by HIST_BLOCK/copies threads, so
+    // it sees at most copy_max samples; each adds at most one tap to a bin (coarse
+    // taps ≤ 2/3, fine taps < 2^-FINE_T). Every counter must stay below 2^32 and every
+    // rounded tap below 2^22 (the magic-add rounding): k ≤ 22, kf ≤ FINE_T + 22. The global
+    // u64 bin, in units of 2^-kf, takes at most n_samples·(2/3)·2^kf.
     {
         // both forms' histogram grids (the form can be switched after creation)
         const int64_t hgrid = ws.can_fuse ? std::min(ws.grid_hist, ws.grid_eval) : ws.grid_hist;
-        const int64_t ngroups = (warp_units + nwarps_hist - 1) / nwarps_hist;
-        // one chunk per warp per group; the staged-tile pass's bound where it can run
-        const int64_t per_thread = std::max((ngroups + hgrid - 1) / hgrid, m->tile_capable ? m->tile_per_thread : 0);
+        // (and the staged-tile pass's bound, where it can run)
+        const int64_t per_thread = std::max((m->n_samples + hgrid * HIST_BLOCK - 1) / (hgrid * HIST_BLOCK),
+                                            m->tile_capable ? m->tile_per_thread : (int64_t)0);
         const double lim = 4294967295.0 * 0.98;
         const double coarse_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_copies(B)), 1);
         const double fine_max = (double)std::max<int64_t>(per_thread * (HIST_BLOCK / hist_fine_copies(B)), 1);
@@ -1398,13 +1364,12 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
         ws.fine_scale_log2 = kf;
     }
     {
-        // one record per padded sample; padding records keep moving bin 0
-        const size_t ns = (size_t)npad;
+        // padded to whole groups of four samples; padding records keep moving bin 0
+        const size_t ns = pad4(m->n_samples);
         TRY_CUDA(cudaMalloc(&ws.rec_bins, ns * sizeof(uint16_t)));
         TRY_CUDA(cudaMemsetAsync(ws.rec_bins, 0, ns * sizeof(uint16_t), st));
         TRY_CUDA(cudaMalloc(&ws.rec_f, ns * sizeof(float)));
         TRY_CUDA(cudaMalloc(&ws.rec_g, 3 * ns * sizeof(float)));
-        TRY_CUDA(cudaMalloc(&ws.rec4, ns * sizeof(float4)));
     }
     // joint B², fixed counts B, then the joint part's B column sums
     TRY_CUDA(cudaMalloc(&ws.hist, ghist_bytes(B)));
@@ -1412,12 +1377,25 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     // partials serve both forms: the split form's k_deriv grid and, should the form
     // be switched, the fused grid
     {
-        const int pgrid = std::max(ws.grid_deriv, ws.grid_eval);
+        const int pgrid = std::max(ws.grid_deriv, std::max(ws.grid_eval,
+            grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1))));
         ws.grid_split_hist = ws.grid_hist;
-        ws.grid_split_deriv = ws.grid_deriv;
+        ws.grid_split_deriv = grid_for((int64_t)pad4(m->n_samples) / 4, DERIV_BLOCK, ctx->num_sms * std::max(occ_d, 1));
         TRY_CUDA(cudaMalloc(&ws.partials, (size_t)pgrid * NMOM * 8));
     }
     TRY_CUDA(cudaMalloc(&ws.vsum, (size_t)value_slices(B) * 8));
+    {
+        // a grid-stride walk gives a CTA at most ceil(n / (grid·block))·block samples
+        auto cap = [&](int grid) -> uint32_t {
+            if (grid < 1) return 0u;
+            const int64_t per = ((int64_t)m->n_samples + (int64_t)grid * HIST_BLOCK - 1) / ((int64_t)grid * HIST_BLOCK);
+            return (uint32_t)(per * HIST_BLOCK);
+        };
+        ws.exq_cap_hist = cap(ws.grid_hist);
+        ws.exq_cap_eval = cap(ws.grid_eval);
+        const size_t len = std::max((size_t)ws.grid_hist * ws.exq_cap_hist, (size_t)ws.grid_eval * ws.exq_cap_eval);
+        TRY_CUDA(cudaMalloc(&ws.exq, std::max<size_t>(len, 1) * sizeof(uint32_t)));
+    }
     TRY_CUDA(cudaMalloc(&ws.result, RESULT_DOUBLES * 8));
     TRY_CUDA(cudaMalloc(&ws.done_counter, 4 * sizeof(unsigned int)));
     TRY_CUDA(cudaMemsetAsync(ws.done_counter, 0, 4 * sizeof(unsigned int), st));
@@ -1574,15 +1552,12 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
     SamplerParams P;
     mi_status s = fill_params(m, stages, nstage, P);
     if (s != MI_OK) return s;
-    const int64_t np = m->nchunks * BRICK_CHUNK;
-    const size_t cap = (size_t)std::max<int64_t>(np, 1);
+    const int64_t ns = m->n_samples;
+    const size_t cap = (size_t)std::max<int64_t>(ns, 1);
     int8_t *d_st = nullptr, *d_ex = nullptr;
     int32_t *d_fb = nullptr, *d_mb = nullptr;
     int64_t* d_fl = nullptr;
     cudaStream_t st = ctx->stream;
-    std::vector<int8_t> h_st(cap), h_ex(cap);
-    std::vector<int32_t> h_fb(cap), h_mb(cap);
-    std::vector<int64_t> h_fl(cap);
     cudaError_t e = cudaMalloc(&d_st, cap);
     if (e == cudaSuccess) e = cudaMalloc(&d_ex, cap);
     if (e == cudaSuccess) e = cudaMalloc(&d_fb, cap * 4);
@@ -1590,15 +1565,15 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
     if (e == cudaSuccess) e = cudaMalloc(&d_fl, cap * 8);
     if (e == cudaSuccess) {
         const int block = 256;
-        k_decisions<<<grid_for(np, block, ctx->num_sms * 8), block, 0, st>>>(
-            P, m->moving, m->mmask, m->codes, m->chunk_run, m->run_brick, np, d_st, d_fb, d_mb, d_fl, d_ex);
+        k_decisions<<<grid_for(ns, block, ctx->num_sms * 8), block, 0, st>>>(P, m->moving, m->mmask, m->samples, m->fbin,
+                                                                             ns, d_st, d_fb, d_mb, d_fl, d_ex);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_st.data(), d_st, (size_t)np, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_ex.data(), d_ex, (size_t)np, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_fb.data(), d_fb, (size_t)np * 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_mb.data(), d_mb, (size_t)np * 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_fl.data(), d_fl, (size_t)np * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && status) e = cudaMemcpyAsync(status, d_st, (size_t)ns, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && exact) e = cudaMemcpyAsync(exact, d_ex, (size_t)ns, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && fixed_bin) e = cudaMemcpyAsync(fixed_bin, d_fb, (size_t)ns * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && moving_bin) e = cudaMemcpyAsync(moving_bin, d_mb, (size_t)ns * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && flat) e = cudaMemcpyAsync(flat, d_fl, (size_t)ns * 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(d_st);
     cudaFree(d_ex);
@@ -1606,19 +1581,6 @@ mi_status mi_metric_sample_decisions(mi_metric* m, const double* stages, int nst
     cudaFree(d_mb);
     cudaFree(d_fl);
     if (e != cudaSuccess) return cuda_status(ctx, e, "mi_metric_sample_decisions");
-    // the padded walk without its padding lanes is the sample order
-    int64_t o = 0;
-    for (int64_t p = 0; p < np; ++p) {
-        if (h_st[p] < 0) continue;
-        if (o >= m->n_samples) return set_error(ctx, MI_ERR_CUDA, "brick layout holds more samples than the metric");
-        if (status) status[o] = h_st[p];
-        if (fixed_bin) fixed_bin[o] = h_fb[p];
-        if (moving_bin) moving_bin[o] = h_mb[p];
-        if (flat) flat[o] = h_fl[p];
-        if (exact) exact[o] = h_ex[p];
-        ++o;
-    }
-    if (o != m->n_samples) return set_error(ctx, MI_ERR_CUDA, "brick layout holds fewer samples than the metric");
     return MI_OK;
 }
 

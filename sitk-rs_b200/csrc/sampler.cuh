@@ -267,9 +267,9 @@ enum : int { SAMPLE_EXACT = 3 };
 // SAMPLE_OUTSIDE; otherwise the cell's fractions are kept and its eight corners
 // requested (SAMPLE_VALID). The value-only and the value+derivative passes hand the
 // same samples to the exact chain, so both form the same histogram bits.
-template <bool GRAD>
-__device__ __forceinline__ int prep_fast(const SamplerParams& P, uint32_t flat, const uint8_t* __restrict__ mmask,
-                                         Prep& p) {
+template <bool GRAD, class Corners>
+__device__ __forceinline__ int prep_fast_src(const SamplerParams& P, uint32_t flat, const uint8_t* __restrict__ mmask,
+                                             Prep& p, Corners corners) {
     p.flat = flat;
     uint32_t i, j, k;
     grid_index(P, flat, i, j, k);
@@ -322,9 +322,15 @@ __device__ __forceinline__ int prep_fast(const SamplerParams& P, uint32_t flat, 
     // The eight corners of the cell of c. c passed the inside test, so floor(c) ∈
     // [−1, size − 1]; the texture's point sampling at voxel centres returns the stored
     // voxel unchanged and its clamp addressing is the reference's clamp-to-edge of each
-    // corner index.
-    fetch_corners(P, fl, p.v);
+    // corner index. (prep_fast_src takes another source of the same values.)
+    corners(fl, p.v);
     return SAMPLE_VALID;
+}
+
+template <bool GRAD>
+__device__ __forceinline__ int prep_fast(const SamplerParams& P, uint32_t flat, const uint8_t* __restrict__ mmask,
+                                         Prep& p) {
+    return prep_fast_src<GRAD>(P, flat, mmask, p, [&](const double* fl, float* v) { fetch_corners(P, fl, v); });
 }
 
 // The trilinear value at fractions fr of the cell with corners v (x-lerps, then y,

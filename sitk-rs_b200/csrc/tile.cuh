@@ -13,10 +13,15 @@
 // time-out the warp raises the evaluation's error word and leaves its loop, so a launch
 // that lost a load ends instead of hanging; the host then reports MI_ERR_TIMEOUT.
 //
-// A brick is staged only when every cell its samples can use lies inside the moving
-// volume (no clamp-to-edge needed) and inside the box; otherwise its samples take the
-// texture path (brick_prep). The box's x origin is a multiple of four voxels (16 bytes,
-// the TMA rule for the innermost coordinate); loads only, no multicast.
+// Per sample the pass runs the texture pass's chain (prep_fast, finish_fast, the exact
+// chain where a decision is open, hist_phase's taps and records) with the corners read
+// from the tile, so it takes the same decisions, routes the same samples to the exact
+// chain and forms the same histogram and records, to the bit. A brick is staged only
+// when every cell its samples can use lies inside the moving volume (no clamp-to-edge
+// needed) and inside the box; a staged sample whose cell would fall outside the box
+// (which the construction excludes) and every sample of an unstaged brick read the
+// texture. The box's x origin is a multiple of four voxels (16 bytes, the TMA rule for
+// the innermost coordinate); loads only, no multicast.
 #pragma once
 
 #include <cuda.h>
@@ -115,53 +120,45 @@ __device__ __forceinline__ TileMeta tile_meta(const SamplerParams& P, const Tile
     return t;
 }
 
-// A staged brick's sample: brick_prep's index, face and mask decisions (the inside test
-// holds for the whole brick), the corners from the tile. A cell outside the tile, which
-// the construction excludes, is handed to the exact chain rather than read.
-template <bool MASK>
-__device__ __forceinline__ int tile_prep(const SamplerParams& P, const TileArgs& T, const TileMeta& t,
-                                         const float* tile, uint32_t code, const uint8_t* __restrict__ mmask, Prep& p) {
-    const int bl = P.brick_bl;
-    const uint32_t msk = (1u << bl) - 1u;
-    const double dx = (double)(code & msk), dy = (double)((code >> bl) & msk), dz = (double)((code >> (2 * bl)) & msk);
-    double c[3], fl[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        c[d] = fma(P.cA[d * 3 + 2], dz, fma(P.cA[d * 3 + 1], dy, fma(P.cA[d * 3 + 0], dx, t.b.co[d])));
-        fl[d] = floor(c[d]);
-        p.fr[d] = (float)(c[d] - fl[d]);
+// One sample of the walk (flat index `flat`, walk position `ws`, fixed bin `fi`): the
+// texture pass's chain with the corners from the staged tile when the brick is staged.
+template <bool RECORD>
+__device__ __forceinline__ void tile_sample(const SamplerParams& P, const EvalArgs& a, const BrickHist& h,
+                                            const TileArgs& T, const TileMeta& t, const float* tile, uint32_t flat,
+                                            uint32_t ws, int fi) {
+    Prep p;
+    int st;
+    if (t.ok) {
+        st = prep_fast_src<RECORD>(P, flat, a.mmask, p, [&](const double* fl, float* v) {
+            const int x = (int)fl[0] - t.ox, y = (int)fl[1] - t.oy, z = (int)fl[2] - t.oz;
+            if ((unsigned)x < (unsigned)(T.bx - 1) && (unsigned)y < (unsigned)(T.by - 1) &&
+                (unsigned)z < (unsigned)(T.bz - 1)) {
+                const int sx = T.bx, sxy = T.bx * T.by;
+                const float* q = tile + (z * T.by + y) * T.bx + x;
+                v[0] = q[0];
+                v[1] = q[1];
+                v[2] = q[sx];
+                v[3] = q[sx + 1];
+                v[4] = q[sxy];
+                v[5] = q[sxy + 1];
+                v[6] = q[sxy + sx];
+                v[7] = q[sxy + sx + 1];
+            } else {
+                fetch_corners(P, fl, v);
+            }
+        });
+    } else {
+        st = prep_fast<RECORD>(P, flat, a.mmask, p);
     }
-    const float flo = fminf(fminf(p.fr[0], p.fr[1]), p.fr[2]);
-    const float fhi = fmaxf(fmaxf(p.fr[0], p.fr[1]), p.fr[2]);
-    if (!(flo > P.face_lo && fhi < P.face_hi)) return SAMPLE_EXACT;
-    if (MASK) {
-        const double ce = 2.0 * P.cerr;
-        uint32_t mflat = 0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double h = c[d] + 0.5;
-            const double r = floor(h);
-            if (floor(h - ce) != floor(h + ce)) return SAMPLE_EXACT;
-            if (!(r >= 0.0 && r < (double)P.msz[d])) return SAMPLE_OUTSIDE;
-            const uint32_t ri = (uint32_t)r;
-            mflat += d == 0 ? ri : (d == 1 ? ri * P.ms1 : ri * P.ms2);
-        }
-        if (!__ldg(mmask + mflat)) return SAMPLE_OUTSIDE;
+    Sample o;
+    if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
+    if (st == SAMPLE_EXACT) {
+        Sample e;
+        st = sample_exact<RECORD>(P, flat, a.moving, a.mmask, e);
+        brick_account<RECORD>(a, h, P.bins, st, e, ws, fi);
+    } else {
+        brick_account<RECORD>(a, h, P.bins, st, o, ws, fi);
     }
-    const int x = (int)fl[0] - t.ox, y = (int)fl[1] - t.oy, z = (int)fl[2] - t.oz;
-    if ((unsigned)x >= (unsigned)(T.bx - 1) || (unsigned)y >= (unsigned)(T.by - 1) || (unsigned)z >= (unsigned)(T.bz - 1))
-        return SAMPLE_EXACT;
-    const int sx = T.bx, sxy = T.bx * T.by;
-    const float* q = tile + (z * T.by + y) * T.bx + x;
-    p.v[0] = q[0];
-    p.v[1] = q[1];
-    p.v[2] = q[sx];
-    p.v[3] = q[sx + 1];
-    p.v[4] = q[sxy];
-    p.v[5] = q[sxy + 1];
-    p.v[6] = q[sxy + sx];
-    p.v[7] = q[sxy + sx + 1];
-    return SAMPLE_VALID;
 }
 
 // Pass 1 with staged tiles (see the file comment). Launched with TILE_BLOCK threads.
@@ -215,7 +212,7 @@ __device__ __forceinline__ void tile_hist_phase(const SamplerParams& P, const Ev
         } else {
             const BrickHist h = brick_hist_lane(a, sh, B);
             const uint32_t* __restrict__ codes = a.codes;
-            const uint8_t* __restrict__ mmask = a.mmask;
+            const int fshift = 3 * P.brick_bl;
             for (uint32_t ri = 0; ri < nr; ++ri) {
                 const int s = (int)(ri % (uint32_t)S);
                 if (!mbar_wait(full + s, (ri / (uint32_t)S) & 1u)) {
@@ -228,18 +225,20 @@ __device__ __forceinline__ void tile_hist_phase(const SamplerParams& P, const Ev
                 const uint32_t cr0 = max(__ldg(T.run_chunk0 + r), c0), cr1 = min(__ldg(T.run_chunk0 + r + 1), c1);
                 // this warp's chunks of the brick: index ≡ warp (mod 16)
                 const uint32_t first = cr0 + (((uint32_t)warp + 16u - (cr0 & 15u)) & 15u);
+                // walk position of the run's padded position 0
+                const uint32_t wbase = __ldg(a.run_start + r) - __ldg(T.run_chunk0 + r) * BRICK_CHUNK;
+                uint32_t code = first < cr1 ? __ldg(codes + (size_t)first * BRICK_CHUNK + lane) : BRICK_PAD;
                 for (uint32_t c = first; c < cr1; c += TILE_CONSUMER_WARPS) {
-                    const uint32_t code = __ldg(codes + (size_t)c * BRICK_CHUNK + lane);
-                    if (code == BRICK_PAD) continue;
-                    Prep p;
-                    int st;
-                    if (t.ok)
-                        st = P.has_mmask ? tile_prep<true>(P, T, t, tile, code, mmask, p)
-                                         : tile_prep<false>(P, T, t, tile, code, mmask, p);
-                    else
-                        st = P.has_mmask ? brick_prep<true>(P, t.b, code, mmask, p)
-                                         : brick_prep<false>(P, t.b, code, mmask, p);
-                    brick_settle<RECORD>(P, a, h, st, p, code, t.b.packed, c * BRICK_CHUNK + lane);
+                    const uint32_t cn = c + TILE_CONSUMER_WARPS;
+                    const uint32_t code_n = cn < cr1 ? __ldg(codes + (size_t)cn * BRICK_CHUNK + lane) : BRICK_PAD;
+                    if (code != BRICK_PAD) {
+                        // the record's position in the walk: from the run's start, or the voxel
+                        // itself when the walk is the whole grid in voxel order
+                        const uint32_t flat = brick_flat(P, t.b.packed, code);
+                        tile_sample<RECORD>(P, a, h, T, t, tile, flat, a.samples ? wbase + c * BRICK_CHUNK + lane : flat,
+                                            (int)(code >> fshift));
+                    }
+                    code = code_n;
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(empty + s);
