@@ -20,6 +20,8 @@ the 64-pair batched registration (device-timed per-pair completion), and the bat
 learned-initialiser form against the plain single-pair driver on held-out 128³ pairs
 (the committed weights). `--storage-study`, `--initnet` and `--gemm-study` run the
 512³ storage study, the initialiser's training study and its GEMM timings instead.
+`--corners tiles` times the histogram pass with TMA-staged moving tiles (the opt-in
+corner source) instead of the moving volume's texture.
 
 --impl reference times the reference algorithm's CPU implementation on this host's
 cores (the C++ restatement under oracle/, all threads), since the Rust reference
@@ -435,6 +437,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if args.form == "fused":
         set_fused(metric, True)
     fused = get_fused(metric)
+    if args.corners == "tiles":
+        # the histogram pass's opt-in corner source: TMA-staged moving tiles
+        from sitk_b200.metric import set_tile_staging
+        set_tile_staging(metric, True)
+        if full_metric is not None:
+            set_tile_staging(full_metric, True)
     launches_per_eval = 1 if fused else 2
     l2 = torch.cuda.get_device_properties(dev).L2_cache_size
     nflush = max(2 * l2, 256 << 20) // 4
@@ -527,8 +535,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         kern = {"k_eval": ms_k[1] / nev_k}
         dom, bytes_alg = "k_eval", 2 * pass_bytes  # both passes in one launch
     else:
-        kern = {"k_hist": ms_k[1] / nev_k, "k_deriv": ms_k[2] / nev_k}  # k_deriv forms the tail itself
-        dom, bytes_alg = "k_hist", pass_bytes
+        hname = "k_hist_tile" if args.corners == "tiles" else "k_hist"
+        kern = {hname: ms_k[1] / nev_k, "k_deriv": ms_k[2] / nev_k}  # k_deriv forms the tail itself
+        dom, bytes_alg = hname, pass_bytes
     peak, peak_kind = _peaks()
     achieved = bytes_alg / (kern[dom] / 1e3) / 1e9
     traffic = _traffic(dom)
@@ -599,6 +608,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "vs_baseline": None, "dtype": DTYPE, "data": "synthetic",
         "config": workload_config(S, world),
         "form": "fused (one cooperative kernel)" if fused else "split (two kernels)",
+        "corners": ("TMA-staged moving tiles" if args.corners == "tiles" else "moving-volume texture"),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * (6 + 3),
                 "d2h_bytes_per_step": 8 * (2 + 6)},
         "gpu_launches": launches_per_eval * args.steps,  # in the timed loop of `value`
@@ -703,6 +713,10 @@ def run_gemm_study(args, rank: int, world: int, local_rank: int):
               ("conv0 weight gradient", 16, 56, 262144), ("conv1 weight gradient", 32, 432, 32768),
               ("conv2 weight gradient", 64, 864, 4096), ("square 4096", 4096, 4096, 4096),
               ("square 8192", 8192, 8192, 8192)]
+    if args.gemm_shape:
+        # one product only (e.g. for a profiler capture): "MxNxK"
+        M_, N_, K_ = (int(x) for x in args.gemm_shape.lower().split("x"))
+        shapes = [(f"{M_}x{N_}x{K_}", M_, N_, K_)]
     peak_t = None
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -865,6 +879,10 @@ def main():
                     help="skip the mean-squares and correlation timings reported beside the metric")
     ap.add_argument("--form", default="split", choices=["split", "fused"],
                     help="launch form of an evaluation: two kernels, or one cooperative kernel")
+    ap.add_argument("--gemm-shape", default=None,
+                    help="with --gemm-study: time this one product only, given as MxNxK")
+    ap.add_argument("--corners", default="texture", choices=["texture", "tiles"],
+                    help="corner source of the histogram pass: the moving volume's texture, or TMA-staged tiles")
     ap.add_argument("--settle", type=float, default=1.0,
                     help="seconds of untimed evaluations before the timed region (clock ramp)")
     ap.add_argument("--initnet", action="store_true",
