@@ -53,10 +53,11 @@ constexpr int GHIST_REPS = MI_GHIST_REPS;
 #define MI_HIST_CLUSTER 1
 #endif
 constexpr int HIST_CLUSTER = MI_HIST_CLUSTER;
-// Samples the fast path cannot decide: 1 queues them and runs the exact chain after the
-// histogram phase's main loop, 0 runs it inside the loop (out of line, see
-// MI_EXACT_NOINLINE). Inside measured faster: a few exact samples per CTA, drained after
-// the loop, held back the CTA's flush by their dependent loads.
+// Samples whose cell the fast path cannot settle (SAMPLE_EXACT): 1 queues them and runs
+// the whole exact chain after the histogram phase's main loop, 0 runs it inside the loop
+// (out of line, see MI_EXACT_NOINLINE). Inside measured faster: a few exact samples per
+// CTA, drained after the loop, held back the CTA's flush by their dependent loads. The
+// exact value part on the corners already fetched (SAMPLE_EXACT_CELL) runs in the loop.
 #ifndef MI_EXACT_DEFERRED
 #define MI_EXACT_DEFERRED 0
 #endif
@@ -349,11 +350,16 @@ __device__ __forceinline__ void hist_phase(const SamplerParams& P, const EvalArg
     // Whole warps iterate together (the loop bound is the warp's first sample).
     const uint32_t wbase = r.begin + r.warp_first;
     // A sample the fast path cannot decide goes to the exact chain: queued (or, without
-    // a queue, run here, out of line).
+    // a queue, run here, out of line: the whole chain, or only its value part on the
+    // corners already fetched when just a range or Parzen decision was uncertain).
     auto settle = [&](int st, const Prep& p, uint32_t s, int fi) {
         Sample o;
         if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
-        if (st == SAMPLE_EXACT) {
+        if (st == SAMPLE_EXACT_CELL) {
+            Sample e;
+            st = sample_exact_cell<RECORD>(P, p.flat, p.v, e);
+            account(st, e, s, fi);
+        } else if (st == SAMPLE_EXACT) {
             if (exq.base) {
                 exq.base[atomicAdd(&exq_count, 1u)] = s;
             } else {

@@ -120,6 +120,24 @@ __device__ __forceinline__ void exact_index(const SamplerParams& P, uint32_t i, 
 // running product ((w0·w1)·w2) (its leading 1.0· is exact), summed in corner order.
 // The eight clamped corners it reads are left in v (corner t at bit offsets
 // (t & 1, (t >> 1) & 1, t >> 2)), for a caller that also needs the gradient.
+// The FP64 trilinear sum on the cell's corners v at the fractions fr (om = 1 − fr), in
+// the reference's order.
+__device__ __forceinline__ double exact_trilinear(const double* fr, const double* om, const float* v) {
+    const double w00 = __dmul_rn(om[0], om[1]);
+    const double w10 = __dmul_rn(fr[0], om[1]);
+    const double w01 = __dmul_rn(om[0], fr[1]);
+    const double w11 = __dmul_rn(fr[0], fr[1]);
+    double mv = __dmul_rn(__dmul_rn(w00, om[2]), (double)v[0]);
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, om[2]), (double)v[1]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, om[2]), (double)v[2]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, om[2]), (double)v[3]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w00, fr[2]), (double)v[4]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, fr[2]), (double)v[5]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, fr[2]), (double)v[6]));
+    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, fr[2]), (double)v[7]));
+    return mv;
+}
+
 __device__ __forceinline__ double exact_value_corners(const SamplerParams& P, const double* c,
                                                       const float* __restrict__ moving, float* v) {
     double fr[3], om[3];
@@ -136,10 +154,6 @@ __device__ __forceinline__ double exact_value_corners(const SamplerParams& P, co
     }
     const int64_t oy0 = b0[1] * P.mstride1, oy1 = b1[1] * P.mstride1;
     const int64_t oz0 = b0[2] * P.mstride2, oz1 = b1[2] * P.mstride2;
-    const double w00 = __dmul_rn(om[0], om[1]);
-    const double w10 = __dmul_rn(fr[0], om[1]);
-    const double w01 = __dmul_rn(om[0], fr[1]);
-    const double w11 = __dmul_rn(fr[0], fr[1]);
     v[0] = __ldg(moving + (b0[0] + oy0 + oz0));
     v[1] = __ldg(moving + (b1[0] + oy0 + oz0));
     v[2] = __ldg(moving + (b0[0] + oy1 + oz0));
@@ -148,15 +162,7 @@ __device__ __forceinline__ double exact_value_corners(const SamplerParams& P, co
     v[5] = __ldg(moving + (b1[0] + oy0 + oz1));
     v[6] = __ldg(moving + (b0[0] + oy1 + oz1));
     v[7] = __ldg(moving + (b1[0] + oy1 + oz1));
-    double mv = __dmul_rn(__dmul_rn(w00, om[2]), (double)v[0]);
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, om[2]), (double)v[1]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, om[2]), (double)v[2]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, om[2]), (double)v[3]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w00, fr[2]), (double)v[4]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w10, fr[2]), (double)v[5]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w01, fr[2]), (double)v[6]));
-    mv = __dadd_rn(mv, __dmul_rn(__dmul_rn(w11, fr[2]), (double)v[7]));
-    return mv;
+    return exact_trilinear(fr, om, v);
 }
 
 __device__ __forceinline__ double exact_value(const SamplerParams& P, const double* c,
@@ -256,8 +262,12 @@ struct Prep {
     float v[8];
 };
 
-// Outcome of a fast-path stage: a decision, or the sample handed to the exact chain.
-enum : int { SAMPLE_EXACT = 3 };
+// Outcome of a fast-path stage: a decision, or the sample handed to the exact chain —
+// the whole chain (SAMPLE_EXACT, from prep_fast: the cell itself is uncertain), or only
+// its value part on the cell the fast path fetched (SAMPLE_EXACT_CELL, from
+// finish_fast: the cell, inside test and mask are certain, a range or Parzen decision
+// is not).
+enum : int { SAMPLE_EXACT = 3, SAMPLE_EXACT_CELL = 4 };
 
 // prep_fast(): the fast path's first stage. c from the composite map (within cerr of
 // the exact c). A sample whose inside test or mask rounding could flip within ±cerr,
@@ -360,20 +370,20 @@ __device__ __forceinline__ float trilinear(const float* v, const float* fr, floa
 //   rlo_in ≤ mv ≤ rhi_in                    surely in range,
 // the thresholds being the range ends ∓ the bound rounded outward to f32; and the
 // Parzen term's floor is certain when floor(termf − dterm) = floor(termf + dterm)
-// after the clamp to [2, bins − 3]. Anything else is SAMPLE_EXACT. Every operation is
+// after the clamp to [2, bins − 3]. Anything else is SAMPLE_EXACT_CELL. Every operation is
 // an explicitly rounded intrinsic, so every kernel that inlines this takes the same
 // path for a sample.
 template <bool GRAD>
 __device__ __forceinline__ int finish_fast(const SamplerParams& P, const Prep& p, Sample& o) {
     const float mv = trilinear<GRAD>(p.v, p.fr, o.g);
     if (mv < P.rlo_out || mv > P.rhi_out) return SAMPLE_OUT_OF_RANGE;
-    if (!(mv >= P.rlo_in && mv <= P.rhi_in)) return SAMPLE_EXACT;
+    if (!(mv >= P.rlo_in && mv <= P.rhi_in)) return SAMPLE_EXACT_CELL;
     const float termf = __fmaf_rn(mv, P.inv_bin_f, -P.nmin_f);
     // truncation then clamp to [2, bins − 3] equals floor then clamp for every term
     // (anything below 2 clamps to 2)
     const float lo = fminf(fmaxf(floorf(__fsub_rn(termf, P.dterm)), (float)PADDING), P.bin_hi_f);
     const float hi = fminf(fmaxf(floorf(__fadd_rn(termf, P.dterm)), (float)PADDING), P.bin_hi_f);
-    if (lo != hi) return SAMPLE_EXACT;
+    if (lo != hi) return SAMPLE_EXACT_CELL;
     o.mi = (int)lo;
     o.f = __fsub_rn(termf, lo);
     return SAMPLE_VALID;
@@ -394,6 +404,34 @@ __device__ __forceinline__ int finish_fast(const SamplerParams& P, const Prep& p
 #else
 #define MI_EXACT_INLINE __forceinline__
 #endif
+// The value part alone (sample_exact_cell: no loads) inline in its callers by default.
+#ifndef MI_EXACT_CELL_NOINLINE
+#define MI_EXACT_CELL_NOINLINE 0
+#endif
+#if MI_EXACT_CELL_NOINLINE
+#define MI_EXACT_CELL_INLINE __noinline__
+#else
+#define MI_EXACT_CELL_INLINE __forceinline__
+#endif
+// The exact chain's decisions on the reference's value mvx at the exact index c of the
+// cell with corners v: range reject, Parzen bin and fraction, and for GRAD the FP32
+// index-space gradient of the interpolant.
+template <bool GRAD>
+__device__ __forceinline__ int exact_decide(const SamplerParams& P, const double* c, double mvx, const float* v,
+                                            Sample& o) {
+    if (mvx < P.moving_min || mvx > P.moving_max) return SAMPLE_OUT_OF_RANGE;
+    if (GRAD) {
+        float fr[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fr[d] = (float)__dsub_rn(c[d], floor(c[d]));
+        trilinear<true>(v, fr, o.g);
+    }
+    const double term = __dsub_rn(__ddiv_rn(mvx, P.moving_bin_size), P.moving_nmin);
+    o.mi = parzen_bin(term, P.bins);
+    o.f = (float)(term - (double)o.mi);
+    return SAMPLE_VALID;
+}
+
 template <bool GRAD>
 __device__ MI_EXACT_INLINE int sample_exact_ijk(const SamplerParams& P, uint32_t i, uint32_t j, uint32_t k,
                                              const float* __restrict__ moving, const uint8_t* __restrict__ mmask,
@@ -416,17 +454,7 @@ __device__ MI_EXACT_INLINE int sample_exact_ijk(const SamplerParams& P, uint32_t
     }
     float v[8];
     const double mvx = exact_value_corners(P, c, moving, v);
-    if (mvx < P.moving_min || mvx > P.moving_max) return SAMPLE_OUT_OF_RANGE;
-    if (GRAD) {
-        float fr[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) fr[d] = (float)__dsub_rn(c[d], floor(c[d]));
-        trilinear<true>(v, fr, o.g);
-    }
-    const double term = __dsub_rn(__ddiv_rn(mvx, P.moving_bin_size), P.moving_nmin);
-    o.mi = parzen_bin(term, P.bins);
-    o.f = (float)(term - (double)o.mi);
-    return SAMPLE_VALID;
+    return exact_decide<GRAD>(P, c, mvx, v, o);
 }
 
 template <bool GRAD>
@@ -435,6 +463,27 @@ __device__ __forceinline__ int sample_exact(const SamplerParams& P, uint32_t fla
     uint32_t i, j, k;
     grid_index(P, flat, i, j, k);
     return sample_exact_ijk<GRAD>(P, i, j, k, moving, mmask, o);
+}
+
+// The exact chain's value part for a sample whose cell the fast path settled
+// (SAMPLE_EXACT_CELL): the fast c was at least cerr from every cell face, the inside
+// test and the mask byte were certain, so the exact index lies in the same cell, passes
+// the same tests, and the eight corners the fast path fetched (v, each the clamped voxel
+// the reference reads) are the ones the reference's trilinear sum takes. Only the exact
+// index, the FP64 sum and the decisions remain; no corner is read again.
+template <bool GRAD>
+__device__ MI_EXACT_CELL_INLINE int sample_exact_cell(const SamplerParams& P, uint32_t flat, const float* v, Sample& o) {
+    uint32_t i, j, k;
+    grid_index(P, flat, i, j, k);
+    double c[3];
+    exact_index(P, i, j, k, c);
+    double fr[3], om[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        fr[d] = __dsub_rn(c[d], floor(c[d]));
+        om[d] = __dsub_rn(1.0, fr[d]);
+    }
+    return exact_decide<GRAD>(P, c, exact_trilinear(fr, om, v), v, o);
 }
 
 // The whole sampler for one sample: the fast path, handing to the exact chain where it
@@ -446,9 +495,9 @@ __device__ __forceinline__ int sample(const SamplerParams& P, uint32_t flat, con
     o.exact = false;
     int st = prep_fast<GRAD>(P, flat, mmask, p);
     if (st == SAMPLE_VALID) st = finish_fast<GRAD>(P, p, o);
-    if (st == SAMPLE_EXACT) {
+    if (st == SAMPLE_EXACT || st == SAMPLE_EXACT_CELL) {
         Sample e;
-        st = sample_exact<GRAD>(P, flat, moving, mmask, e);
+        st = st == SAMPLE_EXACT ? sample_exact<GRAD>(P, flat, moving, mmask, e) : sample_exact_cell<GRAD>(P, flat, p.v, e);
         o = e;
         o.exact = true;
     }

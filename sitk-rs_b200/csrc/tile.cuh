@@ -152,9 +152,10 @@ __device__ __forceinline__ void tile_sample(const SamplerParams& P, const EvalAr
     }
     Sample o;
     if (st == SAMPLE_VALID) st = finish_fast<RECORD>(P, p, o);
-    if (st == SAMPLE_EXACT) {
+    if (st == SAMPLE_EXACT || st == SAMPLE_EXACT_CELL) {
         Sample e;
-        st = sample_exact<RECORD>(P, flat, a.moving, a.mmask, e);
+        st = st == SAMPLE_EXACT ? sample_exact<RECORD>(P, flat, a.moving, a.mmask, e)
+                                : sample_exact_cell<RECORD>(P, flat, p.v, e);
         brick_account<RECORD>(a, h, P.bins, st, e, ws, fi);
     } else {
         brick_account<RECORD>(a, h, P.bins, st, o, ws, fi);
