@@ -139,7 +139,7 @@ k_batch_deriv(PairDev* __restrict__ pairs, const Chunk* __restrict__ chunks, int
         __syncthreads();
         if (last) {
             __threadfence();
-            deriv_fold(sP, pd.J, pd.a, t.degenerate, pd.a.partials, (unsigned int)pd.nchunks);
+            deriv_fold(sP, pd.J, pd.a, t, pd.a.partials, (unsigned int)pd.nchunks);
             if (threadIdx.x < 32) fold_value(sP.bins, pd.a, t);
             if (threadIdx.x == 0) pd.done = 0u;
             const int nb = sP.bins * sP.bins + sP.bins;

@@ -606,6 +606,20 @@ __device__ __forceinline__ unsigned long long least_joint(double dt) {
     return c > 0ull ? c : 1ull;
 }
 
+// The least integer c ≥ 1 with (double)c / d > ε, for the whole calling warp (every lane
+// calls it, every lane gets it): the test is monotone in c, so lanes 0..7 try eight
+// candidates around ε·d at once, and the serial search (least_joint) runs only when the
+// boundary is not among them.
+__device__ __forceinline__ unsigned long long least_passing(double d) {
+    const int lane = threadIdx.x & 31;
+    const long long c0 = (long long)(DBL_EPSILON * d);
+    const long long cand = c0 - 3 + lane;
+    const bool pass = lane < 8 && cand >= 1 && (double)cand / d > DBL_EPSILON;
+    const unsigned int hit = __ballot_sync(0xffffffffu, pass) & 0xffu;
+    const int k = hit ? __ffs(hit) - 1 : 8;
+    return k >= 1 && k < 8 ? (unsigned long long)(c0 - 3 + k) : least_joint(d);
+}
+
 // The rest of the tail on the fetched histogram.
 __device__ TailCtx tail_finish(int B, double moving_bin_size, const EvalArgs& a, const TailSmem& ts) {
     const int B2 = B * B;
@@ -912,16 +926,27 @@ __device__ __forceinline__ GroupWork grid_groups(const EvalArgs& a) {
 // them coalesced.
 __device__ __forceinline__ void store_moments(const float* acc, double* red, double* part, int64_t part_stride) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    double accd[NMOM];
+    // reduce-scatter over the warp: the 12 moments (padded to 16 slots) are halved at
+    // each xor step (a lane keeps the half its step bit selects and adds its partner's
+    // copy of it), so after four steps lane pair (2s, 2s + 1) holds slot s summed over
+    // 16 lanes and the fifth step adds the pair: 16 shuffles instead of 60
+    double x[16];
 #pragma unroll
-    for (int i = 0; i < NMOM; ++i) {
-        double v = (double)acc[i];
+    for (int i = 0; i < 16; ++i) x[i] = i < NMOM ? (double)acc[i] : 0.0;
+    int slot = 0;
 #pragma unroll
-        for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        accd[i] = v;
+    for (int h = 8, off = 16; h >= 1; h >>= 1, off >>= 1) {
+        const bool hi = (lane & off) != 0;
+#pragma unroll
+        for (int j = 0; j < h; ++j) {
+            const double keep = hi ? x[j + h] : x[j];
+            const double give = hi ? x[j] : x[j + h];
+            x[j] = keep + __shfl_xor_sync(0xffffffffu, give, off);
+        }
+        slot += hi ? h : 0;
     }
-    if (lane == 0)
-        for (int i = 0; i < NMOM; ++i) red[warp * NMOM + i] = accd[i];
+    x[0] += __shfl_xor_sync(0xffffffffu, x[0], 1);
+    if ((lane & 1) == 0 && slot < NMOM) red[warp * NMOM + slot] = x[0];
     __syncthreads();
     if (threadIdx.x < NMOM) {
         double v = 0.0;
@@ -1022,17 +1047,16 @@ __device__ TailCtx deriv_phase(const SamplerParams& P, const EvalArgs& a, double
 // The split form's derivative pass with its own tail. Every CTA forms the pRatio·nFactor
 // table itself from the integer histogram, in one round of requests: this thread's
 // bins, the column sums and fixed counts, and the first group of its records all go out
-// together; the marginals' totals and ε flags, their FP64 logarithms and the least
-// passing joint count follow (tail_scalars, margin_terms, least_joint), then each
-// thread's bins' entries, one FP64 logarithm each (pr_entry). The value's 32-bin
+// together; the marginals' totals and the least passing joint and fixed counts follow
+// in every warp (tail_scalars, least_passing), then each thread's bins' entries
+// (pr_entry). The value's 32-bin
 // slices are summed where they fall: the warp holding slice u in CTA u (u < the CTA
 // count; the rest in CTA u mod count) forms its terms from the same logarithms
 // (value_term, slice_sum) into a.vsum, and the last CTA folds them (fold_slices), so
 // the value has the bits of every other form. No CTA waits for another before its
 // record stream, and the histogram pass ends at its flush.
 __host__ __device__ inline size_t stream_smem(int B) {
-    return 32 * (size_t)NMOM * sizeof(double) + (size_t)B * B * sizeof(float) + (size_t)2 * B * 8 +
-           (((size_t)2 * B + 7) & ~(size_t)7) + 8;
+    return 32 * (size_t)NMOM * sizeof(double) + (size_t)B * B * sizeof(float) + (size_t)2 * B * 8;
 }
 
 // Returns the tail state (for the last CTA's fold).
@@ -1043,9 +1067,6 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
     float* pr = reinterpret_cast<float*>(dsh + 32 * NMOM);
     unsigned long long* col = reinterpret_cast<unsigned long long*>(pr + B2);
     unsigned long long* cnt = col + B;
-    uint8_t* okm = reinterpret_cast<uint8_t*>(cnt + B);
-    uint8_t* okf = okm + B;
-    unsigned long long* jmin_s = reinterpret_cast<unsigned long long*>(okm + ((2 * B + 7) & ~7));
     const int lane = threadIdx.x & 31;
     const int bd = (int)blockDim.x;
     const int wfirst = (int)threadIdx.x - lane;
@@ -1073,40 +1094,37 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
     typename Src::Group cur;
     if (q < w.end) Src::load(a, q, cur);
     __syncthreads();
-    // The pRatio table needs the ε flags of the margins and the least passing joint
-    // count, not the margins' logarithms: those feed only the value, whose slices are
-    // summed after this CTA's records (off the path to its moments).
+    // The pRatio table needs the ε tests of the joint counts and the margins, not the
+    // margins' logarithms (those feed only the value, whose slices are summed after this
+    // CTA's records). Each test (count/total > ε for a joint count or column sum,
+    // count/joint_sum > ε for a fixed count; mattes.rs:305-320) is monotone in the
+    // integer count, so each warp finds the two least passing counts itself
+    // (least_passing) and the tests become integer compares: the table follows the
+    // fetch with no further barrier.
     const TailCtx t = tail_scalars(B, col, cnt, a.hist_inv, P.moving_bin_size);
-    if ((int)threadIdx.x < B) {
-        const int m = threadIdx.x;
-        okm[m] = (double)col[m] / t.dt > DBL_EPSILON;
-        okf[m] = (double)cnt[m] / t.joint_sum > DBL_EPSILON;
-    }
-    if (threadIdx.x < 32) {
-        // the least jv ≥ 1 with jv/total > ε (monotone in jv): eight candidates around
-        // ε·total tested at once; the serial search (least_joint) only when the boundary
-        // is not among them
-        const long long c0 = (long long)(DBL_EPSILON * t.dt);
-        const long long cand = c0 - 3 + lane;
-        const bool pass = lane < 8 && cand >= 1 && (double)cand / t.dt > DBL_EPSILON;
-        const unsigned int hit = __ballot_sync(0xffffffffu, pass) & 0xffu;
-        if (lane == 0) {
-            const int k = hit ? __ffs(hit) - 1 : 8;
-            *jmin_s = k >= 1 && k < 8 ? (unsigned long long)(c0 - 3 + k) : least_joint(t.dt);
-        }
-    }
-    __syncthreads();
-    const unsigned long long jmin = *jmin_s;
+    const unsigned long long jmin = least_passing(t.dt);
+    const unsigned long long fmin = least_passing(t.joint_sum);
     const float nf = (float)t.n_factor;
-    for (int i0 = wfirst; i0 < ns * 32; i0 += R * bd) {
-        if (i0 != wfirst) load_round(i0);
+    {
+        // this thread's bins i = wfirst + lane + k·bd (k = 0, 1, …), row f and column m
+        // advanced with i
+        const int df = bd / B, dm = bd - df * B;
+        int f = (wfirst + lane) / B, m = wfirst + lane - f * B;
+        for (int i0 = wfirst; i0 < ns * 32; i0 += R * bd) {
+            if (i0 != wfirst) load_round(i0);
 #pragma unroll
-        for (int u = 0; u < R; ++u) {
-            const int i = i0 + u * bd + lane;
-            if (i < B2) {
-                const int f = i / B, m = i - f * B;
-                const bool take = !t.degenerate && okf[f] && okm[m] && jv[u] >= jmin;
-                pr[i] = pr_entry(take, jv[u], col[m], nf);
+            for (int u = 0; u < R; ++u) {
+                const int i = i0 + u * bd + lane;
+                if (i < B2) {
+                    const bool take = !t.degenerate && cnt[f] >= fmin && col[m] >= jmin && jv[u] >= jmin;
+                    pr[i] = pr_entry(take, jv[u], col[m], nf);
+                }
+                f += df;
+                m += dm;
+                if (m >= B) {
+                    m -= B;
+                    ++f;
+                }
             }
         }
     }
@@ -1124,7 +1142,7 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
             if (i < B2) {
                 const int f = i / B, m = i - f * B;
                 const unsigned long long v = __ldcg(a.ghist + i);
-                if (okf[f] && okm[m] && v >= jmin) {
+                if (cnt[f] >= fmin && col[m] >= jmin && v >= jmin) {
                     const double lcol = log((double)col[m]);
                     const double lfm = log((double)cnt[f] / t.joint_sum);
                     term = value_term(v, true, log((double)v), lcol, lfm, t);
@@ -1139,28 +1157,34 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
 }
 
 // Run by the last CTA to finish the derivative phase: fold the `count` partials of
-// each slot ([slot][count]) in a fixed order (lane l of a slot sums entries l, l+21,
-// …, in batches of sixteen loads issued together, so up to 336 partials per slot
-// take one round trip; the 21 lane sums of a slot are then added in lane order) and
+// each slot ([slot][count]) in a fixed order (lane l of a slot sums entries l, l+18,
+// …, in batches of twenty loads issued together, so up to 360 partials per slot take
+// one round trip; the 18 lane sums of a slot are then added in lane order) and
 // contract with the Jacobian form: ∂/∂p_k = Σ_d J(x_ref)[d][k]·A_d + Σ_{d,e} C_e[d][k]·B[d][e],
-// J(x_ref) = J(0) + Σ_e x_ref,e·C_e.
-__device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const EvalArgs& a, bool degenerate,
+// J(x_ref) = J(0) + Σ_e x_ref,e·C_e. The fold takes the first 216 threads; with
+// WITH_VALUE the CTA's last warp (a CTA of more than 216 threads) folds the value
+// slices (fold_value) meanwhile.
+template <bool WITH_VALUE = false>
+__device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const EvalArgs& a, const TailCtx& tc,
                            const double* partials, unsigned int count) {
-    constexpr int FOLD = 21;
+    constexpr int FOLD = 18, BATCH = 20;
+    const bool degenerate = tc.degenerate;
     __shared__ double fold[FOLD * NMOM];
     __shared__ double mom[NMOM];
     if (threadIdx.x < FOLD * NMOM) {
         const int slot = threadIdx.x / FOLD, ln = threadIdx.x % FOLD;
         const double* src = partials + (int64_t)slot * count;
         double v = 0.0;
-        for (unsigned int b = ln; b < count; b += 16 * FOLD) {
-            double t[16];
+        for (unsigned int b = ln; b < count; b += BATCH * FOLD) {
+            double t[BATCH];
 #pragma unroll
-            for (int u = 0; u < 16; ++u) t[u] = b + u * FOLD < count ? __ldcg(src + b + u * FOLD) : 0.0;
+            for (int u = 0; u < BATCH; ++u) t[u] = b + u * FOLD < count ? __ldcg(src + b + u * FOLD) : 0.0;
 #pragma unroll
-            for (int u = 0; u < 16; ++u) v += t[u];
+            for (int u = 0; u < BATCH; ++u) v += t[u];
         }
         fold[slot * FOLD + ln] = v;
+    } else if (WITH_VALUE && threadIdx.x >= blockDim.x - 32) {
+        fold_value(P.bins, a, tc);
     }
     __syncthreads();
     if (threadIdx.x < NMOM) {
@@ -1201,14 +1225,20 @@ __device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const 
 }
 
 // Arrival at the end of a kernel: returns true in the last CTA to arrive (after
-// which every other CTA's global writes are visible to it).
+// which every other CTA's global writes are visible to it). The CTA's writes are
+// ordered before its arrival by the barrier and one thread's device-scope fence (the
+// fence is cumulative over what the barrier ordered before it), as in a grid-wide
+// barrier's arrival.
 __device__ __forceinline__ bool last_to_arrive(unsigned int* counter) {
     __shared__ bool last;
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const bool l = atomicAdd(counter, 1u) == gridDim.x - 1;
+        if (l) __threadfence();
+        last = l;
+    }
     __syncthreads();
-    if (last) __threadfence();
     return last;
 }
 

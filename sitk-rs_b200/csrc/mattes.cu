@@ -97,7 +97,7 @@ k_eval(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobian
     }
     if (!last_to_arrive(a.sync)) return;
     // every CTA has left the barrier and is done with the histogram
-    if (DERIV) deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
+    if (DERIV) deriv_fold(P, J, a, t, a.partials, gridDim.x);
     if (threadIdx.x < 32) fold_value(B, a, t);
     if (threadIdx.x == 0) {
         a.sync[0] = 0u;
@@ -135,9 +135,10 @@ k_deriv(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobia
     pdl_wait();
     const TailCtx t = stream_phase(P, a, dsh, grid_groups(a));
     if (!last_to_arrive(a.sync)) return;
-    // every CTA has read the histogram and written its value slices and moments
-    deriv_fold(P, J, a, t.degenerate, a.partials, gridDim.x);
-    if (threadIdx.x < 32) fold_value(P.bins, a, t);
+    // every CTA has read the histogram and written its value slices and moments; the
+    // last warp folds the value while the others fold the derivative
+    static_assert(DERIV_BLOCK >= 18 * NMOM + 32, "deriv_fold's value warp");
+    deriv_fold<true>(P, J, a, t, a.partials, gridDim.x);
     publish_seq(a);
     if (threadIdx.x == 0) a.sync[0] = 0u;
     for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
