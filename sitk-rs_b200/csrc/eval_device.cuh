@@ -881,11 +881,9 @@ __device__ __forceinline__ void accumulate_moments(const SamplerParams& P, const
                                                    float* acc) {
     uint32_t i, j, k;
     grid_index(P, flat, i, j, k);
-    const float fi_ = (float)i, fj = (float)j, fk = (float)k;
-    float dx[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-        dx[d] = fmaf(P.xA[d * 3 + 2], fk, fmaf(P.xA[d * 3 + 1], fj, fmaf(P.xA[d * 3 + 0], fi_, P.xb[d])));
+    // the sample's offset from the fixed grid's centre in index units, exact in FP32
+    const float dx[3] = {__fsub_rn((float)i, P.xmid[0]), __fsub_rn((float)j, P.xmid[1]),
+                         __fsub_rn((float)k, P.xmid[2])};
     float dw[4];
     bspline3_deriv_taps(f, dw);
     const float* row = pr + fi * B + (mi - 1);
@@ -1159,7 +1157,8 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
 // Run by the last CTA to finish the derivative phase: fold the `count` partials of
 // each slot ([slot][count]) in a fixed order (lane l of a slot sums entries l, l+18,
 // …, in batches of twenty loads issued together, so up to 360 partials per slot take
-// one round trip; the 18 lane sums of a slot are then added in lane order) and
+// one round trip; the 18 lane sums of a slot are then added by one warp in a fixed xor
+// tree) and
 // contract with the Jacobian form: ∂/∂p_k = Σ_d J(x_ref)[d][k]·A_d + Σ_{d,e} C_e[d][k]·B[d][e],
 // J(x_ref) = J(0) + Σ_e x_ref,e·C_e. The fold takes the first 216 threads; with
 // WITH_VALUE the CTA's last warp (a CTA of more than 216 threads) folds the value
@@ -1170,6 +1169,7 @@ __device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const 
     constexpr int FOLD = 18, BATCH = 20;
     const bool degenerate = tc.degenerate;
     __shared__ double fold[FOLD * NMOM];
+    __shared__ double sums[NMOM];
     __shared__ double mom[NMOM];
     if (threadIdx.x < FOLD * NMOM) {
         const int slot = threadIdx.x / FOLD, ln = threadIdx.x % FOLD;
@@ -1187,23 +1187,35 @@ __device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const 
         fold_value(P.bins, a, tc);
     }
     __syncthreads();
-    if (threadIdx.x < NMOM) {
-        double v = 0.0;
-        for (int l = 0; l < FOLD; ++l) v += fold[threadIdx.x * FOLD + l];
-        fold[threadIdx.x] = v;
+    {
+        // each slot's FOLD lane sums, added by one warp in a fixed xor tree
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int slot = warp; slot < NMOM; slot += nw) {
+            double v = lane < FOLD ? fold[slot * FOLD + lane] : 0.0;
+            v = slice_sum(v);
+            if (lane == 0) sums[slot] = v;
+        }
     }
     __syncthreads();
-    // The records carry the interpolant's gradient in index space; the physical
+    // The records carry the interpolant's gradient in index space and the position
+    // moments are taken in fixed index units about the grid centre; the physical
     // gradient is g_phys[d] = Σ_j g_idx[j]·M[j][d] (M the moving physical→index matrix,
-    // registration/metric.rs:848-861), a linear map applied here once to the sums:
-    // A_d = Σ_j M[j][d]·A_j, B[d][e] = Σ_j M[j][d]·B[j][e].
+    // registration/metric.rs:848-861) and x − x_ref = M_f·(idx − mid) (M_f the fixed
+    // index→physical matrix), linear maps applied here once to the sums:
+    // A_d = Σ_j M[j][d]·A_j, B[d][e] = Σ_j M[j][d]·Σ_k M_f[e][k]·S[j][k].
     if (threadIdx.x < NMOM) {
         const int t = threadIdx.x;
-        const int d = t < 3 ? t : (t - 3) / 3;
-        const int src = t < 3 ? 0 : 3 + (t - 3) % 3;
-        const int step = t < 3 ? 1 : 3;
         double v = 0.0;
-        for (int j = 0; j < 3; ++j) v += P.mp2i[j * 3 + d] * fold[src + j * step];
+        if (t < 3) {
+            for (int j = 0; j < 3; ++j) v += P.mp2i[j * 3 + t] * sums[j];
+        } else {
+            const int d = (t - 3) / 3, e = (t - 3) % 3;
+            for (int j = 0; j < 3; ++j) {
+                double sj = 0.0;
+                for (int k = 0; k < 3; ++k) sj += P.fi2p[e * 3 + k] * sums[3 + j * 3 + k];
+                v += P.mp2i[j * 3 + d] * sj;
+            }
+        }
         mom[t] = v;
     }
     __syncthreads();

@@ -57,8 +57,10 @@ struct SamplerParams {
     // surely outside c < olo or c ≥ ohi
     double ilo, olo, ihi[3], ohi[3];
     double bin_hi;  // (double)(bins − 3), the top Parzen bin
-    // fast path: fixed physical point relative to xref in FP32, x − xref ≈ xA·(i,j,k) + xb
-    float xA[9], xb[3];
+    // the fixed grid's centre in index units ((size − 1)/2 per axis, exact in FP32): the
+    // derivative pass's position moments are taken in (i,j,k) − xmid, exact integers or
+    // half-integers, and mapped to x − x_ref = M_f·((i,j,k) − xmid) once, in FP64, by the fold
+    float xmid[3];
     int msz[3];      // moving size, 32-bit (the volume is below 2^32 voxels)
     uint32_t ms1, ms2;  // moving strides, 32-bit
     cudaTextureObject_t mtex;  // the moving volume as a texture (point, clamp, unnormalised)

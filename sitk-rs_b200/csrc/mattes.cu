@@ -1290,8 +1290,7 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     const double mid[3] = {0.5 * (double)(P.fsize0 - 1), 0.5 * (double)(P.fsize1 - 1), 0.5 * (double)(P.fsize2 - 1)};
     for (int r = 0; r < 3; ++r) {
         P.xref[r] = P.forigin[r] + f_i2p[r * 3] * mid[0] + f_i2p[r * 3 + 1] * mid[1] + f_i2p[r * 3 + 2] * mid[2];
-        P.xb[r] = (float)(P.forigin[r] - P.xref[r]);
-        for (int c = 0; c < 3; ++c) P.xA[r * 3 + c] = (float)f_i2p[r * 3 + c];
+        P.xmid[r] = (float)mid[r];
     }
 
     if (!mattes) {
