@@ -270,8 +270,12 @@ mi_status shape_batch(mi_batch* b, int chunk, int copies) {
     b->copies = copies;
     b->fine_copies = fine;
     const size_t hs = batch_hist_smem(B, copies, fine), ds = deriv_smem(B);
-    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_batch_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hs));
-    MI_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_batch_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ds));
+    // raise-only limits: another batch with fewer bins must not lower them under this one
+    {
+        mi_status ls = raise_smem_limit(ctx, (const void*)k_batch_hist, hs);
+        if (ls == MI_OK) ls = raise_smem_limit(ctx, (const void*)k_batch_deriv, ds);
+        if (ls != MI_OK) return ls;
+    }
     int occ_h = 0, occ_d = 0;
     MI_CHECK_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_batch_hist, HIST_BLOCK, hs));
     MI_CHECK_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_batch_deriv, DERIV_BLOCK, ds));

@@ -85,8 +85,8 @@ struct SamplerParams {
     // The fast path's range and Parzen decisions (sampler.cuh finish_fast): FP32 copies
     // of the reciprocal bin size and normalised minimum, the top bin, and the metric's
     // global bounds, formed per point map by point_map_fill from vmax (the largest
-    // |voxel| of the moving volume): the fast value is within dv = vmax·(8·cerr +
-    // 32·2^-24) of the reference's for every sample, the range thresholds are the
+    // |voxel| of the moving volume): the fast value is within dv = vmax·(16·cerr +
+    // 13·2^-24) of the reference's for every sample, the range thresholds are the
     // range ends ∓ (dv plus rounding slack) rounded outward to f32, and dterm bounds
     // the Parzen term's distance from the reference's.
     double vmax;

@@ -1315,11 +1315,19 @@ mi_status mi_metric_create_ex(mi_context* ctx, const mi_image* fixed, const mi_i
     // Workspace and launch shapes.
     Workspace& ws = m->ws;
     const int B = bins;
-    TRY_CUDA(cudaFuncSetAttribute(k_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_kernel_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist_kernel_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stream_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_eval<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
-    TRY_CUDA(cudaFuncSetAttribute(k_eval<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eval_smem(B)));
+    // dynamic shared-memory limits only ever raised (a metric with fewer bins must not
+    // lower them under another metric's launches)
+#define TRY_STATUS(expr)                 \
+    do {                                 \
+        mi_status _s = (expr);           \
+        if (_s != MI_OK) return fail(_s); \
+    } while (0)
+    TRY_STATUS(raise_smem_limit(ctx, (const void*)k_hist<true>, hist_kernel_smem(B)));
+    TRY_STATUS(raise_smem_limit(ctx, (const void*)k_hist<false>, hist_kernel_smem(B)));
+    TRY_STATUS(raise_smem_limit(ctx, (const void*)k_deriv, stream_smem(B)));
+    TRY_STATUS(raise_smem_limit(ctx, (const void*)k_eval<true>, eval_smem(B)));
+    TRY_STATUS(raise_smem_limit(ctx, (const void*)k_eval<false>, eval_smem(B)));
+#undef TRY_STATUS
     int occ_h = 0, occ_d = 0, occ_e1 = 0, occ_e0 = 0, coop = 0;
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_h, k_hist<true>, HIST_BLOCK, hist_kernel_smem(B)));
     TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_deriv, DERIV_BLOCK, stream_smem(B)));

@@ -104,12 +104,14 @@ MI_HD inline bool point_map_fill(SamplerParams& P, const double* stages, int nst
     if (!(cmax <= DBL_MAX)) return false;
     P.cerr = mul(mul(0x1p-40, add(1.0, cmax)), (double)(1 + nstage));
     {
-        // the fast path's global decision bounds (sampler.cuh finish_fast): the FP32
-        // trilinear value is within 32·2^-24·vmax of the value at the fast c (three
-        // levels of lerps add at most 12 such units), and the fast c's error (cerr, or
-        // 2·cerr on the brick path) moves it by at most 6·vmax per voxel of it (16·cerr
-        // allowed)
-        const double dv = mul(P.vmax, add(mul(16.0, P.cerr), 32.0 * 0x1p-24));
+        // the fast path's global decision bounds (sampler.cuh finish_fast), u = 2^-24,
+        // M = vmax: a lerp fmaf(f, fl(b − a), a) of values within M is within 3uM of
+        // a + f(b − a) (2uM from the rounded difference, uM from the FMA), and a lerp
+        // passes its inputs' errors on unweighted, so the three levels give 9uM; the
+        // FP32 fractions are within 2^-25 + cerr of the exact ones, each moving the value
+        // by at most 2M, another 3uM + 6M·cerr. 13u covers the 12u and the reference's
+        // own FP64 rounding; 16·cerr covers the brick path's 2·cerr.
+        const double dv = mul(P.vmax, add(mul(16.0, P.cerr), 13.0 * 0x1p-24));
         const double rmag = fmax(fabs(P.moving_min), fabs(P.moving_max));
         const double e = add(mul(dv, 1.001), mul(add(mul(2.0, P.vmax), rmag), 0x1p-20));
         P.rlo_out = f32_down(sub(P.moving_min, e));
