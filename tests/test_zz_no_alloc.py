@@ -152,3 +152,43 @@ def test_noalloc_reports_sample_indices_beyond_the_grid():
         st = np.zeros(12 * max(nstage, 1))
         s = _call(L, ctx, f.device_ptr(), f, m, None, 0, info, st, nstage, result)
         assert _lib.STATUS_NAMES[s] == "MI_ERR_POINT_MAP_STAGE_COUNT"
+
+
+def test_noalloc_replays_from_a_captured_graph():
+    # The documented use under stream capture: one call outside any capture (it looks
+    # the scratch array up), then one call captured into a CUDA graph on the context's
+    # stream; each replay gives the direct call's value bits.
+    import torch
+    import sitk_b200 as sb
+    from sitk_b200 import _lib
+
+    L = _lib.load()
+    ctx = sb.Context(0)
+    n = 32
+    p = small_pair(n=n, seed=13, rot=6.0, trans=2.0)
+    f = sb.DeviceImage.upload(p.fixed, ctx=ctx)
+    m = sb.DeviceImage.upload(p.moving, ctx=ctx)
+    metric = sb.DeviceMattesMetric.from_device(f, m, 32)
+    info = _lib.MiMetricInfo()
+    _lib.check(L.mi_metric_info_get(metric.handle, ctypes.byref(info)), ctx.handle)
+    t = sb.VersorRigid3DTransform((0.02, 0.01, -0.015), (0.5, 0.2, -0.4), [(n - 1) / 2.0] * 3)
+    stage = np.ascontiguousarray(sb.transform_stage(t), dtype=np.float64)
+    samples = torch.arange(0, n ** 3, 3, dtype=torch.int32, device="cuda")
+    result = torch.zeros(2, dtype=torch.float64, device="cuda")
+    _lib.check(_call(L, ctx, f.device_ptr(), f, m, samples, samples.numel(), info, stage, 1, result), ctx.handle)
+    ctx.sync()
+    direct = result.cpu().tolist()
+    assert direct[1] > 0 and np.isfinite(direct[0])
+
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        _lib.check(_call(L, ctx, f.device_ptr(), f, m, samples, samples.numel(), info, stage, 1, result),
+                   ctx.handle)
+    for _ in range(2):
+        result.fill_(-1.0)
+        torch.cuda.synchronize()
+        graph.replay()
+        torch.cuda.synchronize()
+        assert result.cpu().tolist() == direct
+    del graph
