@@ -139,7 +139,7 @@ k_deriv(const __grid_constant__ SamplerParams P, const __grid_constant__ Jacobia
     // last warp folds the value while the others fold the derivative
     static_assert(DERIV_BLOCK >= 18 * NMOM + 32, "deriv_fold's value warp");
     deriv_fold<true>(P, J, a, t, a.partials, gridDim.x);
-    publish_seq(a);
+    publish_seq(a, J.nparams);
     if (threadIdx.x == 0) a.sync[0] = 0u;
     for (int i = threadIdx.x; i < P.bins * P.bins + P.bins; i += blockDim.x) a.ghist[i] = 0ull;
     for (int i = threadIdx.x; i < P.bins; i += blockDim.x) a.gcols[i] = 0ull;
@@ -1036,14 +1036,15 @@ mi_status evaluate(mi_metric* m, const double* stages, int nstage, const double*
         // evaluation); the stream is queried every 256 polls, so a failed launch still
         // ends the wait with its error, and a finished stream without the number is
         // reported as an error
-        const volatile unsigned long long* flag =
-            reinterpret_cast<const volatile unsigned long long*>(ws.host_result + RESULT_ERR + 1);
+        const volatile unsigned long long* words = reinterpret_cast<const volatile unsigned long long*>(ws.host_result);
+        const int np = want_derivative ? nparams : 0;
+        auto published = [&]() { return words[RESULT_ERR + 1] == publish_tag(a.seq, words, np); };
         for (uint32_t spin = 1;; ++spin) {
-            if (*flag == a.seq) break;
+            if (published()) break;
             if ((spin & 255u) == 0u) {
                 const cudaError_t q = cudaStreamQuery(st);
                 if (q == cudaSuccess) {
-                    if (*flag == a.seq) break;
+                    if (published()) break;
                     return set_error(ctx, MI_ERR_CUDA, "the evaluation finished without publishing its result");
                 }
                 if (q != cudaErrorNotReady) return cuda_status(ctx, q, "cudaStreamQuery");
