@@ -231,17 +231,16 @@ __device__ __forceinline__ unsigned int* error_word(const EvalArgs& a) {
 
 // The error word a histogram pass with staged tiles raises (sync[3], a wait that timed
 // out), as the result's error slot, and cleared for the next evaluation. Run by the one
-// thread that publishes the result.
+// thread that writes the value.
 __device__ __forceinline__ double carry_error(const EvalArgs& a) {
     const unsigned int e = *reinterpret_cast<volatile unsigned int*>(a.sync + 3);
     if (e) a.sync[3] = 0u;
     return e ? __longlong_as_double((long long)e) : 0.0;
 }
 
-// One step of the publication tag: the word folded in, then SplitMix64's finaliser
-// (Steele, Lea and Flood, OOPSLA 2014), the same on the device and on the host.
-__host__ __device__ inline unsigned long long publish_mix(unsigned long long h, unsigned long long w) {
-    h ^= w;
+// SplitMix64's finaliser (Steele, Lea and Flood, OOPSLA 2014): a bijection of 64-bit
+// words whose every output bit depends on every input bit.
+__host__ __device__ inline unsigned long long publish_mix(unsigned long long h) {
     h *= 0xbf58476d1ce4e5b9ull;
     h ^= h >> 27;
     h *= 0x94d049bb133111ebull;
@@ -249,41 +248,51 @@ __host__ __device__ inline unsigned long long publish_mix(unsigned long long h, 
     return h;
 }
 
-// The tag of a published result: the sequence number, then the value, the valid count,
-// the np derivative components and the error word, in that order.
-__host__ __device__ inline unsigned long long publish_tag(unsigned long long seq, const volatile unsigned long long* w,
-                                                          int np) {
-    unsigned long long h = seq;
-    for (int i = 0; i < 2 + np; ++i) h = publish_mix(h, w[i]);
-    return publish_mix(h, w[RESULT_ERR]);
+// One published word's share of the tag: the word salted with its slot, then mixed.
+__host__ __device__ inline unsigned long long publish_word(int slot, unsigned long long w) {
+    return publish_mix(w ^ ((unsigned long long)(slot + 1) * 0x9e3779b97f4a7c15ull));
 }
 
-// The CTA's copy of the words it publishes (value, valid, derivative), written beside
-// the mirror's so the tag is formed from shared memory.
+// The tag of a published result: the mixed sequence number XOR every published word's
+// share (value, valid count, the np derivative components, the error word). A result
+// whose words have not all arrived differs from the tag by the XOR of the late words'
+// old and new shares, which is not zero but by a 2^-64 chance; a previous evaluation's
+// tag carries another sequence number.
+__host__ __device__ inline unsigned long long publish_tag(unsigned long long seq, const volatile unsigned long long* w,
+                                                          int np) {
+    unsigned long long h = publish_mix(seq);
+    for (int i = 0; i < 2 + np; ++i) h ^= publish_word(i, w[i]);
+    return h ^ publish_word(RESULT_ERR, w[RESULT_ERR]);
+}
+
+// The CTA's copy of the words it publishes (value, valid, derivative and, at
+// RESULT_ERR, the error word), written beside the mirror's so the tag is formed from
+// shared memory.
 __device__ __forceinline__ double* published_words() {
-    __shared__ double pub[RESULT_ERR];
+    __shared__ double pub[RESULT_ERR + 1];
     return pub;
 }
 
-// Run by the whole last CTA after it has written the result into the mirror (and its
-// words into published_words): one thread writes the error word (carry_error) and,
-// into the mirror's last slot, a tag that hashes the evaluation's sequence number with
-// every published word (value, valid, the np derivative components, the error word).
-// The mirror's words may reach the host in any order and no system-scope fence orders
-// them (it cost 1.8 µs of every evaluation): the host takes the result once the tag
-// matches the words it reads (publish_tag), which a partly arrived result does not,
-// and a stale tag never does (the sequence number).
+// Run by the whole last CTA after it has written the result into the mirror and its
+// words into published_words: warp 0 writes, into the mirror's last slot, a tag that
+// hashes the evaluation's sequence number with every published word (publish_tag; one
+// lane per word, then an xor tree). The mirror's words may reach the host in any order
+// and no system-scope fence orders them (it cost 1.8 µs of every evaluation): the host
+// takes the result once the tag matches the words it reads, which a partly arrived
+// result does not.
 __device__ __forceinline__ void publish_seq(const EvalArgs& a, int np) {
     if (!a.result_host) return;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const double e = carry_error(a);
-        a.result_host[RESULT_ERR] = e;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
         const double* w = published_words();
-        unsigned long long h = a.seq;
-        for (int i = 0; i < 2 + np; ++i) h = publish_mix(h, (unsigned long long)__double_as_longlong(w[i]));
-        h = publish_mix(h, (unsigned long long)__double_as_longlong(e));
-        *reinterpret_cast<volatile unsigned long long*>(a.result_host + RESULT_ERR + 1) = h;
+        const int slot = lane < 2 + np ? lane : RESULT_ERR;
+        unsigned long long h =
+            lane <= 2 + np ? publish_word(slot, (unsigned long long)__double_as_longlong(w[slot])) : 0ull;
+#pragma unroll
+        for (int off = 16; off; off >>= 1) h ^= __shfl_xor_sync(0xffffffffu, h, off);
+        if (lane == 0)
+            *reinterpret_cast<volatile unsigned long long*>(a.result_host + RESULT_ERR + 1) = h ^ publish_mix(a.seq);
     }
 }
 
@@ -800,10 +809,13 @@ __device__ void fold_value(int B, const EvalArgs& a, const TailCtx& t) {
         a.result[0] = r0;
         a.result[1] = r1;
         if (a.result_host) {
+            const double e = carry_error(a);  // a staged-tile wait that timed out
             a.result_host[0] = r0;
             a.result_host[1] = r1;
+            a.result_host[RESULT_ERR] = e;
             published_words()[0] = r0;
             published_words()[1] = r1;
+            published_words()[RESULT_ERR] = e;
         }
     }
 }
@@ -896,10 +908,13 @@ __device__ __forceinline__ void tail_once(int B, double moving_bin_size, const E
             a.result[0] = r0;
             a.result[1] = r1;
             if (mirror && a.result_host) {
+                const double e = carry_error(a);
                 a.result_host[0] = r0;
                 a.result_host[1] = r1;
+                a.result_host[RESULT_ERR] = e;
                 published_words()[0] = r0;
                 published_words()[1] = r1;
+                published_words()[RESULT_ERR] = e;
             }
         }
     }
