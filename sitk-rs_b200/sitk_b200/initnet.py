@@ -5,7 +5,7 @@ registers itself.
 The reference starts every registration from CenteredTransformInitializer
 (registration/initializer.rs:56-105); this module adds a learned proposal in front of
 the same regular-step optimizer, and the acceptance rule keeps the plain optimizer
-as the judge: a proposal is used only when its refined result reaches the plain
+as the arbiter: a proposal is used only when its refined result reaches the plain
 run's final metric value within a tolerance.
 
 The network (csrc/initnet.cu) reads a fixed/moving pair resampled to 32³ and
