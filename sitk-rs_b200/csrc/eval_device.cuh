@@ -1215,7 +1215,8 @@ __device__ TailCtx stream_phase(const SamplerParams& P, const EvalArgs& a, doubl
 // one round trip; the 18 lane sums of a slot are then added by one warp in a fixed xor
 // tree) and
 // contract with the Jacobian form: ∂/∂p_k = Σ_d J(x_ref)[d][k]·A_d + Σ_{d,e} C_e[d][k]·B[d][e],
-// J(x_ref) = J(0) + Σ_e x_ref,e·C_e. The fold takes the first 216 threads; with
+// J(x_ref) = J(0) + Σ_e x_ref,e·C_e, through one linear map of the slot sums formed
+// while the partials load. The fold takes the first 216 threads; with
 // WITH_VALUE the CTA's last warp (a CTA of more than 216 threads) folds the value
 // slices (fold_value) meanwhile.
 template <bool WITH_VALUE = false>
@@ -1223,15 +1224,44 @@ __device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const 
                            const double* partials, unsigned int count) {
     constexpr int FOLD = 18, BATCH = 20;
     const bool degenerate = tc.degenerate;
+    const int np = J.nparams;
     __shared__ double fold[FOLD * NMOM];
     __shared__ double sums[NMOM];
-    __shared__ double mom[NMOM];
+    __shared__ double wmap[MI_MAX_PARAMS * NMOM];
     if (threadIdx.x < FOLD * NMOM) {
         const int slot = threadIdx.x / FOLD, ln = threadIdx.x % FOLD;
         const double* src = partials + (int64_t)slot * count;
+        // the first batch of loads goes out before W is formed, the rest after
+        double t[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) t[u] = ln + u * FOLD < count ? __ldcg(src + ln + u * FOLD) : 0.0;
+        if ((int)threadIdx.x < np * NMOM) {
+            // While the loads are in flight: the derivative is linear in the 12 slot sums,
+            // ∂_k = Σ_t W[k][t]·sums[t]; W composes the gradient's index→physical map (M,
+            // moving physical→index, registration/metric.rs:848-861), the position's
+            // x − x_ref = M_f·(idx − mid) (M_f fixed index→physical) and the Jacobian form
+            // J(x) = J(0) + Σ_e x_e·C_e at x_ref:
+            //   W[k][j] = Σ_d J(x_ref)[d][k]·M[j][d],
+            //   W[k][3 + 3j + m] = Σ_{d,e} C_e[d][k]·M[j][d]·M_f[e][m].
+            const int k = threadIdx.x / NMOM, col = threadIdx.x % NMOM;
+            double w = 0.0;
+            if (col < 3) {
+                for (int d = 0; d < 3; ++d) {
+                    double jr = J.jac0[d * np + k];
+                    for (int e = 0; e < 3; ++e) jr += P.xref[e] * J.jacc[e][d * np + k];
+                    w += jr * P.mp2i[col * 3 + d];
+                }
+            } else {
+                const int j = (col - 3) / 3, m = (col - 3) % 3;
+                for (int d = 0; d < 3; ++d)
+                    for (int e = 0; e < 3; ++e) w += J.jacc[e][d * np + k] * (P.mp2i[j * 3 + d] * P.fi2p[e * 3 + m]);
+            }
+            wmap[threadIdx.x] = w;
+        }
         double v = 0.0;
-        for (unsigned int b = ln; b < count; b += BATCH * FOLD) {
-            double t[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) v += t[u];
+        for (unsigned int b = ln + BATCH * FOLD; b < count; b += BATCH * FOLD) {
 #pragma unroll
             for (int u = 0; u < BATCH; ++u) t[u] = b + u * FOLD < count ? __ldcg(src + b + u * FOLD) : 0.0;
 #pragma unroll
@@ -1252,39 +1282,12 @@ __device__ void deriv_fold(const SamplerParams& P, const JacobianForm& J, const 
         }
     }
     __syncthreads();
-    // The records carry the interpolant's gradient in index space and the position
-    // moments are taken in fixed index units about the grid centre; the physical
-    // gradient is g_phys[d] = Σ_j g_idx[j]·M[j][d] (M the moving physical→index matrix,
-    // registration/metric.rs:848-861) and x − x_ref = M_f·(idx − mid) (M_f the fixed
-    // index→physical matrix), linear maps applied here once to the sums:
-    // A_d = Σ_j M[j][d]·A_j, B[d][e] = Σ_j M[j][d]·Σ_k M_f[e][k]·S[j][k].
-    if (threadIdx.x < NMOM) {
-        const int t = threadIdx.x;
-        double v = 0.0;
-        if (t < 3) {
-            for (int j = 0; j < 3; ++j) v += P.mp2i[j * 3 + t] * sums[j];
-        } else {
-            const int d = (t - 3) / 3, e = (t - 3) % 3;
-            for (int j = 0; j < 3; ++j) {
-                double sj = 0.0;
-                for (int k = 0; k < 3; ++k) sj += P.fi2p[e * 3 + k] * sums[3 + j * 3 + k];
-                v += P.mp2i[j * 3 + d] * sj;
-            }
-        }
-        mom[t] = v;
-    }
-    __syncthreads();
-    const int np = J.nparams;
     if (threadIdx.x < np) {
         const int k = threadIdx.x;
         double dk = 0.0;
         if (!degenerate) {
-            for (int d = 0; d < 3; ++d) {
-                double jr = J.jac0[d * np + k];
-                for (int e = 0; e < 3; ++e) jr += P.xref[e] * J.jacc[e][d * np + k];
-                dk += jr * mom[d];
-                for (int e = 0; e < 3; ++e) dk += J.jacc[e][d * np + k] * mom[3 + d * 3 + e];
-            }
+#pragma unroll
+            for (int t = 0; t < NMOM; ++t) dk += wmap[k * NMOM + t] * sums[t];
         }
         a.result[2 + k] = dk;
         if (a.result_host) {
